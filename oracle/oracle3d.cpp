@@ -1,0 +1,313 @@
+// ORACLE — test infrastructure only.
+//
+// CPU restatement of the reference's default 3D velocity path
+// (VELOCITY_3D_TYPE 1: fmm3D::calcVelocityFast), used by tests/, smoke() and
+// bench.py's cpu_baseline leg as the checker; never part of the product.
+//
+//   * octree                  src/FMM/fast3DFMM.cpp:485-745 (FMMCell::generateTree)
+//   * octant rule             src/FMM/fast3DFMM.hpp:17-22
+//   * 10-term P2M / M2M       src/FMM/fmm3D.cpp:84-132, fast3DFMM.cpp:164-302
+//   * M2P multipliers         src/FMM/fmm3D.cpp:147-200
+//   * per-target traversal    src/FMM/fast3DFMM.cpp:318-472 (far iff R^2 > (2 size)^2)
+// plus the FP64 direct Biot-Savart sum u_i = sum_j (a_j x r_ij) / |r_ij|^3.
+//
+// Geometry decisions (octant comparisons, R^2 against (2 size)^2) use separate
+// IEEE operations in the reference's order; build without -march.
+
+#include <array>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+struct Oct {
+    std::vector<int> npar, chd_flag, parent;
+    std::vector<double> xc, yc, zc, size;
+    std::vector<char> active;
+    std::vector<std::vector<int>> pids;
+    std::vector<std::array<int, 8>> chd;
+    std::vector<int> level_start;
+    int max_level = 0;
+    int cap = 30;
+    double root = 0;
+    int ncell() const { return (int)npar.size(); }
+    bool leaf(int c) const { return npar[c] < cap; }
+};
+
+thread_local std::string g_err3;
+
+// fast3DFMM.cpp:485-745. The root box is the particle box joined with the
+// domain centre (0,0,0) (global.cpp:609-611), side = max extent * (1+exp/100).
+bool build_oct(Oct& t, const double* x, const double* y, const double* z, const uint8_t* act,
+               int64_t n, int cap, double exp_pct) {
+    t.cap = cap;
+    double mn[3] = {0.0, 0.0, 0.0}, mx[3] = {0.0, 0.0, 0.0};
+    for (int64_t i = 0; i < n; ++i) {
+        const double p[3] = {x[i], y[i], z[i]};
+        for (int d = 0; d < 3; ++d) {
+            if (p[d] < mn[d]) mn[d] = p[d];
+            if (p[d] > mx[d]) mx[d] = p[d];
+        }
+    }
+    double cen[3];
+    t.root = 0.0;
+    for (int d = 0; d < 3; ++d) {
+        double len = mx[d] - mn[d];
+        t.root = std::max(len, t.root);
+        cen[d] = 0.5 * (mx[d] + mn[d]);
+    }
+    t.root *= (1 + (exp_pct / 100));
+    auto add_cell = [&](int parent, double cx, double cy, double cz, double sz) {
+        t.npar.push_back(0); t.chd_flag.push_back(0); t.parent.push_back(parent);
+        t.xc.push_back(cx); t.yc.push_back(cy); t.zc.push_back(cz); t.size.push_back(sz);
+        t.active.push_back(0); t.pids.emplace_back();
+        std::array<int, 8> z8; z8.fill(0); t.chd.push_back(z8);
+        return t.ncell() - 1;
+    };
+    add_cell(-1, cen[0], cen[1], cen[2], t.root);
+    t.npar[0] = (int)n;
+    t.active[0] = 1;
+    t.level_start.assign(1, 0);
+
+    std::vector<char> settled(n, 0);
+    std::vector<int> cell_of(n, 0);
+    int64_t remaining = n;
+    int L = 0;
+    while (remaining > 0) {
+        ++L;
+        if (L > 60) { g_err3 = "octree deeper than 60 levels (coincident particles)"; return false; }
+        t.level_start.push_back(t.ncell());
+        for (int64_t i = 0; i < n; ++i) {
+            if (settled[i]) continue;
+            int c = cell_of[i];
+            int oct = (x[i] > t.xc[c]) * 1 + (y[i] > t.yc[c]) * 2 + (z[i] > t.zc[c]) * 4;
+            if (((t.chd_flag[c] >> oct) & 1) == 0) {
+                double h = t.size[c] / 2.0;
+                double cx = t.xc[c] + h * (((oct >> 0) & 1) - 0.5);
+                double cy = t.yc[c] + h * (((oct >> 1) & 1) - 0.5);
+                double cz = t.zc[c] + h * (((oct >> 2) & 1) - 0.5);
+                int k = add_cell(c, cx, cy, cz, h);
+                t.chd[c][oct] = k;
+                t.chd_flag[c] |= (1 << oct);
+            }
+            int k = t.chd[c][oct];
+            cell_of[i] = k;
+            t.npar[k]++;
+        }
+        for (int64_t i = 0; i < n; ++i) {
+            if (settled[i]) continue;
+            int c = cell_of[i];
+            if (t.npar[c] < cap) {
+                t.pids[c].push_back((int)i);
+                if (act[i]) t.active[c] = 1;
+                settled[i] = 1;
+                --remaining;
+            }
+        }
+    }
+    t.max_level = L;
+    t.level_start.push_back(t.ncell());
+    for (int lv = t.max_level - 1; lv > 0; --lv) {
+        for (int c = t.level_start[lv]; c < t.level_start[lv + 1]; ++c) {
+            if (t.leaf(c)) continue;
+            for (int o = 0; o < 8; ++o) {
+                if (((t.chd_flag[c] >> o) & 1) == 0) continue;
+                if (t.active[t.chd[c][o]]) { t.active[c] = 1; break; }
+            }
+        }
+    }
+    return true;
+}
+
+// Moments (q, q d, q d^2/2, cross terms) with d = centre - particle
+// (fmm3D.cpp:84-103) and their shift to the parent (fmm3D.cpp:114-132).
+inline void p2m(double* m, double s, double dx, double dy, double dz) {
+    m[0] += s;
+    m[1] += s * dx; m[2] += s * dy; m[3] += s * dz;
+    m[4] += s * dx * dx * 0.5; m[5] += s * dy * dy * 0.5; m[6] += s * dz * dz * 0.5;
+    m[7] += s * dx * dy; m[8] += s * dy * dz; m[9] += s * dx * dz;
+}
+
+inline void m2m(double* m, const double* c, double dx, double dy, double dz) {
+    m[0] += c[0];
+    m[1] += c[1] + c[0] * dx;
+    m[2] += c[2] + c[0] * dy;
+    m[3] += c[3] + c[0] * dz;
+    m[4] += c[4] + (c[0] * dx * dx * 0.5) + (c[1] * dx);
+    m[5] += c[5] + (c[0] * dy * dy * 0.5) + (c[2] * dy);
+    m[6] += c[6] + (c[0] * dz * dz * 0.5) + (c[3] * dz);
+    m[7] += c[7] + (c[0] * dx * dy) + (c[1] * dy) + (c[2] * dx);
+    m[8] += c[8] + (c[0] * dy * dz) + (c[2] * dz) + (c[3] * dy);
+    m[9] += c[9] + (c[0] * dx * dz) + (c[1] * dz) + (c[3] * dx);
+}
+
+// Derivatives of r/|r|^3 paired with the 10 moments (fmm3D.cpp:147-200).
+inline void m2p_mul(double R2, double dx, double dy, double dz, double* gx, double* gy, double* gz) {
+    double R = std::sqrt(R2), R3 = R * R2, R5 = R3 * R2, R7 = R5 * R2;
+    gx[0] = dx / R3;
+    gx[1] = -(3 * dx * dx / R5) + (1 / R3);
+    gx[2] = -(3 * dx * dy / R5);
+    gx[3] = -(3 * dx * dz / R5);
+    gx[4] = (15 * dx * dx * dx / R7) - (9 * dx / R5);
+    gx[5] = (15 * dx * dy * dy / R7) - (3 * dx / R5);
+    gx[6] = (15 * dx * dz * dz / R7) - (3 * dx / R5);
+    gx[7] = (15 * dx * dx * dy / R7) - (3 * dy / R5);
+    gx[8] = (15 * dx * dy * dz / R7);
+    gx[9] = (15 * dx * dx * dz / R7) - (3 * dz / R5);
+    gy[0] = dy / R3;
+    gy[1] = -(3 * dy * dx / R5);
+    gy[2] = -(3 * dy * dy / R5) + (1 / R3);
+    gy[3] = -(3 * dy * dz / R5);
+    gy[4] = (15 * dy * dx * dx / R7) - (3 * dy / R5);
+    gy[5] = (15 * dy * dy * dy / R7) - (9 * dy / R5);
+    gy[6] = (15 * dy * dz * dz / R7) - (3 * dy / R5);
+    gy[7] = (15 * dy * dx * dy / R7) - (3 * dx / R5);
+    gy[8] = (15 * dy * dy * dz / R7) - (3 * dz / R5);
+    gy[9] = (15 * dy * dx * dz / R7);
+    gz[0] = dz / R3;
+    gz[1] = -(3 * dz * dx / R5);
+    gz[2] = -(3 * dz * dy / R5);
+    gz[3] = -(3 * dz * dz / R5) + (1 / R3);
+    gz[4] = (15 * dz * dx * dx / R7) - (3 * dz / R5);
+    gz[5] = (15 * dz * dy * dy / R7) - (3 * dz / R5);
+    gz[6] = (15 * dz * dz * dz / R7) - (9 * dz / R5);
+    gz[7] = (15 * dz * dx * dy / R7);
+    gz[8] = (15 * dz * dy * dz / R7) - (3 * dy / R5);
+    gz[9] = (15 * dz * dx * dz / R7) - (3 * dx / R5);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* orc3_last_error() { return g_err3.c_str(); }
+
+// Treecode velocity (reference calcVelocityFast with every particle a target).
+int orc_fmm3d_velocity(const double* x, const double* y, const double* z,
+                       const double* ax, const double* ay, const double* az, const uint8_t* act,
+                       int64_t n, int leaf_cap, double exp_pct, double* u, double* v, double* w) {
+    Oct t;
+    if (!build_oct(t, x, y, z, act, n, leaf_cap, exp_pct)) return -1;
+    const int nc = t.ncell();
+    std::vector<double> mx((size_t)nc * 10, 0.0), my((size_t)nc * 10, 0.0), mz((size_t)nc * 10, 0.0);
+    #pragma omp parallel for schedule(dynamic, 16)
+    for (int c = 0; c < nc; ++c) {
+        if (!t.leaf(c) || !t.active[c]) continue;
+        for (int i : t.pids[c]) {
+            if (!act[i]) continue;
+            double dx = t.xc[c] - x[i], dy = t.yc[c] - y[i], dz = t.zc[c] - z[i];
+            p2m(&mx[(size_t)c * 10], ax[i], dx, dy, dz);
+            p2m(&my[(size_t)c * 10], ay[i], dx, dy, dz);
+            p2m(&mz[(size_t)c * 10], az[i], dx, dy, dz);
+        }
+    }
+    for (int lv = t.max_level - 1; lv > 0; --lv) {
+        for (int c = t.level_start[lv]; c < t.level_start[lv + 1]; ++c) {
+            if (!t.active[c] || t.leaf(c)) continue;
+            for (int o = 0; o < 8; ++o) {
+                if (((t.chd_flag[c] >> o) & 1) == 0) continue;
+                int k = t.chd[c][o];
+                double dx = t.xc[c] - t.xc[k], dy = t.yc[c] - t.yc[k], dz = t.zc[c] - t.zc[k];
+                m2m(&mx[(size_t)c * 10], &mx[(size_t)k * 10], dx, dy, dz);
+                m2m(&my[(size_t)c * 10], &my[(size_t)k * 10], dx, dy, dz);
+                m2m(&mz[(size_t)c * 10], &mz[(size_t)k * 10], dx, dy, dz);
+            }
+        }
+    }
+    #pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t i = 0; i < n; ++i) {
+        const double xp = x[i], yp = y[i], zp = z[i];
+        double vx = 0, vy = 0, vz = 0;
+        std::vector<int> cur, nxt;
+        for (int o = 0; o < 8; ++o)
+            if ((t.chd_flag[0] >> o) & 1) cur.push_back(t.chd[0][o]);
+        double gx[10], gy[10], gz[10];
+        for (int lv = 1; lv < t.max_level; ++lv) {
+            nxt.clear();
+            for (int c : cur) {
+                for (int o = 0; o < 8; ++o) {
+                    if (((t.chd_flag[c] >> o) & 1) == 0) continue;
+                    int k = t.chd[c][o];
+                    if (!t.active[k]) continue;
+                    double dx = xp - t.xc[k], dy = yp - t.yc[k], dz = zp - t.zc[k];
+                    double R2 = dx * dx + dy * dy + dz * dz;
+                    double Rc = t.size[k] * 2.0;
+                    if (R2 > Rc * Rc) {
+                        m2p_mul(R2, dx, dy, dz, gx, gy, gz);
+                        const double* Mx = &mx[(size_t)k * 10];
+                        const double* My = &my[(size_t)k * 10];
+                        const double* Mz = &mz[(size_t)k * 10];
+                        for (int m = 0; m < 10; ++m) {
+                            vx += My[m] * gz[m] - Mz[m] * gy[m];
+                            vy += Mz[m] * gx[m] - Mx[m] * gz[m];
+                            vz += Mx[m] * gy[m] - My[m] * gx[m];
+                        }
+                    } else if (t.chd_flag[k] != 0) {
+                        nxt.push_back(k);
+                    } else {
+                        for (int j : t.pids[k]) {
+                            if (!act[j] || j == i) continue;
+                            double ex = xp - x[j], ey = yp - y[j], ez = zp - z[j];
+                            double r2 = ex * ex + ey * ey + ez * ez;
+                            double r3 = std::sqrt(r2) * r2;
+                            vx += (ay[j] * ez - az[j] * ey) / r3;
+                            vy += (az[j] * ex - ax[j] * ez) / r3;
+                            vz += (ax[j] * ey - ay[j] * ex) / r3;
+                        }
+                    }
+                }
+            }
+            cur.swap(nxt);
+        }
+        u[i] = vx; v[i] = vy; w[i] = vz;
+    }
+    return 0;
+}
+
+// Octree dump in creation order: ints per cell = nPar, chdFlag, parent,
+// active, level, (max_level on cell 0); geom = xc, yc, zc, size.
+int64_t orc_tree3d(const double* x, const double* y, const double* z, const uint8_t* act, int64_t n,
+                   int leaf_cap, double exp_pct, int32_t* ints, double* geom) {
+    Oct t;
+    if (!build_oct(t, x, y, z, act, n, leaf_cap, exp_pct)) return -1;
+    if (ints && geom) {
+        for (int lv = 0; lv <= t.max_level; ++lv) {
+            for (int c = t.level_start[lv]; c < t.level_start[lv + 1]; ++c) {
+                int32_t* r = ints + 6 * c;
+                r[0] = t.npar[c]; r[1] = t.chd_flag[c]; r[2] = t.parent[c]; r[3] = t.active[c];
+                r[4] = lv; r[5] = (c == 0) ? t.max_level : 0;
+                geom[4 * c] = t.xc[c]; geom[4 * c + 1] = t.yc[c]; geom[4 * c + 2] = t.zc[c]; geom[4 * c + 3] = t.size[c];
+            }
+        }
+    }
+    return t.ncell();
+}
+
+// FP64 direct velocity at m sampled targets from all active sources.
+void orc_direct3d_velocity(const double* x, const double* y, const double* z,
+                           const double* ax, const double* ay, const double* az, const uint8_t* act,
+                           int64_t n, const int64_t* tgt, int64_t m, double* u, double* v, double* w) {
+    #pragma omp parallel for schedule(static)
+    for (int64_t k = 0; k < m; ++k) {
+        int64_t i = tgt[k];
+        double vx = 0, vy = 0, vz = 0;
+        for (int64_t j = 0; j < n; ++j) {
+            if (j == i || !act[j]) continue;
+            double ex = x[i] - x[j], ey = y[i] - y[j], ez = z[i] - z[j];
+            double r2 = ex * ex + ey * ey + ez * ez;
+            double r3 = std::sqrt(r2) * r2;
+            vx += (ay[j] * ez - az[j] * ey) / r3;
+            vy += (az[j] * ex - ax[j] * ez) / r3;
+            vz += (ax[j] * ey - ay[j] * ex) / r3;
+        }
+        u[k] = vx; v[k] = vy; w[k] = vz;
+    }
+}
+
+}  // extern "C"
