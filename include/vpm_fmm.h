@@ -1,0 +1,166 @@
+/*
+ * vpm_fmm.h — C ABI of the B200 FMM velocity step for the LSMPS vortex
+ * particle method (drop-in for the velocity evaluation of
+ * anggarapangestu/LSMPS_VPM_v2, src/FMM + src/velocity_calculation).
+ *
+ * Plain pointers and sizes only. Every function returns a status code
+ * (VPM_OK = 0) and never lets an exception cross the ABI; the text of the last
+ * failure is available from vpm_last_error(ctx). Calls on one context are
+ * stream-ordered on the context's stream and are not re-entrant: use one
+ * context per host thread. The caller owns every input and output buffer; no
+ * pointer is retained after a call returns.
+ *
+ * Host-buffer entry points (vpm_fmm2d_field, vpm_velocity2d, ...) copy inputs
+ * to the device, run, copy results back and synchronise. The *_device entry
+ * points take device pointers, enqueue the whole evaluation on the context's
+ * stream and return without synchronising; their device-side error word is
+ * checked by vpm_ctx_sync().
+ */
+#ifndef VPM_FMM_H
+#define VPM_FMM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes (errno-style values). */
+#define VPM_OK 0
+#define VPM_EDEVICE 5      /* CUDA runtime error                                   */
+#define VPM_ENOMEM 12      /* device allocation failed                             */
+#define VPM_EINVAL 22      /* bad argument or degenerate input (e.g. all particles coincide) */
+#define VPM_EOVERFLOW 75   /* a tree / list capacity was exceeded                  */
+#define VPM_ETIMEDOUT 110  /* a bounded device-side wait gave up                   */
+
+/* Arithmetic of the evaluation. */
+#define VPM_PREC_FP64 0    /* plain form: FP64 everywhere                           */
+#define VPM_PREC_MIXED 1   /* chosen form: FP32 near field, split-precision M2L      */
+
+/* Binomial coefficients of the translations. */
+#define VPM_BINOM_REFERENCE 0 /* as the reference's binComb computes them in 32-bit
+                                 int, wrapping for the largest orders
+                                 (src/FMM/fmm2D.cpp:28-58); needed for 1e-10 parity */
+#define VPM_BINOM_EXACT 1     /* true binomial coefficients                          */
+
+typedef struct vpm_ctx vpm_ctx;
+
+/*
+ * Knobs of the evaluation. Defaults (vpm_fmm_params_default) are the
+ * reference's 2D values: global.cpp:303 (expTree = 1.0), :311 (P_max = 10),
+ * :312 (par_count_max = 75), :313 (src_count_max = 50); treeCell.cpp:5
+ * (EPSILON_TOLERANCE = 1e-9); fast3DFMM.cpp:4 (support factor 2.0) with the
+ * 3D leaf cap src_count_max = 30 (global.cpp:779).
+ */
+typedef struct vpm_fmm_params {
+    int32_t p;            /* expansion order, 1..30                                 */
+    int32_t max_src;      /* 2D leaf cap on active (source) particles               */
+    int32_t max_par;      /* 2D leaf cap on all particles                           */
+    int32_t leaf_cap_3d;  /* 3D leaf iff particle count < leaf_cap_3d               */
+    double exp_tree_pct;  /* root box expansion, percent                            */
+    double eps;           /* list distance tolerance                                */
+    int32_t precision;    /* VPM_PREC_*                                             */
+    int32_t binom;        /* VPM_BINOM_*                                            */
+    int32_t max_depth;    /* deepest tree level the keys resolve (2D: 16 or 31)     */
+    int32_t reserved;
+} vpm_fmm_params;
+
+/* Per-call figures (counts are exact; times are CUDA-event milliseconds). */
+typedef struct vpm_fmm_stats {
+    int64_t n;            /* particles                                              */
+    int64_t n_cells;      /* cells in the tree (reference treeData.size())          */
+    int64_t n_leaves;     /* leaves (reference leafList.size())                     */
+    int32_t min_level;    /* reference TreeCell::min_level                          */
+    int32_t max_level;    /* reference TreeCell::max_level                          */
+    int64_t p2p_pairs;    /* (target, source) pairs over list 1, j != i             */
+    int64_t m2l_pairs;    /* (cell, cell) pairs over lists 2 and 4                  */
+    int64_t m2p_pairs;    /* (target, cell) pairs over list 3                       */
+    int64_t list1_len;
+    int64_t list3_len;
+    float ms_tree;        /* bounding box, keys, sort, level splits                 */
+    float ms_lists;       /* lists 1-4                                              */
+    float ms_upward;      /* P2M + M2M                                              */
+    float ms_m2l;
+    float ms_eval;        /* L2L chain + L2P + M2P                                  */
+    float ms_p2p;
+    float ms_total;       /* device time of the whole evaluation                    */
+    int32_t kernels;      /* kernel launches of this call                           */
+    int32_t depth_retry;  /* 1 when the host entry point rebuilt with deeper keys   */
+} vpm_fmm_stats;
+
+/* Fill *p with the reference's 2D/3D defaults listed above. */
+void vpm_fmm_params_default(vpm_fmm_params* p);
+
+/* Create a context on CUDA device `device` (buffers, stream, events). */
+int vpm_ctx_create(int device, vpm_ctx** out);
+int vpm_ctx_destroy(vpm_ctx* ctx);
+/* Run subsequent calls on `cuda_stream` (a cudaStream_t; NULL = the context's own stream). */
+int vpm_ctx_set_stream(vpm_ctx* ctx, void* cuda_stream);
+/* Wait for the context's stream and report any device-side error word. */
+int vpm_ctx_sync(vpm_ctx* ctx);
+/* Message of the last failure on this context (static storage of the context). */
+const char* vpm_last_error(vpm_ctx* ctx);
+
+/*
+ * 2D field of the point sources (x_j, y_j, q_j):
+ *   E(x_i) = sum_j q_j (x_i - x_j) / |x_i - x_j|^2
+ * approximated by the adaptive-quadtree FMM. Replaces
+ *   TreeCell::initializeTree(pos, active)          src/FMM/treeCell.cpp:1043
+ *   fmm2D::calcField(tree, pos, active, src)        src/FMM/fmm2D.cpp:907
+ *   fmm2D::get_Field_x / get_Field_y                src/FMM/fmm2D.cpp:1146-1157
+ * ex/ey are the reference's Ex/Ey (the velocity is u = Ey, v = -Ex).
+ * Host buffers of n elements. stats may be NULL.
+ */
+int vpm_fmm2d_field(vpm_ctx* ctx, const double* x, const double* y, const double* q,
+                    const uint8_t* active, int64_t n, const vpm_fmm_params* prm,
+                    double* ex, double* ey, vpm_fmm_stats* stats);
+
+/* Same with device pointers, asynchronous on the context's stream. */
+int vpm_fmm2d_field_device(vpm_ctx* ctx, const double* x, const double* y, const double* q,
+                           const uint8_t* active, int64_t n, const vpm_fmm_params* prm,
+                           double* ex, double* ey);
+
+/*
+ * The FMM body of VelocityCalc::velocity_fmm_2d
+ * (src/velocity_calculation/velocity_calc.cpp:455-578): sources
+ * q = -omega s^2 / (2 pi), then u = Ey + u_inf, v = -Ex + v_inf
+ * (the free stream of VelocityCalc::get_velocity, velocity_calc.cpp:226-230).
+ * Host buffers.
+ */
+int vpm_velocity2d(vpm_ctx* ctx, const double* x, const double* y, const double* omega,
+                   const double* s, const uint8_t* active, int64_t n, const vpm_fmm_params* prm,
+                   double u_inf, double v_inf, double* u, double* v, vpm_fmm_stats* stats);
+
+/*
+ * Build only the tree and lists 1-4 of a 2D particle set (host buffers), for
+ * the parity dumps below. Replaces TreeCell::initializeTree
+ * (src/FMM/treeCell.cpp:1043) when no field is wanted.
+ */
+int vpm_tree2d_build(vpm_ctx* ctx, const double* x, const double* y, const uint8_t* active, int64_t n,
+                     const vpm_fmm_params* prm, vpm_fmm_stats* stats);
+
+/* Statistics of the last evaluation on this context (synchronises). */
+int vpm_last_stats(vpm_ctx* ctx, vpm_fmm_stats* stats);
+
+/*
+ * Parity dumps of the tree and lists built by the last 2D call on this
+ * context, in the reference's vocabulary (treeCell.hpp:16-75, 112-128):
+ *   cells sorted by reference cell ID: ids[k]; ints6[6k..6k+5] = level, ix, iy,
+ *   parNum, srcParNum, flags (1 = isLeaf, 2 = isActive); centers2[2k..] = centre.
+ *   leaves in the reference's leafList order with each leaf's particle IDs
+ *   (ascending, parIDList) as CSR.
+ *   list `which` (1..4) as CSR over the reference's cells in ID order: lists 1
+ *   and 3 for every leaf (TreeCell::intList, treeCell.cpp:636), lists 2 and 4
+ *   for every cell at level >= 2 (TreeCell::extList, treeCell.cpp:818).
+ * Call vpm_tree2d_counts first to size the outputs.
+ */
+int vpm_tree2d_counts(vpm_ctx* ctx, int64_t* n_cells, int64_t* n_leaves, int64_t list_len[4]);
+int vpm_tree2d_cells(vpm_ctx* ctx, int64_t* ids, int32_t* ints6, double* centers2);
+int vpm_tree2d_leaves(vpm_ctx* ctx, int64_t* leaf_ids, int64_t* offs, int32_t* pids);
+int vpm_tree2d_list(vpm_ctx* ctx, int which, int64_t* cell_ids, int64_t* offs, int64_t* ids);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VPM_FMM_H */

@@ -1,0 +1,14 @@
+"""B200-native FMM velocity step of the LSMPS vortex particle method.
+
+The compute path is libvpm_fmm.so (hand-written sm_100a CUDA kernels behind
+the C ABI in include/vpm_fmm.h); this package binds it and mirrors the
+reference's operator interface for the path.
+"""
+from ._lib import (BINOM_EXACT, BINOM_REFERENCE, PREC_FP64, PREC_MIXED, Params, Stats, VpmError,
+                   default_params, lib)
+from .fmm import Context, Particle, TreeCell, VelocityCalc, default_context, fmm2D
+
+__all__ = [
+    "BINOM_EXACT", "BINOM_REFERENCE", "PREC_FP64", "PREC_MIXED", "Params", "Stats", "VpmError",
+    "default_params", "lib", "Context", "Particle", "TreeCell", "VelocityCalc", "default_context", "fmm2D",
+]

@@ -1,0 +1,127 @@
+"""ctypes binding of the C ABI in include/vpm_fmm.h (libvpm_fmm.so, built
+in-tree by ``python -m lsmps_vpm_v2_b200.build``).
+
+There is no fallback: if the shared library is missing or cannot be loaded,
+every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SO_PATH = os.path.join(HERE, "libvpm_fmm.so")
+
+VPM_OK = 0
+VPM_EDEVICE = 5
+VPM_ENOMEM = 12
+VPM_EINVAL = 22
+VPM_EOVERFLOW = 75
+VPM_ETIMEDOUT = 110
+
+PREC_FP64 = 0
+PREC_MIXED = 1
+BINOM_REFERENCE = 0
+BINOM_EXACT = 1
+
+
+class Params(C.Structure):
+    """vpm_fmm_params (include/vpm_fmm.h)."""
+    _fields_ = [
+        ("p", C.c_int32),
+        ("max_src", C.c_int32),
+        ("max_par", C.c_int32),
+        ("leaf_cap_3d", C.c_int32),
+        ("exp_tree_pct", C.c_double),
+        ("eps", C.c_double),
+        ("precision", C.c_int32),
+        ("binom", C.c_int32),
+        ("max_depth", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
+class Stats(C.Structure):
+    """vpm_fmm_stats (include/vpm_fmm.h)."""
+    _fields_ = [
+        ("n", C.c_int64),
+        ("n_cells", C.c_int64),
+        ("n_leaves", C.c_int64),
+        ("min_level", C.c_int32),
+        ("max_level", C.c_int32),
+        ("p2p_pairs", C.c_int64),
+        ("m2l_pairs", C.c_int64),
+        ("m2p_pairs", C.c_int64),
+        ("list1_len", C.c_int64),
+        ("list3_len", C.c_int64),
+        ("ms_tree", C.c_float),
+        ("ms_lists", C.c_float),
+        ("ms_upward", C.c_float),
+        ("ms_m2l", C.c_float),
+        ("ms_eval", C.c_float),
+        ("ms_p2p", C.c_float),
+        ("ms_total", C.c_float),
+        ("kernels", C.c_int32),
+        ("depth_retry", C.c_int32),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_vp = C.c_void_p
+_dp = C.POINTER(C.c_double)
+_i64p = C.POINTER(C.c_int64)
+_i32p = C.POINTER(C.c_int32)
+
+# name -> (restype, argtypes); every symbol declared in include/vpm_fmm.h.
+SIGNATURES = {
+    "vpm_fmm_params_default": (None, [C.POINTER(Params)]),
+    "vpm_ctx_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
+    "vpm_ctx_destroy": (C.c_int, [_vp]),
+    "vpm_ctx_set_stream": (C.c_int, [_vp, _vp]),
+    "vpm_ctx_sync": (C.c_int, [_vp]),
+    "vpm_last_error": (C.c_char_p, [_vp]),
+    "vpm_fmm2d_field": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int64, C.POINTER(Params), _vp, _vp,
+                                  C.POINTER(Stats)]),
+    "vpm_fmm2d_field_device": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int64, C.POINTER(Params), _vp, _vp]),
+    "vpm_velocity2d": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, C.c_int64, C.POINTER(Params), C.c_double,
+                                 C.c_double, _vp, _vp, C.POINTER(Stats)]),
+    "vpm_tree2d_build": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int64, C.POINTER(Params), C.POINTER(Stats)]),
+    "vpm_last_stats": (C.c_int, [_vp, C.POINTER(Stats)]),
+    "vpm_tree2d_counts": (C.c_int, [_vp, _i64p, _i64p, _i64p]),
+    "vpm_tree2d_cells": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "vpm_tree2d_leaves": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "vpm_tree2d_list": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp]),
+}
+
+_LIB = None
+
+
+def lib() -> C.CDLL:
+    """The loaded product library (raises when it is missing)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(SO_PATH):
+            raise RuntimeError(f"{SO_PATH} is missing: build it with `python -m lsmps_vpm_v2_b200.build`")
+        L = C.CDLL(SO_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _LIB = L
+    return _LIB
+
+
+def default_params(**over) -> Params:
+    p = Params()
+    lib().vpm_fmm_params_default(C.byref(p))
+    for k, v in over.items():
+        setattr(p, k, v)
+    return p
+
+
+class VpmError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"[{status}] {msg}")
+        self.status = status

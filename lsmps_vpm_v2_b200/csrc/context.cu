@@ -1,0 +1,85 @@
+// Context lifetime and interaction counting.
+#include "context.h"
+
+namespace vpm {
+
+namespace {
+
+// Exact interaction counts of the last 2D evaluation (for the statistics and
+// the roofline figures): list-1 pairs j != i, M2L pairs, list-3 pairs.
+__global__ void count2d(Tree2D t, Lists2D l, unsigned long long* out, const unsigned* err) {
+    if (fatal(err)) return;
+    const int nl = t.info->n_leaves, nc = t.info->n_cells;
+    unsigned long long p2p = 0, m2p = 0, m2l = 0;
+    for (int li = blockIdx.x * blockDim.x + threadIdx.x; li < nl; li += gridDim.x * blockDim.x) {
+        const int c = t.leaf_cells[li];
+        const long long T = t.c_hi[c] - t.c_lo[c];
+        long long S = 0;
+        bool self = false;
+        for (uint32_t k = l.l1_off[li]; k < l.l1_off[li + 1]; ++k) {
+            const int s = l.l1_src[k];
+            S += t.c_hi[s] - t.c_lo[s];
+            self |= (s == c);
+        }
+        p2p += (unsigned long long)(T * S - (self ? T : 0));
+        m2p += (unsigned long long)(T * (long long)(l.l3_off[li + 1] - l.l3_off[li]));
+    }
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x)
+        m2l += l.l2_n[c] + l.l4_n[c];
+    atomicAdd(&out[0], p2p);
+    atomicAdd(&out[1], m2l);
+    atomicAdd(&out[2], m2p);
+}
+
+}  // namespace
+
+Ctx::~Ctx() {
+    if (device >= 0) cudaSetDevice(device);
+    if (arena2d) cudaFree(arena2d);
+    if (d_err) cudaFree(d_err);
+    for (auto& e : ev)
+        if (e) cudaEventDestroy(e);
+    if (own_stream) cudaStreamDestroy(own_stream);
+}
+
+int Ctx::init(int dev) {
+    device = dev;
+    cudaError_t e = cudaSetDevice(dev);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaSetDevice");
+    e = cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaStreamCreate");
+    stream = own_stream;
+    e = cudaMalloc(&d_err, 64);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc");
+    e = cudaMemset(d_err, 0, 64);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaMemset");
+    for (auto& x : ev) {
+        e = cudaEventCreate(&x);
+        if (e != cudaSuccess) return fail_cuda(e, "cudaEventCreate");
+    }
+    return VPM_OK;
+}
+
+int Ctx::count_interactions(vpm_fmm_stats* s) {
+    unsigned long long* d = (unsigned long long*)(d_err + 2);  // 3 counters after the error word
+    cudaError_t e = cudaMemsetAsync(d, 0, 3 * sizeof(unsigned long long), stream);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaMemsetAsync");
+    count2d<<<148, 256, 0, stream>>>(tree, lists, d, d_err);
+    unsigned long long h[3];
+    e = cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return fail_cuda(e, "count interactions");
+    s->p2p_pairs = (int64_t)h[0];
+    s->m2l_pairs = (int64_t)h[1];
+    s->m2p_pairs = (int64_t)h[2];
+    return VPM_OK;
+}
+
+size_t mixed_bytes(int n, int cap_cells, int P) { return 256; }
+
+int Ctx::enqueue_mixed2d(const vpm_fmm_params& p, double* o0, double* o1, int velocity, double uinf, double vinf,
+                         int* launches) {
+    return fail(VPM_EINVAL, "mixed precision is not available in this build");
+}
+
+}  // namespace vpm

@@ -1,0 +1,85 @@
+// The context behind `vpm_ctx`: device, stream, one device arena per
+// dimension, timing events and the state of the last evaluation.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "fmm2d.cuh"
+
+namespace vpm {
+
+struct Caps2D {
+    int n = 0, cells = 0, P = 0;
+    long long l1 = 0, l3 = 0;
+};
+
+// Host copy of a 2D tree for the parity dumps.
+struct HostTree2D {
+    int nc = 0, nl = 0, n = 0;
+    std::vector<int32_t> lo, hi, src, ix, iy, leafidx, leaf_cells, l2, l4, l1, l3;
+    std::vector<uint8_t> flags, level, l2n, l4n;
+    std::vector<double> cx, cy;
+    std::vector<uint32_t> perm, l1off, l3off;
+    std::vector<int64_t> id;
+    std::vector<int> by_id;
+};
+
+// Size of the mixed-precision work area inside the 2D arena.
+size_t mixed_bytes(int n, int cap_cells, int P);
+
+struct Ctx {
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    std::string last_error;
+    unsigned* d_err = nullptr;
+    cudaEvent_t ev[8] = {};
+
+    // 2D arena
+    void* arena2d = nullptr;
+    size_t arena2d_bytes = 0;
+    Caps2D cap;
+    bool grow = false;
+    double *in_x = nullptr, *in_y = nullptr, *in_q = nullptr, *out0 = nullptr, *out1 = nullptr;
+    uint8_t* in_act = nullptr;
+    Tree2D tree{};
+    TreeScratch2D ts{};
+    Lists2D lists{};
+    Expansions2D ex2{};
+    void* mixed_base = nullptr;
+    int coef_P = -1, coef_binom = -1;
+
+    // last evaluation
+    bool have_tree = false;
+    int last_n = 0;
+    int last_launches = 0;
+    int depth_retry = 0;
+    vpm_fmm_params last_params{};
+    HostTree2D host_tree;
+
+    ~Ctx();
+    int init(int dev);
+    int fail(int status, const std::string& msg);
+    int fail_cuda(cudaError_t e, const char* what);
+    int map_err(unsigned bits);
+    int check_params(const vpm_fmm_params* prm, vpm_fmm_params& out);
+    int plan_caps(int n, const vpm_fmm_params& p, int& cells, long long& l1, long long& l3);
+    int reserve2d(int n, int cap_cells, int P, long long cap_l1, long long cap_l3);
+    int enqueue2d(const double* x, const double* y, const double* q, const uint8_t* act, int n,
+                  const vpm_fmm_params& p, int K, double* o0, double* o1, int velocity, double uinf, double vinf,
+                  bool tree_only);
+    int enqueue_mixed2d(const vpm_fmm_params& p, double* o0, double* o1, int velocity, double uinf, double vinf,
+                        int* launches);
+    int run2d_host(const double* x, const double* y, const double* q_or_omega, const double* s, const uint8_t* act,
+                   int64_t n, const vpm_fmm_params* prm, double* o0, double* o1, int velocity, double uinf,
+                   double vinf, vpm_fmm_stats* stats, bool tree_only);
+    int collect_stats(vpm_fmm_stats* s);
+    int count_interactions(vpm_fmm_stats* s);
+    int fetch_tree(HostTree2D& h);
+};
+
+cudaError_t fmm2d_p2p_out(const Tree2D& t, const Lists2D& l, const Expansions2D& e, double* out0, double* out1,
+                          int velocity, double u_inf, double v_inf, unsigned* err, cudaStream_t st, int* launches);
+
+}  // namespace vpm

@@ -1,0 +1,131 @@
+// Device data layout of one 2D evaluation (all arrays live in HBM, owned by
+// the context and reused across calls).
+//
+// Particles are kept in tree (Morton) order as SoA doubles; `perm` maps a
+// sorted slot back to the caller's particle index. Cells are level-major and,
+// within a level, in Morton order of (ix, iy); every cell covers the
+// contiguous particle range [lo, hi) of the sorted arrays. Leaves are listed
+// in the same order in `leaf_cells`.
+#pragma once
+
+#include "prims.cuh"
+
+namespace vpm {
+
+constexpr int kMaxLevels2D = 31;   // key resolution limit (2 bits per level, 62-bit keys)
+constexpr int kList2Cap = 27;      // list 2 of a cell has at most 27 members
+constexpr int kList4Cap = 16;      // list 4 (coarser leaves next to the parent) slots
+constexpr int kQueueCap = 160;     // BFS queue of TreeCell::intList / extList
+constexpr int kMaxP = 30;          // largest expansion order
+
+enum CellFlags : uint8_t { CELL_LEAF = 1, CELL_ACTIVE = 2 };
+
+// Geometry record written by the bounding-box kernel (exact IEEE arithmetic,
+// treeCell.cpp:1061-1092).
+struct Geom2D {
+    double minx, maxx, miny, maxy;
+    double root;        // rootLength
+    double pivx, pivy;  // pivotCoord
+    double size_k;      // cell size at the key level
+};
+
+// Counts produced on the device by the tree build.
+struct TreeInfo2D {
+    int level_start[kMaxLevels2D + 3];  // first cell index of each level
+    int leaf_start[kMaxLevels2D + 3];   // first leaf index of each level
+    int n_cells;
+    int n_leaves;
+    int depth;           // deepest level holding a cell
+    int min_leaf_level;
+    int max_leaf_level;
+    int pad;
+    unsigned long long list1_len, list3_len;     // CSR totals
+    unsigned long long p2p_pairs, m2l_pairs, m2p_pairs;
+};
+
+struct Tree2D {
+    int n;
+    int key_levels;       // Lk
+    int cap_cells;
+    Geom2D* geom;
+    TreeInfo2D* info;
+    // sorted particles
+    uint64_t* key;
+    uint32_t* perm;
+    double *px, *py, *pq;
+    uint8_t* pact;
+    uint32_t* actscan;    // n + 1 entries: exclusive prefix of active flags
+    // cells
+    int32_t *c_lo, *c_hi, *c_src, *c_parent, *c_child0, *c_ix, *c_iy, *c_leafidx;
+    uint8_t *c_flags, *c_chmask, *c_level;
+    double *c_cx, *c_cy;
+    uint64_t* c_code;
+    int32_t* leaf_cells;
+};
+
+// Interaction lists. Lists 2 and 4 are fixed-width per cell; lists 1 and 3 are
+// CSR over leaves.
+struct Lists2D {
+    int32_t* l2_src;     // [cap_cells][27] source cell
+    uint8_t* l2_slot;    // [cap_cells][27] offset slot 0..39 of the source
+    uint8_t* l2_n;       // [cap_cells]
+    int32_t* l4_src;     // [cap_cells][16]
+    uint8_t* l4_n;       // [cap_cells]
+    uint32_t* l1_cnt;    // [cap_leaves] then CSR offsets (cap_leaves + 1)
+    uint32_t* l1_off;
+    int32_t* l1_src;     // [cap_l1]
+    uint32_t* l3_cnt;
+    uint32_t* l3_off;
+    int32_t* l3_src;     // [cap_l3]
+    int cap_leaves;
+    long long cap_l1, cap_l3;
+};
+
+// Scratch of the tree build.
+constexpr int kBBoxBlocks = 296;
+
+struct TreeScratch2D {
+    double* bbox_partial;   // [kBBoxBlocks * 4]
+    uint64_t* key_alt;
+    uint32_t* val_alt;
+    uint32_t* act_u32;
+    uint64_t* lvl_status;   // [kMaxLevels2D + 1][max_tiles]
+    unsigned* lvl_ticket;   // [kMaxLevels2D + 2]
+    int lvl_max_tiles;
+    SortScratch sort;
+    ScanScratch scan;
+};
+
+// Tree build: bounding box through level splits. All launches are enqueued on
+// `st`; nothing is read back. Returns the number of launches in *launches.
+cudaError_t build_tree2d(const double* x, const double* y, const double* q, const uint8_t* act, Tree2D& t,
+                         TreeScratch2D& s, int max_src, int max_par, double exp_pct, unsigned* err, cudaStream_t st,
+                         int* launches);
+
+// Lists 1-4 (count, scan, fill). Requires the tree on `st`.
+cudaError_t build_lists2d(const Tree2D& t, Lists2D& l, ScanScratch& scan, double eps, unsigned* err,
+                          cudaStream_t st, int* launches);
+
+// Coefficient tables of the translations for order P (host side), uploaded
+// to constant memory by set_coefficients2d.
+cudaError_t set_coefficients2d(int P, bool exact_binom, cudaStream_t st);
+
+// FP64 evaluation (plain form): P2M+M2M, M2L, L2L chain + M2P + L2P, P2P.
+// ex/ey are written in the caller's particle order.
+struct Expansions2D {
+    double2* a;          // [cap_cells][P+1] multipole
+    double2* b;          // [cap_cells][P+1] local (M2L part only)
+    unsigned* up_count;  // [cap_cells] children completed (upward pass)
+    double* fx;          // [n] far-field Ex in sorted order
+    double* fy;
+};
+
+cudaError_t fmm2d_upward(const Tree2D& t, Expansions2D& e, int P, unsigned* err, cudaStream_t st, int* launches);
+cudaError_t fmm2d_m2l(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, unsigned* err, cudaStream_t st,
+                      int* launches);
+cudaError_t fmm2d_eval(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, unsigned* err, cudaStream_t st,
+                       int* launches);
+cudaError_t fmm2d_p2p(const Tree2D& t, const Lists2D& l, const Expansions2D& e, double* ex, double* ey,
+                      unsigned* err, cudaStream_t st, int* launches);
+
+}  // namespace vpm

@@ -1,0 +1,392 @@
+// Adaptive quadtree of the reference (TreeCell::initializeTree,
+// src/FMM/treeCell.cpp:1043-1243), rebuilt for the GPU.
+//
+// The reference bins the unsettled particles level by level with
+//   index_L = (int)((x - pivot) / (rootLength / 2^L))       treeCell.cpp:290-303
+// and makes a cell a leaf when srcParNum <= max_src && parNum <= max_par
+// (treeCell.cpp:1195-1196). Dividing by 2^L is exact in binary floating point,
+// so RN(d / size_L) = RN(d / size_K) / 2^(K-L) and index_L is the top L bits of
+// index_K. One Morton key at level K therefore determines the cell of every
+// particle at every level: one stable radix sort of the keys, then each level's
+// cells are the distinct key prefixes inside the non-leaf cells of the level
+// above. A leaf at level L covers a contiguous range of the sorted particles.
+//
+// This file is compiled with --fmad=false: every geometric value (root box,
+// pivot, index, cell centre) is formed by separate IEEE operations in the
+// reference's order.
+#include "fmm2d.cuh"
+
+namespace vpm {
+
+namespace {
+
+constexpr int kLvlThreads = 256;
+constexpr uint64_t kLvA = 1ull << 62;
+constexpr uint64_t kLvP = 2ull << 62;
+constexpr uint64_t kLvMask = (1ull << 62) - 1;
+
+__device__ __forceinline__ uint64_t ld_relaxed(const uint64_t* p) {
+    uint64_t v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed(uint64_t* p, uint64_t v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Bounding box and root geometry (treeCell.cpp:1061-1092).
+__global__ void __launch_bounds__(256)
+bbox2d(const double* __restrict__ x, const double* __restrict__ y, int n, double exp_pct, int key_levels,
+       Geom2D* g, double* partial, unsigned* done, unsigned* err) {
+    double mnx = x[0], mxx = x[0], mny = y[0], mxy = y[0];
+    bool bad = false;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        double a = x[i], b = y[i];
+        bad |= !isfinite(a) || !isfinite(b);
+        mnx = fmin(mnx, a); mxx = fmax(mxx, a);
+        mny = fmin(mny, b); mxy = fmax(mxy, b);
+    }
+    if (bad) set_err(err, ERR_NONFINITE);
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mnx = fmin(mnx, __shfl_xor_sync(0xffffffffu, mnx, o));
+        mxx = fmax(mxx, __shfl_xor_sync(0xffffffffu, mxx, o));
+        mny = fmin(mny, __shfl_xor_sync(0xffffffffu, mny, o));
+        mxy = fmax(mxy, __shfl_xor_sync(0xffffffffu, mxy, o));
+    }
+    __shared__ double sh[4][8];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) { sh[0][warp] = mnx; sh[1][warp] = mxx; sh[2][warp] = mny; sh[3][warp] = mxy; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+            mnx = fmin(mnx, sh[0][w]); mxx = fmax(mxx, sh[1][w]);
+            mny = fmin(mny, sh[2][w]); mxy = fmax(mxy, sh[3][w]);
+        }
+        double* p = partial + 4 * blockIdx.x;
+        p[0] = mnx; p[1] = mxx; p[2] = mny; p[3] = mxy;
+        __threadfence();
+        last = atomicAdd(done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last || threadIdx.x != 0) return;
+    __threadfence();
+    for (unsigned b = 0; b < gridDim.x; ++b) {
+        const double* p = partial + 4 * b;
+        mnx = fmin(mnx, __ldcg(p)); mxx = fmax(mxx, __ldcg(p + 1));
+        mny = fmin(mny, __ldcg(p + 2)); mxy = fmax(mxy, __ldcg(p + 3));
+    }
+    double root = 0.0;
+    double ex = fabs(xsub(mxx, mnx)), ey = fabs(xsub(mxy, mny));
+    if (ex > root) root = ex;
+    if (ey > root) root = ey;
+    double expansion = xadd(1.0, xdiv(exp_pct, 100.0));
+    root = xmul(root, expansion);
+    g->minx = mnx; g->maxx = mxx; g->miny = mny; g->maxy = mxy;
+    g->root = root;
+    g->pivx = xdiv(xsub(xadd(mxx, mnx), root), 2.0);
+    g->pivy = xdiv(xsub(xadd(mxy, mny), root), 2.0);
+    g->size_k = xdiv(root, ldexp(1.0, key_levels));
+    if (!(root > 0.0) || !isfinite(root)) set_err(err, ERR_NONFINITE);
+    *done = 0;
+}
+
+// Morton key of each particle at the key level (treeCell.cpp:290-303).
+__global__ void keys2d(const double* __restrict__ x, const double* __restrict__ y, int n, const Geom2D* g,
+                       int key_levels, uint64_t* key, uint32_t* idx, unsigned* err) {
+    const double pivx = g->pivx, pivy = g->pivy, s = g->size_k;
+    const double lim = ldexp(1.0, key_levels);
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        double tx = xdiv(xsub(x[i], pivx), s);
+        double ty = xdiv(xsub(y[i], pivy), s);
+        uint32_t ix = 0, iy = 0;
+        if (tx >= 0.0 && tx < lim && ty >= 0.0 && ty < lim) {
+            ix = (uint32_t)__double2ull_rz(tx);
+            iy = (uint32_t)__double2ull_rz(ty);
+        } else {
+            set_err(err, ERR_RANGE);
+        }
+        key[i] = morton2(ix, iy);
+        idx[i] = (uint32_t)i;
+    }
+}
+
+// Sorted copies of the particle data and the active flags as 0/1 words.
+__global__ void gather2d(const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ q,
+                         const uint8_t* __restrict__ act, const uint32_t* __restrict__ perm, int n, double* px,
+                         double* py, double* pq, uint8_t* pact, uint32_t* act_u32, unsigned* err) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        uint32_t j = perm[i];
+        if (j >= (uint32_t)n) {
+            set_err(err, ERR_INDEX);
+            continue;
+        }
+        px[i] = x[j];
+        py[i] = y[j];
+        pq[i] = q[j];
+        uint8_t a = act[j] ? 1 : 0;
+        pact[i] = a;
+        act_u32[i] = a;
+    }
+}
+
+// Root cell (treeCell.cpp:1117-1133): never a leaf.
+__global__ void tree_root2d(Tree2D t) {
+    const Geom2D* g = t.geom;
+    TreeInfo2D* info = t.info;
+    t.c_lo[0] = 0;
+    t.c_hi[0] = t.n;
+    int src = (int)t.actscan[t.n];
+    t.c_src[0] = src;
+    t.c_flags[0] = src != 0 ? CELL_ACTIVE : 0;
+    t.c_parent[0] = -1;
+    t.c_child0[0] = -1;
+    t.c_chmask[0] = 0;
+    t.c_level[0] = 0;
+    t.c_ix[0] = 0;
+    t.c_iy[0] = 0;
+    t.c_code[0] = 0;
+    t.c_leafidx[0] = -1;
+    t.c_cx[0] = xadd(g->pivx, xmul(0.5, g->root));
+    t.c_cy[0] = xadd(g->pivy, xmul(0.5, g->root));
+    for (int L = 0; L < kMaxLevels2D + 3; ++L) {
+        info->level_start[L] = L == 0 ? 0 : 1;
+        info->leaf_start[L] = 0;
+    }
+    info->n_cells = 1;
+    info->n_leaves = 0;
+    info->depth = 0;
+}
+
+// First index in [lo, hi) whose level code (key >> shift) is >= v.
+__device__ __forceinline__ int lower_code(const uint64_t* __restrict__ key, int lo, int hi, int shift, uint64_t v) {
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if ((key[mid] >> shift) < v) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Cells of level L from the non-leaf cells of level L-1. Tiles of 256 parents
+// take ordered tickets; a packed (cells, leaves) count per tile is combined by
+// decoupled look-back so children are emitted in parent order, i.e. Morton
+// order within the level.
+__global__ void __launch_bounds__(kLvlThreads)
+tree_level2d(Tree2D t, int L, int max_src, int max_par, uint64_t* status, unsigned* ticket, unsigned* err) {
+    __shared__ unsigned s_tile;
+    __shared__ uint64_t warp_sums[kLvlThreads / 32];
+    __shared__ uint64_t s_prefix;
+    TreeInfo2D* info = t.info;
+    if (*(volatile const unsigned*)err & (ERR_CELL_CAP | ERR_TIMEOUT | ERR_NONFINITE)) return;
+    const int p0 = info->level_start[L - 1];
+    const int np = info->level_start[L] - p0;
+    const int ntiles = np > 0 ? ceil_div(np, kLvlThreads) : 1;
+    const int base_cell = info->level_start[L];
+    const int base_leaf = info->leaf_start[L];
+    const int shift = 2 * (t.key_levels - L);
+    const double len = xdiv(t.geom->root, ldexp(1.0, L));
+    const double pivx = t.geom->pivx, pivy = t.geom->pivy;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+
+    for (;;) {
+        if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
+        __syncthreads();
+        const int tile = (int)s_tile;
+        __syncthreads();
+        if (tile >= ntiles) return;
+        const int p = p0 + tile * kLvlThreads + threadIdx.x;
+        int bnd[5];
+        int nchild = 0, nleaf = 0;
+        unsigned mask = 0;
+        bool parent_ok = tile * kLvlThreads + (int)threadIdx.x < np;
+        if (parent_ok && !(t.c_flags[p] & CELL_LEAF)) {
+            const int lo = t.c_lo[p], hi = t.c_hi[p];
+            const uint64_t pc = t.c_code[p] << 2;
+            bnd[0] = lo;
+            bnd[4] = hi;
+            bnd[1] = lower_code(t.key, lo, hi, shift, pc + 1);
+            bnd[2] = lower_code(t.key, bnd[1], hi, shift, pc + 2);
+            bnd[3] = lower_code(t.key, bnd[2], hi, shift, pc + 3);
+            for (int d = 0; d < 4; ++d) {
+                if (bnd[d + 1] > bnd[d]) {
+                    mask |= 1u << d;
+                    ++nchild;
+                    int par = bnd[d + 1] - bnd[d];
+                    int src = (int)(t.actscan[bnd[d + 1]] - t.actscan[bnd[d]]);
+                    if (src <= max_src && par <= max_par) ++nleaf;
+                }
+            }
+        }
+        // Block-wide exclusive scan of the packed (cells, leaves) counts.
+        uint64_t v = (uint64_t)nchild | ((uint64_t)nleaf << 31);
+        uint64_t x = v;
+        #pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint64_t yv = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += yv;
+        }
+        if (lane == 31) warp_sums[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            uint64_t w = lane < kLvlThreads / 32 ? warp_sums[lane] : 0;
+            #pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                uint64_t yv = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += yv;
+            }
+            if (lane < kLvlThreads / 32) warp_sums[lane] = w;
+        }
+        __syncthreads();
+        const uint64_t excl = (warp ? warp_sums[warp - 1] : 0) + x - v;
+        const uint64_t agg = warp_sums[kLvlThreads / 32 - 1];
+        if (threadIdx.x == 0) {
+            uint64_t prefix = 0;
+            if (tile == 0) {
+                st_relaxed(&status[0], kLvP | agg);
+            } else {
+                st_relaxed(&status[tile], kLvA | agg);
+                int k = tile - 1;
+                long long spins = 0;
+                while (k >= 0) {
+                    uint64_t w = ld_relaxed(&status[k]);
+                    if ((w & ~kLvMask) == 0) {
+                        if (++spins > kSpinLimit) { set_err(err, ERR_TIMEOUT); break; }
+                        continue;
+                    }
+                    prefix += w & kLvMask;
+                    if ((w & ~kLvMask) == kLvP) break;
+                    --k;
+                }
+                st_relaxed(&status[tile], kLvP | (prefix + agg));
+            }
+            s_prefix = prefix;
+            if (tile == ntiles - 1) {
+                uint64_t tot = prefix + agg;
+                int ncell = (int)(tot & 0x7FFFFFFFull), nlf = (int)(tot >> 31);
+                for (int k2 = L + 1; k2 < kMaxLevels2D + 3; ++k2) {
+                    info->level_start[k2] = base_cell + ncell;
+                    info->leaf_start[k2] = base_leaf + nlf;
+                }
+                info->n_cells = base_cell + ncell;
+                info->n_leaves = base_leaf + nlf;
+                if (ncell > 0) info->depth = L;
+                if (base_cell + ncell > t.cap_cells) set_err(err, ERR_CELL_CAP);
+            }
+        }
+        __syncthreads();
+        const uint64_t mine = s_prefix + excl;
+        int ci = base_cell + (int)(mine & 0x7FFFFFFFull);
+        int li = base_leaf + (int)(mine >> 31);
+        if (nchild > 0) {
+            const int pix = t.c_ix[p], piy = t.c_iy[p];
+            const uint64_t pc = t.c_code[p] << 2;
+            if (ci + nchild <= t.cap_cells) {
+                t.c_child0[p] = ci;
+                t.c_chmask[p] = (uint8_t)mask;
+            } else {
+                t.c_child0[p] = -1;
+                t.c_chmask[p] = 0;
+            }
+            for (int d = 0; d < 4; ++d) {
+                if (!(mask & (1u << d))) continue;
+                if (ci >= t.cap_cells) { set_err(err, ERR_CELL_CAP); break; }
+                const int lo = bnd[d], hi = bnd[d + 1];
+                const int par = hi - lo;
+                const int src = (int)(t.actscan[hi] - t.actscan[lo]);
+                const bool leaf = src <= max_src && par <= max_par;
+                const int ix = 2 * pix + (d & 1), iy = 2 * piy + (d >> 1);
+                t.c_lo[ci] = lo;
+                t.c_hi[ci] = hi;
+                t.c_src[ci] = src;
+                t.c_flags[ci] = (leaf ? CELL_LEAF : 0) | (src != 0 ? CELL_ACTIVE : 0);
+                t.c_parent[ci] = p;
+                t.c_child0[ci] = -1;
+                t.c_chmask[ci] = 0;
+                t.c_level[ci] = (uint8_t)L;
+                t.c_ix[ci] = ix;
+                t.c_iy[ci] = iy;
+                t.c_code[ci] = pc + d;
+                t.c_cx[ci] = xadd(pivx, xmul(xadd(0.5, (double)ix), len));
+                t.c_cy[ci] = xadd(pivy, xmul(xadd(0.5, (double)iy), len));
+                if (leaf) {
+                    t.c_leafidx[ci] = li;
+                    t.leaf_cells[li] = ci;
+                    ++li;
+                } else {
+                    t.c_leafidx[ci] = -1;
+                    if (L == t.key_levels) set_err(err, ERR_DEPTH);
+                }
+                ++ci;
+            }
+        } else if (parent_ok && !(t.c_flags[p] & CELL_LEAF)) {
+            t.c_child0[p] = -1;
+            t.c_chmask[p] = 0;
+        }
+        __syncthreads();
+    }
+}
+
+// Leaf level range (TreeCell::min_level / max_level, treeCell.cpp:1236-1240).
+__global__ void tree_finish2d(TreeInfo2D* info) {
+    int mn = -1, mx = -1;
+    for (int L = 0; L <= kMaxLevels2D; ++L) {
+        if (info->leaf_start[L + 1] > info->leaf_start[L]) {
+            if (mn < 0) mn = L;
+            mx = L;
+        }
+    }
+    info->min_leaf_level = mn;
+    info->max_leaf_level = mx;
+}
+
+}  // namespace
+
+cudaError_t build_tree2d(const double* x, const double* y, const double* q, const uint8_t* act, Tree2D& t,
+                         TreeScratch2D& s, int max_src, int max_par, double exp_pct, unsigned* err, cudaStream_t st,
+                         int* launches) {
+    const int n = t.n;
+    const int K = t.key_levels;
+    const int gridN = std::max(1, std::min(148 * 8, ceil_div(n, 256)));
+    unsigned* done = s.lvl_ticket + kMaxLevels2D + 1;
+    const int bb_blocks = std::max(1, std::min(kBBoxBlocks, ceil_div(n, 256)));
+    cudaError_t e = cudaMemsetAsync(s.lvl_ticket, 0, sizeof(unsigned) * (kMaxLevels2D + 2), st);
+    if (e != cudaSuccess) return e;
+    bbox2d<<<bb_blocks, 256, 0, st>>>(x, y, n, exp_pct, K, t.geom, s.bbox_partial, done, err);
+    keys2d<<<gridN, 256, 0, st>>>(x, y, n, t.geom, K, t.key, t.perm, err);
+    *launches += 2;
+    uint64_t* keys = t.key;
+    uint32_t* vals = t.perm;
+    e = radix_sort_pairs(&keys, &vals, s.key_alt, s.val_alt, n, 2 * K, s.sort, err, st, launches);
+    if (e != cudaSuccess) return e;
+    if (keys != t.key) {
+        e = cudaMemcpyAsync(t.key, keys, sizeof(uint64_t) * n, cudaMemcpyDeviceToDevice, st);
+        if (e != cudaSuccess) return e;
+        e = cudaMemcpyAsync(t.perm, vals, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st);
+        if (e != cudaSuccess) return e;
+    }
+    gather2d<<<gridN, 256, 0, st>>>(x, y, q, act, t.perm, n, t.px, t.py, t.pq, t.pact, s.act_u32, err);
+    *launches += 1;
+    e = scan_exclusive(s.act_u32, t.actscan, n, t.actscan + n, s.scan, err, st);
+    if (e != cudaSuccess) return e;
+    *launches += 1;
+    e = cudaMemsetAsync(s.lvl_status, 0, sizeof(uint64_t) * (size_t)(K + 1) * s.lvl_max_tiles, st);
+    if (e != cudaSuccess) return e;
+    tree_root2d<<<1, 1, 0, st>>>(t);
+    *launches += 1;
+    for (int L = 1; L <= K; ++L) {
+        long long bound = std::min<long long>(t.cap_cells, 1ll << std::min(2 * (L - 1), 40));
+        int tiles = std::max(1, ceil_div(bound, kLvlThreads));
+        if (tiles > s.lvl_max_tiles) return cudaErrorInvalidValue;
+        int grid = std::min(tiles, 148 * 4);
+        tree_level2d<<<grid, kLvlThreads, 0, st>>>(t, L, max_src, max_par, s.lvl_status + (size_t)L * s.lvl_max_tiles,
+                                                   s.lvl_ticket + L, err);
+        *launches += 1;
+    }
+    tree_finish2d<<<1, 1, 0, st>>>(t.info);
+    *launches += 1;
+    return cudaGetLastError();
+}
+
+}  // namespace vpm

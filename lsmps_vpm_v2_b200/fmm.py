@@ -1,0 +1,249 @@
+"""Host-side front end of the B200 FMM velocity step.
+
+``Context`` wraps one ``vpm_ctx`` (device buffers, stream). On top of it sit
+mirrors of the reference's operator interface for this path, with the same
+names, argument meaning and error behaviour (exceptions on failure):
+
+* ``TreeCell``      — src/FMM/treeCell.hpp:83-195 (initializeTree, intList,
+                      extList, leafList, min_level / max_level)
+* ``fmm2D``         — src/FMM/fmm2D.hpp:15-68 (calcField, get_Field_x/y)
+* ``Particle``, ``VelocityCalc`` — Utils.hpp:77-159 and
+  src/velocity_calculation/velocity_calc.hpp:15-47 (get_velocity with the 2D
+  FMM branch, velocity_calc.cpp:455-578)
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from ._lib import Params, Stats, VpmError, default_params, lib
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _u8(a):
+    return np.ascontiguousarray(a, dtype=np.uint8)
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class Context:
+    """One device context: buffers, stream and the last tree (for dumps)."""
+
+    def __init__(self, device: int = 0):
+        self._h = C.c_void_p()
+        st = lib().vpm_ctx_create(int(device), C.byref(self._h))
+        if st != 0:
+            raise VpmError(st, "vpm_ctx_create failed")
+        self.device = device
+
+    def close(self):
+        if self._h:
+            lib().vpm_ctx_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st: int):
+        if st != 0:
+            raise VpmError(st, lib().vpm_last_error(self._h).decode())
+
+    def set_stream(self, stream_ptr: int | None):
+        self._check(lib().vpm_ctx_set_stream(self._h, C.c_void_p(stream_ptr or 0)))
+
+    def sync(self):
+        self._check(lib().vpm_ctx_sync(self._h))
+
+    # ---- 2D -----------------------------------------------------------------
+    def field2d(self, x, y, q, active, params: Params | None = None, stats: bool = False):
+        """(Ex, Ey) of the reference's fmm2D::calcField, host arrays in/out."""
+        x, y, q, a = _f64(x), _f64(y), _f64(q), _u8(active)
+        n = x.size
+        ex, ey = np.empty(n), np.empty(n)
+        p = params or default_params()
+        s = Stats()
+        self._check(lib().vpm_fmm2d_field(self._h, _ptr(x), _ptr(y), _ptr(q), _ptr(a), n, C.byref(p),
+                                          _ptr(ex), _ptr(ey), C.byref(s)))
+        return (ex, ey, s) if stats else (ex, ey)
+
+    def field2d_device(self, x, y, q, active, ex, ey, params: Params | None = None):
+        """Asynchronous field on device buffers (objects with .data_ptr(), e.g. torch CUDA tensors)."""
+        p = params or default_params()
+        n = int(x.numel())
+        self._check(lib().vpm_fmm2d_field_device(self._h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()),
+                                                 C.c_void_p(q.data_ptr()), C.c_void_p(active.data_ptr()), n,
+                                                 C.byref(p), C.c_void_p(ex.data_ptr()), C.c_void_p(ey.data_ptr())))
+
+    def velocity2d(self, x, y, omega, s, active, u_inf=0.0, v_inf=0.0, params: Params | None = None,
+                   stats: bool = False):
+        x, y, w, sz, a = _f64(x), _f64(y), _f64(omega), _f64(s), _u8(active)
+        n = x.size
+        u, v = np.empty(n), np.empty(n)
+        p = params or default_params()
+        st = Stats()
+        self._check(lib().vpm_velocity2d(self._h, _ptr(x), _ptr(y), _ptr(w), _ptr(sz), _ptr(a), n, C.byref(p),
+                                         float(u_inf), float(v_inf), _ptr(u), _ptr(v), C.byref(st)))
+        return (u, v, st) if stats else (u, v)
+
+    def last_stats(self) -> Stats:
+        s = Stats()
+        self._check(lib().vpm_last_stats(self._h, C.byref(s)))
+        return s
+
+    def build_tree2d(self, x, y, active, params: Params | None = None) -> Stats:
+        x, y, a = _f64(x), _f64(y), _u8(active)
+        p = params or default_params()
+        s = Stats()
+        self._check(lib().vpm_tree2d_build(self._h, _ptr(x), _ptr(y), _ptr(a), x.size, C.byref(p), C.byref(s)))
+        return s
+
+    def dump_tree2d(self):
+        """The last 2D tree in the reference's vocabulary (see include/vpm_fmm.h)."""
+        nc, nl = C.c_int64(), C.c_int64()
+        ll = (C.c_int64 * 4)()
+        self._check(lib().vpm_tree2d_counts(self._h, C.byref(nc), C.byref(nl), ll))
+        nc, nl = nc.value, nl.value
+        ids = np.zeros(nc, np.int64)
+        ints = np.zeros((nc, 6), np.int32)
+        cen = np.zeros((nc, 2))
+        self._check(lib().vpm_tree2d_cells(self._h, _ptr(ids), _ptr(ints), _ptr(cen)))
+        n = int(ints[0, 3]) if nc else 0
+        lid = np.zeros(nl, np.int64)
+        loff = np.zeros(nl + 1, np.int64)
+        lp = np.zeros(max(n, 1), np.int32)
+        self._check(lib().vpm_tree2d_leaves(self._h, _ptr(lid), _ptr(loff), _ptr(lp)))
+        lists = {}
+        for which in (1, 2, 3, 4):
+            m = nl if which in (1, 3) else int(np.count_nonzero(ints[:, 0] >= 2))
+            cid = np.zeros(m, np.int64)
+            offs = np.zeros(m + 1, np.int64)
+            out = np.zeros(max(int(ll[which - 1]), 1), np.int64)
+            self._check(lib().vpm_tree2d_list(self._h, which, _ptr(cid), _ptr(offs), _ptr(out)))
+            lists[which] = (cid, offs, out[: int(offs[-1])])
+        return dict(ids=ids, level=ints[:, 0], ix=ints[:, 1], iy=ints[:, 2], par=ints[:, 3], src=ints[:, 4],
+                    leaf=(ints[:, 5] & 1).astype(bool), active=(ints[:, 5] & 2).astype(bool), centers=cen,
+                    leaf_ids=lid, leaf_offs=loff, leaf_pids=lp[:n], lists=lists)
+
+
+_default_ctx: Context | None = None
+
+
+def default_context() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx
+
+
+# ---- mirrors of the reference's operator interface ---------------------------
+
+class TreeCell:
+    """Mirror of TreeCell (src/FMM/treeCell.hpp:83-195) backed by the GPU tree.
+
+    Cells are addressed by the reference's cell ID; lists come from the GPU
+    interaction lists."""
+
+    def __init__(self, ctx: Context | None = None, params: Params | None = None):
+        self.ctx = ctx or default_context()
+        self.params = params or default_params()
+        self.min_level = 2
+        self.max_level = 2
+        self.leafList: list[int] = []
+        self.cellCount = 0
+        self._dump = None
+
+    def initializeTree(self, parPos, activeFlag):
+        pos = np.asarray(parPos, dtype=np.float64)
+        s = self.ctx.build_tree2d(pos[:, 0], pos[:, 1], np.asarray(activeFlag, dtype=np.uint8), self.params)
+        self._dump = self.ctx.dump_tree2d()
+        self.min_level, self.max_level = int(s.min_level), int(s.max_level)
+        self.leafList = [int(v) for v in self._dump["leaf_ids"]]
+        self.cellCount = int(s.n_cells)
+
+    updateTree = initializeTree  # the reference rebuilds too (treeCell.cpp:1245-1249)
+
+    def _list(self, which, cell_id):
+        cid, offs, out = self._dump["lists"][which]
+        k = int(np.searchsorted(cid, cell_id))
+        if k >= cid.size or cid[k] != cell_id:
+            raise IndexError(f"cell {cell_id} has no list {which}")
+        return [int(v) for v in out[offs[k]:offs[k + 1]]]
+
+    def intList(self, currID):
+        """(list 1, list 3) of a leaf."""
+        return self._list(1, currID), self._list(3, currID)
+
+    def extList(self, currID):
+        """(list 2, list 4) of a cell at level >= 2."""
+        return self._list(2, currID), self._list(4, currID)
+
+
+class fmm2D:
+    """Mirror of fmm2D (src/FMM/fmm2D.hpp:15-68) on the GPU FMM."""
+
+    def __init__(self, ctx: Context | None = None, params: Params | None = None):
+        self.ctx = ctx or default_context()
+        self.params = params or default_params()
+        self._ex = self._ey = None
+        self.stats: Stats | None = None
+
+    def calcField(self, _cellTree, parPos, activeFlag, srcVal):
+        """The tree argument is accepted for interface parity; the GPU rebuilds
+        it from the particles (the reference's tree is also a pure function of
+        positions and marks)."""
+        pos = np.asarray(parPos, dtype=np.float64)
+        self._ex, self._ey, self.stats = self.ctx.field2d(pos[:, 0], pos[:, 1], srcVal, activeFlag, self.params,
+                                                          stats=True)
+
+    def get_Field_x(self):
+        return self._ex
+
+    def get_Field_y(self):
+        return self._ey
+
+
+@dataclass
+class Particle:
+    """The fields of the reference's Particle (Utils.hpp:77-159) that the
+    velocity step reads and writes."""
+    x: np.ndarray
+    y: np.ndarray
+    s: np.ndarray
+    vorticity: np.ndarray
+    isActive: np.ndarray
+    z: np.ndarray | None = None
+    u: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    v: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    w: np.ndarray = field(default_factory=lambda: np.zeros(0))
+
+    @property
+    def num(self) -> int:
+        return int(np.asarray(self.x).size)
+
+
+class VelocityCalc:
+    """Mirror of VelocityCalc::get_velocity (velocity_calc.cpp:48-139) for the
+    FMM branch (VELOCITY_2D_TYPE 2): u = Ey + u_inf, v = -Ex + v_inf."""
+
+    def __init__(self, ctx: Context | None = None, params: Params | None = None, u_inf: float = 0.0,
+                 v_inf: float = 0.0):
+        self.ctx = ctx or default_context()
+        self.params = params or default_params()
+        self.u_inf, self.v_inf = u_inf, v_inf
+        self.stats: Stats | None = None
+
+    def get_velocity(self, p: Particle, step: int = 0) -> None:
+        u, v, self.stats = self.ctx.velocity2d(p.x, p.y, p.vorticity, p.s, p.isActive, self.u_inf, self.v_inf,
+                                               self.params, stats=True)
+        p.u, p.v = u, v
