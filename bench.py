@@ -1,0 +1,311 @@
+"""Benchmark of the 2D FMM velocity step on the boundary-layer workload
+(N = 778,377 particles: flat-plate field, spacings 0.005/0.02/0.04 x 0.66,
+p = 10, leaf caps 50/75).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--form mixed|fp64]
+
+Prints one JSON line (rank 0). Our arm: `value` is particle velocities per
+second of device-resident evaluations (inputs in HBM, CUDA events on the
+launching stream, L2 flushed by a 256 MiB write between steps); `e2e` is the
+same metric through the public host API (pinned host buffers, H2D + D2H
+inside the timed region); `roofline` covers the dominant kernel; and
+`cpu_baseline` is the reference's own FMM compiled from its sources
+(oracle/_ref), timed on the host cores. With --gpus N (torchrun) each rank
+evaluates its own copy of the workload (independent solves, no collective)
+and `value` is the aggregate.
+
+--impl reference times the reference's CPU implementation of the same
+evaluation on this host (rank 0 only; other ranks exit).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from lsmps_vpm_v2_b200 import workloads  # noqa: E402
+
+METRIC = "2D FMM particle velocities/sec @780k, mixed vs FP64 GPU at ≤1e-4 rel L2"
+UNIT = "particle velocities/s"
+L2_FLUSH_BYTES = 256 << 20
+P2P_FLOPS_PER_PAIR = 12  # 2 sub, 3 for r^2, 1 reciprocal, 2 x 3 multiply-add
+
+
+def workload():
+    return workloads.boundary_layer_2d(scale=0.66)
+
+
+def _dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def _oracle():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle  # noqa: E402  (checker / CPU baseline only)
+    if oracle.ref_available():
+        return oracle.Reference(), "reference"
+    return oracle.Port(), "port"
+
+
+def cpu_baseline(wl, budget_s=12.0, max_reps=20):
+    """Reference CPU FMM (tree + calcField) on the full workload, repeated
+    until ~budget_s of CPU time; all host threads (OpenMP)."""
+    checker, kind = _oracle()
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    x, y, q, a = wl["x"], wl["y"], wl["q"], wl["active"]
+    checker.fmm2d_field(x[:20000], y[:20000], q[:20000], a[:20000])  # warm-up (page-in, thread pool)
+    times = []
+    t_all = time.perf_counter()
+    while len(times) < max_reps and (time.perf_counter() - t_all) < budget_s:
+        t0 = time.perf_counter()
+        checker.fmm2d_field(x, y, q, a)
+        times.append(time.perf_counter() - t0)
+    med = statistics.median(times)
+    return {"value": x.size / med, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"{len(times)} full evaluations of the {x.size}-particle workload (tree + calcField), "
+                      f"median {med:.3f} s"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [v.strip() for v in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def run_reference(args):
+    world, rank, _ = _dist_env()
+    if rank != 0:
+        return 0
+    wl = workload()
+    checker, kind = _oracle()
+    x, y, q, a = wl["x"], wl["y"], wl["q"], wl["active"]
+    for _ in range(args.warmup):
+        checker.fmm2d_field(x, y, q, a)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        checker.fmm2d_field(x, y, q, a)
+    dt = (time.perf_counter() - t0) / max(args.steps, 1)
+    value = x.size / dt
+    threads = os.cpu_count() or 1
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"boundary_layer_2d N={x.size} p=10 caps 50/75", "n": int(x.size), "p": 10,
+                   "max_src": 50, "max_par": 75, "parallelism": "replicas"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                         "sample": f"{args.steps} full evaluations (TreeCell::initializeTree + fmm2D::calcField)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from lsmps_vpm_v2_b200 import Context, default_params, PREC_FP64, PREC_MIXED
+
+    world, rank, local = _dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    wl = workload()
+    n = int(wl["x"].size)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+    ctx = Context(local)
+    ctx.set_stream(stream.cuda_stream)
+    form = args.form
+    prm = default_params(precision=PREC_MIXED if form == "mixed" else PREC_FP64)
+
+    x = torch.from_numpy(wl["x"]).to(dev)
+    y = torch.from_numpy(wl["y"]).to(dev)
+    q = torch.from_numpy(wl["q"]).to(dev)
+    act = torch.from_numpy(wl["active"]).to(dev)
+    ex = torch.empty(n, dtype=torch.float64, device=dev)
+    ey = torch.empty(n, dtype=torch.float64, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
+
+    for _ in range(max(args.warmup, 3)):
+        ctx.field2d_device(x, y, q, act, ex, ey, prm)
+    ctx.sync()
+
+    # ---- timed region: device-resident evaluations ----
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        flush.fill_(k)
+        starts[k].record(stream)
+        ctx.field2d_device(x, y, q, act, ex, ey, prm)
+        ends[k].record(stream)
+    torch.cuda.synchronize()
+    ctx.sync()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    ms_step = float(np.mean(ms))
+    if world > 1:
+        t = torch.tensor([ms_step], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_step = float(t.item())
+    value = world * n / (ms_step * 1e-3)
+    st = ctx.last_stats()
+    launches_per_step = int(st.kernels)
+
+    # ---- stage profile (same workload, per-stage CUDA events) ----
+    stage = {k: [] for k in ("ms_tree", "ms_lists", "ms_upward", "ms_m2l", "ms_eval", "ms_p2p", "ms_total")}
+    for k in range(min(args.steps, 20)):
+        flush.fill_(k)
+        ctx.field2d_device(x, y, q, act, ex, ey, prm)
+        s = ctx.last_stats()
+        for key in stage:
+            stage[key].append(getattr(s, key))
+    stage = {k: float(np.mean(v)) for k, v in stage.items()}
+
+    # ---- end to end through the public host API (pinned buffers) ----
+    hx = torch.from_numpy(wl["x"]).pin_memory().numpy()
+    hy = torch.from_numpy(wl["y"]).pin_memory().numpy()
+    hw = torch.from_numpy(wl["omega"]).pin_memory().numpy()
+    hs = torch.from_numpy(wl["s"]).pin_memory().numpy()
+    ha = torch.from_numpy(wl["active"]).pin_memory().numpy()
+    e2e_ms = []
+    for k in range(max(3, min(args.steps, 20)) + 2):
+        flush.fill_(k)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        u, v = ctx.velocity2d(hx, hy, hw, hs, ha, 0.0, 0.0, prm)
+        t1 = time.perf_counter()
+        if k >= 2:
+            e2e_ms.append((t1 - t0) * 1e3)
+    e2e_step = float(np.mean(e2e_ms))
+    if world > 1:
+        t = torch.tensor([e2e_step], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_step = float(t.item())
+
+    # ---- roofline of the dominant kernel (near-field P2P) ----
+    fp64_peak, fp32_peak = ctx.fma_peaks()
+    pairs = int(st.p2p_pairs)
+    flops = P2P_FLOPS_PER_PAIR * pairs
+    p2p_ms = stage["ms_p2p"]
+    achieved = flops / (p2p_ms * 1e-3) / 1e12
+    peak = fp64_peak if form == "fp64" else fp32_peak
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get(f"p2p_{form}")
+    roofline = {"bound": "fp64" if form == "fp64" else "fp32", "kernel": "p2p2d" if form == "fp64" else "p2p2d_mixed",
+                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "traffic": traffic, "peak_source": "measured FMA-chain peak (vpm_measure_fma_peaks)",
+                "work": f"{P2P_FLOPS_PER_PAIR} flops x {pairs} list-1 pairs per launch"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if form == "fp64" else "f32+f64", "data": "synthetic",
+        "config": {"workload": f"boundary_layer_2d N={n} p=10 caps 50/75", "n": n, "p": 10, "max_src": 50,
+                   "max_par": 75, "form": form, "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "256 MiB write between steps (outside the per-step events)"},
+        "e2e": {"value": world * n / (e2e_step * 1e-3), "unit": UNIT, "ms_per_step": e2e_step,
+                "h2d_bytes_per_step": n * (8 * 4 + 1), "d2h_bytes_per_step": n * 16,
+                "api": "vpm_velocity2d (host buffers)"},
+        "gpu_launches": launches_per_step * args.steps,
+        "stages_ms": stage,
+        "interactions": {"p2p_pairs": pairs, "m2l_pairs": int(st.m2l_pairs), "m2p_pairs": int(st.m2p_pairs),
+                         "cells": int(st.n_cells), "leaves": int(st.n_leaves)},
+        "roofline": roofline,
+        "clocks": clk,
+        "fma_peaks_tflops": {"fp64": fp64_peak, "fp32": fp32_peak},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(wl)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--form", choices=["mixed", "fp64"], default="fp64")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -159,6 +159,13 @@ int vpm_tree2d_cells(vpm_ctx* ctx, int64_t* ids, int32_t* ints6, double* centers
 int vpm_tree2d_leaves(vpm_ctx* ctx, int64_t* leaf_ids, int64_t* offs, int32_t* pids);
 int vpm_tree2d_list(vpm_ctx* ctx, int which, int64_t* cell_ids, int64_t* offs, int64_t* ids);
 
+/*
+ * FMA-throughput microbenchmark of the device (TFLOP/s of dependent FMA
+ * chains in FP64 and FP32): the pipe peaks the near-field roofline fractions
+ * are quoted against. No counterpart in the reference (measurement utility).
+ */
+int vpm_measure_fma_peaks(vpm_ctx* ctx, double* fp64_tflops, double* fp32_tflops);
+
 #ifdef __cplusplus
 }
 #endif

@@ -93,6 +93,7 @@ SIGNATURES = {
     "vpm_tree2d_cells": (C.c_int, [_vp, _vp, _vp, _vp]),
     "vpm_tree2d_leaves": (C.c_int, [_vp, _vp, _vp, _vp]),
     "vpm_tree2d_list": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp]),
+    "vpm_measure_fma_peaks": (C.c_int, [_vp, _dp, _dp]),
 }
 
 _LIB = None

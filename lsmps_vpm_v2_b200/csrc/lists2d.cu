@@ -21,7 +21,7 @@ struct TreeView {
     // Index of the cell (L, ix, iy) or -1 when it does not exist.
     __device__ int find(int L, int ix, int iy) const {
         if (L < 0 || L > t.info->depth) return -1;
-        const int cnt = 1 << L;
+        const long long cnt = 1ll << L;
         if (ix < 0 || iy < 0 || ix >= cnt || iy >= cnt) return -1;
         int lo = t.info->level_start[L], hi = t.info->level_start[L + 1];
         const uint64_t code = morton2((uint32_t)ix, (uint32_t)iy);
@@ -60,7 +60,7 @@ __device__ void int_list(const TreeView& v, int c, double eps, int mode, uint32_
     Queue q;
     const int L = t.c_level[c], cx = t.c_ix[c], cy = t.c_iy[c];
     const double cur_len = v.len(L), ccx = t.c_cx[c], ccy = t.c_cy[c];
-    const int cnt = 1 << L;
+    const long long cnt = 1ll << L;
     for (int k = 0; k < 9; ++k) {
         int jx = cx + k % 3 - 1, jy = cy + k / 3 - 1;
         if (jx < 0 || jy < 0 || jx >= cnt || jy >= cnt) continue;
@@ -139,7 +139,7 @@ __device__ void ext_list(const TreeView& v, int c, double eps, int32_t* l2, uint
     const double cur_len = v.len(L), ccx = t.c_cx[c], ccy = t.c_cy[c];
     const int p = t.c_parent[c];
     const int PL = L - 1, px = t.c_ix[p], py = t.c_iy[p];
-    const int cnt = 1 << PL;
+    const long long cnt = 1ll << PL;
     Queue q;  // list-4 candidates
     int k2 = 0;
     const double min2 = xadd(cur_len, eps);

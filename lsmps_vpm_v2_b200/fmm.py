@@ -74,7 +74,7 @@ class Context:
         p = params or default_params()
         s = Stats()
         self._check(lib().vpm_fmm2d_field(self._h, _ptr(x), _ptr(y), _ptr(q), _ptr(a), n, C.byref(p),
-                                          _ptr(ex), _ptr(ey), C.byref(s)))
+                                          _ptr(ex), _ptr(ey), C.byref(s) if stats else None))
         return (ex, ey, s) if stats else (ex, ey)
 
     def field2d_device(self, x, y, q, active, ex, ey, params: Params | None = None):
@@ -93,8 +93,15 @@ class Context:
         p = params or default_params()
         st = Stats()
         self._check(lib().vpm_velocity2d(self._h, _ptr(x), _ptr(y), _ptr(w), _ptr(sz), _ptr(a), n, C.byref(p),
-                                         float(u_inf), float(v_inf), _ptr(u), _ptr(v), C.byref(st)))
+                                         float(u_inf), float(v_inf), _ptr(u), _ptr(v),
+                                         C.byref(st) if stats else None))
         return (u, v, st) if stats else (u, v)
+
+    def fma_peaks(self):
+        """(FP64, FP32) FMA throughput of the device in TFLOP/s."""
+        a, b = C.c_double(), C.c_double()
+        self._check(lib().vpm_measure_fma_peaks(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def last_stats(self) -> Stats:
         s = Stats()

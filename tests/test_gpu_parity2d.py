@@ -1,0 +1,129 @@
+"""CUDA FP64 2D path against the oracle, through the C ABI: tree, leafList,
+parIDList and lists 1-4 bit-exact; field within 1e-10 relative L2 with the
+reference's binomials (and with exact ones), NaN exactly where the reference
+gives NaN; full-size workload and linearity."""
+import numpy as np
+import pytest
+
+import cases2d
+from lsmps_vpm_v2_b200 import BINOM_EXACT, VpmError, default_params, workloads
+from lsmps_vpm_v2_b200.workloads import rel_l2
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-10
+
+
+def _tree_equal(g, t):
+    for k, v in (("ids", t.ids), ("par", t.par), ("src", t.src), ("leaf", t.leaf), ("active", t.active),
+                 ("centers", t.centers), ("leaf_ids", t.leaf_ids), ("leaf_offs", t.leaf_offs),
+                 ("leaf_pids", t.leaf_pids)):
+        assert np.array_equal(g[k], v), k
+    assert np.array_equal(g["level"], t.level) and np.array_equal(g["ix"], t.ix) and np.array_equal(g["iy"], t.iy)
+
+
+@pytest.mark.parametrize("name", list(cases2d.CASES))
+def test_tree_and_lists_bit_exact(ctx, port, name):
+    d = cases2d.CASES[name]()
+    x, y, a = d["x"], d["y"], d["active"]
+    ctx.build_tree2d(x, y, a)
+    g = ctx.dump_tree2d()
+    _tree_equal(g, port.tree2d(x, y, a))
+    for which in (1, 2, 3, 4):
+        cid, offs, out = g["lists"][which]
+        po, pv = port.lists2d(x, y, a, which, cid)
+        assert np.array_equal(offs, po), which
+        for k in range(cid.size):
+            assert sorted(out[offs[k]:offs[k + 1]]) == sorted(pv[po[k]:po[k + 1]]), (which, cid[k])
+
+
+@pytest.mark.parametrize("name", list(cases2d.CASES))
+def test_field_fp64(ctx, port, name):
+    d = cases2d.CASES[name]()
+    x, y, q, a = d["x"], d["y"], d["q"], d["active"]
+    ex, ey = ctx.field2d(x, y, q, a)
+    rx, ry = port.fmm2d_field(x, y, q, a)
+    fin = np.isfinite(rx) & np.isfinite(ry)
+    assert np.array_equal(fin, np.isfinite(ex) & np.isfinite(ey))
+    assert rel_l2((ex[fin], ey[fin]), (rx[fin], ry[fin])) <= TOL
+
+
+@pytest.mark.parametrize("p,caps", [(4, (50, 75)), (12, (50, 75)), (16, (20, 30)), (20, (100, 150)), (30, (50, 75))])
+def test_field_orders_and_caps(ctx, port, p, caps):
+    d = cases2d.clustered()
+    x, y, q, a = d["x"], d["y"], d["q"], d["active"]
+    prm = default_params(p=p, max_src=caps[0], max_par=caps[1])
+    ex, ey = ctx.field2d(x, y, q, a, prm)
+    rx, ry = port.fmm2d_field(x, y, q, a, p=p, max_src=caps[0], max_par=caps[1])
+    assert rel_l2((ex, ey), (rx, ry)) <= TOL
+
+
+def test_exact_binomials(ctx, port):
+    d = cases2d.plate_small()
+    x, y, q, a = d["x"], d["y"], d["q"], d["active"]
+    ex, ey = ctx.field2d(x, y, q, a, default_params(p=16, binom=BINOM_EXACT))
+    rx, ry = port.fmm2d_field(x, y, q, a, p=16, exact_binom=True)
+    assert rel_l2((ex, ey), (rx, ry)) <= TOL
+
+
+def test_golden_fixtures(ctx):
+    import glob
+    import os
+    for f in sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "fmm2d_*.npz"))):
+        g = dict(np.load(f))
+        prm = default_params(p=int(g["p"]), max_src=int(g["max_src"]), max_par=int(g["max_par"]))
+        ex, ey = ctx.field2d(g["x"], g["y"], g["q"], g["active"], prm)
+        assert rel_l2((ex, ey), (g["ex"], g["ey"])) <= TOL, f
+        d = ctx.dump_tree2d()
+        assert np.array_equal(d["ids"], g["ids"]) and np.array_equal(d["leaf_ids"], g["leaf_ids"]), f
+
+
+def test_velocity_entry(ctx):
+    d = workloads.lamb_oseen_2d(n_side=96, seed=2)
+    ex, ey = ctx.field2d(d["x"], d["y"], d["q"], d["active"])
+    u, v = ctx.velocity2d(d["x"], d["y"], d["omega"], d["s"], d["active"], 0.5, -0.25)
+    # u = Ey + u_inf, v = -Ex + v_inf (velocity_calc.cpp:572-575, 226-230)
+    assert np.max(np.abs(u - (ey + 0.5))) <= 1e-12 * np.max(np.abs(ey)) + 1e-15
+    assert np.max(np.abs(v - (-ex - 0.25))) <= 1e-12 * np.max(np.abs(ex)) + 1e-15
+
+
+def test_full_size_workload(ctx, port):
+    d = workloads.boundary_layer_2d(scale=0.66)
+    x, y, q, a = d["x"], d["y"], d["q"], d["active"]
+    ex, ey, st = ctx.field2d(x, y, q, a, stats=True)
+    assert st.depth_retry == 0 and st.n_cells > 20000
+    rx, ry = port.fmm2d_field(x, y, q, a)
+    assert rel_l2((ex, ey), (rx, ry)) <= TOL
+    # linearity in the sources (size-independent property)
+    ex2, ey2 = ctx.field2d(x, y, 2.5 * q, a)
+    assert rel_l2((ex2, ey2), (2.5 * ex, 2.5 * ey)) <= 1e-13
+
+
+def test_errors(ctx):
+    with pytest.raises(VpmError) as e:
+        ctx.field2d(np.zeros(1), np.zeros(1), np.ones(1), np.ones(1, np.uint8))
+    assert e.value.status == 22
+    x = np.linspace(0, 1, 100)
+    y = x.copy()
+    y[5] = np.nan
+    with pytest.raises(VpmError) as e:
+        ctx.field2d(x, y, np.ones(100), np.ones(100, np.uint8))
+    assert e.value.status == 22
+    with pytest.raises(VpmError):
+        ctx.field2d(x, x, np.ones(100), np.ones(100, np.uint8), default_params(p=31))
+    # still usable after errors
+    d = cases2d.CASES["tiny300"]()
+    ctx.field2d(d["x"], d["y"], d["q"], d["active"])
+
+
+def test_coincident_cluster_retries_deeper_keys(ctx, port):
+    """More than max_par particles in a cell of size 2^-16 root: the 16-level
+    keys cannot separate them, the host entry point rebuilds with 31 levels."""
+    rng = np.random.default_rng(3)
+    x = np.concatenate([rng.uniform(-1, 1, 500), 0.3 + rng.uniform(0, 1e-7, 200)])
+    y = np.concatenate([rng.uniform(-1, 1, 500), 0.2 + rng.uniform(0, 1e-7, 200)])
+    q = rng.normal(0, 1, x.size)
+    a = np.ones(x.size, np.uint8)
+    ex, ey, st = ctx.field2d(x, y, q, a, stats=True)
+    assert st.depth_retry == 1
+    rx, ry = port.fmm2d_field(x, y, q, a)
+    assert rel_l2((ex, ey), (rx, ry)) <= TOL
