@@ -62,7 +62,9 @@ typedef struct vpm_fmm_params {
     int32_t precision;    /* VPM_PREC_*                                             */
     int32_t binom;        /* VPM_BINOM_*                                            */
     int32_t max_depth;    /* deepest tree level the keys resolve (2D: 16 or 31)     */
-    int32_t reserved;
+    int32_t use_graph;    /* device entry points: capture the evaluation once as a
+                             CUDA graph and replay it while the buffers, n and the
+                             parameters are unchanged (no per-stage timings then)  */
 } vpm_fmm_params;
 
 /* Per-call figures (counts are exact; times are CUDA-event milliseconds). */

@@ -37,7 +37,7 @@ class Params(C.Structure):
         ("precision", C.c_int32),
         ("binom", C.c_int32),
         ("max_depth", C.c_int32),
-        ("reserved", C.c_int32),
+        ("use_graph", C.c_int32),
     ]
 
 

@@ -98,8 +98,10 @@ int Ctx::reserve2d(int n, int cap_cells, int P, long long cap_l1, long long cap_
     size_t o_a = L.take<double2>(C * (P + 1)), o_b = L.take<double2>(C * (P + 1)), o_cnt = L.take<unsigned>(C);
     size_t o_fx = L.take<double>(n), o_fy = L.take<double>(n);
     size_t o_geom = L.take<Geom2D>(1), o_info = L.take<TreeInfo2D>(1);
+    size_t o_coef = L.take<double>(3 * kCoefTable);
     size_t o_mixed = L.take<char>(mixed_bytes(n, cap_cells, P));
 
+    drop_graph();
     if (arena2d) cudaFree(arena2d);
     arena2d = nullptr;
     cap = Caps2D{};
@@ -139,6 +141,8 @@ int Ctx::reserve2d(int n, int cap_cells, int P, long long cap_l1, long long cap_
     lists.cap_l3 = cap_l3;
     ex2.a = (double2*)P_(o_a); ex2.b = (double2*)P_(o_b); ex2.up_count = (unsigned*)P_(o_cnt);
     ex2.fx = (double*)P_(o_fx); ex2.fy = (double*)P_(o_fy);
+    ex2.coef = (double*)P_(o_coef);
+    coef_P = -1;  // the new arena holds no coefficients yet
     mixed_base = P_(o_mixed);
     cap.n = n; cap.cells = cap_cells; cap.P = P; cap.l1 = cap_l1; cap.l3 = cap_l3;
     return VPM_OK;
@@ -187,34 +191,94 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
     tree.key_levels = K;
     VPM_CUDA_TRY(cudaMemsetAsync(d_err, 0, sizeof(unsigned), st));
     if (coef_P != p.p || coef_binom != p.binom) {
-        VPM_CUDA_TRY(set_coefficients2d(p.p, p.binom == VPM_BINOM_EXACT, st));
+        VPM_CUDA_TRY(set_coefficients2d(p.p, p.binom == VPM_BINOM_EXACT, ex2.coef, st));
         coef_P = p.p;
         coef_binom = p.binom;
     }
-    VPM_CUDA_TRY(cudaEventRecord(ev[0], st));
+    if (int r = record(0)) return r;
     VPM_CUDA_TRY(build_tree2d(x, y, q, act, tree, ts, p.max_src, p.max_par, p.exp_tree_pct, d_err, st, &launches));
-    VPM_CUDA_TRY(cudaEventRecord(ev[1], st));
+    if (int r = record(1)) return r;
     VPM_CUDA_TRY(build_lists2d(tree, lists, ts.scan, p.eps, d_err, st, &launches));
-    VPM_CUDA_TRY(cudaEventRecord(ev[2], st));
+    if (int r = record(2)) return r;
     if (tree_only) {
-        for (int i = 3; i <= 6; ++i) VPM_CUDA_TRY(cudaEventRecord(ev[i], st));
+        for (int i = 3; i <= 6; ++i)
+            if (int r = record(i)) return r;
     } else if (p.precision == VPM_PREC_MIXED) {
         int r = enqueue_mixed2d(p, o0, o1, velocity, uinf, vinf, &launches);
         if (r != VPM_OK) return r;
     } else {
         VPM_CUDA_TRY(fmm2d_upward(tree, ex2, p.p, d_err, st, &launches));
-        VPM_CUDA_TRY(cudaEventRecord(ev[3], st));
+        if (int r = record(3)) return r;
         VPM_CUDA_TRY(fmm2d_m2l(tree, lists, ex2, p.p, d_err, st, &launches));
-        VPM_CUDA_TRY(cudaEventRecord(ev[4], st));
+        if (int r = record(4)) return r;
         VPM_CUDA_TRY(fmm2d_eval(tree, lists, ex2, p.p, d_err, st, &launches));
-        VPM_CUDA_TRY(cudaEventRecord(ev[5], st));
+        if (int r = record(5)) return r;
         VPM_CUDA_TRY(fmm2d_p2p_out(tree, lists, ex2, o0, o1, velocity, uinf, vinf, d_err, st, &launches));
     }
-    VPM_CUDA_TRY(cudaEventRecord(ev[6], st));
+    if (int r = record(6)) return r;
     last_launches = launches;
     last_params = p;
     last_n = n;
     have_tree = true;
+    return VPM_OK;
+}
+
+int Ctx::record(int i) {
+    if (!timing) return VPM_OK;
+    VPM_CUDA_TRY(cudaEventRecord(ev[i], stream));
+    return VPM_OK;
+}
+
+void Ctx::drop_graph() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    gexec = nullptr;
+}
+
+// Enqueue (or replay) one evaluation on device buffers. With p.use_graph the
+// whole evaluation is captured once per (buffers, n, parameters, stream,
+// arena) and replayed as a CUDA graph: every launch in it reads its sizes from
+// device memory, so the same graph is valid for any particle set of this size.
+int Ctx::launch2d(const double* x, const double* y, const double* q, const uint8_t* act, int n,
+                  const vpm_fmm_params& p, int K, double* o0, double* o1, int velocity, double uinf,
+                  double vinf) {
+    if (!p.use_graph) return enqueue2d(x, y, q, act, n, p, K, o0, o1, velocity, uinf, vinf, false);
+    GraphKey k;
+    std::memset(&k, 0, sizeof(k));  // padding included: the key is compared bytewise
+    k.ptr[0] = x; k.ptr[1] = y; k.ptr[2] = q; k.ptr[3] = act; k.ptr[4] = o0; k.ptr[5] = o1;
+    k.n = n; k.K = K; k.velocity = velocity; k.uinf = uinf; k.vinf = vinf; k.p = p; k.stream = stream;
+    k.arena = arena2d;
+    if (gexec && std::memcmp(&k, &gkey, sizeof(k)) == 0) {
+        VPM_CUDA_TRY(cudaGraphLaunch(gexec, stream));
+        last_launches = graph_launches;
+        last_n = n;
+        return VPM_OK;
+    }
+    drop_graph();
+    if (coef_P != p.p || coef_binom != p.binom) {
+        VPM_CUDA_TRY(set_coefficients2d(p.p, p.binom == VPM_BINOM_EXACT, ex2.coef, stream));
+        coef_P = p.p;
+        coef_binom = p.binom;
+    }
+    VPM_CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    timing = false;
+    int r = enqueue2d(x, y, q, act, n, p, K, o0, o1, velocity, uinf, vinf, false);
+    timing = true;
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(stream, &g);
+    if (r != VPM_OK) {
+        if (g) cudaGraphDestroy(g);
+        return r;
+    }
+    if (e != cudaSuccess) return fail_cuda(e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&gexec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        gexec = nullptr;
+        return fail_cuda(e, "cudaGraphInstantiate");
+    }
+    std::memcpy(&gkey, &k, sizeof(k));
+    graph_launches = last_launches;
+    VPM_CUDA_TRY(cudaGraphLaunch(gexec, stream));
     return VPM_OK;
 }
 
@@ -232,14 +296,15 @@ int Ctx::collect_stats(vpm_fmm_stats* s) {
     s->list1_len = (int64_t)info.list1_len;
     s->list3_len = (int64_t)info.list3_len;
     float ms[7] = {0};
-    for (int i = 1; i <= 6; ++i) cudaEventElapsedTime(&ms[i], ev[i - 1], ev[i]);
+    if (!last_was_graph)
+        for (int i = 1; i <= 6; ++i) cudaEventElapsedTime(&ms[i], ev[i - 1], ev[i]);
     s->ms_tree = ms[1];
     s->ms_lists = ms[2];
     s->ms_upward = ms[3];
     s->ms_m2l = ms[4];
     s->ms_eval = ms[5];
     s->ms_p2p = ms[6];
-    cudaEventElapsedTime(&s->ms_total, ev[0], ev[6]);
+    if (!last_was_graph) cudaEventElapsedTime(&s->ms_total, ev[0], ev[6]);
     s->kernels = last_launches;
     s->depth_retry = depth_retry;
     // Interaction counts (exact, from the lists).
@@ -288,7 +353,9 @@ int Ctx::run2d_host(const double* x, const double* y, const double* q_or_omega, 
         } else {
             VPM_CUDA_TRY(cudaMemcpyAsync(in_q, q_or_omega, sizeof(double) * n, cudaMemcpyHostToDevice, stream));
         }
-        r = enqueue2d(in_x, in_y, in_q, in_act, n, p, K, out0, out1, velocity, uinf, vinf, tree_only);
+        last_was_graph = p.use_graph != 0 && !tree_only;
+        r = tree_only ? enqueue2d(in_x, in_y, in_q, in_act, n, p, K, out0, out1, velocity, uinf, vinf, true)
+                      : launch2d(in_x, in_y, in_q, in_act, n, p, K, out0, out1, velocity, uinf, vinf);
         if (r) return r;
         unsigned bits = 0;
         VPM_CUDA_TRY(cudaMemcpyAsync(&bits, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
@@ -469,7 +536,8 @@ int vpm_fmm2d_field_device(vpm_ctx* ctx, const double* x, const double* y, const
     if (r) return r;
     r = c->reserve2d(n, cells, p.p, l1, l3);
     if (r) return r;
-    return c->enqueue2d(x, y, q, active, n, p, p.max_depth, ex, ey, 0, 0.0, 0.0, false);
+    c->last_was_graph = p.use_graph != 0;
+    return c->launch2d(x, y, q, active, n, p, p.max_depth, ex, ey, 0, 0.0, 0.0);
 }
 
 int vpm_last_stats(vpm_ctx* ctx, vpm_fmm_stats* stats) {

@@ -35,6 +35,7 @@ __global__ void count2d(Tree2D t, Lists2D l, unsigned long long* out, const unsi
 
 Ctx::~Ctx() {
     if (device >= 0) cudaSetDevice(device);
+    drop_graph();
     if (arena2d) cudaFree(arena2d);
     if (d_err) cudaFree(d_err);
     for (auto& e : ev)
@@ -75,11 +76,23 @@ int Ctx::count_interactions(vpm_fmm_stats* s) {
     return VPM_OK;
 }
 
-size_t mixed_bytes(int n, int cap_cells, int P) { return 256; }
+// Mixed-form work area: leaf-relative FP32 particles (float4 per particle).
+size_t mixed_bytes(int n, int cap_cells, int P) { return sizeof(float4) * (size_t)n + 256; }
 
+// Mixed form: the upward pass, M2L and the far-field evaluation in FP64 and
+// the near field (P2P, the dominant stage) in FP32 with compensated sums.
 int Ctx::enqueue_mixed2d(const vpm_fmm_params& p, double* o0, double* o1, int velocity, double uinf, double vinf,
                          int* launches) {
-    return fail(VPM_EINVAL, "mixed precision is not available in this build");
+    cudaStream_t st = stream;
+    VPM_CUDA_TRY(fmm2d_upward(tree, ex2, p.p, d_err, st, launches));
+    if (int r = record(3)) return r;
+    VPM_CUDA_TRY(fmm2d_m2l(tree, lists, ex2, p.p, d_err, st, launches));
+    if (int r = record(4)) return r;
+    VPM_CUDA_TRY(fmm2d_eval(tree, lists, ex2, p.p, d_err, st, launches));
+    if (int r = record(5)) return r;
+    float4* rel = (float4*)mixed_base;
+    VPM_CUDA_TRY(fmm2d_p2p_f32(tree, lists, ex2, rel, o0, o1, velocity, uinf, vinf, d_err, st, launches));
+    return VPM_OK;
 }
 
 }  // namespace vpm

@@ -50,6 +50,21 @@ struct Ctx {
     void* mixed_base = nullptr;
     int coef_P = -1, coef_binom = -1;
 
+    // CUDA graph of the device entry point (capture once, replay)
+    struct GraphKey {
+        const void* ptr[6];
+        int n, K, velocity;
+        double uinf, vinf;
+        vpm_fmm_params p;
+        cudaStream_t stream;
+        void* arena;
+    };
+    cudaGraphExec_t gexec = nullptr;
+    GraphKey gkey{};
+    bool timing = true;  // record the per-stage events (off while capturing)
+    bool last_was_graph = false;
+    int graph_launches = 0;
+
     // last evaluation
     bool have_tree = false;
     int last_n = 0;
@@ -77,8 +92,15 @@ struct Ctx {
     int collect_stats(vpm_fmm_stats* s);
     int count_interactions(vpm_fmm_stats* s);
     int fetch_tree(HostTree2D& h);
+    int launch2d(const double* x, const double* y, const double* q, const uint8_t* act, int n,
+                 const vpm_fmm_params& p, int K, double* o0, double* o1, int velocity, double uinf, double vinf);
+    void drop_graph();
+    int record(int i);
 };
 
+cudaError_t fmm2d_p2p_f32(const Tree2D& t, const Lists2D& l, const Expansions2D& e, float4* rel, double* out0,
+                          double* out1, int velocity, double u_inf, double v_inf, unsigned* err, cudaStream_t st,
+                          int* launches);
 cudaError_t fmm2d_p2p_out(const Tree2D& t, const Lists2D& l, const Expansions2D& e, double* out0, double* out1,
                           int velocity, double u_inf, double v_inf, unsigned* err, cudaStream_t st, int* launches);
 

@@ -106,9 +106,16 @@ cudaError_t build_tree2d(const double* x, const double* y, const double* q, cons
 cudaError_t build_lists2d(const Tree2D& t, Lists2D& l, ScanScratch& scan, double eps, unsigned* err,
                           cudaStream_t st, int* launches);
 
-// Coefficient tables of the translations for order P (host side), uploaded
-// to constant memory by set_coefficients2d.
-cudaError_t set_coefficients2d(int P, bool exact_binom, cudaStream_t st);
+// Translation coefficients for order P, three (kMaxP+1)^2 tables of doubles
+// in device memory owned by the caller (each context keeps its own):
+//   m2m[p][k] = C(p-1,k-1) * (p/k)                (fmm2D.cpp:372-374)
+//   m2l[p][k] = C(p+k-1,k-1) * (-1)^k / k         (fmm2D.cpp:477-479)
+//   l2l[p][k] = C(k,p)                            (fmm2D.cpp:640-641)
+// with C from the reference's 32-bit binComb or exact. The upload
+// synchronises `st` (the host table is temporary).
+constexpr int kCoefTable = (kMaxP + 1) * (kMaxP + 1);
+constexpr int kCoefM2M = 0, kCoefM2L = kCoefTable, kCoefL2L = 2 * kCoefTable;
+cudaError_t set_coefficients2d(int P, bool exact_binom, double* dst, cudaStream_t st);
 
 // FP64 evaluation (plain form): P2M+M2M, M2L, L2L chain + M2P + L2P, P2P.
 // ex/ey are written in the caller's particle order.
@@ -116,6 +123,7 @@ struct Expansions2D {
     double2* a;          // [cap_cells][P+1] multipole
     double2* b;          // [cap_cells][P+1] local (M2L part only)
     unsigned* up_count;  // [cap_cells] children completed (upward pass)
+    double* coef;        // [3 * kCoefTable] translation coefficients
     double* fx;          // [n] far-field Ex in sorted order
     double* fy;
 };

@@ -20,15 +20,6 @@
 
 namespace vpm {
 
-// Translation coefficients for the current order, in global memory:
-//   m2m[p][k] = C(p-1,k-1) * (p/k)                (fmm2D.cpp:372-374)
-//   m2l[p][k] = C(p+k-1,k-1) * (-1)^k / k         (fmm2D.cpp:477-479)
-//   l2l[p][k] = C(k,p)                            (fmm2D.cpp:640-641)
-// with C from the reference's 32-bit binComb or exact.
-__device__ double g_m2m[(kMaxP + 1) * (kMaxP + 1)];
-__device__ double g_m2l[(kMaxP + 1) * (kMaxP + 1)];
-__device__ double g_l2l[(kMaxP + 1) * (kMaxP + 1)];
-
 namespace {
 
 constexpr int W = kMaxP + 1;
@@ -76,7 +67,9 @@ __device__ __forceinline__ double2 warp_sum2(double2 v) {
 
 // One warp per leaf. Lane k holds coefficient k (P <= 30 < 32).
 __global__ void __launch_bounds__(128)
-upward2d(Tree2D t, double2* __restrict__ a, unsigned* __restrict__ cnt, int P, unsigned* err) {
+upward2d(Tree2D t, double2* __restrict__ a, unsigned* __restrict__ cnt, const double* __restrict__ coef, int P,
+         unsigned* err) {
+    const double* g_m2m = coef + kCoefM2M;
     __shared__ double2 s_child[4][W];
     if (fatal(err)) return;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -155,7 +148,9 @@ upward2d(Tree2D t, double2* __restrict__ a, unsigned* __restrict__ cnt, int P, u
 // list 4. Powers w^m = (z_src - z_tgt)^(-m), m = 1..2P, go through shared
 // memory per group.
 __global__ void __launch_bounds__(128)
-m2l2d(Tree2D t, Lists2D l, const double2* __restrict__ a, double2* __restrict__ b, int P, unsigned* err) {
+m2l2d(Tree2D t, Lists2D l, const double2* __restrict__ a, double2* __restrict__ b, const double* __restrict__ coef,
+      int P, unsigned* err) {
+    const double* g_m2l = coef + kCoefM2L;
     extern __shared__ double2 sm[];
     if (fatal(err)) return;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -223,7 +218,8 @@ constexpr int kEvalThreads = 64;
 
 __global__ void __launch_bounds__(kEvalThreads)
 eval2d(Tree2D t, Lists2D l, const double2* __restrict__ a, const double2* __restrict__ b, double* __restrict__ fx,
-       double* __restrict__ fy, int P, unsigned* err) {
+       double* __restrict__ fy, const double* __restrict__ coef, int P, unsigned* err) {
+    const double* g_l2l = coef + kCoefL2L;
     __shared__ double2 s_b[W];
     __shared__ double2 s_nb[W];
     __shared__ int s_path[kMaxLevels2D + 1];
@@ -376,25 +372,138 @@ p2p2d(Tree2D t, Lists2D l, const double* __restrict__ fx, const double* __restri
     }
 }
 
+// ---- mixed form: FP32 near field ---------------------------------------------
+
+// Leaf-relative FP32 coordinates and FP32 strengths: x - c_leaf is formed in
+// FP64 (exact enough: |x - c| <= cell size) and rounded once.
+__global__ void leaf_relative_f32(Tree2D t, float4* __restrict__ rel, unsigned* err) {
+    if (fatal(err)) return;
+    const int nl = t.info->n_leaves;
+    for (int li = blockIdx.x; li < nl; li += gridDim.x) {
+        const int c = t.leaf_cells[li];
+        const double cx = t.c_cx[c], cy = t.c_cy[c];
+        for (int i = t.c_lo[c] + threadIdx.x; i < t.c_hi[c]; i += blockDim.x)
+            rel[i] = make_float4((float)(t.px[i] - cx), (float)(t.py[i] - cy), (float)t.pq[i], __int_as_float(i));
+    }
+}
+
+constexpr int kP2PStageF = 512;
+
+// FP32 P2P over list 1. Targets and sources are expressed relative to the
+// target leaf's centre: source = (c_src - c_tgt) [FP64 difference, rounded
+// once] + (x - c_src) [FP32], so every pair offset keeps ~1e-7 relative
+// accuracy. Each thread sums a staged block of sources in FP32 and adds the
+// block sum into an FP64 accumulator (compensated per-target summation).
+__global__ void __launch_bounds__(kP2PThreads)
+p2p2d_f32(Tree2D t, Lists2D l, const float4* __restrict__ rel, const double* __restrict__ fx,
+          const double* __restrict__ fy, double* __restrict__ out0, double* __restrict__ out1, int velocity,
+          double u_inf, double v_inf, unsigned* err) {
+    __shared__ float4 s_src[kP2PStageF];
+    __shared__ double s_px[kP2PThreads], s_py[kP2PThreads];
+    if (fatal(err)) return;
+    const int nl = t.info->n_leaves;
+    for (int li = blockIdx.x; li < nl; li += gridDim.x) {
+        const int c = t.leaf_cells[li];
+        const int lo = t.c_lo[c], hi = t.c_hi[c];
+        const double ccx = t.c_cx[c], ccy = t.c_cy[c];
+        const uint32_t o1 = l.l1_off[li], e1 = l.l1_off[li + 1];
+        for (int tb = lo; tb < hi; tb += kP2PThreads) {
+            const int T = min(kP2PThreads, hi - tb);
+            const int ns = kP2PThreads / T;
+            const int tt = threadIdx.x % T, split = threadIdx.x / T;
+            const bool on = split < ns;
+            const int ti = tb + tt;
+            const float4 tg = rel[ti];
+            const int tid = __float_as_int(tg.w);
+            double ex = 0.0, ey = 0.0;
+            uint32_t k = o1;
+            int s_lo = 0, s_hi = 0;
+            float ox = 0.f, oy = 0.f;
+            if (k < e1) {
+                const int sc = l.l1_src[k];
+                s_lo = t.c_lo[sc]; s_hi = t.c_hi[sc];
+                ox = (float)(t.c_cx[sc] - ccx); oy = (float)(t.c_cy[sc] - ccy);
+            }
+            while (k < e1) {
+                int m = 0;
+                __syncthreads();
+                while (k < e1 && m < kP2PStageF) {
+                    const int take = min(kP2PStageF - m, s_hi - s_lo);
+                    for (int j = threadIdx.x; j < take; j += blockDim.x) {
+                        float4 v = rel[s_lo + j];
+                        v.x += ox;
+                        v.y += oy;
+                        s_src[m + j] = v;
+                    }
+                    m += take;
+                    s_lo += take;
+                    if (s_lo >= s_hi) {
+                        ++k;
+                        if (k < e1) {
+                            const int sc = l.l1_src[k];
+                            s_lo = t.c_lo[sc]; s_hi = t.c_hi[sc];
+                            ox = (float)(t.c_cx[sc] - ccx); oy = (float)(t.c_cy[sc] - ccy);
+                        }
+                    }
+                }
+                __syncthreads();
+                if (on) {
+                    float bx = 0.f, by = 0.f;
+                    for (int j = split; j < m; j += ns) {
+                        const float4 sv = s_src[j];
+                        const float dx = tg.x - sv.x, dy = tg.y - sv.y;
+                        const float r2 = fmaf(dx, dx, dy * dy);
+                        float inv;
+                        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(inv) : "f"(r2));
+                        const float f = (__float_as_int(sv.w) == tid) ? 0.f : sv.z * inv;
+                        bx = fmaf(f, dx, bx);
+                        by = fmaf(f, dy, by);
+                    }
+                    ex += bx;
+                    ey += by;
+                }
+            }
+            __syncthreads();
+            if (on && split > 0) { s_px[threadIdx.x] = ex; s_py[threadIdx.x] = ey; }
+            __syncthreads();
+            if (split == 0) {
+                for (int s2 = 1; s2 < ns; ++s2) { ex += s_px[s2 * T + tt]; ey += s_py[s2 * T + tt]; }
+                ex += fx[ti];
+                ey += fy[ti];
+                const uint32_t orig = t.perm[ti];
+                if (orig >= (uint32_t)t.n) {
+                    set_err(err, ERR_INDEX);
+                } else if (velocity) {
+                    out0[orig] = ey + u_inf;
+                    out1[orig] = -ex + v_inf;
+                } else {
+                    out0[orig] = ex;
+                    out1[orig] = ey;
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
 __global__ void zero_u32(unsigned* p, int n) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = 0;
 }
 
 }  // namespace
 
-cudaError_t set_coefficients2d(int P, bool exact, cudaStream_t st) {
-    std::vector<double> m2m(W * W, 0.0), m2l(W * W, 0.0), l2l(W * W, 0.0);
+cudaError_t set_coefficients2d(int P, bool exact, double* dst, cudaStream_t st) {
+    std::vector<double> tab(3 * W * W, 0.0);
+    double* m2m = tab.data() + kCoefM2M;
+    double* m2l = tab.data() + kCoefM2L;
+    double* l2l = tab.data() + kCoefL2L;
     for (int p = 0; p <= P; ++p) {
         for (int k = 1; k <= p; ++k) m2m[p * W + k] = (double)binom_host(p - 1, k - 1, exact) * ((double)p / (double)k);
         for (int k = 1; k <= P; ++k)
             m2l[p * W + k] = (double)binom_host(p + k - 1, k - 1, exact) * ((k & 1) ? -1.0 : 1.0) / (double)k;
         for (int k = p; k <= P; ++k) l2l[p * W + k] = (double)binom_host(k, p, exact);
     }
-    cudaError_t e = cudaMemcpyToSymbolAsync(g_m2m, m2m.data(), sizeof(double) * W * W, 0, cudaMemcpyHostToDevice, st);
-    if (e != cudaSuccess) return e;
-    e = cudaMemcpyToSymbolAsync(g_m2l, m2l.data(), sizeof(double) * W * W, 0, cudaMemcpyHostToDevice, st);
-    if (e != cudaSuccess) return e;
-    e = cudaMemcpyToSymbolAsync(g_l2l, l2l.data(), sizeof(double) * W * W, 0, cudaMemcpyHostToDevice, st);
+    cudaError_t e = cudaMemcpyAsync(dst, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return e;
     // The host vectors go out of scope: wait for the copies.
     return cudaStreamSynchronize(st);
@@ -404,7 +513,7 @@ cudaError_t fmm2d_upward(const Tree2D& t, Expansions2D& e, int P, unsigned* err,
     cudaError_t r = cudaMemsetAsync(e.a, 0, sizeof(double2) * (size_t)t.cap_cells * (P + 1), st);
     if (r != cudaSuccess) return r;
     zero_u32<<<148, 256, 0, st>>>(e.up_count, t.cap_cells);
-    upward2d<<<148 * 8, 128, 0, st>>>(t, e.a, e.up_count, P, err);
+    upward2d<<<148 * 8, 128, 0, st>>>(t, e.a, e.up_count, e.coef, P, err);
     *launches += 2;
     return cudaGetLastError();
 }
@@ -413,14 +522,14 @@ cudaError_t fmm2d_m2l(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P,
                       int* launches) {
     const int G = 32 / P;
     const size_t smem = sizeof(double2) * 4 * (size_t)(G * (2 * P + 1) + 2 * G * (P + 1));
-    m2l2d<<<148 * 16, 128, smem, st>>>(t, l, e.a, e.b, P, err);
+    m2l2d<<<148 * 16, 128, smem, st>>>(t, l, e.a, e.b, e.coef, P, err);
     *launches += 1;
     return cudaGetLastError();
 }
 
 cudaError_t fmm2d_eval(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, unsigned* err, cudaStream_t st,
                        int* launches) {
-    eval2d<<<148 * 16, kEvalThreads, 0, st>>>(t, l, e.a, e.b, e.fx, e.fy, P, err);
+    eval2d<<<148 * 16, kEvalThreads, 0, st>>>(t, l, e.a, e.b, e.fx, e.fy, e.coef, P, err);
     *launches += 1;
     return cudaGetLastError();
 }
@@ -429,6 +538,15 @@ cudaError_t fmm2d_p2p_out(const Tree2D& t, const Lists2D& l, const Expansions2D&
                           int velocity, double u_inf, double v_inf, unsigned* err, cudaStream_t st, int* launches) {
     p2p2d<<<148 * 16, kP2PThreads, 0, st>>>(t, l, e.fx, e.fy, out0, out1, velocity, u_inf, v_inf, err);
     *launches += 1;
+    return cudaGetLastError();
+}
+
+cudaError_t fmm2d_p2p_f32(const Tree2D& t, const Lists2D& l, const Expansions2D& e, float4* rel, double* out0,
+                          double* out1, int velocity, double u_inf, double v_inf, unsigned* err, cudaStream_t st,
+                          int* launches) {
+    leaf_relative_f32<<<148 * 8, 128, 0, st>>>(t, rel, err);
+    p2p2d_f32<<<148 * 16, kP2PThreads, 0, st>>>(t, l, rel, e.fx, e.fy, out0, out1, velocity, u_inf, v_inf, err);
+    *launches += 2;
     return cudaGetLastError();
 }
 
