@@ -173,7 +173,8 @@ def run_ours(args):
     ctx = Context(local)
     ctx.set_stream(stream.cuda_stream)
     form = args.form
-    prm = default_params(precision=PREC_MIXED if form == "mixed" else PREC_FP64)
+    prm = default_params(precision=PREC_MIXED if form == "mixed" else PREC_FP64, use_graph=0 if args.no_graph else 1)
+    prm_stage = default_params(precision=prm.precision)  # eager launches: per-stage events
 
     x = torch.from_numpy(wl["x"]).to(dev)
     y = torch.from_numpy(wl["y"]).to(dev)
@@ -220,7 +221,7 @@ def run_ours(args):
     stage = {k: [] for k in ("ms_tree", "ms_lists", "ms_upward", "ms_m2l", "ms_eval", "ms_p2p", "ms_total")}
     for k in range(min(args.steps, 20)):
         flush.fill_(k)
-        ctx.field2d_device(x, y, q, act, ex, ey, prm)
+        ctx.field2d_device(x, y, q, act, ex, ey, prm_stage)
         s = ctx.last_stats()
         for key in stage:
             stage[key].append(getattr(s, key))
@@ -270,7 +271,8 @@ def run_ours(args):
         "vs_baseline": None, "dtype": "f64" if form == "fp64" else "f32+f64", "data": "synthetic",
         "config": {"workload": f"boundary_layer_2d N={n} p=10 caps 50/75", "n": n, "p": 10, "max_src": 50,
                    "max_par": 75, "form": form, "parallelism": "replicas" if world > 1 else "single",
-                   "l2": "256 MiB write between steps (outside the per-step events)"},
+                   "l2": "256 MiB write between steps (outside the per-step events)",
+                   "launch": "CUDA graph replay" if prm.use_graph else "eager"},
         "e2e": {"value": world * n / (e2e_step * 1e-3), "unit": UNIT, "ms_per_step": e2e_step,
                 "h2d_bytes_per_step": n * (8 * 4 + 1), "d2h_bytes_per_step": n * 16,
                 "api": "vpm_velocity2d (host buffers)"},
@@ -301,6 +303,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--form", choices=["mixed", "fp64"], default="fp64")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-graph", action="store_true", help="launch stage by stage instead of replaying a CUDA graph")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

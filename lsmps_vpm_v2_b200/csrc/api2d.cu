@@ -69,7 +69,7 @@ int Ctx::reserve2d(int n, int cap_cells, int P, long long cap_l1, long long cap_
     cap_l1 = std::max(cap_l1, cap.l1);
     cap_l3 = std::max(cap_l3, cap.l3);
     const int K = kMaxLevels2D;
-    const int lvl_tiles = ceil_div(cap_cells, 256) + 1;
+    const int lvl_tiles = ceil_div(cap_cells, 8) + 1;   // tiles of 8 parents
     const int s_tiles = sort_tiles(n);
     const int sc_tiles = scan_tiles(std::max(n, cap_cells) + 1);
     Layout2D L;
@@ -99,6 +99,9 @@ int Ctx::reserve2d(int n, int cap_cells, int P, long long cap_l1, long long cap_
     size_t o_fx = L.take<double>(n), o_fy = L.take<double>(n);
     size_t o_geom = L.take<Geom2D>(1), o_info = L.take<TreeInfo2D>(1);
     size_t o_coef = L.take<double>(3 * kCoefTable);
+    size_t o_op = L.take<double2>((size_t)49 * (P + 1) * P);
+    const int dlev = dense_levels_for(n);
+    size_t o_dense = L.take<int32_t>((size_t)dense_entries(dlev));
     size_t o_mixed = L.take<char>(mixed_bytes(n, cap_cells, P));
 
     drop_graph();
@@ -131,6 +134,8 @@ int Ctx::reserve2d(int n, int cap_cells, int P, long long cap_l1, long long cap_
     tree.c_cx = (double*)P_(o_ccx); tree.c_cy = (double*)P_(o_ccy); tree.c_code = (uint64_t*)P_(o_ccode);
     tree.leaf_cells = (int32_t*)P_(o_leaves);
     tree.geom = (Geom2D*)P_(o_geom); tree.info = (TreeInfo2D*)P_(o_info);
+    tree.dense = (int32_t*)P_(o_dense);
+    tree.dense_levels = dlev;
     tree.cap_cells = cap_cells;
     lists.l2_src = (int32_t*)P_(o_l2); lists.l2_slot = (uint8_t*)P_(o_l2s); lists.l2_n = (uint8_t*)P_(o_l2n);
     lists.l4_src = (int32_t*)P_(o_l4); lists.l4_n = (uint8_t*)P_(o_l4n);
@@ -142,6 +147,7 @@ int Ctx::reserve2d(int n, int cap_cells, int P, long long cap_l1, long long cap_
     ex2.a = (double2*)P_(o_a); ex2.b = (double2*)P_(o_b); ex2.up_count = (unsigned*)P_(o_cnt);
     ex2.fx = (double*)P_(o_fx); ex2.fy = (double*)P_(o_fy);
     ex2.coef = (double*)P_(o_coef);
+    ex2.op = (double2*)P_(o_op);
     coef_P = -1;  // the new arena holds no coefficients yet
     mixed_base = P_(o_mixed);
     cap.n = n; cap.cells = cap_cells; cap.P = P; cap.l1 = cap_l1; cap.l3 = cap_l3;
@@ -192,6 +198,7 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
     VPM_CUDA_TRY(cudaMemsetAsync(d_err, 0, sizeof(unsigned), st));
     if (coef_P != p.p || coef_binom != p.binom) {
         VPM_CUDA_TRY(set_coefficients2d(p.p, p.binom == VPM_BINOM_EXACT, ex2.coef, st));
+        VPM_CUDA_TRY(set_m2l_operators2d(p.p, p.binom == VPM_BINOM_EXACT, ex2.op, st));
         coef_P = p.p;
         coef_binom = p.binom;
     }
@@ -256,6 +263,7 @@ int Ctx::launch2d(const double* x, const double* y, const double* q, const uint8
     drop_graph();
     if (coef_P != p.p || coef_binom != p.binom) {
         VPM_CUDA_TRY(set_coefficients2d(p.p, p.binom == VPM_BINOM_EXACT, ex2.coef, stream));
+        VPM_CUDA_TRY(set_m2l_operators2d(p.p, p.binom == VPM_BINOM_EXACT, ex2.op, stream));
         coef_P = p.p;
         coef_binom = p.binom;
     }

@@ -61,7 +61,20 @@ struct Tree2D {
     double *c_cx, *c_cy;
     uint64_t* c_code;
     int32_t* leaf_cells;
+    // Dense lookup grid: dense[reference cell ID] = cell index for levels
+    // <= dense_levels (nullptr: none). Entries are never cleared: a lookup
+    // accepts an entry only if that cell has the queried level and index.
+    int32_t* dense;
+    int dense_levels;
 };
+
+// Dense grid levels for n particles (<= 11, i.e. <= 5.6M entries).
+inline int dense_levels_for(int n) {
+    int L = 4;
+    while (L < 11 && (1ll << (2 * (L - 2))) < (long long)n) ++L;
+    return L;
+}
+inline long long dense_entries(int levels) { return ((1ll << (2 * (levels + 1))) - 1) / 3; }
 
 // Interaction lists. Lists 2 and 4 are fixed-width per cell; lists 1 and 3 are
 // CSR over leaves.
@@ -91,7 +104,7 @@ struct TreeScratch2D {
     uint32_t* act_u32;
     uint64_t* lvl_status;   // [kMaxLevels2D + 1][max_tiles]
     unsigned* lvl_ticket;   // [kMaxLevels2D + 2]
-    int lvl_max_tiles;
+    int lvl_max_tiles;      // in tiles of 8 parents
     SortScratch sort;
     ScanScratch scan;
 };
@@ -116,6 +129,7 @@ cudaError_t build_lists2d(const Tree2D& t, Lists2D& l, ScanScratch& scan, double
 constexpr int kCoefTable = (kMaxP + 1) * (kMaxP + 1);
 constexpr int kCoefM2M = 0, kCoefM2L = kCoefTable, kCoefL2L = 2 * kCoefTable;
 cudaError_t set_coefficients2d(int P, bool exact_binom, double* dst, cudaStream_t st);
+cudaError_t set_m2l_operators2d(int P, bool exact_binom, double2* dst, cudaStream_t st);
 
 // FP64 evaluation (plain form): P2M+M2M, M2L, L2L chain + M2P + L2P, P2P.
 // ex/ey are written in the caller's particle order.
@@ -124,6 +138,7 @@ struct Expansions2D {
     double2* b;          // [cap_cells][P+1] local (M2L part only)
     unsigned* up_count;  // [cap_cells] children completed (upward pass)
     double* coef;        // [3 * kCoefTable] translation coefficients
+    double2* op;         // [49][P+1][P] list-2 M2L operators, or nullptr (direct formula)
     double* fx;          // [n] far-field Ex in sorted order
     double* fy;
 };

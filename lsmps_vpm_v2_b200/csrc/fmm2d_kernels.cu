@@ -16,6 +16,7 @@
 //                 added to the far field and written in the caller's order.
 #include "fmm2d.cuh"
 
+#include <complex>
 #include <vector>
 
 namespace vpm {
@@ -65,79 +66,113 @@ __device__ __forceinline__ double2 warp_sum2(double2 v) {
 
 // ---- upward pass -----------------------------------------------------------
 
-// One warp per leaf. Lane k holds coefficient k (P <= 30 < 32).
-__global__ void __launch_bounds__(128)
-upward2d(Tree2D t, double2* __restrict__ a, unsigned* __restrict__ cnt, const double* __restrict__ coef, int P,
-         unsigned* err) {
-    const double* g_m2m = coef + kCoefM2M;
-    __shared__ double2 s_child[4][W];
+constexpr int kP2MWarps = 2;
+constexpr int kAccPad = 33;  // padded lane stride of the P2M accumulators
+
+// P2M, one warp per leaf: lane j takes particles j, j+32, ... and adds
+// q (z - z_c)^k into its own shared-memory accumulator column k; the columns
+// are then summed in a fixed order (deterministic).
+__global__ void __launch_bounds__(32 * kP2MWarps)
+p2m2d(Tree2D t, double2* __restrict__ a, int P, unsigned* err) {
+    extern __shared__ double2 acc_sm[];
     if (fatal(err)) return;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    double2* acc = acc_sm + (size_t)wib * (P + 1) * kAccPad;
     const int nl = t.info->n_leaves;
-    const int warps = gridDim.x * (blockDim.x >> 5);
-    for (int li = blockIdx.x * (blockDim.x >> 5) + wib; li < nl; li += warps) {
+    const int warps = gridDim.x * kP2MWarps;
+    for (int li = blockIdx.x * kP2MWarps + wib; li < nl; li += warps) {
         const int c = t.leaf_cells[li];
-        if (t.c_flags[c] & CELL_ACTIVE) {
-            const double zx = t.c_cx[c], zy = t.c_cy[c];
-            const int lo = t.c_lo[c], hi = t.c_hi[c];
-            double2 acc = make_double2(0.0, 0.0);
-            for (int j0 = lo; j0 < hi; j0 += 32) {
-                const int j = j0 + lane;
-                double q = 0.0;
-                double2 w = make_double2(0.0, 0.0);
-                if (j < hi && t.pact[j]) {
-                    q = t.pq[j];
-                    w = make_double2(t.px[j] - zx, t.py[j] - zy);
-                }
-                double2 wk = make_double2(q, 0.0);  // q w^k
-                for (int k = 0; k <= P; ++k) {
-                    double2 s = warp_sum2(wk);
-                    if (lane == k) acc = cadd(acc, s);
-                    wk = cmul(wk, w);
-                }
+        if (!(t.c_flags[c] & CELL_ACTIVE)) continue;
+        for (int k = 0; k <= P; ++k) acc[k * kAccPad + lane] = make_double2(0.0, 0.0);
+        const double zx = t.c_cx[c], zy = t.c_cy[c];
+        const int lo = t.c_lo[c], hi = t.c_hi[c];
+        for (int j = lo + lane; j < hi; j += 32) {
+            if (!t.pact[j]) continue;
+            const double2 w = make_double2(t.px[j] - zx, t.py[j] - zy);
+            double2 wk = make_double2(t.pq[j], 0.0);
+            for (int k = 0; k <= P; ++k) {
+                double2* ak = &acc[k * kAccPad + lane];
+                *ak = cadd(*ak, wk);
+                wk = cmul(wk, w);
             }
-            if (lane <= P) a[(size_t)c * (P + 1) + lane] = acc;
         }
-        // Walk up: the last child of a parent to finish computes the parent.
-        int cur = c;
-        for (;;) {
-            const int par = t.c_parent[cur];
-            if (par <= 0) break;  // the root's expansion is never used
-            __threadfence();
+        __syncwarp();
+        if (lane <= P) {
+            double2 sum = make_double2(0.0, 0.0);
+            for (int l = 0; l < 32; ++l) sum = cadd(sum, acc[lane * kAccPad + l]);
+            a[(size_t)c * (P + 1) + lane] = sum;
+        }
+        __syncwarp();
+    }
+}
+
+// M2M into the active non-leaf cells of level L (fmm2D.cpp:309-379), one warp
+// per cell, lane p computing a_p by Horner's rule in t = z_child - z_parent:
+//   a_p += a0 t^p + sum_{k=1..p} m2m[p][k] a_k t^(p-k).
+__global__ void __launch_bounds__(128)
+m2m_level2d(Tree2D t, double2* __restrict__ a, const double* __restrict__ coef, int P, int L, unsigned* err) {
+    __shared__ double2 s_child[4][W];
+    if (fatal(err)) return;
+    const double* g_m2m = coef + kCoefM2M;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int c0 = t.info->level_start[L], c1 = t.info->level_start[L + 1];
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    for (int c = c0 + blockIdx.x * (blockDim.x >> 5) + wib; c < c1; c += warps) {
+        const uint8_t f = t.c_flags[c];
+        if ((f & CELL_LEAF) || !(f & CELL_ACTIVE)) continue;
+        const double px = t.c_cx[c], py = t.c_cy[c];
+        const unsigned m = t.c_chmask[c];
+        const int ch0 = t.c_child0[c];
+        if (ch0 < 0) continue;
+        double2 acc = make_double2(0.0, 0.0);
+        for (int r = 0; r < __popc(m); ++r) {
+            const int ch = ch0 + r;
+            if (lane <= P) s_child[wib][lane] = a[(size_t)ch * (P + 1) + lane];
             __syncwarp();
-            unsigned old = 0;
-            if (lane == 0) old = atomicAdd(&cnt[par], 1u);
-            old = __shfl_sync(0xffffffffu, old, 0);
-            const unsigned m = t.c_chmask[par];
-            if (old != (unsigned)__popc(m) - 1u) break;
-            __threadfence();
-            if (t.c_flags[par] & CELL_ACTIVE) {
-                const double px = t.c_cx[par], py = t.c_cy[par];
-                double2 acc = make_double2(0.0, 0.0);
-                const int c0 = t.c_child0[par];
-                for (int r = 0; r < __popc(m); ++r) {
-                    const int ch = c0 + r;
-                    if (lane <= P) s_child[wib][lane] = ldcg2(&a[(size_t)ch * (P + 1) + lane]);
-                    __syncwarp();
-                    const double2 tt = make_double2(t.c_cx[ch] - px, t.c_cy[ch] - py);
-                    if (lane == 0) {
-                        acc = cadd(acc, s_child[wib][0]);
-                    } else if (lane <= P) {
-                        // sum_{j=0..p} coef_j t^j with coef_p = a0, coef_{p-k} = m2m[p][k] a_k
-                        const int p = lane;
-                        double2 S = s_child[wib][0];
-                        for (int j = p - 1; j >= 0; --j) {
-                            const int k = p - j;
-                            S = cfma(S, tt, cscale(s_child[wib][k], g_m2m[p * W + k]));
-                        }
-                        acc = cadd(acc, S);
-                    }
-                    __syncwarp();
+            const double2 tt = make_double2(t.c_cx[ch] - px, t.c_cy[ch] - py);
+            if (lane == 0) {
+                acc = cadd(acc, s_child[wib][0]);
+            } else if (lane <= P) {
+                const int p = lane;
+                double2 S = s_child[wib][0];
+                for (int j = p - 1; j >= 0; --j) {
+                    const int k = p - j;
+                    S = cfma(S, tt, cscale(s_child[wib][k], g_m2m[p * W + k]));
                 }
-                if (lane <= P) a[(size_t)par * (P + 1) + lane] = acc;
+                acc = cadd(acc, S);
             }
-            cur = par;
+            __syncwarp();
         }
+        if (lane <= P) a[(size_t)c * (P + 1) + lane] = acc;
+    }
+}
+
+// L2L pull into every cell of level L >= 3 from its parent (fmm2D.cpp:587-651,
+// where each non-leaf parent at levels 2..max-1 pushes into its children):
+//   b_p(c) += sum_{k=p..P} l2l[p][k] b_k(parent) t^(k-p),  t = z_c - z_parent.
+// The parent's expansion is final because level L-1 ran in the previous launch.
+__global__ void __launch_bounds__(128)
+l2l_level2d(Tree2D t, double2* __restrict__ b, const double* __restrict__ coef, int P, int L, unsigned* err) {
+    __shared__ double2 s_par[4][W];
+    if (fatal(err)) return;
+    const double* g_l2l = coef + kCoefL2L;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int c0 = t.info->level_start[L], c1 = t.info->level_start[L + 1];
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    for (int c = c0 + blockIdx.x * (blockDim.x >> 5) + wib; c < c1; c += warps) {
+        const int par = t.c_parent[c];
+        if (lane <= P) s_par[wib][lane] = b[(size_t)par * (P + 1) + lane];
+        __syncwarp();
+        if (lane <= P) {
+            const double2 tt = make_double2(t.c_cx[c] - t.c_cx[par], t.c_cy[c] - t.c_cy[par]);
+            const int pp = lane;
+            const double* cf = g_l2l + pp * W;
+            double2 S = cscale(s_par[wib][P], cf[P]);
+            for (int kk = P - 1; kk >= pp; --kk) S = cfma(S, tt, cscale(s_par[wib][kk], cf[kk]));
+            double2* bc = &b[(size_t)c * (P + 1) + pp];
+            *bc = cadd(*bc, S);
+        }
+        __syncwarp();
     }
 }
 
@@ -212,53 +247,123 @@ m2l2d(Tree2D t, Lists2D l, const double2* __restrict__ a, double2* __restrict__ 
     }
 }
 
-// ---- leaf evaluation: L2L chain, M2P (list 3), L2P --------------------------
+// M2L with precomputed list-2 operators. For a list-2 pair the source sits
+// at the integer offset tau = (dx, dy) in {-3..3}^2 cell lengths r, and with
+// scaled expansions a~_k = a_k / r^k, b~_p = r^p b_p the translation
+//   b~_p = sum_{k=0..P} T_tau[p][k] a~_k,
+//   T_tau[p][0] = -(1/p) tau^-p,  T_tau[p][k] = -m2l[p][k] tau^-(p+k)
+// does not depend on the level (the same algebra as fmm2D.cpp:471-481). The
+// 49 operators (stored [slot][k][p], p fastest) replace the per-pair powers.
+// List-4 sources (coarser leaves, arbitrary offsets) use the direct formula.
+// One warp per target cell, split into G = 32/P groups of P lanes.
+__global__ void __launch_bounds__(128)
+m2l2d_op(Tree2D t, Lists2D l, const double2* __restrict__ a, double2* __restrict__ b,
+         const double2* __restrict__ op, const double* __restrict__ coef, int P, unsigned* err) {
+    extern __shared__ double2 sm[];
+    if (fatal(err)) return;
+    const double* g_m2l = coef + kCoefM2L;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int G = 32 / P;
+    const int g = lane / P, p = lane % P + 1;
+    const bool on = g < G;
+    // per warp: as[G][P+1] (scaled sources), pw[G][2P+1] (list-4 powers), part[G][P+1]
+    double2* as = sm + (size_t)wib * (G * (P + 1) * 2 + G * (2 * P + 1));
+    double2* part = as + G * (P + 1);
+    double2* pw = part + G * (P + 1);
+    const double root = t.geom->root;
+    const int c_begin = t.info->level_start[2], c_end = t.info->n_cells;
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    for (int c = c_begin + blockIdx.x * (blockDim.x >> 5) + wib; c < c_end; c += warps) {
+        const int n2 = l.l2_n[c], n4 = l.l4_n[c];
+        const double rinv = ldexp(1.0, (int)t.c_level[c]) / root;  // 1 / cell length
+        const double zx = t.c_cx[c], zy = t.c_cy[c];
+        double2 acc_s = make_double2(0.0, 0.0);  // scaled (list 2)
+        double2 acc = make_double2(0.0, 0.0);    // unscaled (list 4)
+        // rinv^k for the lanes' k = p (and k = 0 handled by p == 1 lanes)
+        double rk = 1.0;
+        for (int e = 0; e < p; ++e) rk *= rinv;  // rinv^p
+        for (int s0 = 0; s0 < n2; s0 += G) {
+            const int si = s0 + g;
+            const bool has = on && si < n2;
+            int src = 0, slot = 0;
+            if (has) {
+                src = l.l2_src[(size_t)c * kList2Cap + si];
+                slot = l.l2_slot[(size_t)c * kList2Cap + si];
+                as[g * (P + 1) + p] = cscale(a[(size_t)src * (P + 1) + p], rk);
+                if (p == 1) as[g * (P + 1)] = a[(size_t)src * (P + 1)];
+            }
+            __syncwarp();
+            if (has) {
+                const double2* A = as + g * (P + 1);
+                const double2* T = op + (size_t)slot * (P + 1) * P + (p - 1);
+                double2 sacc = acc_s;
+                for (int k = 0; k <= P; ++k) sacc = cfma(T[(size_t)k * P], A[k], sacc);
+                acc_s = sacc;
+            }
+            __syncwarp();
+        }
+        for (int s0 = 0; s0 < n4; s0 += G) {
+            const int si = s0 + g;
+            const bool has = on && si < n4;
+            int src = 0;
+            if (has) src = l.l4_src[(size_t)c * kList4Cap + si];
+            double2 w = make_double2(0.0, 0.0);
+            if (has) w = cinv(make_double2(t.c_cx[src] - zx, t.c_cy[src] - zy));
+            double2 wp = make_double2(1.0, 0.0), base = w;
+            for (int e = p; e > 0; e >>= 1) {
+                if (e & 1) wp = cmul(wp, base);
+                base = cmul(base, base);
+            }
+            const double2 wP = make_double2(__shfl_sync(0xffffffffu, wp.x, on ? g * P + P - 1 : lane),
+                                            __shfl_sync(0xffffffffu, wp.y, on ? g * P + P - 1 : lane));
+            double2* Wg = pw + g * (2 * P + 1);
+            if (has) {
+                Wg[p] = wp;
+                Wg[p + P] = cmul(wp, wP);
+                as[g * (P + 1) + p] = a[(size_t)src * (P + 1) + p];
+                if (p == 1) as[g * (P + 1)] = a[(size_t)src * (P + 1)];
+            }
+            __syncwarp();
+            if (has) {
+                const double2* A = as + g * (P + 1);
+                double2 sv = cscale(cmul(A[0], Wg[p]), 1.0 / (double)p);
+                const double* cf = g_m2l + p * W;
+                for (int k = 1; k <= P; ++k) sv = cfma(cscale(A[k], cf[k]), Wg[p + k], sv);
+                acc = csub(acc, sv);
+            }
+            __syncwarp();
+        }
+        if (on) part[g * (P + 1) + p] = cadd(cscale(acc_s, rk), acc);
+        __syncwarp();
+        if (lane < P) {
+            double2 tot = make_double2(0.0, 0.0);
+            for (int gg = 0; gg < G; ++gg) tot = cadd(tot, part[gg * (P + 1) + lane + 1]);
+            b[(size_t)c * (P + 1) + lane + 1] = tot;
+        }
+        if (lane == 0) b[(size_t)c * (P + 1)] = make_double2(0.0, 0.0);
+        __syncwarp();
+    }
+}
+
+// ---- leaf evaluation: M2P (list 3), L2P --------------------------------------
 
 constexpr int kEvalThreads = 64;
 
+// Far field of every particle of a leaf: M2P over list 3 (fmm2D.cpp:1040-1066)
+// and L2P of the leaf's complete local expansion (fmm2D.cpp:1076-1093). Cells
+// above level 2 carry no local expansion (M2L starts at level 2).
 __global__ void __launch_bounds__(kEvalThreads)
 eval2d(Tree2D t, Lists2D l, const double2* __restrict__ a, const double2* __restrict__ b, double* __restrict__ fx,
-       double* __restrict__ fy, const double* __restrict__ coef, int P, unsigned* err) {
-    const double* g_l2l = coef + kCoefL2L;
+       double* __restrict__ fy, int P, unsigned* err) {
     __shared__ double2 s_b[W];
-    __shared__ double2 s_nb[W];
-    __shared__ int s_path[kMaxLevels2D + 1];
     if (fatal(err)) return;
     const int nl = t.info->n_leaves;
     for (int li = blockIdx.x; li < nl; li += gridDim.x) {
         const int c = t.leaf_cells[li];
         const int L = t.c_level[c];
-        // Local expansion of the leaf: b(level 2 ancestor) pushed down.
-        if (threadIdx.x == 0) {
-            int cur = c;
-            for (int k = L; k >= 0; --k) {
-                s_path[k] = cur < 0 ? 0 : cur;
-                if (cur >= 0) cur = t.c_parent[cur];
-            }
-        }
+        if (threadIdx.x <= P)
+            s_b[threadIdx.x] = L >= 2 ? b[(size_t)c * (P + 1) + threadIdx.x] : make_double2(0.0, 0.0);
         __syncthreads();
-        if (L >= 2) {
-            const int lane = threadIdx.x;
-            if (lane <= P) s_b[lane] = b[(size_t)s_path[2] * (P + 1) + lane];
-            __syncthreads();
-            for (int k = 3; k <= L; ++k) {
-                const int ch = s_path[k], par = s_path[k - 1];
-                if (lane <= P) {
-                    const double2 tt = make_double2(t.c_cx[ch] - t.c_cx[par], t.c_cy[ch] - t.c_cy[par]);
-                    const int pp = lane;
-                    const double* cf = g_l2l + pp * W;
-                    double2 S = cscale(s_b[P], cf[P]);
-                    for (int kk = P - 1; kk >= pp; --kk) S = cfma(S, tt, cscale(s_b[kk], cf[kk]));
-                    s_nb[pp] = cadd(b[(size_t)ch * (P + 1) + pp], S);
-                }
-                __syncthreads();
-                if (lane <= P) s_b[lane] = s_nb[lane];
-                __syncthreads();
-            }
-        } else {
-            if (threadIdx.x <= P) s_b[threadIdx.x] = make_double2(0.0, 0.0);
-            __syncthreads();
-        }
         const int lo = t.c_lo[c], hi = t.c_hi[c];
         const double zx = t.c_cx[c], zy = t.c_cy[c];
         const uint32_t o3 = l.l3_off[li], e3 = l.l3_off[li + 1];
@@ -290,16 +395,21 @@ eval2d(Tree2D t, Lists2D l, const double2* __restrict__ a, const double2* __rest
 // ---- P2P over list 1 --------------------------------------------------------
 
 constexpr int kP2PThreads = 128;
-constexpr int kP2PStage = 256;
 
+// One block per leaf (grid-stride). Thread (t, split) owns target t and the
+// sources split, split + ns, ... of every list-1 cell; sources are read from
+// global memory (L1-resident, nearly warp-uniform addresses), so the pair
+// loop has no barrier. The partial sums of a target's splits are combined in
+// a fixed order at the end.
 __global__ void __launch_bounds__(kP2PThreads)
 p2p2d(Tree2D t, Lists2D l, const double* __restrict__ fx, const double* __restrict__ fy, double* __restrict__ out0,
       double* __restrict__ out1, int velocity, double u_inf, double v_inf, unsigned* err) {
-    __shared__ double s_x[kP2PStage], s_y[kP2PStage], s_q[kP2PStage];
-    __shared__ int s_i[kP2PStage];
     __shared__ double s_px[kP2PThreads], s_py[kP2PThreads];
     if (fatal(err)) return;
     const int nl = t.info->n_leaves;
+    const double* __restrict__ px = t.px;
+    const double* __restrict__ py = t.py;
+    const double* __restrict__ pq = t.pq;
     for (int li = blockIdx.x; li < nl; li += gridDim.x) {
         const int c = t.leaf_cells[li];
         const int lo = t.c_lo[c], hi = t.c_hi[c];
@@ -310,46 +420,35 @@ p2p2d(Tree2D t, Lists2D l, const double* __restrict__ fx, const double* __restri
             const int tt = threadIdx.x % T, split = threadIdx.x / T;
             const bool on = split < ns;
             const int ti = tb + tt;
-            const double xt = t.px[ti], yt = t.py[ti];
-            double ex = 0.0, ey = 0.0;
-            // Stage list-1 sources in chunks.
-            uint32_t k = o1;
-            int s_lo = 0, s_hi = 0;  // remaining range of the current source cell
-            if (k < e1) { const int sc = l.l1_src[k]; s_lo = t.c_lo[sc]; s_hi = t.c_hi[sc]; }
-            while (k < e1) {
-                int m = 0;
-                __syncthreads();
-                // fill the stage (uniform control flow: all threads walk the same ranges)
-                while (k < e1 && m < kP2PStage) {
-                    const int take = min(kP2PStage - m, s_hi - s_lo);
-                    for (int j = threadIdx.x; j < take; j += blockDim.x) {
-                        const int gj = s_lo + j;
-                        s_x[m + j] = t.px[gj];
-                        s_y[m + j] = t.py[gj];
-                        s_q[m + j] = t.pq[gj];
-                        s_i[m + j] = gj;
+            const double xt = px[ti], yt = py[ti];
+            double ex0 = 0.0, ey0 = 0.0, ex1 = 0.0, ey1 = 0.0;
+            if (on) {
+                for (uint32_t k = o1; k < e1; ++k) {
+                    const int sc = l.l1_src[k];
+                    const int s_hi = t.c_hi[sc];
+                    int j = t.c_lo[sc] + split;
+                    for (; j + ns < s_hi; j += 2 * ns) {
+                        const int j1 = j + ns;
+                        const double dx0 = xt - __ldg(px + j), dy0 = yt - __ldg(py + j);
+                        const double dx1 = xt - __ldg(px + j1), dy1 = yt - __ldg(py + j1);
+                        const double r0 = fma(dx0, dx0, dy0 * dy0), r1 = fma(dx1, dx1, dy1 * dy1);
+                        const double f0 = (j == ti) ? 0.0 : __ldg(pq + j) * rcp_nr(r0);
+                        const double f1 = (j1 == ti) ? 0.0 : __ldg(pq + j1) * rcp_nr(r1);
+                        ex0 = fma(f0, dx0, ex0);
+                        ey0 = fma(f0, dy0, ey0);
+                        ex1 = fma(f1, dx1, ex1);
+                        ey1 = fma(f1, dy1, ey1);
                     }
-                    m += take;
-                    s_lo += take;
-                    if (s_lo >= s_hi) {
-                        ++k;
-                        if (k < e1) { const int sc = l.l1_src[k]; s_lo = t.c_lo[sc]; s_hi = t.c_hi[sc]; }
-                    }
-                }
-                __syncthreads();
-                if (on) {
-                    for (int j = split; j < m; j += ns) {
-                        if (s_i[j] == ti) continue;
-                        const double dx = xt - s_x[j], dy = yt - s_y[j];
-                        const double r2 = fma(dx, dx, dy * dy);
-                        const double f = s_q[j] * rcp_nr(r2);
-                        ex = fma(f, dx, ex);
-                        ey = fma(f, dy, ey);
+                    if (j < s_hi) {
+                        const double dx0 = xt - __ldg(px + j), dy0 = yt - __ldg(py + j);
+                        const double r0 = fma(dx0, dx0, dy0 * dy0);
+                        const double f0 = (j == ti) ? 0.0 : __ldg(pq + j) * rcp_nr(r0);
+                        ex0 = fma(f0, dx0, ex0);
+                        ey0 = fma(f0, dy0, ey0);
                     }
                 }
             }
-            // Reduce the splits of each target.
-            __syncthreads();
+            double ex = ex0 + ex1, ey = ey0 + ey1;
             if (on && split > 0) { s_px[threadIdx.x] = ex; s_py[threadIdx.x] = ey; }
             __syncthreads();
             if (split == 0) {
@@ -387,18 +486,16 @@ __global__ void leaf_relative_f32(Tree2D t, float4* __restrict__ rel, unsigned* 
     }
 }
 
-constexpr int kP2PStageF = 512;
-
 // FP32 P2P over list 1. Targets and sources are expressed relative to the
 // target leaf's centre: source = (c_src - c_tgt) [FP64 difference, rounded
-// once] + (x - c_src) [FP32], so every pair offset keeps ~1e-7 relative
-// accuracy. Each thread sums a staged block of sources in FP32 and adds the
-// block sum into an FP64 accumulator (compensated per-target summation).
+// once per source cell] + (x - c_src) [FP32, precomputed], so every pair
+// offset keeps ~1e-7 relative accuracy. Each thread sums one source cell's
+// contributions in FP32 and adds that block sum into an FP64 accumulator
+// (compensated per-target summation). Same thread mapping as p2p2d.
 __global__ void __launch_bounds__(kP2PThreads)
 p2p2d_f32(Tree2D t, Lists2D l, const float4* __restrict__ rel, const double* __restrict__ fx,
           const double* __restrict__ fy, double* __restrict__ out0, double* __restrict__ out1, int velocity,
           double u_inf, double v_inf, unsigned* err) {
-    __shared__ float4 s_src[kP2PStageF];
     __shared__ double s_px[kP2PThreads], s_py[kP2PThreads];
     if (fatal(err)) return;
     const int nl = t.info->n_leaves;
@@ -414,56 +511,45 @@ p2p2d_f32(Tree2D t, Lists2D l, const float4* __restrict__ rel, const double* __r
             const bool on = split < ns;
             const int ti = tb + tt;
             const float4 tg = rel[ti];
-            const int tid = __float_as_int(tg.w);
             double ex = 0.0, ey = 0.0;
-            uint32_t k = o1;
-            int s_lo = 0, s_hi = 0;
-            float ox = 0.f, oy = 0.f;
-            if (k < e1) {
-                const int sc = l.l1_src[k];
-                s_lo = t.c_lo[sc]; s_hi = t.c_hi[sc];
-                ox = (float)(t.c_cx[sc] - ccx); oy = (float)(t.c_cy[sc] - ccy);
-            }
-            while (k < e1) {
-                int m = 0;
-                __syncthreads();
-                while (k < e1 && m < kP2PStageF) {
-                    const int take = min(kP2PStageF - m, s_hi - s_lo);
-                    for (int j = threadIdx.x; j < take; j += blockDim.x) {
-                        float4 v = rel[s_lo + j];
-                        v.x += ox;
-                        v.y += oy;
-                        s_src[m + j] = v;
+            if (on) {
+                for (uint32_t k = o1; k < e1; ++k) {
+                    const int sc = l.l1_src[k];
+                    const int s_hi = t.c_hi[sc];
+                    // target minus source offset, per source cell
+                    const float ox = tg.x - (float)(t.c_cx[sc] - ccx), oy = tg.y - (float)(t.c_cy[sc] - ccy);
+                    float bx0 = 0.f, by0 = 0.f, bx1 = 0.f, by1 = 0.f;
+                    int j = t.c_lo[sc] + split;
+                    for (; j + ns < s_hi; j += 2 * ns) {
+                        const int j1 = j + ns;
+                        const float4 s0 = __ldg(rel + j), s1 = __ldg(rel + j1);
+                        const float dx0 = ox - s0.x, dy0 = oy - s0.y;
+                        const float dx1 = ox - s1.x, dy1 = oy - s1.y;
+                        const float r0 = fmaf(dx0, dx0, dy0 * dy0), r1 = fmaf(dx1, dx1, dy1 * dy1);
+                        float i0, i1;
+                        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(i0) : "f"(r0));
+                        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(i1) : "f"(r1));
+                        const float f0 = (j == ti) ? 0.f : s0.z * i0;
+                        const float f1 = (j1 == ti) ? 0.f : s1.z * i1;
+                        bx0 = fmaf(f0, dx0, bx0);
+                        by0 = fmaf(f0, dy0, by0);
+                        bx1 = fmaf(f1, dx1, bx1);
+                        by1 = fmaf(f1, dy1, by1);
                     }
-                    m += take;
-                    s_lo += take;
-                    if (s_lo >= s_hi) {
-                        ++k;
-                        if (k < e1) {
-                            const int sc = l.l1_src[k];
-                            s_lo = t.c_lo[sc]; s_hi = t.c_hi[sc];
-                            ox = (float)(t.c_cx[sc] - ccx); oy = (float)(t.c_cy[sc] - ccy);
-                        }
+                    if (j < s_hi) {
+                        const float4 s0 = __ldg(rel + j);
+                        const float dx0 = ox - s0.x, dy0 = oy - s0.y;
+                        const float r0 = fmaf(dx0, dx0, dy0 * dy0);
+                        float i0;
+                        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(i0) : "f"(r0));
+                        const float f0 = (j == ti) ? 0.f : s0.z * i0;
+                        bx0 = fmaf(f0, dx0, bx0);
+                        by0 = fmaf(f0, dy0, by0);
                     }
-                }
-                __syncthreads();
-                if (on) {
-                    float bx = 0.f, by = 0.f;
-                    for (int j = split; j < m; j += ns) {
-                        const float4 sv = s_src[j];
-                        const float dx = tg.x - sv.x, dy = tg.y - sv.y;
-                        const float r2 = fmaf(dx, dx, dy * dy);
-                        float inv;
-                        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(inv) : "f"(r2));
-                        const float f = (__float_as_int(sv.w) == tid) ? 0.f : sv.z * inv;
-                        bx = fmaf(f, dx, bx);
-                        by = fmaf(f, dy, by);
-                    }
-                    ex += bx;
-                    ey += by;
+                    ex += (double)bx0 + (double)bx1;
+                    ey += (double)by0 + (double)by1;
                 }
             }
-            __syncthreads();
             if (on && split > 0) { s_px[threadIdx.x] = ex; s_py[threadIdx.x] = ey; }
             __syncthreads();
             if (split == 0) {
@@ -509,27 +595,69 @@ cudaError_t set_coefficients2d(int P, bool exact, double* dst, cudaStream_t st) 
     return cudaStreamSynchronize(st);
 }
 
+// Upward pass: P2M of every active leaf, then M2M level by level from the
+// deepest possible level up to level 1 (levels below the tree's depth exit
+// at once; the launch count does not depend on the data, so the sequence can
+// be captured in a CUDA graph).
 cudaError_t fmm2d_upward(const Tree2D& t, Expansions2D& e, int P, unsigned* err, cudaStream_t st, int* launches) {
     cudaError_t r = cudaMemsetAsync(e.a, 0, sizeof(double2) * (size_t)t.cap_cells * (P + 1), st);
     if (r != cudaSuccess) return r;
-    zero_u32<<<148, 256, 0, st>>>(e.up_count, t.cap_cells);
-    upward2d<<<148 * 8, 128, 0, st>>>(t, e.a, e.up_count, e.coef, P, err);
-    *launches += 2;
+    const size_t smem = sizeof(double2) * kP2MWarps * (P + 1) * kAccPad;
+    p2m2d<<<148 * 16, 32 * kP2MWarps, smem, st>>>(t, e.a, P, err);
+    *launches += 1;
+    for (int L = t.key_levels - 1; L >= 1; --L) {
+        m2m_level2d<<<148 * 4, 128, 0, st>>>(t, e.a, e.coef, P, L, err);
+        *launches += 1;
+    }
     return cudaGetLastError();
+}
+
+// List-2 operators T_tau (see m2l2d_op) for the 49 offset slots, from the
+// same M2L coefficients as the direct formula (so the reference's binomials
+// carry over). Upload synchronises `st`.
+cudaError_t set_m2l_operators2d(int P, bool exact, double2* dst, cudaStream_t st) {
+    std::vector<double2> op((size_t)49 * (P + 1) * P);
+    for (int slot = 0; slot < 49; ++slot) {
+        const int dx = slot % 7 - 3, dy = slot / 7 - 3;
+        std::complex<double> tau(dx, dy), inv = (dx == 0 && dy == 0) ? 0.0 : 1.0 / tau;
+        std::vector<std::complex<double>> ip(2 * P + 2);
+        ip[0] = 1.0;
+        for (int m = 1; m <= 2 * P; ++m) ip[m] = ip[m - 1] * inv;
+        for (int p = 1; p <= P; ++p) {
+            for (int k = 0; k <= P; ++k) {
+                std::complex<double> v;
+                if (k == 0) v = -(1.0 / (double)p) * ip[p];
+                else v = -((double)binom_host(p + k - 1, k - 1, exact) * ((k & 1) ? -1.0 : 1.0) / (double)k) * ip[p + k];
+                op[((size_t)slot * (P + 1) + k) * P + (p - 1)] = make_double2(v.real(), v.imag());
+            }
+        }
+    }
+    cudaError_t e = cudaMemcpyAsync(dst, op.data(), sizeof(double2) * op.size(), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return e;
+    return cudaStreamSynchronize(st);
 }
 
 cudaError_t fmm2d_m2l(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, unsigned* err, cudaStream_t st,
                       int* launches) {
     const int G = 32 / P;
-    const size_t smem = sizeof(double2) * 4 * (size_t)(G * (2 * P + 1) + 2 * G * (P + 1));
-    m2l2d<<<148 * 16, 128, smem, st>>>(t, l, e.a, e.b, e.coef, P, err);
+    if (e.op) {
+        const size_t smem = sizeof(double2) * 4 * (size_t)(2 * G * (P + 1) + G * (2 * P + 1));
+        m2l2d_op<<<148 * 16, 128, smem, st>>>(t, l, e.a, e.b, e.op, e.coef, P, err);
+    } else {
+        const size_t smem = sizeof(double2) * 4 * (size_t)(G * (2 * P + 1) + 2 * G * (P + 1));
+        m2l2d<<<148 * 16, 128, smem, st>>>(t, l, e.a, e.b, e.coef, P, err);
+    }
     *launches += 1;
+    for (int L = 3; L <= t.key_levels; ++L) {
+        l2l_level2d<<<148 * 4, 128, 0, st>>>(t, e.b, e.coef, P, L, err);
+        *launches += 1;
+    }
     return cudaGetLastError();
 }
 
 cudaError_t fmm2d_eval(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, unsigned* err, cudaStream_t st,
                        int* launches) {
-    eval2d<<<148 * 16, kEvalThreads, 0, st>>>(t, l, e.a, e.b, e.fx, e.fy, e.coef, P, err);
+    eval2d<<<148 * 16, kEvalThreads, 0, st>>>(t, l, e.a, e.b, e.fx, e.fy, P, err);
     *launches += 1;
     return cudaGetLastError();
 }

@@ -17,12 +17,22 @@ namespace {
 struct TreeView {
     Tree2D t;
     double root;
+    int depth, n_cells;
+    __device__ TreeView(const Tree2D& tt) : t(tt), root(tt.geom->root), depth(tt.info->depth), n_cells(tt.info->n_cells) {}
     __device__ __forceinline__ double len(int L) const { return xdiv(root, ldexp(1.0, L)); }
-    // Index of the cell (L, ix, iy) or -1 when it does not exist.
+    // Index of the cell (L, ix, iy) or -1 when it does not exist: one load
+    // from the dense grid (validated against the cell's own level and index,
+    // since the grid is never cleared) or a binary search of the level's
+    // Morton codes.
     __device__ int find(int L, int ix, int iy) const {
-        if (L < 0 || L > t.info->depth) return -1;
+        if (L < 0 || L > depth) return -1;
         const long long cnt = 1ll << L;
         if (ix < 0 || iy < 0 || ix >= cnt || iy >= cnt) return -1;
+        if (t.dense && L <= t.dense_levels) {
+            const int e = t.dense[start_id2(L) + ix + ((int64_t)iy << L)];
+            if (e >= 0 && e < n_cells && t.c_level[e] == L && t.c_ix[e] == ix && t.c_iy[e] == iy) return e;
+            return -1;
+        }
         int lo = t.info->level_start[L], hi = t.info->level_start[L + 1];
         const uint64_t code = morton2((uint32_t)ix, (uint32_t)iy);
         while (lo < hi) {
@@ -112,7 +122,7 @@ __device__ void int_list(const TreeView& v, int c, double eps, int mode, uint32_
 
 __global__ void int_list_kernel(Tree2D t, double eps, int mode, Lists2D l, unsigned* err) {
     if (fatal(err)) return;
-    TreeView v{t, t.geom->root};
+    TreeView v(t);
     const int nl = t.info->n_leaves;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < l.cap_leaves; i += gridDim.x * blockDim.x) {
         if (i >= nl) {
@@ -201,7 +211,7 @@ __device__ void ext_list(const TreeView& v, int c, double eps, int32_t* l2, uint
 
 __global__ void ext_list_kernel(Tree2D t, double eps, Lists2D l, unsigned* err) {
     if (fatal(err)) return;
-    TreeView v{t, t.geom->root};
+    TreeView v(t);
     const int c0 = t.info->level_start[2], c1 = t.info->n_cells;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < t.cap_cells; i += gridDim.x * blockDim.x) {
         if (i < c0 || i >= c1) {

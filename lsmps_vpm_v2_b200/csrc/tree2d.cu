@@ -20,7 +20,8 @@ namespace vpm {
 
 namespace {
 
-constexpr int kLvlThreads = 256;
+constexpr int kLvlWarps = 8;                 // parents per tile, one warp each
+constexpr int kLvlThreads = 32 * kLvlWarps;
 constexpr uint64_t kLvA = 1ull << 62;
 constexpr uint64_t kLvP = 2ull << 62;
 constexpr uint64_t kLvMask = (1ull << 62) - 1;
@@ -150,6 +151,7 @@ __global__ void tree_root2d(Tree2D t) {
     t.c_leafidx[0] = -1;
     t.c_cx[0] = xadd(g->pivx, xmul(0.5, g->root));
     t.c_cy[0] = xadd(g->pivy, xmul(0.5, g->root));
+    if (t.dense) t.dense[0] = 0;
     for (int L = 0; L < kMaxLevels2D + 3; ++L) {
         info->level_start[L] = L == 0 ? 0 : 1;
         info->leaf_start[L] = 0;
@@ -159,30 +161,52 @@ __global__ void tree_root2d(Tree2D t) {
     info->depth = 0;
 }
 
-// First index in [lo, hi) whose level code (key >> shift) is >= v.
-__device__ __forceinline__ int lower_code(const uint64_t* __restrict__ key, int lo, int hi, int shift, uint64_t v) {
-    while (lo < hi) {
-        int mid = (lo + hi) >> 1;
-        if ((key[mid] >> shift) < v) lo = mid + 1;
-        else hi = mid;
+// First index in [lo, hi) whose level code (key >> shift) is >= v, found by
+// the whole warp: 32 probes per round cut the interval 33-fold, so a range of
+// n keys takes ceil(log33 n) dependent loads instead of log2 n. The result is
+// warp-uniform; every lane must call.
+__device__ __forceinline__ int warp_lower_code(const uint64_t* __restrict__ key, int lo, int hi, int shift,
+                                               uint64_t v, int lane) {
+    int a = lo, b = hi;  // answer in [a, b]
+    while (b - a > 32) {
+        const long long len = b - a;
+        const int pos = a + (int)(((long long)(lane + 1) * len) / 33);
+        const unsigned m = __ballot_sync(0xffffffffu, (key[pos] >> shift) >= v);
+        const int a0 = a;
+        if (m == 0) {
+            a = a0 + (int)((32ll * len) / 33) + 1;
+        } else {
+            const int f = __ffs(m) - 1;
+            b = a0 + (int)(((long long)(f + 1) * len) / 33);
+            if (f > 0) a = a0 + (int)(((long long)f * len) / 33) + 1;
+        }
     }
-    return lo;
+    const int pos = a + lane;
+    const unsigned m = __ballot_sync(0xffffffffu, pos < b && (key[pos] >> shift) >= v);
+    return m ? a + __ffs(m) - 1 : b;
 }
 
-// Cells of level L from the non-leaf cells of level L-1. Tiles of 256 parents
-// take ordered tickets; a packed (cells, leaves) count per tile is combined by
-// decoupled look-back so children are emitted in parent order, i.e. Morton
-// order within the level.
+__device__ __forceinline__ int sel4(int i, int v0, int v1, int v2, int v3) {
+    return i == 0 ? v0 : i == 1 ? v1 : i == 2 ? v2 : v3;
+}
+
+// Cells of level L from the non-leaf cells of level L-1, one warp per parent,
+// kLvlWarps parents per tile. Tiles take ordered tickets and combine their
+// packed (cells, leaves) counts by decoupled look-back, so children are
+// emitted in parent order, i.e. Morton order within the level. Each new cell
+// also lands in the dense lookup grid (indexed by the reference's cell ID)
+// when its level is covered by it.
 __global__ void __launch_bounds__(kLvlThreads)
-tree_level2d(Tree2D t, int L, int max_src, int max_par, uint64_t* status, unsigned* ticket, unsigned* err) {
+tree_level2d(Tree2D t, int L, int max_src, int max_par, int* dense, int dense_levels, uint64_t* status,
+             unsigned* ticket, unsigned* err) {
     __shared__ unsigned s_tile;
-    __shared__ uint64_t warp_sums[kLvlThreads / 32];
     __shared__ uint64_t s_prefix;
+    __shared__ int s_cnt[kLvlWarps], s_lf[kLvlWarps], s_xc[kLvlWarps], s_xl[kLvlWarps];
     TreeInfo2D* info = t.info;
     if (*(volatile const unsigned*)err & (ERR_CELL_CAP | ERR_TIMEOUT | ERR_NONFINITE)) return;
     const int p0 = info->level_start[L - 1];
     const int np = info->level_start[L] - p0;
-    const int ntiles = np > 0 ? ceil_div(np, kLvlThreads) : 1;
+    const int ntiles = np > 0 ? ceil_div(np, kLvlWarps) : 1;
     const int base_cell = info->level_start[L];
     const int base_leaf = info->leaf_start[L];
     const int shift = 2 * (t.key_levels - L);
@@ -194,135 +218,123 @@ tree_level2d(Tree2D t, int L, int max_src, int max_par, uint64_t* status, unsign
         if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
         __syncthreads();
         const int tile = (int)s_tile;
-        __syncthreads();
         if (tile >= ntiles) return;
-        const int p = p0 + tile * kLvlThreads + threadIdx.x;
-        int bnd[5];
-        int nchild = 0, nleaf = 0;
-        unsigned mask = 0;
-        bool parent_ok = tile * kLvlThreads + (int)threadIdx.x < np;
-        if (parent_ok && !(t.c_flags[p] & CELL_LEAF)) {
-            const int lo = t.c_lo[p], hi = t.c_hi[p];
+        const int pi = tile * kLvlWarps + warp;
+        const int p = p0 + pi;
+        const bool nonleaf = pi < np && !(t.c_flags[p] & CELL_LEAF);   // warp-uniform
+        int b0 = 0, b1 = 0, b2 = 0, b3 = 0, b4 = 0;
+        bool has = false, leaf = false;
+        unsigned mask = 0, lmask = 0;
+        int clo = 0, chi = 0, src = 0;
+        if (nonleaf) {
+            b0 = t.c_lo[p];
+            b4 = t.c_hi[p];
             const uint64_t pc = t.c_code[p] << 2;
-            bnd[0] = lo;
-            bnd[4] = hi;
-            bnd[1] = lower_code(t.key, lo, hi, shift, pc + 1);
-            bnd[2] = lower_code(t.key, bnd[1], hi, shift, pc + 2);
-            bnd[3] = lower_code(t.key, bnd[2], hi, shift, pc + 3);
-            for (int d = 0; d < 4; ++d) {
-                if (bnd[d + 1] > bnd[d]) {
-                    mask |= 1u << d;
-                    ++nchild;
-                    int par = bnd[d + 1] - bnd[d];
-                    int src = (int)(t.actscan[bnd[d + 1]] - t.actscan[bnd[d]]);
-                    if (src <= max_src && par <= max_par) ++nleaf;
-                }
+            b1 = warp_lower_code(t.key, b0, b4, shift, pc + 1, lane);
+            b2 = warp_lower_code(t.key, b1, b4, shift, pc + 2, lane);
+            b3 = warp_lower_code(t.key, b2, b4, shift, pc + 3, lane);
+            clo = sel4(lane, b0, b1, b2, b3);
+            chi = sel4(lane, b1, b2, b3, b4);
+            has = lane < 4 && chi > clo;
+            if (has) {
+                src = (int)(t.actscan[chi] - t.actscan[clo]);
+                leaf = src <= max_src && (chi - clo) <= max_par;
             }
+            mask = __ballot_sync(0xffffffffu, has);
+            lmask = __ballot_sync(0xffffffffu, leaf);
         }
-        // Block-wide exclusive scan of the packed (cells, leaves) counts.
-        uint64_t v = (uint64_t)nchild | ((uint64_t)nleaf << 31);
-        uint64_t x = v;
-        #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            uint64_t yv = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += yv;
+        if (lane == 0) {
+            s_cnt[warp] = __popc(mask);
+            s_lf[warp] = __popc(lmask);
         }
-        if (lane == 31) warp_sums[warp] = x;
         __syncthreads();
         if (warp == 0) {
-            uint64_t w = lane < kLvlThreads / 32 ? warp_sums[lane] : 0;
+            int c = lane < kLvlWarps ? s_cnt[lane] : 0, lf = lane < kLvlWarps ? s_lf[lane] : 0;
+            int ic = c, il = lf;
             #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
-                uint64_t yv = __shfl_up_sync(0xffffffffu, w, o);
-                if (lane >= o) w += yv;
+                int yc = __shfl_up_sync(0xffffffffu, ic, o), yl = __shfl_up_sync(0xffffffffu, il, o);
+                if (lane >= o) { ic += yc; il += yl; }
             }
-            if (lane < kLvlThreads / 32) warp_sums[lane] = w;
-        }
-        __syncthreads();
-        const uint64_t excl = (warp ? warp_sums[warp - 1] : 0) + x - v;
-        const uint64_t agg = warp_sums[kLvlThreads / 32 - 1];
-        if (threadIdx.x == 0) {
-            uint64_t prefix = 0;
-            if (tile == 0) {
-                st_relaxed(&status[0], kLvP | agg);
-            } else {
-                st_relaxed(&status[tile], kLvA | agg);
-                int k = tile - 1;
-                long long spins = 0;
-                while (k >= 0) {
-                    uint64_t w = ld_relaxed(&status[k]);
-                    if ((w & ~kLvMask) == 0) {
-                        if (++spins > kSpinLimit) { set_err(err, ERR_TIMEOUT); break; }
-                        continue;
-                    }
-                    prefix += w & kLvMask;
-                    if ((w & ~kLvMask) == kLvP) break;
-                    --k;
-                }
-                st_relaxed(&status[tile], kLvP | (prefix + agg));
-            }
-            s_prefix = prefix;
-            if (tile == ntiles - 1) {
-                uint64_t tot = prefix + agg;
-                int ncell = (int)(tot & 0x7FFFFFFFull), nlf = (int)(tot >> 31);
-                for (int k2 = L + 1; k2 < kMaxLevels2D + 3; ++k2) {
-                    info->level_start[k2] = base_cell + ncell;
-                    info->leaf_start[k2] = base_leaf + nlf;
-                }
-                info->n_cells = base_cell + ncell;
-                info->n_leaves = base_leaf + nlf;
-                if (ncell > 0) info->depth = L;
-                if (base_cell + ncell > t.cap_cells) set_err(err, ERR_CELL_CAP);
-            }
-        }
-        __syncthreads();
-        const uint64_t mine = s_prefix + excl;
-        int ci = base_cell + (int)(mine & 0x7FFFFFFFull);
-        int li = base_leaf + (int)(mine >> 31);
-        if (nchild > 0) {
-            const int pix = t.c_ix[p], piy = t.c_iy[p];
-            const uint64_t pc = t.c_code[p] << 2;
-            if (ci + nchild <= t.cap_cells) {
-                t.c_child0[p] = ci;
-                t.c_chmask[p] = (uint8_t)mask;
-            } else {
-                t.c_child0[p] = -1;
-                t.c_chmask[p] = 0;
-            }
-            for (int d = 0; d < 4; ++d) {
-                if (!(mask & (1u << d))) continue;
-                if (ci >= t.cap_cells) { set_err(err, ERR_CELL_CAP); break; }
-                const int lo = bnd[d], hi = bnd[d + 1];
-                const int par = hi - lo;
-                const int src = (int)(t.actscan[hi] - t.actscan[lo]);
-                const bool leaf = src <= max_src && par <= max_par;
-                const int ix = 2 * pix + (d & 1), iy = 2 * piy + (d >> 1);
-                t.c_lo[ci] = lo;
-                t.c_hi[ci] = hi;
-                t.c_src[ci] = src;
-                t.c_flags[ci] = (leaf ? CELL_LEAF : 0) | (src != 0 ? CELL_ACTIVE : 0);
-                t.c_parent[ci] = p;
-                t.c_child0[ci] = -1;
-                t.c_chmask[ci] = 0;
-                t.c_level[ci] = (uint8_t)L;
-                t.c_ix[ci] = ix;
-                t.c_iy[ci] = iy;
-                t.c_code[ci] = pc + d;
-                t.c_cx[ci] = xadd(pivx, xmul(xadd(0.5, (double)ix), len));
-                t.c_cy[ci] = xadd(pivy, xmul(xadd(0.5, (double)iy), len));
-                if (leaf) {
-                    t.c_leafidx[ci] = li;
-                    t.leaf_cells[li] = ci;
-                    ++li;
+            if (lane < kLvlWarps) { s_xc[lane] = ic - c; s_xl[lane] = il - lf; }
+            const uint64_t agg = (uint64_t)__shfl_sync(0xffffffffu, ic, 31) |
+                                 ((uint64_t)__shfl_sync(0xffffffffu, il, 31) << 31);
+            if (lane == 0) {
+                uint64_t prefix = 0;
+                if (tile == 0) {
+                    st_relaxed(&status[0], kLvP | agg);
                 } else {
-                    t.c_leafidx[ci] = -1;
-                    if (L == t.key_levels) set_err(err, ERR_DEPTH);
+                    st_relaxed(&status[tile], kLvA | agg);
+                    int k = tile - 1;
+                    long long spins = 0;
+                    while (k >= 0) {
+                        uint64_t w = ld_relaxed(&status[k]);
+                        if ((w & ~kLvMask) == 0) {
+                            if (++spins > kSpinLimit) { set_err(err, ERR_TIMEOUT); break; }
+                            continue;
+                        }
+                        prefix += w & kLvMask;
+                        if ((w & ~kLvMask) == kLvP) break;
+                        --k;
+                    }
+                    st_relaxed(&status[tile], kLvP | (prefix + agg));
                 }
-                ++ci;
+                s_prefix = prefix;
+                if (tile == ntiles - 1) {
+                    const uint64_t tot = prefix + agg;
+                    const int ncell = (int)(tot & 0x7FFFFFFFull), nlf = (int)(tot >> 31);
+                    for (int k2 = L + 1; k2 < kMaxLevels2D + 3; ++k2) {
+                        info->level_start[k2] = base_cell + ncell;
+                        info->leaf_start[k2] = base_leaf + nlf;
+                    }
+                    info->n_cells = base_cell + ncell;
+                    info->n_leaves = base_leaf + nlf;
+                    if (ncell > 0) info->depth = L;
+                    if (base_cell + ncell > t.cap_cells) set_err(err, ERR_CELL_CAP);
+                }
             }
-        } else if (parent_ok && !(t.c_flags[p] & CELL_LEAF)) {
-            t.c_child0[p] = -1;
-            t.c_chmask[p] = 0;
+        }
+        __syncthreads();
+        if (nonleaf) {
+            const int nchild = __popc(mask);
+            const int ci0 = base_cell + (int)(s_prefix & 0x7FFFFFFFull) + s_xc[warp];
+            const int li0 = base_leaf + (int)(s_prefix >> 31) + s_xl[warp];
+            if (lane == 0) {
+                const bool fits = ci0 + nchild <= t.cap_cells;
+                t.c_child0[p] = fits ? ci0 : -1;
+                t.c_chmask[p] = fits ? (uint8_t)mask : 0;
+            }
+            if (has) {
+                const unsigned below = (1u << lane) - 1u;
+                const int ci = ci0 + __popc(mask & below);
+                if (ci >= t.cap_cells) {
+                    set_err(err, ERR_CELL_CAP);
+                } else {
+                    const int ix = 2 * t.c_ix[p] + (lane & 1), iy = 2 * t.c_iy[p] + (lane >> 1);
+                    t.c_lo[ci] = clo;
+                    t.c_hi[ci] = chi;
+                    t.c_src[ci] = src;
+                    t.c_flags[ci] = (leaf ? CELL_LEAF : 0) | (src != 0 ? CELL_ACTIVE : 0);
+                    t.c_parent[ci] = p;
+                    t.c_child0[ci] = -1;
+                    t.c_chmask[ci] = 0;
+                    t.c_level[ci] = (uint8_t)L;
+                    t.c_ix[ci] = ix;
+                    t.c_iy[ci] = iy;
+                    t.c_code[ci] = (t.c_code[p] << 2) + lane;
+                    t.c_cx[ci] = xadd(pivx, xmul(xadd(0.5, (double)ix), len));
+                    t.c_cy[ci] = xadd(pivy, xmul(xadd(0.5, (double)iy), len));
+                    if (dense && L <= dense_levels) dense[start_id2(L) + ix + ((int64_t)iy << L)] = ci;
+                    if (leaf) {
+                        const int li = li0 + __popc(lmask & below);
+                        t.c_leafidx[ci] = li;
+                        t.leaf_cells[li] = ci;
+                    } else {
+                        t.c_leafidx[ci] = -1;
+                        if (L == t.key_levels) set_err(err, ERR_DEPTH);
+                    }
+                }
+            }
         }
         __syncthreads();
     }
@@ -377,11 +389,11 @@ cudaError_t build_tree2d(const double* x, const double* y, const double* q, cons
     *launches += 1;
     for (int L = 1; L <= K; ++L) {
         long long bound = std::min<long long>(t.cap_cells, 1ll << std::min(2 * (L - 1), 40));
-        int tiles = std::max(1, ceil_div(bound, kLvlThreads));
+        int tiles = std::max(1, ceil_div(bound, kLvlWarps));
         if (tiles > s.lvl_max_tiles) return cudaErrorInvalidValue;
-        int grid = std::min(tiles, 148 * 4);
-        tree_level2d<<<grid, kLvlThreads, 0, st>>>(t, L, max_src, max_par, s.lvl_status + (size_t)L * s.lvl_max_tiles,
-                                                   s.lvl_ticket + L, err);
+        int grid = std::min(tiles, 148 * 8);
+        tree_level2d<<<grid, kLvlThreads, 0, st>>>(t, L, max_src, max_par, t.dense, t.dense_levels,
+                                                   s.lvl_status + (size_t)L * s.lvl_max_tiles, s.lvl_ticket + L, err);
         *launches += 1;
     }
     tree_finish2d<<<1, 1, 0, st>>>(t.info);
