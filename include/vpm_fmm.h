@@ -19,6 +19,7 @@
 #ifndef VPM_FMM_H
 #define VPM_FMM_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -160,6 +161,30 @@ int vpm_tree2d_counts(vpm_ctx* ctx, int64_t* n_cells, int64_t* n_leaves, int64_t
 int vpm_tree2d_cells(vpm_ctx* ctx, int64_t* ids, int32_t* ints6, double* centers2);
 int vpm_tree2d_leaves(vpm_ctx* ctx, int64_t* leaf_ids, int64_t* offs, int32_t* pids);
 int vpm_tree2d_list(vpm_ctx* ctx, int which, int64_t* cell_ids, int64_t* offs, int64_t* ids);
+
+/*
+ * vpm_fmm2d_field_device_static: the evaluation of vpm_fmm2d_field_device
+ * (device buffers in and out, FP64 or mixed form) without any device
+ * allocation, for callers that cannot call cudaMalloc: code running while a
+ * CUDA stream capture is open (allocation is not permitted there), host
+ * callbacks, and programs whose device memory is owned by another allocator.
+ * No counterpart in the reference (its FMM allocates host memory freely).
+ *
+ * All scratch lives in one static device array of 8 MiB that every GPU
+ * loading this library keeps until the process exits. Limits: n <= 8192,
+ * p <= 12, at most 8192 tree cells; larger requests return VPM_EINVAL, a
+ * tree that outgrows the array returns VPM_EOVERFLOW. The first call on a
+ * device looks up the array's device address (with that device current) and
+ * must come before any stream capture that contains this call. Calls share
+ * the array and overwrite it; calls that overlap on the GPU race, so
+ * serialise them. Runs on `cuda_stream` (a cudaStream_t, NULL = legacy
+ * default stream) and waits for it to report errors. errbuf (may be NULL)
+ * receives a message of at most errlen bytes.
+ */
+int vpm_fmm2d_field_device_static(const double* x, const double* y, const double* q,
+                                  const uint8_t* active, int64_t n, const vpm_fmm_params* prm,
+                                  double* ex, double* ey, void* cuda_stream, char* errbuf,
+                                  size_t errlen);
 
 /*
  * FMA-throughput microbenchmark of the device (TFLOP/s of dependent FMA

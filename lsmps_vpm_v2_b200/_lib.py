@@ -94,6 +94,8 @@ SIGNATURES = {
     "vpm_tree2d_leaves": (C.c_int, [_vp, _vp, _vp, _vp]),
     "vpm_tree2d_list": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp]),
     "vpm_measure_fma_peaks": (C.c_int, [_vp, _dp, _dp]),
+    "vpm_fmm2d_field_device_static": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int64, C.POINTER(Params), _vp, _vp, _vp,
+                                                C.c_char_p, C.c_size_t]),
 }
 
 _LIB = None
