@@ -169,12 +169,14 @@ def run_ours(args):
     wl = workload()
     n = int(wl["x"].size)
     dev = torch.device("cuda", local)
-    stream = torch.cuda.current_stream()
+    # One dedicated stream for the library and the timing events (torch's
+    # default stream has the handle 0, which the library would not run on).
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
     ctx = Context(local)
     ctx.set_stream(stream.cuda_stream)
     form = args.form
     prm = default_params(precision=PREC_MIXED if form == "mixed" else PREC_FP64, use_graph=0 if args.no_graph else 1)
-    prm_stage = default_params(precision=prm.precision)  # eager launches: per-stage events
 
     x = torch.from_numpy(wl["x"]).to(dev)
     y = torch.from_numpy(wl["y"]).to(dev)
@@ -218,14 +220,18 @@ def run_ours(args):
     launches_per_step = int(st.kernels)
 
     # ---- stage profile (same workload, per-stage CUDA events) ----
-    stage = {k: [] for k in ("ms_tree", "ms_lists", "ms_upward", "ms_m2l", "ms_eval", "ms_p2p", "ms_total")}
-    for k in range(min(args.steps, 20)):
+    # one graph per stage, events between them, evaluations back to back
+    prm_stage = default_params(precision=prm.precision, use_graph=0 if args.no_graph else 2)
+    ctx.field2d_device(x, y, q, act, ex, ey, prm_stage)   # capture
+    ctx.stage_history(enable=True)
+    nprof = max(3, min(args.steps, 40))
+    for k in range(nprof):
         flush.fill_(k)
         ctx.field2d_device(x, y, q, act, ex, ey, prm_stage)
-        s = ctx.last_stats()
-        for key in stage:
-            stage[key].append(getattr(s, key))
-    stage = {k: float(np.mean(v)) for k, v in stage.items()}
+    hist = ctx.stage_history(enable=False)
+    stage = {f"ms_{nm}": float(np.mean(hist[:, i])) for i, nm in enumerate(ctx.STAGES)}
+    stage["ms_total"] = float(np.mean(hist.sum(axis=1)))
+    ctx.field2d_device(x, y, q, act, ex, ey, prm)
 
     # ---- end to end through the public host API (pinned buffers) ----
     hx = torch.from_numpy(wl["x"]).pin_memory().numpy()
@@ -233,12 +239,14 @@ def run_ours(args):
     hw = torch.from_numpy(wl["omega"]).pin_memory().numpy()
     hs = torch.from_numpy(wl["s"]).pin_memory().numpy()
     ha = torch.from_numpy(wl["active"]).pin_memory().numpy()
+    hu = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
+    hv = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
     e2e_ms = []
     for k in range(max(3, min(args.steps, 20)) + 2):
         flush.fill_(k)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        u, v = ctx.velocity2d(hx, hy, hw, hs, ha, 0.0, 0.0, prm)
+        ctx.velocity2d(hx, hy, hw, hs, ha, 0.0, 0.0, prm, out=(hu, hv))
         t1 = time.perf_counter()
         if k >= 2:
             e2e_ms.append((t1 - t0) * 1e3)

@@ -63,9 +63,11 @@ typedef struct vpm_fmm_params {
     int32_t precision;    /* VPM_PREC_*                                             */
     int32_t binom;        /* VPM_BINOM_*                                            */
     int32_t max_depth;    /* deepest tree level the keys resolve (2D: 16 or 31)     */
-    int32_t use_graph;    /* device entry points: capture the evaluation once as a
-                             CUDA graph and replay it while the buffers, n and the
-                             parameters are unchanged (no per-stage timings then)  */
+    int32_t use_graph;    /* device entry points: 1 = capture the evaluation once as
+                             a CUDA graph and replay it while the buffers, n and
+                             the parameters are unchanged (no per-stage timings);
+                             2 = one graph per stage, with the stage events
+                             recorded between them (profiling)                    */
 } vpm_fmm_params;
 
 /* Per-call figures (counts are exact; times are CUDA-event milliseconds). */
@@ -84,11 +86,15 @@ typedef struct vpm_fmm_stats {
     float ms_lists;       /* lists 1-4                                              */
     float ms_upward;      /* P2M + M2M                                              */
     float ms_m2l;
-    float ms_eval;        /* L2L chain + L2P + M2P                                  */
+    float ms_eval;        /* M2P + L2P                                              */
     float ms_p2p;
     float ms_total;       /* device time of the whole evaluation                    */
     int32_t kernels;      /* kernel launches of this call                           */
     int32_t depth_retry;  /* 1 when the host entry point rebuilt with deeper keys   */
+    float ms_keys_sort;   /* bounding box, keys, radix sort, gather (part of ms_tree) */
+    float ms_levels;      /* level splits (part of ms_tree)                         */
+    float ms_l2l;         /* L2L levels (not part of ms_m2l)                        */
+    float pad_;
 } vpm_fmm_stats;
 
 /* Fill *p with the reference's 2D/3D defaults listed above. */
@@ -97,7 +103,8 @@ void vpm_fmm_params_default(vpm_fmm_params* p);
 /* Create a context on CUDA device `device` (buffers, stream, events). */
 int vpm_ctx_create(int device, vpm_ctx** out);
 int vpm_ctx_destroy(vpm_ctx* ctx);
-/* Run subsequent calls on `cuda_stream` (a cudaStream_t; NULL = the context's own stream). */
+/* Run subsequent calls on `cuda_stream` (a cudaStream_t; NULL = the context's own stream, a
+ * blocking stream, so it is ordered with work on the legacy default stream). */
 int vpm_ctx_set_stream(vpm_ctx* ctx, void* cuda_stream);
 /* Wait for the context's stream and report any device-side error word. */
 int vpm_ctx_sync(vpm_ctx* ctx);
@@ -141,6 +148,17 @@ int vpm_velocity2d(vpm_ctx* ctx, const double* x, const double* y, const double*
  */
 int vpm_tree2d_build(vpm_ctx* ctx, const double* x, const double* y, const uint8_t* active, int64_t n,
                      const vpm_fmm_params* prm, vpm_fmm_stats* stats);
+
+/*
+ * Stage-time history for profiling (no counterpart in the reference). With
+ * enable = 1 every later timed evaluation (use_graph 0 or 2) records its 8
+ * stage times into a ring of 64 entries, so evaluations can run back to back
+ * without host synchronisation. A call returns the recorded entries (oldest
+ * first) into ms[entry * 8 + stage], stages in the order keys+sort, levels,
+ * lists, P2M+M2M, M2L, L2L, M2P+L2P, P2P, sets *count, clears the ring and
+ * leaves recording on or off as `enable` says. Synchronises the stream.
+ */
+int vpm_stage_history(vpm_ctx* ctx, int32_t enable, int32_t max_entries, float* ms, int32_t* count);
 
 /* Statistics of the last evaluation on this context (synchronises). */
 int vpm_last_stats(vpm_ctx* ctx, vpm_fmm_stats* stats);

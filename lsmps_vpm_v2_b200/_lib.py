@@ -63,6 +63,10 @@ class Stats(C.Structure):
         ("ms_total", C.c_float),
         ("kernels", C.c_int32),
         ("depth_retry", C.c_int32),
+        ("ms_keys_sort", C.c_float),
+        ("ms_levels", C.c_float),
+        ("ms_l2l", C.c_float),
+        ("pad_", C.c_float),
     ]
 
     def as_dict(self):
@@ -94,6 +98,7 @@ SIGNATURES = {
     "vpm_tree2d_leaves": (C.c_int, [_vp, _vp, _vp, _vp]),
     "vpm_tree2d_list": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp]),
     "vpm_measure_fma_peaks": (C.c_int, [_vp, _dp, _dp]),
+    "vpm_stage_history": (C.c_int, [_vp, C.c_int32, C.c_int32, _vp, C.POINTER(C.c_int32)]),
     "vpm_fmm2d_field_device_static": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int64, C.POINTER(Params), _vp, _vp, _vp,
                                                 C.c_char_p, C.c_size_t]),
 }

@@ -80,7 +80,7 @@ int Ctx::reserve2d(int n, int cap_cells, int P, long long cap_l1, long long cap_
     size_t o_actscan = L.take<uint32_t>((size_t)n + 1);
     size_t o_keyalt = L.take<uint64_t>(n), o_valalt = L.take<uint32_t>(n), o_actu = L.take<uint32_t>(n);
     size_t o_bbox = L.take<double>(kBBoxBlocks * 4);
-    size_t o_lstat = L.take<uint64_t>((size_t)(K + 1) * lvl_tiles), o_ltick = L.take<unsigned>(K + 2);
+    size_t o_lstat = L.take<uint64_t>((size_t)(K + 1) * lvl_tiles), o_ltick = L.take<unsigned>(kTicketWords);
     size_t o_sstat = L.take<uint32_t>((size_t)8 * s_tiles * 256), o_stick = L.take<unsigned>(8),
            o_hist = L.take<uint32_t>(8 * 256);
     size_t o_scstat = L.take<uint64_t>(sc_tiles), o_sctick = L.take<unsigned>(1);
@@ -135,6 +135,7 @@ int Ctx::reserve2d(int n, int cap_cells, int P, long long cap_l1, long long cap_
     tree.leaf_cells = (int32_t*)P_(o_leaves);
     tree.geom = (Geom2D*)P_(o_geom); tree.info = (TreeInfo2D*)P_(o_info);
     tree.dense = (int32_t*)P_(o_dense);
+    tree.gbar = ts.lvl_ticket + kBarrierWordsAt;
     tree.dense_levels = dlev;
     tree.cap_cells = cap_cells;
     lists.l2_src = (int32_t*)P_(o_l2); lists.l2_slot = (uint8_t*)P_(o_l2s); lists.l2_n = (uint8_t*)P_(o_l2n);
@@ -203,26 +204,34 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
         coef_binom = p.binom;
     }
     if (int r = record(0)) return r;
-    VPM_CUDA_TRY(build_tree2d(x, y, q, act, tree, ts, p.max_src, p.max_par, p.exp_tree_pct, d_err, st, &launches));
+    VPM_CUDA_TRY(keys_sort2d(x, y, q, act, tree, ts, p.exp_tree_pct, d_err, st, &launches));
     if (int r = record(1)) return r;
-    VPM_CUDA_TRY(build_lists2d(tree, lists, ts.scan, p.eps, d_err, st, &launches));
+    VPM_CUDA_TRY(levels2d(tree, ts, p.max_src, p.max_par, d_err, st, &launches));
     if (int r = record(2)) return r;
+    VPM_CUDA_TRY(build_lists2d(tree, lists, ts.scan, p.eps, d_err, st, &launches));
+    if (int r = record(3)) return r;
     if (tree_only) {
-        for (int i = 3; i <= 6; ++i)
+        for (int i = 4; i < kStageEvents; ++i)
             if (int r = record(i)) return r;
-    } else if (p.precision == VPM_PREC_MIXED) {
-        int r = enqueue_mixed2d(p, o0, o1, velocity, uinf, vinf, &launches);
-        if (r != VPM_OK) return r;
     } else {
         VPM_CUDA_TRY(fmm2d_upward(tree, ex2, p.p, d_err, st, &launches));
-        if (int r = record(3)) return r;
-        VPM_CUDA_TRY(fmm2d_m2l(tree, lists, ex2, p.p, d_err, st, &launches));
         if (int r = record(4)) return r;
-        VPM_CUDA_TRY(fmm2d_eval(tree, lists, ex2, p.p, d_err, st, &launches));
+        VPM_CUDA_TRY(fmm2d_m2l_only(tree, lists, ex2, p.p, d_err, st, &launches));
         if (int r = record(5)) return r;
-        VPM_CUDA_TRY(fmm2d_p2p_out(tree, lists, ex2, o0, o1, velocity, uinf, vinf, d_err, st, &launches));
+        VPM_CUDA_TRY(fmm2d_l2l(tree, ex2, p.p, d_err, st, &launches));
+        if (int r = record(6)) return r;
+        VPM_CUDA_TRY(fmm2d_eval(tree, lists, ex2, p.p, d_err, st, &launches));
+        if (int r = record(7)) return r;
+        if (p.precision == VPM_PREC_MIXED) {
+            float4* rel = (float4*)mixed_base;
+            VPM_CUDA_TRY(fmm2d_p2p_f32(tree, lists, ex2, rel, o0, o1, velocity, uinf, vinf, d_err, st, &launches,
+                                       p.max_par));
+        } else {
+            VPM_CUDA_TRY(fmm2d_p2p_f64_tma(tree, lists, ex2, (double4*)mixed_base, o0, o1, velocity, uinf, vinf, d_err,
+                                           st, &launches, p.max_par));
+        }
+        if (int r = record(8)) return r;
     }
-    if (int r = record(6)) return r;
     last_launches = launches;
     last_params = p;
     last_n = n;
@@ -230,15 +239,51 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
     return VPM_OK;
 }
 
+// Stage mark i. Eager launches record event i. While one graph is being
+// captured (use_graph = 1) marks are skipped: event nodes inside the graph
+// would cost more than the stages they time. While per-stage graphs are
+// being captured (use_graph = 2) a mark closes the graph of the previous
+// stage and opens the next; replay records the events between stage graphs.
 int Ctx::record(int i) {
-    if (!timing) return VPM_OK;
-    VPM_CUDA_TRY(cudaEventRecord(ev[i], stream));
+    if (!capturing) {
+        VPM_CUDA_TRY(cudaEventRecord(ev[i], stream));
+        if (ring_cur >= 0) VPM_CUDA_TRY(cudaEventRecord(ring[ring_cur][i], stream));
+        return VPM_OK;
+    }
+    if (!split_capture || i == 0) return VPM_OK;
+    cudaGraph_t g = nullptr;
+    VPM_CUDA_TRY(cudaStreamEndCapture(stream, &g));
+    cudaGraphExec_t x = nullptr;
+    cudaError_t e = cudaGraphInstantiate(&x, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaGraphInstantiate (stage)");
+    stage_exec[i - 1] = x;
+    if (i < kStageEvents - 1) VPM_CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     return VPM_OK;
 }
+
+// The ring slot for the evaluation about to be enqueued (if the ring is on).
+void Ctx::begin_ring() {
+    ring_cur = -1;
+    if (!ring_on) return;
+    if (!ring[0][0]) {
+        for (auto& row : ring)
+            for (auto& e : row) cudaEventCreate(&e);
+    }
+    ring_cur = (ring_head + ring_count) % kRing;
+    if (ring_count == kRing) ring_head = (ring_head + 1) % kRing;
+    else ++ring_count;
+}
+
+void Ctx::end_ring() { ring_cur = -1; }
 
 void Ctx::drop_graph() {
     if (gexec) cudaGraphExecDestroy(gexec);
     gexec = nullptr;
+    for (auto& x : stage_exec) {
+        if (x) cudaGraphExecDestroy(x);
+        x = nullptr;
+    }
 }
 
 // Enqueue (or replay) one evaluation on device buffers. With p.use_graph the
@@ -248,16 +293,35 @@ void Ctx::drop_graph() {
 int Ctx::launch2d(const double* x, const double* y, const double* q, const uint8_t* act, int n,
                   const vpm_fmm_params& p, int K, double* o0, double* o1, int velocity, double uinf,
                   double vinf) {
-    if (!p.use_graph) return enqueue2d(x, y, q, act, n, p, K, o0, o1, velocity, uinf, vinf, false);
+    if (!p.use_graph) {
+        last_timed = true;
+        begin_ring();
+        int r = enqueue2d(x, y, q, act, n, p, K, o0, o1, velocity, uinf, vinf, false);
+        end_ring();
+        return r;
+    }
     GraphKey k;
     std::memset(&k, 0, sizeof(k));  // padding included: the key is compared bytewise
     k.ptr[0] = x; k.ptr[1] = y; k.ptr[2] = q; k.ptr[3] = act; k.ptr[4] = o0; k.ptr[5] = o1;
     k.n = n; k.K = K; k.velocity = velocity; k.uinf = uinf; k.vinf = vinf; k.p = p; k.stream = stream;
     k.arena = arena2d;
-    if (gexec && std::memcmp(&k, &gkey, sizeof(k)) == 0) {
-        VPM_CUDA_TRY(cudaGraphLaunch(gexec, stream));
+    const bool split = p.use_graph == 2;
+    const bool have = split ? stage_exec[0] != nullptr : gexec != nullptr;
+    if (have && std::memcmp(&k, &gkey, sizeof(k)) == 0) {
+        if (split) {
+            begin_ring();
+            if (int r = record(0)) return r;
+            for (int i = 0; i < kStageEvents - 1; ++i) {
+                VPM_CUDA_TRY(cudaGraphLaunch(stage_exec[i], stream));
+                if (int r = record(i + 1)) return r;
+            }
+            end_ring();
+        } else {
+            VPM_CUDA_TRY(cudaGraphLaunch(gexec, stream));
+        }
         last_launches = graph_launches;
         last_n = n;
+        last_timed = split;
         return VPM_OK;
     }
     drop_graph();
@@ -268,26 +332,36 @@ int Ctx::launch2d(const double* x, const double* y, const double* q, const uint8
         coef_binom = p.binom;
     }
     VPM_CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-    timing = false;
+    capturing = true;
+    split_capture = split;
     int r = enqueue2d(x, y, q, act, n, p, K, o0, o1, velocity, uinf, vinf, false);
-    timing = true;
-    cudaGraph_t g = nullptr;
-    cudaError_t e = cudaStreamEndCapture(stream, &g);
+    capturing = false;
+    split_capture = false;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(stream, &cs);
     if (r != VPM_OK) {
-        if (g) cudaGraphDestroy(g);
+        if (cs != cudaStreamCaptureStatusNone) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(stream, &g);
+            if (g) cudaGraphDestroy(g);
+        }
+        drop_graph();
         return r;
     }
-    if (e != cudaSuccess) return fail_cuda(e, "cudaStreamEndCapture");
-    e = cudaGraphInstantiate(&gexec, g, 0);
-    cudaGraphDestroy(g);
-    if (e != cudaSuccess) {
-        gexec = nullptr;
-        return fail_cuda(e, "cudaGraphInstantiate");
+    if (!split) {
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(stream, &g);
+        if (e != cudaSuccess) return fail_cuda(e, "cudaStreamEndCapture");
+        e = cudaGraphInstantiate(&gexec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            gexec = nullptr;
+            return fail_cuda(e, "cudaGraphInstantiate");
+        }
     }
     std::memcpy(&gkey, &k, sizeof(k));
     graph_launches = last_launches;
-    VPM_CUDA_TRY(cudaGraphLaunch(gexec, stream));
-    return VPM_OK;
+    return launch2d(x, y, q, act, n, p, K, o0, o1, velocity, uinf, vinf);
 }
 
 int Ctx::collect_stats(vpm_fmm_stats* s) {
@@ -303,16 +377,19 @@ int Ctx::collect_stats(vpm_fmm_stats* s) {
     s->max_level = info.max_leaf_level;
     s->list1_len = (int64_t)info.list1_len;
     s->list3_len = (int64_t)info.list3_len;
-    float ms[7] = {0};
-    if (!last_was_graph)
-        for (int i = 1; i <= 6; ++i) cudaEventElapsedTime(&ms[i], ev[i - 1], ev[i]);
-    s->ms_tree = ms[1];
-    s->ms_lists = ms[2];
-    s->ms_upward = ms[3];
-    s->ms_m2l = ms[4];
-    s->ms_eval = ms[5];
-    s->ms_p2p = ms[6];
-    if (!last_was_graph) cudaEventElapsedTime(&s->ms_total, ev[0], ev[6]);
+    float ms[kStageEvents] = {0};
+    if (last_timed)
+        for (int i = 1; i < kStageEvents; ++i) cudaEventElapsedTime(&ms[i], ev[i - 1], ev[i]);
+    s->ms_keys_sort = ms[1];
+    s->ms_levels = ms[2];
+    s->ms_tree = ms[1] + ms[2];
+    s->ms_lists = ms[3];
+    s->ms_upward = ms[4];
+    s->ms_m2l = ms[5];
+    s->ms_l2l = ms[6];
+    s->ms_eval = ms[7];
+    s->ms_p2p = ms[8];
+    if (last_timed) cudaEventElapsedTime(&s->ms_total, ev[0], ev[kStageEvents - 1]);
     s->kernels = last_launches;
     s->depth_retry = depth_retry;
     // Interaction counts (exact, from the lists).
@@ -362,6 +439,7 @@ int Ctx::run2d_host(const double* x, const double* y, const double* q_or_omega, 
             VPM_CUDA_TRY(cudaMemcpyAsync(in_q, q_or_omega, sizeof(double) * n, cudaMemcpyHostToDevice, stream));
         }
         last_was_graph = p.use_graph != 0 && !tree_only;
+        if (tree_only) last_timed = true;
         r = tree_only ? enqueue2d(in_x, in_y, in_q, in_act, n, p, K, out0, out1, velocity, uinf, vinf, true)
                       : launch2d(in_x, in_y, in_q, in_act, n, p, K, out0, out1, velocity, uinf, vinf);
         if (r) return r;
@@ -546,6 +624,32 @@ int vpm_fmm2d_field_device(vpm_ctx* ctx, const double* x, const double* y, const
     if (r) return r;
     c->last_was_graph = p.use_graph != 0;
     return c->launch2d(x, y, q, active, n, p, p.max_depth, ex, ey, 0, 0.0, 0.0);
+}
+
+int vpm_stage_history(vpm_ctx* ctx, int32_t enable, int32_t max_entries, float* ms, int32_t* count) {
+    if (!ctx) return VPM_EINVAL;
+    Ctx* c = (Ctx*)ctx;
+    cudaError_t e = cudaSetDevice(c->device);
+    if (e != cudaSuccess) return c->fail_cuda(e, "cudaSetDevice");
+    int got = 0;
+    if (ms && max_entries > 0 && c->ring_count > 0) {
+        e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) return c->fail_cuda(e, "vpm_stage_history");
+        for (int k = 0; k < c->ring_count && got < max_entries; ++k) {
+            const int slot = (c->ring_head + k) % Ctx::kRing;
+            for (int i = 0; i + 1 < vpm::kStageEvents; ++i) {
+                float v = 0.f;
+                cudaEventElapsedTime(&v, c->ring[slot][i], c->ring[slot][i + 1]);
+                ms[(size_t)got * (vpm::kStageEvents - 1) + i] = v;
+            }
+            ++got;
+        }
+    }
+    if (count) *count = got;
+    c->ring_head = 0;
+    c->ring_count = 0;
+    c->ring_on = enable ? 1 : 0;
+    return VPM_OK;
 }
 
 int vpm_last_stats(vpm_ctx* ctx, vpm_fmm_stats* stats) {

@@ -47,7 +47,9 @@ int Ctx::init(int dev) {
     device = dev;
     cudaError_t e = cudaSetDevice(dev);
     if (e != cudaSuccess) return fail_cuda(e, "cudaSetDevice");
-    e = cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking);
+    // A blocking stream: work the caller puts on the legacy default stream
+    // (e.g. PyTorch's default) is ordered with the context's work.
+    e = cudaStreamCreate(&own_stream);
     if (e != cudaSuccess) return fail_cuda(e, "cudaStreamCreate");
     stream = own_stream;
     e = cudaMalloc(&d_err, 64);
@@ -76,23 +78,10 @@ int Ctx::count_interactions(vpm_fmm_stats* s) {
     return VPM_OK;
 }
 
-// Mixed-form work area: leaf-relative FP32 particles (float4 per particle).
-size_t mixed_bytes(int n, int cap_cells, int P) { return sizeof(float4) * (size_t)n + 256; }
+// Near-field work area: leaf-relative FP32 particles (float4 per particle,
+// mixed form) or the AoS FP64 copy (double4 per particle, plain form).
+size_t mixed_bytes(int n, int cap_cells, int P) { return sizeof(double4) * (size_t)n + 256; }
 
-// Mixed form: the upward pass, M2L and the far-field evaluation in FP64 and
-// the near field (P2P, the dominant stage) in FP32 with compensated sums.
-int Ctx::enqueue_mixed2d(const vpm_fmm_params& p, double* o0, double* o1, int velocity, double uinf, double vinf,
-                         int* launches) {
-    cudaStream_t st = stream;
-    VPM_CUDA_TRY(fmm2d_upward(tree, ex2, p.p, d_err, st, launches));
-    if (int r = record(3)) return r;
-    VPM_CUDA_TRY(fmm2d_m2l(tree, lists, ex2, p.p, d_err, st, launches));
-    if (int r = record(4)) return r;
-    VPM_CUDA_TRY(fmm2d_eval(tree, lists, ex2, p.p, d_err, st, launches));
-    if (int r = record(5)) return r;
-    float4* rel = (float4*)mixed_base;
-    VPM_CUDA_TRY(fmm2d_p2p_f32(tree, lists, ex2, rel, o0, o1, velocity, uinf, vinf, d_err, st, launches));
-    return VPM_OK;
-}
+
 
 }  // namespace vpm

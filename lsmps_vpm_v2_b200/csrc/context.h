@@ -9,6 +9,10 @@
 
 namespace vpm {
 
+// Stage marks of one evaluation: 0 start, 1 keys+sort, 2 tree levels,
+// 3 lists, 4 P2M+M2M, 5 M2L, 6 L2L, 7 M2P+L2P, 8 P2P (end).
+constexpr int kStageEvents = 9;
+
 struct Caps2D {
     int n = 0, cells = 0, P = 0;
     long long l1 = 0, l3 = 0;
@@ -34,7 +38,7 @@ struct Ctx {
     cudaStream_t stream = nullptr;
     std::string last_error;
     unsigned* d_err = nullptr;
-    cudaEvent_t ev[8] = {};
+    cudaEvent_t ev[kStageEvents] = {};
 
     // 2D arena
     void* arena2d = nullptr;
@@ -61,7 +65,16 @@ struct Ctx {
     };
     cudaGraphExec_t gexec = nullptr;
     GraphKey gkey{};
-    bool timing = true;  // record the per-stage events (off while capturing)
+    bool capturing = false;      // a CUDA graph capture is open on `stream`
+    bool split_capture = false;  // ... one graph per stage (use_graph = 2)
+    bool last_timed = false;     // the stage events of the last evaluation are valid
+    cudaGraphExec_t stage_exec[kStageEvents - 1] = {};
+    // Ring of stage-event sets: with the ring on, each timed evaluation records
+    // into the next slot, so many evaluations can run back to back and be
+    // read afterwards (vpm_stage_history).
+    static constexpr int kRing = 64;
+    cudaEvent_t ring[kRing][kStageEvents] = {};
+    int ring_on = 0, ring_head = 0, ring_count = 0, ring_cur = -1;
     bool last_was_graph = false;
     int graph_launches = 0;
 
@@ -84,8 +97,6 @@ struct Ctx {
     int enqueue2d(const double* x, const double* y, const double* q, const uint8_t* act, int n,
                   const vpm_fmm_params& p, int K, double* o0, double* o1, int velocity, double uinf, double vinf,
                   bool tree_only);
-    int enqueue_mixed2d(const vpm_fmm_params& p, double* o0, double* o1, int velocity, double uinf, double vinf,
-                        int* launches);
     int run2d_host(const double* x, const double* y, const double* q_or_omega, const double* s, const uint8_t* act,
                    int64_t n, const vpm_fmm_params* prm, double* o0, double* o1, int velocity, double uinf,
                    double vinf, vpm_fmm_stats* stats, bool tree_only);
@@ -95,12 +106,22 @@ struct Ctx {
     int launch2d(const double* x, const double* y, const double* q, const uint8_t* act, int n,
                  const vpm_fmm_params& p, int K, double* o0, double* o1, int velocity, double uinf, double vinf);
     void drop_graph();
+    void begin_ring();
+    void end_ring();
     int record(int i);
 };
 
+// FP32 P2P of the mixed form: warp per leaf (max_par >= 0), or the block-per-
+// leaf TMA-staged kernel sized for leaves of at most -max_par particles
+// (max_par < 0).
 cudaError_t fmm2d_p2p_f32(const Tree2D& t, const Lists2D& l, const Expansions2D& e, float4* rel, double* out0,
                           double* out1, int velocity, double u_inf, double v_inf, unsigned* err, cudaStream_t st,
-                          int* launches);
+                          int* launches, int max_par);
+// FP64 P2P on an AoS copy of the particles (`aos`, n entries); kernel choice as
+// for fmm2d_p2p_f32.
+cudaError_t fmm2d_p2p_f64_tma(const Tree2D& t, const Lists2D& l, const Expansions2D& e, double4* aos, double* out0,
+                              double* out1, int velocity, double u_inf, double v_inf, unsigned* err, cudaStream_t st,
+                              int* launches, int max_par);
 cudaError_t fmm2d_p2p_out(const Tree2D& t, const Lists2D& l, const Expansions2D& e, double* out0, double* out1,
                           int velocity, double u_inf, double v_inf, unsigned* err, cudaStream_t st, int* launches);
 

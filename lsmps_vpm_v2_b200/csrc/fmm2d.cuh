@@ -66,6 +66,10 @@ struct Tree2D {
     // accepts an entry only if that cell has the queried level and index.
     int32_t* dense;
     int dense_levels;
+    // Grid-barrier words of the cooperative level loops (tree levels at 0,
+    // M2M at 2, L2L at 4), zeroed with the tickets at the start of every
+    // evaluation; nullptr: launch level by level.
+    unsigned* gbar;
 };
 
 // Dense grid levels for n particles (<= 11, i.e. <= 5.6M entries).
@@ -96,6 +100,8 @@ struct Lists2D {
 
 // Scratch of the tree build.
 constexpr int kBBoxBlocks = 296;
+constexpr int kTicketWords = kMaxLevels2D + 2 + 8;  // level tickets, bbox counter, 3 x 2 barrier words
+constexpr int kBarrierWordsAt = kMaxLevels2D + 2;
 
 struct TreeScratch2D {
     double* bbox_partial;   // [kBBoxBlocks * 4]
@@ -103,7 +109,7 @@ struct TreeScratch2D {
     uint32_t* val_alt;
     uint32_t* act_u32;
     uint64_t* lvl_status;   // [kMaxLevels2D + 1][max_tiles]
-    unsigned* lvl_ticket;   // [kMaxLevels2D + 2]
+    unsigned* lvl_ticket;   // [kTicketWords]: level tickets, bbox counter, then the grid-barrier words
     int lvl_max_tiles;      // in tiles of 8 parents
     SortScratch sort;
     ScanScratch scan;
@@ -114,6 +120,13 @@ struct TreeScratch2D {
 cudaError_t build_tree2d(const double* x, const double* y, const double* q, const uint8_t* act, Tree2D& t,
                          TreeScratch2D& s, int max_src, int max_par, double exp_pct, unsigned* err, cudaStream_t st,
                          int* launches);
+
+// The two halves of build_tree2d: bounding box, keys, sort, gather and the
+// active-count scan; then the level-by-level cell construction.
+cudaError_t keys_sort2d(const double* x, const double* y, const double* q, const uint8_t* act, Tree2D& t,
+                        TreeScratch2D& s, double exp_pct, unsigned* err, cudaStream_t st, int* launches);
+cudaError_t levels2d(Tree2D& t, TreeScratch2D& s, int max_src, int max_par, unsigned* err, cudaStream_t st,
+                     int* launches);
 
 // Lists 1-4 (count, scan, fill). Requires the tree on `st`.
 cudaError_t build_lists2d(const Tree2D& t, Lists2D& l, ScanScratch& scan, double eps, unsigned* err,
@@ -145,7 +158,10 @@ struct Expansions2D {
 
 cudaError_t fmm2d_upward(const Tree2D& t, Expansions2D& e, int P, unsigned* err, cudaStream_t st, int* launches);
 cudaError_t fmm2d_m2l(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, unsigned* err, cudaStream_t st,
-                      int* launches);
+                      int* launches);  // M2L followed by the L2L levels
+cudaError_t fmm2d_m2l_only(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, unsigned* err,
+                           cudaStream_t st, int* launches);
+cudaError_t fmm2d_l2l(const Tree2D& t, Expansions2D& e, int P, unsigned* err, cudaStream_t st, int* launches);
 cudaError_t fmm2d_eval(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, unsigned* err, cudaStream_t st,
                        int* launches);
 cudaError_t fmm2d_p2p(const Tree2D& t, const Lists2D& l, const Expansions2D& e, double* ex, double* ey,

@@ -109,10 +109,12 @@ p2m2d(Tree2D t, double2* __restrict__ a, int P, unsigned* err) {
 // M2M into the active non-leaf cells of level L (fmm2D.cpp:309-379), one warp
 // per cell, lane p computing a_p by Horner's rule in t = z_child - z_parent:
 //   a_p += a0 t^p + sum_{k=1..p} m2m[p][k] a_k t^(p-k).
-__global__ void __launch_bounds__(128)
-m2m_level2d(Tree2D t, double2* __restrict__ a, const double* __restrict__ coef, int P, int L, unsigned* err) {
+//
+// Child expansions are read through L2 (ld.cg): in the cooperative kernel the
+// level below was written by other blocks of the same launch.
+__device__ __forceinline__ void m2m_level_body(const Tree2D& t, double2* __restrict__ a,
+                                               const double* __restrict__ coef, int P, int L) {
     __shared__ double2 s_child[4][W];
-    if (fatal(err)) return;
     const double* g_m2m = coef + kCoefM2M;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int c0 = t.info->level_start[L], c1 = t.info->level_start[L + 1];
@@ -127,7 +129,7 @@ m2m_level2d(Tree2D t, double2* __restrict__ a, const double* __restrict__ coef, 
         double2 acc = make_double2(0.0, 0.0);
         for (int r = 0; r < __popc(m); ++r) {
             const int ch = ch0 + r;
-            if (lane <= P) s_child[wib][lane] = a[(size_t)ch * (P + 1) + lane];
+            if (lane <= P) s_child[wib][lane] = __ldcg(&a[(size_t)ch * (P + 1) + lane]);
             __syncwarp();
             const double2 tt = make_double2(t.c_cx[ch] - px, t.c_cy[ch] - py);
             if (lane == 0) {
@@ -147,21 +149,39 @@ m2m_level2d(Tree2D t, double2* __restrict__ a, const double* __restrict__ coef, 
     }
 }
 
+__global__ void __launch_bounds__(128)
+m2m_level2d(Tree2D t, double2* __restrict__ a, const double* __restrict__ coef, int P, int L, unsigned* err) {
+    if (block_fatal(err)) return;
+    m2m_level_body(t, a, coef, P, L);
+}
+
+// All M2M levels (depth-1 down to 1) in one cooperative launch, a grid
+// barrier between levels.
+__global__ void __launch_bounds__(128)
+m2m_levels_coop(Tree2D t, double2* __restrict__ a, const double* __restrict__ coef, int P, unsigned* bar,
+                unsigned* err) {
+    const int depth = t.info->depth;
+    for (int L = depth - 1; L >= 1; --L) {
+        if (!block_fatal(err)) m2m_level_body(t, a, coef, P, L);
+        grid_sync(bar, err);
+    }
+}
+
 // L2L pull into every cell of level L >= 3 from its parent (fmm2D.cpp:587-651,
 // where each non-leaf parent at levels 2..max-1 pushes into its children):
 //   b_p(c) += sum_{k=p..P} l2l[p][k] b_k(parent) t^(k-p),  t = z_c - z_parent.
 // The parent's expansion is final because level L-1 ran in the previous launch.
-__global__ void __launch_bounds__(128)
-l2l_level2d(Tree2D t, double2* __restrict__ b, const double* __restrict__ coef, int P, int L, unsigned* err) {
+// Parent expansions are read through L2 (ld.cg) for the cooperative kernel.
+__device__ __forceinline__ void l2l_level_body(const Tree2D& t, double2* __restrict__ b,
+                                               const double* __restrict__ coef, int P, int L) {
     __shared__ double2 s_par[4][W];
-    if (fatal(err)) return;
     const double* g_l2l = coef + kCoefL2L;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int c0 = t.info->level_start[L], c1 = t.info->level_start[L + 1];
     const int warps = gridDim.x * (blockDim.x >> 5);
     for (int c = c0 + blockIdx.x * (blockDim.x >> 5) + wib; c < c1; c += warps) {
         const int par = t.c_parent[c];
-        if (lane <= P) s_par[wib][lane] = b[(size_t)par * (P + 1) + lane];
+        if (lane <= P) s_par[wib][lane] = __ldcg(&b[(size_t)par * (P + 1) + lane]);
         __syncwarp();
         if (lane <= P) {
             const double2 tt = make_double2(t.c_cx[c] - t.c_cx[par], t.c_cy[c] - t.c_cy[par]);
@@ -170,9 +190,26 @@ l2l_level2d(Tree2D t, double2* __restrict__ b, const double* __restrict__ coef, 
             double2 S = cscale(s_par[wib][P], cf[P]);
             for (int kk = P - 1; kk >= pp; --kk) S = cfma(S, tt, cscale(s_par[wib][kk], cf[kk]));
             double2* bc = &b[(size_t)c * (P + 1) + pp];
-            *bc = cadd(*bc, S);
+            *bc = cadd(__ldcg(bc), S);
         }
         __syncwarp();
+    }
+}
+
+__global__ void __launch_bounds__(128)
+l2l_level2d(Tree2D t, double2* __restrict__ b, const double* __restrict__ coef, int P, int L, unsigned* err) {
+    if (block_fatal(err)) return;
+    l2l_level_body(t, b, coef, P, L);
+}
+
+// All L2L levels (3 down to the depth) in one cooperative launch.
+__global__ void __launch_bounds__(128)
+l2l_levels_coop(Tree2D t, double2* __restrict__ b, const double* __restrict__ coef, int P, unsigned* bar,
+                unsigned* err) {
+    const int depth = t.info->depth;
+    for (int L = 3; L <= depth; ++L) {
+        if (!block_fatal(err)) l2l_level_body(t, b, coef, P, L);
+        grid_sync(bar, err);
     }
 }
 
@@ -396,15 +433,34 @@ eval2d(Tree2D t, Lists2D l, const double2* __restrict__ a, const double2* __rest
 
 constexpr int kP2PThreads = 128;
 
-// One block per leaf (grid-stride). Thread (t, split) owns target t and the
-// sources split, split + ns, ... of every list-1 cell; sources are read from
-// global memory (L1-resident, nearly warp-uniform addresses), so the pair
-// loop has no barrier. The partial sums of a target's splits are combined in
-// a fixed order at the end.
+// Writes one target's total field (near + far) in the caller's order.
+__device__ __forceinline__ void p2p_store(const Tree2D& t, int ti, double ex, double ey, const double* fx,
+                                          const double* fy, double* out0, double* out1, int velocity, double u_inf,
+                                          double v_inf, unsigned* err) {
+    ex += fx[ti];
+    ey += fy[ti];
+    const uint32_t orig = t.perm[ti];
+    if (orig >= (uint32_t)t.n) {
+        set_err(err, ERR_INDEX);
+    } else if (velocity) {
+        out0[orig] = ey + u_inf;
+        out1[orig] = -ex + v_inf;
+    } else {
+        out0[orig] = ex;
+        out1[orig] = ey;
+    }
+}
+
+// One block per leaf (grid-stride). With H = ceil(T/2), thread (t, split)
+// owns targets t and t + H and the sources split, split + ns, ... of every
+// list-1 cell (ns = 128 / H), so each source load serves two targets. Sources
+// come straight from global memory (L1-resident, nearly warp-uniform
+// addresses); the j == i exclusion is only tested inside the target's own
+// leaf. Partial sums are combined in a fixed order.
 __global__ void __launch_bounds__(kP2PThreads)
 p2p2d(Tree2D t, Lists2D l, const double* __restrict__ fx, const double* __restrict__ fy, double* __restrict__ out0,
       double* __restrict__ out1, int velocity, double u_inf, double v_inf, unsigned* err) {
-    __shared__ double s_px[kP2PThreads], s_py[kP2PThreads];
+    __shared__ double s_px[2][kP2PThreads], s_py[2][kP2PThreads];
     if (fatal(err)) return;
     const int nl = t.info->n_leaves;
     const double* __restrict__ px = t.px;
@@ -414,57 +470,58 @@ p2p2d(Tree2D t, Lists2D l, const double* __restrict__ fx, const double* __restri
         const int c = t.leaf_cells[li];
         const int lo = t.c_lo[c], hi = t.c_hi[c];
         const uint32_t o1 = l.l1_off[li], e1 = l.l1_off[li + 1];
-        for (int tb = lo; tb < hi; tb += kP2PThreads) {
-            const int T = min(kP2PThreads, hi - tb);
-            const int ns = kP2PThreads / T;
-            const int tt = threadIdx.x % T, split = threadIdx.x / T;
+        for (int tb = lo; tb < hi; tb += 2 * kP2PThreads) {
+            const int T = min(2 * kP2PThreads, hi - tb);
+            const int H = (T + 1) >> 1;
+            const int ns = kP2PThreads / H;
+            const int tt = threadIdx.x % H, split = threadIdx.x / H;
             const bool on = split < ns;
-            const int ti = tb + tt;
-            const double xt = px[ti], yt = py[ti];
-            double ex0 = 0.0, ey0 = 0.0, ex1 = 0.0, ey1 = 0.0;
+            const int ta = tb + tt, tbb = tb + tt + H;
+            const bool hasb = tt + H < T;
+            const double xa = px[ta], ya = py[ta];
+            const double xb = hasb ? px[tbb] : xa, yb = hasb ? py[tbb] : ya;
+            double exa = 0.0, eya = 0.0, exb = 0.0, eyb = 0.0;
             if (on) {
                 for (uint32_t k = o1; k < e1; ++k) {
                     const int sc = l.l1_src[k];
                     const int s_hi = t.c_hi[sc];
-                    int j = t.c_lo[sc] + split;
-                    for (; j + ns < s_hi; j += 2 * ns) {
-                        const int j1 = j + ns;
-                        const double dx0 = xt - __ldg(px + j), dy0 = yt - __ldg(py + j);
-                        const double dx1 = xt - __ldg(px + j1), dy1 = yt - __ldg(py + j1);
-                        const double r0 = fma(dx0, dx0, dy0 * dy0), r1 = fma(dx1, dx1, dy1 * dy1);
-                        const double f0 = (j == ti) ? 0.0 : __ldg(pq + j) * rcp_nr(r0);
-                        const double f1 = (j1 == ti) ? 0.0 : __ldg(pq + j1) * rcp_nr(r1);
-                        ex0 = fma(f0, dx0, ex0);
-                        ey0 = fma(f0, dy0, ey0);
-                        ex1 = fma(f1, dx1, ex1);
-                        ey1 = fma(f1, dy1, ey1);
-                    }
-                    if (j < s_hi) {
-                        const double dx0 = xt - __ldg(px + j), dy0 = yt - __ldg(py + j);
-                        const double r0 = fma(dx0, dx0, dy0 * dy0);
-                        const double f0 = (j == ti) ? 0.0 : __ldg(pq + j) * rcp_nr(r0);
-                        ex0 = fma(f0, dx0, ex0);
-                        ey0 = fma(f0, dy0, ey0);
+                    if (sc != c) {
+                        for (int j = t.c_lo[sc] + split; j < s_hi; j += ns) {
+                            const double sx = __ldg(px + j), sy = __ldg(py + j), sq = __ldg(pq + j);
+                            const double dxa = xa - sx, dya = ya - sy, dxb = xb - sx, dyb = yb - sy;
+                            const double fa = sq * rcp_nr(fma(dxa, dxa, dya * dya));
+                            const double fb = sq * rcp_nr(fma(dxb, dxb, dyb * dyb));
+                            exa = fma(fa, dxa, exa);
+                            eya = fma(fa, dya, eya);
+                            exb = fma(fb, dxb, exb);
+                            eyb = fma(fb, dyb, eyb);
+                        }
+                    } else {
+                        for (int j = t.c_lo[sc] + split; j < s_hi; j += ns) {
+                            const double sx = __ldg(px + j), sy = __ldg(py + j), sq = __ldg(pq + j);
+                            const double dxa = xa - sx, dya = ya - sy, dxb = xb - sx, dyb = yb - sy;
+                            const double fa = (j == ta) ? 0.0 : sq * rcp_nr(fma(dxa, dxa, dya * dya));
+                            const double fb = (j == tbb) ? 0.0 : sq * rcp_nr(fma(dxb, dxb, dyb * dyb));
+                            exa = fma(fa, dxa, exa);
+                            eya = fma(fa, dya, eya);
+                            exb = fma(fb, dxb, exb);
+                            eyb = fma(fb, dyb, eyb);
+                        }
                     }
                 }
             }
-            double ex = ex0 + ex1, ey = ey0 + ey1;
-            if (on && split > 0) { s_px[threadIdx.x] = ex; s_py[threadIdx.x] = ey; }
+            if (on && split > 0) {
+                s_px[0][threadIdx.x] = exa; s_py[0][threadIdx.x] = eya;
+                s_px[1][threadIdx.x] = exb; s_py[1][threadIdx.x] = eyb;
+            }
             __syncthreads();
             if (split == 0) {
-                for (int s = 1; s < ns; ++s) { ex += s_px[s * T + tt]; ey += s_py[s * T + tt]; }
-                ex += fx[ti];
-                ey += fy[ti];
-                const uint32_t orig = t.perm[ti];
-                if (orig >= (uint32_t)t.n) {
-                    set_err(err, ERR_INDEX);
-                } else if (velocity) {
-                    out0[orig] = ey + u_inf;
-                    out1[orig] = -ex + v_inf;
-                } else {
-                    out0[orig] = ex;
-                    out1[orig] = ey;
+                for (int s = 1; s < ns; ++s) {
+                    exa += s_px[0][s * H + tt]; eya += s_py[0][s * H + tt];
+                    exb += s_px[1][s * H + tt]; eyb += s_py[1][s * H + tt];
                 }
+                p2p_store(t, ta, exa, eya, fx, fy, out0, out1, velocity, u_inf, v_inf, err);
+                if (hasb) p2p_store(t, tbb, exb, eyb, fx, fy, out0, out1, velocity, u_inf, v_inf, err);
             }
             __syncthreads();
         }
@@ -491,12 +548,19 @@ __global__ void leaf_relative_f32(Tree2D t, float4* __restrict__ rel, unsigned* 
 // once per source cell] + (x - c_src) [FP32, precomputed], so every pair
 // offset keeps ~1e-7 relative accuracy. Each thread sums one source cell's
 // contributions in FP32 and adds that block sum into an FP64 accumulator
-// (compensated per-target summation). Same thread mapping as p2p2d.
+// (compensated per-target summation). Same mapping as p2p2d (two targets
+// per thread).
+__device__ __forceinline__ float rcp_approx(float a) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
+    return r;
+}
+
 __global__ void __launch_bounds__(kP2PThreads)
 p2p2d_f32(Tree2D t, Lists2D l, const float4* __restrict__ rel, const double* __restrict__ fx,
           const double* __restrict__ fy, double* __restrict__ out0, double* __restrict__ out1, int velocity,
           double u_inf, double v_inf, unsigned* err) {
-    __shared__ double s_px[kP2PThreads], s_py[kP2PThreads];
+    __shared__ double s_px[2][kP2PThreads], s_py[2][kP2PThreads];
     if (fatal(err)) return;
     const int nl = t.info->n_leaves;
     for (int li = blockIdx.x; li < nl; li += gridDim.x) {
@@ -504,72 +568,497 @@ p2p2d_f32(Tree2D t, Lists2D l, const float4* __restrict__ rel, const double* __r
         const int lo = t.c_lo[c], hi = t.c_hi[c];
         const double ccx = t.c_cx[c], ccy = t.c_cy[c];
         const uint32_t o1 = l.l1_off[li], e1 = l.l1_off[li + 1];
-        for (int tb = lo; tb < hi; tb += kP2PThreads) {
-            const int T = min(kP2PThreads, hi - tb);
-            const int ns = kP2PThreads / T;
-            const int tt = threadIdx.x % T, split = threadIdx.x / T;
+        for (int tb = lo; tb < hi; tb += 2 * kP2PThreads) {
+            const int T = min(2 * kP2PThreads, hi - tb);
+            const int H = (T + 1) >> 1;
+            const int ns = kP2PThreads / H;
+            const int tt = threadIdx.x % H, split = threadIdx.x / H;
             const bool on = split < ns;
-            const int ti = tb + tt;
-            const float4 tg = rel[ti];
-            double ex = 0.0, ey = 0.0;
+            const int ta = tb + tt, tbb = tb + tt + H;
+            const bool hasb = tt + H < T;
+            const float4 ga = rel[ta];
+            const float4 gb = hasb ? rel[tbb] : ga;
+            double exa = 0.0, eya = 0.0, exb = 0.0, eyb = 0.0;
             if (on) {
                 for (uint32_t k = o1; k < e1; ++k) {
                     const int sc = l.l1_src[k];
                     const int s_hi = t.c_hi[sc];
-                    // target minus source offset, per source cell
-                    const float ox = tg.x - (float)(t.c_cx[sc] - ccx), oy = tg.y - (float)(t.c_cy[sc] - ccy);
-                    float bx0 = 0.f, by0 = 0.f, bx1 = 0.f, by1 = 0.f;
-                    int j = t.c_lo[sc] + split;
-                    for (; j + ns < s_hi; j += 2 * ns) {
-                        const int j1 = j + ns;
-                        const float4 s0 = __ldg(rel + j), s1 = __ldg(rel + j1);
-                        const float dx0 = ox - s0.x, dy0 = oy - s0.y;
-                        const float dx1 = ox - s1.x, dy1 = oy - s1.y;
-                        const float r0 = fmaf(dx0, dx0, dy0 * dy0), r1 = fmaf(dx1, dx1, dy1 * dy1);
-                        float i0, i1;
-                        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(i0) : "f"(r0));
-                        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(i1) : "f"(r1));
-                        const float f0 = (j == ti) ? 0.f : s0.z * i0;
-                        const float f1 = (j1 == ti) ? 0.f : s1.z * i1;
-                        bx0 = fmaf(f0, dx0, bx0);
-                        by0 = fmaf(f0, dy0, by0);
-                        bx1 = fmaf(f1, dx1, bx1);
-                        by1 = fmaf(f1, dy1, by1);
+                    const float ox = (float)(t.c_cx[sc] - ccx), oy = (float)(t.c_cy[sc] - ccy);
+                    const float ax = ga.x - ox, ay = ga.y - oy, bx = gb.x - ox, by = gb.y - oy;
+                    float pxa = 0.f, pya = 0.f, pxb = 0.f, pyb = 0.f;
+                    if (sc != c) {
+                        for (int j = t.c_lo[sc] + split; j < s_hi; j += ns) {
+                            const float4 sv = __ldg(rel + j);
+                            const float dxa = ax - sv.x, dya = ay - sv.y, dxb = bx - sv.x, dyb = by - sv.y;
+                            const float fa = sv.z * rcp_approx(fmaf(dxa, dxa, dya * dya));
+                            const float fb = sv.z * rcp_approx(fmaf(dxb, dxb, dyb * dyb));
+                            pxa = fmaf(fa, dxa, pxa);
+                            pya = fmaf(fa, dya, pya);
+                            pxb = fmaf(fb, dxb, pxb);
+                            pyb = fmaf(fb, dyb, pyb);
+                        }
+                    } else {
+                        for (int j = t.c_lo[sc] + split; j < s_hi; j += ns) {
+                            const float4 sv = __ldg(rel + j);
+                            const float dxa = ax - sv.x, dya = ay - sv.y, dxb = bx - sv.x, dyb = by - sv.y;
+                            const float fa = (j == ta) ? 0.f : sv.z * rcp_approx(fmaf(dxa, dxa, dya * dya));
+                            const float fb = (j == tbb) ? 0.f : sv.z * rcp_approx(fmaf(dxb, dxb, dyb * dyb));
+                            pxa = fmaf(fa, dxa, pxa);
+                            pya = fmaf(fa, dya, pya);
+                            pxb = fmaf(fb, dxb, pxb);
+                            pyb = fmaf(fb, dyb, pyb);
+                        }
                     }
-                    if (j < s_hi) {
-                        const float4 s0 = __ldg(rel + j);
-                        const float dx0 = ox - s0.x, dy0 = oy - s0.y;
-                        const float r0 = fmaf(dx0, dx0, dy0 * dy0);
-                        float i0;
-                        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(i0) : "f"(r0));
-                        const float f0 = (j == ti) ? 0.f : s0.z * i0;
-                        bx0 = fmaf(f0, dx0, bx0);
-                        by0 = fmaf(f0, dy0, by0);
-                    }
-                    ex += (double)bx0 + (double)bx1;
-                    ey += (double)by0 + (double)by1;
+                    exa += (double)pxa; eya += (double)pya;
+                    exb += (double)pxb; eyb += (double)pyb;
                 }
             }
-            if (on && split > 0) { s_px[threadIdx.x] = ex; s_py[threadIdx.x] = ey; }
+            if (on && split > 0) {
+                s_px[0][threadIdx.x] = exa; s_py[0][threadIdx.x] = eya;
+                s_px[1][threadIdx.x] = exb; s_py[1][threadIdx.x] = eyb;
+            }
             __syncthreads();
             if (split == 0) {
-                for (int s2 = 1; s2 < ns; ++s2) { ex += s_px[s2 * T + tt]; ey += s_py[s2 * T + tt]; }
-                ex += fx[ti];
-                ey += fy[ti];
-                const uint32_t orig = t.perm[ti];
-                if (orig >= (uint32_t)t.n) {
-                    set_err(err, ERR_INDEX);
-                } else if (velocity) {
-                    out0[orig] = ey + u_inf;
-                    out1[orig] = -ex + v_inf;
-                } else {
-                    out0[orig] = ex;
-                    out1[orig] = ey;
+                for (int s2 = 1; s2 < ns; ++s2) {
+                    exa += s_px[0][s2 * H + tt]; eya += s_py[0][s2 * H + tt];
+                    exb += s_px[1][s2 * H + tt]; eyb += s_py[1][s2 * H + tt];
                 }
+                p2p_store(t, ta, exa, eya, fx, fy, out0, out1, velocity, u_inf, v_inf, err);
+                if (hasb) p2p_store(t, tbb, exb, eyb, fx, fy, out0, out1, velocity, u_inf, v_inf, err);
             }
             __syncthreads();
         }
     }
+}
+
+// ---- TMA-staged FP32 P2P ------------------------------------------------------
+
+constexpr int kStageCells = 64;  // list-1 cells of one leaf held in the stage descriptor
+
+struct StageCell {
+    int start, end;  // staged slots [start, end)
+    float ox, oy;    // c_src - c_tgt (FP64 difference rounded once)
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// Bounded wait on the phase with the given parity; false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+    const uint32_t a = smem_u32(bar);
+    for (long long i = 0; i < kSpinLimit; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+// One bulk copy global -> this CTA's shared memory, completing on `bar`.
+// Both addresses 16-byte aligned, size a multiple of 16 (float4 elements).
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// Stage the list-1 sources of leaf `li` into buffer (buf, cells): one thread.
+// Returns the number of staged slots, or -1 when the leaf does not fit (the
+// barrier is still armed, with zero bytes, so its phase completes).
+__device__ int stage_leaf(const Tree2D& t, const Lists2D& l, const float4* rel, int li, float4* buf, int cap,
+                          StageCell* cells, uint64_t* bar) {
+    const int c = t.leaf_cells[li];
+    const double ccx = t.c_cx[c], ccy = t.c_cy[c];
+    const uint32_t o1 = l.l1_off[li], e1 = l.l1_off[li + 1];
+    int total = 0;
+    bool fits = (int)(e1 - o1) <= kStageCells;
+    if (fits) {
+        for (uint32_t k = o1; k < e1; ++k) {
+            const int sc = l.l1_src[k];
+            total += t.c_hi[sc] - t.c_lo[sc];
+        }
+        fits = total <= cap;
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_arrive_expect_tx(bar, fits ? (unsigned)total * 16u : 0u);
+    if (!fits) return -1;
+    int pos = 0, kk = 0;
+    for (uint32_t k = o1; k < e1; ++k, ++kk) {
+        const int sc = l.l1_src[k];
+        const int lo = t.c_lo[sc], hi = t.c_hi[sc];
+        cells[kk].start = pos;
+        cells[kk].end = pos + (hi - lo);
+        cells[kk].ox = (float)(t.c_cx[sc] - ccx);
+        cells[kk].oy = (float)(t.c_cy[sc] - ccy);
+        bulk_g2s(buf + pos, rel + lo, (unsigned)(hi - lo) * 16u, bar);
+        pos += hi - lo;
+    }
+    return total;
+}
+
+// Per-precision pieces of the TMA-staged P2P.
+struct P2PF32 {
+    using Elem = float4;   // (x - c_leaf, y - c_leaf, q, -) in FP32
+    using Acc = float;
+    static __device__ __forceinline__ void shift(Elem& e, float ox, float oy) { e.x += ox; e.y += oy; }
+    static __device__ __forceinline__ float inv(float r2) { return rcp_approx(r2); }
+};
+struct P2PF64 {
+    using Elem = double4;  // (x, y, q, -) in FP64, absolute coordinates
+    using Acc = double;
+    static __device__ __forceinline__ void shift(Elem&, float, float) {}
+    static __device__ __forceinline__ double inv(double r2) { return rcp_nr(r2); }
+};
+
+// Stage the list-1 sources of leaf `li` into `buf` with one bulk copy per
+// source cell (one thread). Returns the staged slot count, or -1 when the
+// leaf does not fit (the barrier is still armed, with zero bytes, so its
+// phase completes); cells[k] receives each cell's slot range and its centre
+// offset relative to the target leaf (FP64 difference rounded once).
+template <class Elem>
+__device__ int stage_leaf(const Tree2D& t, const Lists2D& l, const Elem* src, int li, Elem* buf, int cap,
+                          StageCell* cells, uint64_t* bar) {
+    const int c = t.leaf_cells[li];
+    const double ccx = t.c_cx[c], ccy = t.c_cy[c];
+    const uint32_t o1 = l.l1_off[li], e1 = l.l1_off[li + 1];
+    int total = 0;
+    bool fits = (int)(e1 - o1) <= kStageCells;
+    if (fits) {
+        for (uint32_t k = o1; k < e1; ++k) {
+            const int sc = l.l1_src[k];
+            total += t.c_hi[sc] - t.c_lo[sc];
+        }
+        fits = total <= cap;
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_arrive_expect_tx(bar, fits ? (unsigned)(total * sizeof(Elem)) : 0u);
+    if (!fits) return -1;
+    int pos = 0, kk = 0;
+    for (uint32_t k = o1; k < e1; ++k, ++kk) {
+        const int sc = l.l1_src[k];
+        const int lo = t.c_lo[sc], hi = t.c_hi[sc];
+        cells[kk].start = pos;
+        cells[kk].end = pos + (hi - lo);
+        cells[kk].ox = (float)(t.c_cx[sc] - ccx);
+        cells[kk].oy = (float)(t.c_cy[sc] - ccy);
+        bulk_g2s(buf + pos, src + lo, (unsigned)((hi - lo) * sizeof(Elem)), bar);
+        pos += hi - lo;
+    }
+    return total;
+}
+
+constexpr int kTPT = 4;  // targets per thread in the TMA P2P
+
+// Pair loop of one thread over source slots [j0, j1) (step ns) for kTPT
+// targets; slot self[k] is excluded for target k (-1: none). FP32 sums are
+// flushed into the FP64 accumulators every 64 sources.
+template <class Tr>
+__device__ __forceinline__ void pair_loop4(const typename Tr::Elem* __restrict__ buf, int j0, int j1, int ns,
+                                           const double* tx, const double* ty, const int* self, double* ex,
+                                           double* ey) {
+    using A = typename Tr::Acc;
+    A x[kTPT], y[kTPT];
+    #pragma unroll
+    for (int k = 0; k < kTPT; ++k) { x[k] = (A)tx[k]; y[k] = (A)ty[k]; }
+    const bool has_self = self[0] >= 0 || self[1] >= 0 || self[2] >= 0 || self[3] >= 0;
+    for (int jb = j0; jb < j1; jb += 64 * ns) {
+        const int je = min(j1, jb + 64 * ns);
+        A px[kTPT], py[kTPT];
+        #pragma unroll
+        for (int k = 0; k < kTPT; ++k) { px[k] = 0; py[k] = 0; }
+        if (!has_self) {
+            for (int j = jb; j < je; j += ns) {
+                const typename Tr::Elem sv = buf[j];
+                const A sx = (A)sv.x, sy = (A)sv.y, sq = (A)sv.z;
+                #pragma unroll
+                for (int k = 0; k < kTPT; ++k) {
+                    const A dx = x[k] - sx, dy = y[k] - sy;
+                    const A f = sq * Tr::inv(dx * dx + dy * dy);
+                    px[k] += f * dx;
+                    py[k] += f * dy;
+                }
+            }
+        } else {
+            for (int j = jb; j < je; j += ns) {
+                const typename Tr::Elem sv = buf[j];
+                const A sx = (A)sv.x, sy = (A)sv.y, sq = (A)sv.z;
+                #pragma unroll
+                for (int k = 0; k < kTPT; ++k) {
+                    const A dx = x[k] - sx, dy = y[k] - sy;
+                    A f = sq * Tr::inv(dx * dx + dy * dy);
+                    if (j == self[k]) f = 0;
+                    px[k] += f * dx;
+                    py[k] += f * dy;
+                }
+            }
+        }
+        #pragma unroll
+        for (int k = 0; k < kTPT; ++k) { ex[k] += (double)px[k]; ey[k] += (double)py[k]; }
+    }
+}
+
+// TMA-staged P2P. Each block walks its leaves (grid-stride) with two stage
+// buffers: while the block computes leaf i from one buffer, thread 0 has bulk
+// copies of leaf i+1's list-1 sources in flight into the other (one mbarrier
+// per buffer, bounded waits). After a stage lands the block adds each source
+// cell's centre offset (FP32 form: sources then share the target leaf's
+// frame), so the pair loop is one flat loop over the staged slots. Thread
+// (t, split) owns targets t and t + H (H = ceil(T/2)) and slots split,
+// split + ns, ... A leaf whose sources do not fit is computed from global
+// memory cell by cell.
+template <class Tr>
+__global__ void __launch_bounds__(kP2PThreads)
+p2p2d_tma(Tree2D t, Lists2D l, const typename Tr::Elem* __restrict__ src, const double* __restrict__ fx,
+          const double* __restrict__ fy, double* __restrict__ out0, double* __restrict__ out1, int velocity,
+          double u_inf, double v_inf, int cap, unsigned* err) {
+    using Elem = typename Tr::Elem;
+    extern __shared__ __align__(16) unsigned char p2p_sm[];
+    Elem* bufs = (Elem*)p2p_sm;                                        // [2][cap]
+    StageCell* scells = (StageCell*)(bufs + 2 * (size_t)cap);          // [2][kStageCells]
+    uint64_t* bars = (uint64_t*)(scells + 2 * kStageCells);            // [2]
+    int* s_count = (int*)(bars + 2);                                   // [2]
+    __shared__ double s_px[kTPT][kP2PThreads], s_py[kTPT][kP2PThreads];
+    if (fatal(err)) return;
+    const int nl = t.info->n_leaves;
+    if ((int)blockIdx.x >= nl) return;
+    if (threadIdx.x == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_count[0] = stage_leaf<Elem>(t, l, src, blockIdx.x, bufs, cap, scells, &bars[0]);
+    }
+    __syncthreads();
+    int iter = 0;
+    for (int li = blockIdx.x; li < nl; li += gridDim.x, ++iter) {
+        const int b = iter & 1;
+        const int nxt = li + gridDim.x;
+        if (threadIdx.x == 0 && nxt < nl)
+            s_count[b ^ 1] = stage_leaf<Elem>(t, l, src, nxt, bufs + (size_t)(b ^ 1) * cap, cap,
+                                              scells + (b ^ 1) * kStageCells, &bars[b ^ 1]);
+        const bool ok = mbar_wait(&bars[b], (iter >> 1) & 1);
+        if (!ok) set_err(err, ERR_TIMEOUT);
+        const int staged = s_count[b];
+        Elem* buf = bufs + (size_t)b * cap;
+        const StageCell* cells = scells + b * kStageCells;
+        const int c = t.leaf_cells[li];
+        const int lo = t.c_lo[c], hi = t.c_hi[c];
+        const double ccx = t.c_cx[c], ccy = t.c_cy[c];
+        const uint32_t o1 = l.l1_off[li], e1 = l.l1_off[li + 1];
+        const int ncell = (int)(e1 - o1);
+        // Own-leaf slot range, and the frame shift of the staged sources.
+        int own0 = -1;
+        if (staged >= 0 && ok) {
+            for (int kk = 0; kk < ncell; ++kk) {
+                const StageCell ci = cells[kk];
+                if (l.l1_src[o1 + kk] == c) own0 = ci.start;
+                for (int j = ci.start + threadIdx.x; j < ci.end; j += blockDim.x) Tr::shift(buf[j], ci.ox, ci.oy);
+            }
+        }
+        __syncthreads();
+        for (int tb = lo; tb < hi; tb += kTPT * kP2PThreads) {
+            const int T = min(kTPT * kP2PThreads, hi - tb);
+            const int H = (T + kTPT - 1) / kTPT;
+            const int ns = kP2PThreads / H;
+            const int tt = threadIdx.x % H, split = threadIdx.x / H;
+            const bool on = split < ns && ok;
+            int ti[kTPT];
+            double tx[kTPT], ty[kTPT], ex[kTPT], ey[kTPT];
+            #pragma unroll
+            for (int k = 0; k < kTPT; ++k) {
+                const int off = tt + k * H;
+                ti[k] = off < T ? tb + off : -1;
+                const Elem g = src[ti[k] >= 0 ? ti[k] : tb + tt];
+                tx[k] = g.x;
+                ty[k] = g.y;
+                ex[k] = 0.0;
+                ey[k] = 0.0;
+            }
+            if (on) {
+                if (staged >= 0) {
+                    int self[kTPT];
+                    #pragma unroll
+                    for (int k = 0; k < kTPT; ++k) self[k] = (own0 >= 0 && ti[k] >= 0) ? own0 + (ti[k] - lo) : -1;
+                    // Slots of the own leaf need the j == i test; the others do not.
+                    if (own0 >= 0) {
+                        const int own1 = own0 + (hi - lo);
+                        const int none[kTPT] = {-1, -1, -1, -1};
+                        pair_loop4<Tr>(buf, split, own0, ns, tx, ty, none, ex, ey);
+                        const int j0 = own0 + ((split - own0) % ns + ns) % ns;
+                        pair_loop4<Tr>(buf, j0, own1, ns, tx, ty, self, ex, ey);
+                        const int j2 = own1 + ((split - own1) % ns + ns) % ns;
+                        pair_loop4<Tr>(buf, j2, staged, ns, tx, ty, none, ex, ey);
+                    } else {
+                        pair_loop4<Tr>(buf, split, staged, ns, tx, ty, self, ex, ey);
+                    }
+                } else {
+                    for (int kk = 0; kk < ncell; ++kk) {
+                        const int sc = l.l1_src[o1 + kk];
+                        const int slo = t.c_lo[sc], shi = t.c_hi[sc];
+                        double sx = 0.0, sy = 0.0;
+                        if (sizeof(Elem) == sizeof(float4)) {
+                            sx = (double)(float)(t.c_cx[sc] - ccx);
+                            sy = (double)(float)(t.c_cy[sc] - ccy);
+                        }
+                        double tx2[kTPT], ty2[kTPT];
+                        int self[kTPT];
+                        #pragma unroll
+                        for (int k = 0; k < kTPT; ++k) {
+                            tx2[k] = tx[k] - sx;
+                            ty2[k] = ty[k] - sy;
+                            self[k] = (sc == c) ? ti[k] : -1;
+                        }
+                        pair_loop4<Tr>(src, slo + split, shi, ns, tx2, ty2, self, ex, ey);
+                    }
+                }
+            }
+            if (on && split > 0) {
+                #pragma unroll
+                for (int k = 0; k < kTPT; ++k) { s_px[k][threadIdx.x] = ex[k]; s_py[k][threadIdx.x] = ey[k]; }
+            }
+            __syncthreads();
+            if (split == 0 && ok) {
+                for (int s2 = 1; s2 < ns; ++s2) {
+                    #pragma unroll
+                    for (int k = 0; k < kTPT; ++k) { ex[k] += s_px[k][s2 * H + tt]; ey[k] += s_py[k][s2 * H + tt]; }
+                }
+                #pragma unroll
+                for (int k = 0; k < kTPT; ++k)
+                    if (ti[k] >= 0) p2p_store(t, ti[k], ex[k], ey[k], fx, fy, out0, out1, velocity, u_inf, v_inf, err);
+            }
+            __syncthreads();
+        }
+    }
+    // Copies are only issued for leaves this block then waits on; after a
+    // timed-out wait, wait once more (bounded) so no copy lands in freed
+    // shared memory.
+    if (threadIdx.x == 0 && iter > 0) {
+        const int last = iter - 1;
+        (void)mbar_wait(&bars[last & 1], (last >> 1) & 1);
+    }
+}
+
+// Warp-per-leaf P2P (the default near field). Each warp owns one leaf at a
+// time (grid-stride over leaves), so no block-wide barrier sits in the loop.
+// With H = ceil(T/4) lanes per split, lane (t, split) owns targets t, t+H,
+// t+2H, t+3H and the sources split, split + ns, ... (ns = 32/H) of every
+// list-1 cell, read straight from global memory (nearly warp-uniform
+// addresses, L1-resident). Split partials are summed in a fixed order through
+// a per-warp shared-memory tile. FP32 form: coordinates relative to the
+// target leaf (source-cell offset rounded once per cell).
+constexpr int kWarpP2PWarps = 4;
+
+template <class Tr>
+__global__ void __launch_bounds__(32 * kWarpP2PWarps)
+p2p2d_warp(Tree2D t, Lists2D l, const typename Tr::Elem* __restrict__ src, const double* __restrict__ fx,
+           const double* __restrict__ fy, double* __restrict__ out0, double* __restrict__ out1, int velocity,
+           double u_inf, double v_inf, unsigned* err) {
+    using Elem = typename Tr::Elem;
+    __shared__ double s_red[kWarpP2PWarps][2 * kTPT][32];
+    if (fatal(err)) return;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int nl = t.info->n_leaves;
+    const bool rel = sizeof(Elem) == sizeof(float4);
+    for (int li = blockIdx.x * kWarpP2PWarps + wib; li < nl; li += gridDim.x * kWarpP2PWarps) {
+        const int c = t.leaf_cells[li];
+        const int lo = t.c_lo[c], hi = t.c_hi[c];
+        const double ccx = t.c_cx[c], ccy = t.c_cy[c];
+        const uint32_t o1 = l.l1_off[li], e1 = l.l1_off[li + 1];
+        for (int tb = lo; tb < hi; tb += kTPT * 32) {
+            const int T = min(kTPT * 32, hi - tb);
+            const int H = (T + kTPT - 1) / kTPT;
+            const int ns = 32 / H;
+            const int tt = lane % H, split = lane / H;
+            const bool on = split < ns;
+            int ti[kTPT];
+            double tx[kTPT], ty[kTPT], ex[kTPT], ey[kTPT];
+            #pragma unroll
+            for (int k = 0; k < kTPT; ++k) {
+                const int off = tt + k * H;
+                ti[k] = off < T ? tb + off : -1;
+                const Elem g = src[ti[k] >= 0 ? ti[k] : tb];
+                tx[k] = g.x;
+                ty[k] = g.y;
+                ex[k] = 0.0;
+                ey[k] = 0.0;
+            }
+            if (on) {
+                for (uint32_t kk = o1; kk < e1; ++kk) {
+                    const int sc = l.l1_src[kk];
+                    const int slo = t.c_lo[sc], shi = t.c_hi[sc];
+                    double sx = 0.0, sy = 0.0;
+                    if (rel) {
+                        sx = (double)(float)(t.c_cx[sc] - ccx);
+                        sy = (double)(float)(t.c_cy[sc] - ccy);
+                    }
+                    double tx2[kTPT], ty2[kTPT];
+                    int self[kTPT];
+                    #pragma unroll
+                    for (int k = 0; k < kTPT; ++k) {
+                        tx2[k] = tx[k] - sx;
+                        ty2[k] = ty[k] - sy;
+                        self[k] = (sc == c) ? ti[k] : -1;
+                    }
+                    pair_loop4<Tr>(src, slo + split, shi, ns, tx2, ty2, self, ex, ey);
+                }
+            }
+            // sum the splits of each target: lanes tt, tt + H, ... hold its parts
+            #pragma unroll
+            for (int k = 0; k < kTPT; ++k) {
+                s_red[wib][2 * k][lane] = on ? ex[k] : 0.0;
+                s_red[wib][2 * k + 1][lane] = on ? ey[k] : 0.0;
+            }
+            __syncwarp();
+            if (split == 0) {
+                #pragma unroll
+                for (int k = 0; k < kTPT; ++k) {
+                    double sx2 = 0.0, sy2 = 0.0;
+                    for (int s2 = 0; s2 < ns; ++s2) {
+                        sx2 += s_red[wib][2 * k][s2 * H + tt];
+                        sy2 += s_red[wib][2 * k + 1][s2 * H + tt];
+                    }
+                    if (ti[k] >= 0) p2p_store(t, ti[k], sx2, sy2, fx, fy, out0, out1, velocity, u_inf, v_inf, err);
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// AoS (x, y, q) copy of the sorted particles for the FP64 TMA P2P (bulk
+// copies need 16-byte aligned ranges).
+__global__ void particles_aos(Tree2D t, double4* __restrict__ aos, unsigned* err) {
+    if (fatal(err)) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < t.n; i += gridDim.x * blockDim.x)
+        aos[i] = make_double4(t.px[i], t.py[i], t.pq[i], 0.0);
+}
+
+template <class Tr>
+cudaError_t launch_p2p_tma(const Tree2D& t, const Lists2D& l, const typename Tr::Elem* src, const Expansions2D& e,
+                           double* out0, double* out1, int velocity, double u_inf, double v_inf, unsigned* err,
+                           cudaStream_t st, int max_par) {
+    // Room for twelve full leaves: the nine neighbours at the leaf's level plus finer ones.
+    const int cap = std::min(4096, std::max(512, 12 * max_par));
+    const size_t smem = 2 * (size_t)cap * sizeof(typename Tr::Elem) + 2 * kStageCells * sizeof(StageCell) + 64;
+    static size_t smem_set = 0;
+    if (smem > smem_set) {
+        cudaError_t r = cudaFuncSetAttribute(p2p2d_tma<Tr>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (r != cudaSuccess) return r;
+        smem_set = smem;
+    }
+    p2p2d_tma<Tr><<<148 * 8, kP2PThreads, smem, st>>>(t, l, src, e.fx, e.fy, out0, out1, velocity, u_inf, v_inf, cap,
+                                                      err);
+    return cudaGetLastError();
 }
 
 __global__ void zero_u32(unsigned* p, int n) {
@@ -605,6 +1094,15 @@ cudaError_t fmm2d_upward(const Tree2D& t, Expansions2D& e, int P, unsigned* err,
     const size_t smem = sizeof(double2) * kP2MWarps * (P + 1) * kAccPad;
     p2m2d<<<148 * 16, 32 * kP2MWarps, smem, st>>>(t, e.a, P, err);
     *launches += 1;
+    if (t.gbar) {
+        int grid = 0;
+        r = launch_coop(m2m_levels_coop, 128, 0, st, 4, &grid, t, e.a, (const double*)e.coef, P, t.gbar + 2, err);
+        if (r == cudaSuccess) {
+            *launches += 1;
+            return cudaGetLastError();
+        }
+        (void)cudaGetLastError();  // cooperative launch refused: one launch per level instead
+    }
     for (int L = t.key_levels - 1; L >= 1; --L) {
         m2m_level2d<<<148 * 4, 128, 0, st>>>(t, e.a, e.coef, P, L, err);
         *launches += 1;
@@ -637,8 +1135,8 @@ cudaError_t set_m2l_operators2d(int P, bool exact, double2* dst, cudaStream_t st
     return cudaStreamSynchronize(st);
 }
 
-cudaError_t fmm2d_m2l(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, unsigned* err, cudaStream_t st,
-                      int* launches) {
+cudaError_t fmm2d_m2l_only(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, unsigned* err,
+                           cudaStream_t st, int* launches) {
     const int G = 32 / P;
     if (e.op) {
         const size_t smem = sizeof(double2) * 4 * (size_t)(2 * G * (P + 1) + G * (2 * P + 1));
@@ -648,11 +1146,32 @@ cudaError_t fmm2d_m2l(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P,
         m2l2d<<<148 * 16, 128, smem, st>>>(t, l, e.a, e.b, e.coef, P, err);
     }
     *launches += 1;
+    return cudaGetLastError();
+}
+
+cudaError_t fmm2d_l2l(const Tree2D& t, Expansions2D& e, int P, unsigned* err, cudaStream_t st, int* launches) {
+    if (t.gbar) {
+        int grid = 0;
+        cudaError_t r = launch_coop(l2l_levels_coop, 128, 0, st, 4, &grid, t, e.b, (const double*)e.coef, P,
+                                    t.gbar + 4, err);
+        if (r == cudaSuccess) {
+            *launches += 1;
+            return cudaGetLastError();
+        }
+        (void)cudaGetLastError();  // cooperative launch refused: one launch per level instead
+    }
     for (int L = 3; L <= t.key_levels; ++L) {
         l2l_level2d<<<148 * 4, 128, 0, st>>>(t, e.b, e.coef, P, L, err);
         *launches += 1;
     }
     return cudaGetLastError();
+}
+
+cudaError_t fmm2d_m2l(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, unsigned* err, cudaStream_t st,
+                      int* launches) {
+    cudaError_t r = fmm2d_m2l_only(t, l, e, P, err, st, launches);
+    if (r != cudaSuccess) return r;
+    return fmm2d_l2l(t, e, P, err, st, launches);
 }
 
 cudaError_t fmm2d_eval(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, unsigned* err, cudaStream_t st,
@@ -671,10 +1190,23 @@ cudaError_t fmm2d_p2p_out(const Tree2D& t, const Lists2D& l, const Expansions2D&
 
 cudaError_t fmm2d_p2p_f32(const Tree2D& t, const Lists2D& l, const Expansions2D& e, float4* rel, double* out0,
                           double* out1, int velocity, double u_inf, double v_inf, unsigned* err, cudaStream_t st,
-                          int* launches) {
+                          int* launches, int max_par) {
     leaf_relative_f32<<<148 * 8, 128, 0, st>>>(t, rel, err);
-    p2p2d_f32<<<148 * 16, kP2PThreads, 0, st>>>(t, l, rel, e.fx, e.fy, out0, out1, velocity, u_inf, v_inf, err);
     *launches += 2;
+    if (max_par < 0) return launch_p2p_tma<P2PF32>(t, l, rel, e, out0, out1, velocity, u_inf, v_inf, err, st, -max_par);
+    p2p2d_warp<P2PF32><<<148 * 16, 32 * kWarpP2PWarps, 0, st>>>(t, l, rel, e.fx, e.fy, out0, out1, velocity, u_inf,
+                                                               v_inf, err);
+    return cudaGetLastError();
+}
+
+cudaError_t fmm2d_p2p_f64_tma(const Tree2D& t, const Lists2D& l, const Expansions2D& e, double4* aos, double* out0,
+                              double* out1, int velocity, double u_inf, double v_inf, unsigned* err, cudaStream_t st,
+                              int* launches, int max_par) {
+    particles_aos<<<148 * 8, 256, 0, st>>>(t, aos, err);
+    *launches += 2;
+    if (max_par < 0) return launch_p2p_tma<P2PF64>(t, l, aos, e, out0, out1, velocity, u_inf, v_inf, err, st, -max_par);
+    p2p2d_warp<P2PF64><<<148 * 16, 32 * kWarpP2PWarps, 0, st>>>(t, l, aos, e.fx, e.fy, out0, out1, velocity, u_inf,
+                                                               v_inf, err);
     return cudaGetLastError();
 }
 

@@ -153,7 +153,7 @@ extern "C" int vpm_fmm2d_field_device_static(const double* x, const double* y, c
     ts.act_u32 = cv.take<uint32_t>(base, kStaticMaxN);
     ts.bbox_partial = cv.take<double>(base, kBBoxBlocks * 4);
     ts.lvl_status = cv.take<uint64_t>(base, (size_t)(kMaxLevels2D + 1) * lvl_tiles);
-    ts.lvl_ticket = cv.take<unsigned>(base, kMaxLevels2D + 2);
+    ts.lvl_ticket = cv.take<unsigned>(base, kTicketWords);
     ts.lvl_max_tiles = lvl_tiles;
     ts.sort.status = cv.take<uint32_t>(base, (size_t)8 * s_tiles * 256);
     ts.sort.tickets = cv.take<unsigned>(base, 8);
@@ -174,6 +174,7 @@ extern "C" int vpm_fmm2d_field_device_static(const double* x, const double* y, c
     t.cap_cells = kStaticMaxCells;
     t.dense = nullptr;  // lookups fall back to binary search
     t.dense_levels = 0;
+    t.gbar = ts.lvl_ticket + kBarrierWordsAt;
     l.l2_src = cv.take<int32_t>(base, C * kList2Cap); l.l2_slot = cv.take<uint8_t>(base, C * kList2Cap);
     l.l2_n = cv.take<uint8_t>(base, C);
     l.l4_src = cv.take<int32_t>(base, C * kList4Cap); l.l4_n = cv.take<uint8_t>(base, C);
@@ -223,7 +224,7 @@ extern "C" int vpm_fmm2d_field_device_static(const double* x, const double* y, c
     if (r == cudaSuccess) r = fmm2d_eval(t, l, xe, P, err, st, &launches);
     if (r == cudaSuccess) {
         if (p.precision == VPM_PREC_MIXED)
-            r = fmm2d_p2p_f32(t, l, xe, rel, ex, ey, 0, 0.0, 0.0, err, st, &launches);
+            r = fmm2d_p2p_f32(t, l, xe, rel, ex, ey, 0, 0.0, 0.0, err, st, &launches, 0);
         else
             r = fmm2d_p2p(t, l, xe, ex, ey, err, st, &launches);
     }

@@ -71,12 +71,28 @@ bbox2d(const double* __restrict__ x, const double* __restrict__ y, int n, double
         last = atomicAdd(done, 1u) == gridDim.x - 1;
     }
     __syncthreads();
-    if (!last || threadIdx.x != 0) return;
+    if (!last) return;
     __threadfence();
-    for (unsigned b = 0; b < gridDim.x; ++b) {
+    // The last block reduces the per-block partials, all threads in parallel.
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
         const double* p = partial + 4 * b;
         mnx = fmin(mnx, __ldcg(p)); mxx = fmax(mxx, __ldcg(p + 1));
         mny = fmin(mny, __ldcg(p + 2)); mxy = fmax(mxy, __ldcg(p + 3));
+    }
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mnx = fmin(mnx, __shfl_xor_sync(0xffffffffu, mnx, o));
+        mxx = fmax(mxx, __shfl_xor_sync(0xffffffffu, mxx, o));
+        mny = fmin(mny, __shfl_xor_sync(0xffffffffu, mny, o));
+        mxy = fmax(mxy, __shfl_xor_sync(0xffffffffu, mxy, o));
+    }
+    __syncthreads();
+    if (lane == 0) { sh[0][warp] = mnx; sh[1][warp] = mxx; sh[2][warp] = mny; sh[3][warp] = mxy; }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+        mnx = fmin(mnx, sh[0][w]); mxx = fmax(mxx, sh[1][w]);
+        mny = fmin(mny, sh[2][w]); mxy = fmax(mxy, sh[3][w]);
     }
     double root = 0.0;
     double ex = fabs(xsub(mxx, mnx)), ey = fabs(xsub(mxy, mny));
@@ -161,29 +177,73 @@ __global__ void tree_root2d(Tree2D t) {
     info->depth = 0;
 }
 
-// First index in [lo, hi) whose level code (key >> shift) is >= v, found by
-// the whole warp: 32 probes per round cut the interval 33-fold, so a range of
-// n keys takes ceil(log33 n) dependent loads instead of log2 n. The result is
-// warp-uniform; every lane must call.
-__device__ __forceinline__ int warp_lower_code(const uint64_t* __restrict__ key, int lo, int hi, int shift,
-                                               uint64_t v, int lane) {
-    int a = lo, b = hi;  // answer in [a, b]
-    while (b - a > 32) {
-        const long long len = b - a;
-        const int pos = a + (int)(((long long)(lane + 1) * len) / 33);
-        const unsigned m = __ballot_sync(0xffffffffu, (key[pos] >> shift) >= v);
-        const int a0 = a;
-        if (m == 0) {
-            a = a0 + (int)((32ll * len) / 33) + 1;
-        } else {
-            const int f = __ffs(m) - 1;
-            b = a0 + (int)(((long long)(f + 1) * len) / 33);
-            if (f > 0) a = a0 + (int)(((long long)f * len) / 33) + 1;
+// The three inner child boundaries of a parent range [lo, hi): the first
+// index whose level code (key >> shift) is >= v+1, v+2 and v+3. The three
+// 33-ary searches run interleaved, each lane issuing up to three independent
+// loads per round, so the warp waits on one chain of dependent loads instead
+// of three; the first round's probes are shared. Results are warp-uniform.
+__device__ __forceinline__ void warp_split3(const uint64_t* __restrict__ key, int lo, int hi, int shift, uint64_t v,
+                                            int lane, int& r1, int& r2, int& r3) {
+    int a[3] = {lo, lo, lo}, b[3] = {hi, hi, hi};
+    if (hi - lo > 32) {
+        const long long len = hi - lo;
+        const uint64_t kv = key[lo + (int)(((long long)(lane + 1) * len) / 33)] >> shift;
+        #pragma unroll
+        for (int t = 0; t < 3; ++t) {
+            const unsigned m = __ballot_sync(0xffffffffu, kv >= v + 1 + t);
+            if (m == 0) {
+                a[t] = lo + (int)((32ll * len) / 33) + 1;
+            } else {
+                const int f = __ffs(m) - 1;
+                b[t] = lo + (int)(((long long)(f + 1) * len) / 33);
+                if (f > 0) a[t] = lo + (int)(((long long)f * len) / 33) + 1;
+            }
         }
     }
-    const int pos = a + lane;
-    const unsigned m = __ballot_sync(0xffffffffu, pos < b && (key[pos] >> shift) >= v);
-    return m ? a + __ffs(m) - 1 : b;
+    for (;;) {
+        bool more = false;
+        uint64_t kv[3];
+        #pragma unroll
+        for (int t = 0; t < 3; ++t) {
+            const long long len = b[t] - a[t];
+            kv[t] = 0;
+            if (len > 32) {
+                more = true;
+                kv[t] = key[a[t] + (int)(((long long)(lane + 1) * len) / 33)] >> shift;
+            }
+        }
+        if (!more) break;
+        #pragma unroll
+        for (int t = 0; t < 3; ++t) {
+            const long long len = b[t] - a[t];
+            if (len <= 32) continue;
+            const unsigned m = __ballot_sync(0xffffffffu, kv[t] >= v + 1 + t);
+            const int a0 = a[t];
+            if (m == 0) {
+                a[t] = a0 + (int)((32ll * len) / 33) + 1;
+            } else {
+                const int f = __ffs(m) - 1;
+                b[t] = a0 + (int)(((long long)(f + 1) * len) / 33);
+                if (f > 0) a[t] = a0 + (int)(((long long)f * len) / 33) + 1;
+            }
+        }
+    }
+    int r[3];
+    uint64_t kv[3];
+    #pragma unroll
+    for (int t = 0; t < 3; ++t) {
+        const int pos = a[t] + lane;
+        kv[t] = pos < b[t] ? key[pos] >> shift : 0;
+    }
+    #pragma unroll
+    for (int t = 0; t < 3; ++t) {
+        const int pos = a[t] + lane;
+        const unsigned m = __ballot_sync(0xffffffffu, pos < b[t] && kv[t] >= v + 1 + t);
+        r[t] = m ? a[t] + __ffs(m) - 1 : b[t];
+    }
+    r1 = r[0];
+    r2 = r[1];
+    r3 = r[2];
 }
 
 __device__ __forceinline__ int sel4(int i, int v0, int v1, int v2, int v3) {
@@ -196,19 +256,26 @@ __device__ __forceinline__ int sel4(int i, int v0, int v1, int v2, int v3) {
 // emitted in parent order, i.e. Morton order within the level. Each new cell
 // also lands in the dense lookup grid (indexed by the reference's cell ID)
 // when its level is covered by it.
-__global__ void __launch_bounds__(kLvlThreads)
-tree_level2d(Tree2D t, int L, int max_src, int max_par, int* dense, int dense_levels, uint64_t* status,
-             unsigned* ticket, unsigned* err) {
+//
+// Everything this step reads that an earlier level wrote (level starts,
+// parent cells) is loaded through L2 (ld.cg): in the cooperative kernel all
+// levels run in one launch and L1 is not coherent across blocks.
+__device__ void level_step(const Tree2D& t, int L, int max_src, int max_par, int* dense, int dense_levels,
+                           uint64_t* status, unsigned* ticket, unsigned* err) {
     __shared__ unsigned s_tile;
     __shared__ uint64_t s_prefix;
     __shared__ int s_cnt[kLvlWarps], s_lf[kLvlWarps], s_xc[kLvlWarps], s_xl[kLvlWarps];
+    __shared__ unsigned s_stop;
     TreeInfo2D* info = t.info;
-    if (*(volatile const unsigned*)err & (ERR_CELL_CAP | ERR_TIMEOUT | ERR_NONFINITE)) return;
-    const int p0 = info->level_start[L - 1];
-    const int np = info->level_start[L] - p0;
+    // One read of the error word per block, so the whole block takes the same exit.
+    if (threadIdx.x == 0) s_stop = *(volatile const unsigned*)err & (ERR_CELL_CAP | ERR_TIMEOUT | ERR_NONFINITE);
+    __syncthreads();
+    if (s_stop) return;
+    const int p0 = __ldcg(&info->level_start[L - 1]);
+    const int np = __ldcg(&info->level_start[L]) - p0;
     const int ntiles = np > 0 ? ceil_div(np, kLvlWarps) : 1;
-    const int base_cell = info->level_start[L];
-    const int base_leaf = info->leaf_start[L];
+    const int base_cell = __ldcg(&info->level_start[L]);
+    const int base_leaf = __ldcg(&info->leaf_start[L]);
     const int shift = 2 * (t.key_levels - L);
     const double len = xdiv(t.geom->root, ldexp(1.0, L));
     const double pivx = t.geom->pivx, pivy = t.geom->pivy;
@@ -221,18 +288,16 @@ tree_level2d(Tree2D t, int L, int max_src, int max_par, int* dense, int dense_le
         if (tile >= ntiles) return;
         const int pi = tile * kLvlWarps + warp;
         const int p = p0 + pi;
-        const bool nonleaf = pi < np && !(t.c_flags[p] & CELL_LEAF);   // warp-uniform
+        const bool nonleaf = pi < np && !(__ldcg(&t.c_flags[p]) & CELL_LEAF);   // warp-uniform
         int b0 = 0, b1 = 0, b2 = 0, b3 = 0, b4 = 0;
         bool has = false, leaf = false;
         unsigned mask = 0, lmask = 0;
         int clo = 0, chi = 0, src = 0;
         if (nonleaf) {
-            b0 = t.c_lo[p];
-            b4 = t.c_hi[p];
-            const uint64_t pc = t.c_code[p] << 2;
-            b1 = warp_lower_code(t.key, b0, b4, shift, pc + 1, lane);
-            b2 = warp_lower_code(t.key, b1, b4, shift, pc + 2, lane);
-            b3 = warp_lower_code(t.key, b2, b4, shift, pc + 3, lane);
+            b0 = __ldcg(&t.c_lo[p]);
+            b4 = __ldcg(&t.c_hi[p]);
+            const uint64_t pc = __ldcg(&t.c_code[p]) << 2;
+            warp_split3(t.key, b0, b4, shift, pc, lane, b1, b2, b3);
             clo = sel4(lane, b0, b1, b2, b3);
             chi = sel4(lane, b1, b2, b3, b4);
             has = lane < 4 && chi > clo;
@@ -310,7 +375,7 @@ tree_level2d(Tree2D t, int L, int max_src, int max_par, int* dense, int dense_le
                 if (ci >= t.cap_cells) {
                     set_err(err, ERR_CELL_CAP);
                 } else {
-                    const int ix = 2 * t.c_ix[p] + (lane & 1), iy = 2 * t.c_iy[p] + (lane >> 1);
+                    const int ix = 2 * __ldcg(&t.c_ix[p]) + (lane & 1), iy = 2 * __ldcg(&t.c_iy[p]) + (lane >> 1);
                     t.c_lo[ci] = clo;
                     t.c_hi[ci] = chi;
                     t.c_src[ci] = src;
@@ -321,7 +386,7 @@ tree_level2d(Tree2D t, int L, int max_src, int max_par, int* dense, int dense_le
                     t.c_level[ci] = (uint8_t)L;
                     t.c_ix[ci] = ix;
                     t.c_iy[ci] = iy;
-                    t.c_code[ci] = (t.c_code[p] << 2) + lane;
+                    t.c_code[ci] = (__ldcg(&t.c_code[p]) << 2) + lane;
                     t.c_cx[ci] = xadd(pivx, xmul(xadd(0.5, (double)ix), len));
                     t.c_cy[ci] = xadd(pivy, xmul(xadd(0.5, (double)iy), len));
                     if (dense && L <= dense_levels) dense[start_id2(L) + ix + ((int64_t)iy << L)] = ci;
@@ -340,6 +405,26 @@ tree_level2d(Tree2D t, int L, int max_src, int max_par, int* dense, int dense_le
     }
 }
 
+__global__ void __launch_bounds__(kLvlThreads)
+tree_level2d(Tree2D t, int L, int max_src, int max_par, int* dense, int dense_levels, uint64_t* status,
+             unsigned* ticket, unsigned* err) {
+    level_step(t, L, max_src, max_par, dense, dense_levels, status, ticket, err);
+}
+
+// All levels in one cooperative launch: a grid barrier between levels, and a
+// stop as soon as a level creates no cells (that test reads a value written
+// before the barrier, so every block takes the same decision).
+__global__ void __launch_bounds__(kLvlThreads)
+tree_levels_coop(Tree2D t, int max_src, int max_par, int* dense, int dense_levels, uint64_t* status, int stride,
+                 unsigned* tickets, unsigned* bar, unsigned* err) {
+    for (int L = 1; L <= t.key_levels; ++L) {
+        level_step(t, L, max_src, max_par, dense, dense_levels, status + (size_t)L * stride, tickets + L, err);
+        grid_sync(bar, err);
+        const int created = __ldcg(&t.info->level_start[L + 1]) - __ldcg(&t.info->level_start[L]);
+        if (created == 0) break;
+    }
+}
+
 // Leaf level range (TreeCell::min_level / max_level, treeCell.cpp:1236-1240).
 __global__ void tree_finish2d(TreeInfo2D* info) {
     int mn = -1, mx = -1;
@@ -355,15 +440,14 @@ __global__ void tree_finish2d(TreeInfo2D* info) {
 
 }  // namespace
 
-cudaError_t build_tree2d(const double* x, const double* y, const double* q, const uint8_t* act, Tree2D& t,
-                         TreeScratch2D& s, int max_src, int max_par, double exp_pct, unsigned* err, cudaStream_t st,
-                         int* launches) {
+cudaError_t keys_sort2d(const double* x, const double* y, const double* q, const uint8_t* act, Tree2D& t,
+                        TreeScratch2D& s, double exp_pct, unsigned* err, cudaStream_t st, int* launches) {
     const int n = t.n;
     const int K = t.key_levels;
     const int gridN = std::max(1, std::min(148 * 8, ceil_div(n, 256)));
     unsigned* done = s.lvl_ticket + kMaxLevels2D + 1;
     const int bb_blocks = std::max(1, std::min(kBBoxBlocks, ceil_div(n, 256)));
-    cudaError_t e = cudaMemsetAsync(s.lvl_ticket, 0, sizeof(unsigned) * (kMaxLevels2D + 2), st);
+    cudaError_t e = cudaMemsetAsync(s.lvl_ticket, 0, sizeof(unsigned) * kTicketWords, st);
     if (e != cudaSuccess) return e;
     bbox2d<<<bb_blocks, 256, 0, st>>>(x, y, n, exp_pct, K, t.geom, s.bbox_partial, done, err);
     keys2d<<<gridN, 256, 0, st>>>(x, y, n, t.geom, K, t.key, t.perm, err);
@@ -383,10 +467,28 @@ cudaError_t build_tree2d(const double* x, const double* y, const double* q, cons
     e = scan_exclusive(s.act_u32, t.actscan, n, t.actscan + n, s.scan, err, st);
     if (e != cudaSuccess) return e;
     *launches += 1;
-    e = cudaMemsetAsync(s.lvl_status, 0, sizeof(uint64_t) * (size_t)(K + 1) * s.lvl_max_tiles, st);
+    return cudaGetLastError();
+}
+
+cudaError_t levels2d(Tree2D& t, TreeScratch2D& s, int max_src, int max_par, unsigned* err, cudaStream_t st,
+                     int* launches) {
+    const int K = t.key_levels;
+    cudaError_t e = cudaMemsetAsync(s.lvl_status, 0, sizeof(uint64_t) * (size_t)(K + 1) * s.lvl_max_tiles, st);
     if (e != cudaSuccess) return e;
     tree_root2d<<<1, 1, 0, st>>>(t);
     *launches += 1;
+    if (t.gbar) {
+        int grid = 0;
+        e = launch_coop(tree_levels_coop, kLvlThreads, 0, st, 8, &grid, t, max_src, max_par, t.dense, t.dense_levels,
+                        s.lvl_status, s.lvl_max_tiles, s.lvl_ticket, t.gbar, err);
+        if (e == cudaSuccess) {
+            *launches += 1;
+            tree_finish2d<<<1, 1, 0, st>>>(t.info);
+            *launches += 1;
+            return cudaGetLastError();
+        }
+        (void)cudaGetLastError();  // cooperative launch refused: one launch per level instead
+    }
     for (int L = 1; L <= K; ++L) {
         long long bound = std::min<long long>(t.cap_cells, 1ll << std::min(2 * (L - 1), 40));
         int tiles = std::max(1, ceil_div(bound, kLvlWarps));
@@ -399,6 +501,14 @@ cudaError_t build_tree2d(const double* x, const double* y, const double* q, cons
     tree_finish2d<<<1, 1, 0, st>>>(t.info);
     *launches += 1;
     return cudaGetLastError();
+}
+
+cudaError_t build_tree2d(const double* x, const double* y, const double* q, const uint8_t* act, Tree2D& t,
+                         TreeScratch2D& s, int max_src, int max_par, double exp_pct, unsigned* err, cudaStream_t st,
+                         int* launches) {
+    cudaError_t e = keys_sort2d(x, y, q, act, t, s, exp_pct, err, st, launches);
+    if (e != cudaSuccess) return e;
+    return levels2d(t, s, max_src, max_par, err, st, launches);
 }
 
 }  // namespace vpm

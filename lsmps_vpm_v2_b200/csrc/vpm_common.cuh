@@ -40,6 +40,48 @@ __device__ __forceinline__ bool fatal(const unsigned* err) {
 }
 
 // ---------------------------------------------------------------------------
+// Grid-wide barrier for cooperative (co-resident) launches: bar[0] counts
+// arrivals, bar[1] is the generation. The last block to arrive resets the
+// count and bumps the generation; the others poll the generation, at most
+// kSpinLimit times (then ERR_TIMEOUT and continue). bar[0] must be zero at
+// launch. Every block must call it the same number of times.
+// ---------------------------------------------------------------------------
+// The error word's fatal bits, read once per block so that every thread of
+// the block takes the same branch (safe around __syncthreads).
+__device__ __forceinline__ bool block_fatal(const unsigned* err) {
+    __shared__ int s_fatal;
+    __syncthreads();
+    if (threadIdx.x == 0) s_fatal = fatal(err);
+    __syncthreads();
+    return s_fatal != 0;
+}
+
+__device__ __forceinline__ void grid_sync(unsigned* bar, unsigned* err) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* gen = bar + 1;
+        const unsigned g = *gen;
+        __threadfence();
+        if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            long long spins = 0;
+            while (*gen == g) {
+                if (++spins > kSpinLimit) {
+                    set_err(err, ERR_TIMEOUT);
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
 // Exact IEEE double operations (round-to-nearest, never contracted): used for
 // every value that decides an integer (cell index, adjacency, separation).
 // ---------------------------------------------------------------------------
@@ -87,6 +129,36 @@ __host__ __device__ __forceinline__ uint64_t morton2(uint32_t ix, uint32_t iy) {
 __host__ __device__ __forceinline__ int64_t start_id2(int L) { return (((int64_t)1 << (2 * L)) - 1) / 3; }
 
 __host__ __device__ inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+// Cooperative launch with every block co-resident: grid = SMs x the
+// occupancy of `kernel` at `block` threads (at most max_blocks_per_sm). The
+// grid size is returned in *grid. Fails (no launch) when the device cannot
+// make the blocks co-resident.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_coop(void (*kernel)(KArgs...), int block, size_t smem, cudaStream_t st, int max_blocks_per_sm,
+                        int* grid, Args... args) {
+    int dev = 0, sms = 0, occ = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, block, smem);
+    if (e != cudaSuccess) return e;
+    if (occ < 1) return cudaErrorCooperativeLaunchTooLarge;
+    if (occ > max_blocks_per_sm) occ = max_blocks_per_sm;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(sms * occ);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (grid) *grid = sms * occ;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
 
 }  // namespace vpm
 

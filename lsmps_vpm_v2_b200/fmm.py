@@ -85,11 +85,27 @@ class Context:
                                                  C.c_void_p(q.data_ptr()), C.c_void_p(active.data_ptr()), n,
                                                  C.byref(p), C.c_void_p(ex.data_ptr()), C.c_void_p(ey.data_ptr())))
 
+    STAGES = ("keys_sort", "levels", "lists", "upward", "m2l", "l2l", "eval", "p2p")
+
+    def stage_history(self, enable: bool = True, max_entries: int = 64):
+        """Stage times (ms, one row per evaluation, columns STAGES) recorded
+        since the last call; recording stays on if `enable`."""
+        ms = np.zeros((max_entries, len(self.STAGES)), np.float32)
+        cnt = C.c_int32()
+        self._check(lib().vpm_stage_history(self._h, int(enable), max_entries, _ptr(ms), C.byref(cnt)))
+        return ms[: cnt.value]
+
     def velocity2d(self, x, y, omega, s, active, u_inf=0.0, v_inf=0.0, params: Params | None = None,
-                   stats: bool = False):
+                   stats: bool = False, out=None):
+        """u = Ey + u_inf, v = -Ex + v_inf (host arrays). `out` = (u, v)
+        preallocated float64 arrays (e.g. pinned) to write into."""
         x, y, w, sz, a = _f64(x), _f64(y), _f64(omega), _f64(s), _u8(active)
         n = x.size
-        u, v = np.empty(n), np.empty(n)
+        if out is not None:
+            u, v = out
+            assert u.dtype == np.float64 and v.dtype == np.float64 and u.flags.c_contiguous and v.flags.c_contiguous
+        else:
+            u, v = np.empty(n), np.empty(n)
         p = params or default_params()
         st = Stats()
         self._check(lib().vpm_velocity2d(self._h, _ptr(x), _ptr(y), _ptr(w), _ptr(sz), _ptr(a), n, C.byref(p),
