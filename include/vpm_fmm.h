@@ -68,6 +68,8 @@ typedef struct vpm_fmm_params {
                              the parameters are unchanged (no per-stage timings);
                              2 = one graph per stage, with the stage events
                              recorded between them (profiling)                    */
+    double center_3d[3];  /* 3D domain centre joined into the root box
+                             (Pars::xcenter/ycenter/zcenter, fast3DFMM.cpp:506-508) */
 } vpm_fmm_params;
 
 /* Per-call figures (counts are exact; times are CUDA-event milliseconds). */
@@ -203,6 +205,56 @@ int vpm_fmm2d_field_device_static(const double* x, const double* y, const double
                                   const uint8_t* active, int64_t n, const vpm_fmm_params* prm,
                                   double* ex, double* ey, void* cuda_stream, char* errbuf,
                                   size_t errlen);
+
+/*
+ * 3D velocity of the vortex particles (x_j, alpha_j) by the octree treecode
+ * of the reference's default 3D path (VELOCITY_3D_TYPE 1):
+ *   u(x_i) = sum_j alpha_j x (x_i - x_j) / |x_i - x_j|^3
+ * with far cells (R^2 > (2 size)^2) through their 10-term Cartesian moments.
+ * Replaces
+ *   fmm3D::calcVelocityFast(pos, active, target, ax, ay, az)   src/FMM/fmm3D.cpp (fast3DFMM.cpp:32-92)
+ *   FMMCell::generateTree                                     src/FMM/fast3DFMM.cpp:485-745
+ *   fastFMM3Dutils::evaluateFMM                               src/FMM/fast3DFMM.cpp:318-472
+ *   fmm3D::get_Field_x / _y / _z                              src/FMM/fmm3D.hpp:106-138
+ * Every particle is a target, as in the reference (which ignores the target
+ * flags); `target` may be NULL. precision = VPM_PREC_MIXED evaluates the P2P
+ * and M2P terms in FP32 (FP64 geometry, decisions and per-target sums).
+ * Leaf iff particle count < prm->leaf_cap_3d; the root box is the particle
+ * box joined with prm->center_3d. Host buffers; stats may be NULL.
+ */
+int vpm_fmm3d_velocity(vpm_ctx* ctx, const double* x, const double* y, const double* z, const double* ax,
+                       const double* ay, const double* az, const uint8_t* active, const uint8_t* target, int64_t n,
+                       const vpm_fmm_params* prm, double* u, double* v, double* w, vpm_fmm_stats* stats);
+
+/* Same with device pointers, asynchronous on the context's stream. */
+int vpm_fmm3d_velocity_device(vpm_ctx* ctx, const double* x, const double* y, const double* z, const double* ax,
+                              const double* ay, const double* az, const uint8_t* active, int64_t n,
+                              const vpm_fmm_params* prm, double* u, double* v, double* w);
+
+/*
+ * The FMM body of VelocityCalc::velocity_fmm_3d_fast
+ * (src/velocity_calculation/velocity_calc.cpp:2384-2524, all particles
+ * evaluated): alpha = omega s^3 / (4 pi), then the free stream of
+ * VelocityCalc::get_velocity (velocity_calc.cpp:226-236). Host buffers.
+ */
+int vpm_velocity3d(vpm_ctx* ctx, const double* x, const double* y, const double* z, const double* omega_x,
+                   const double* omega_y, const double* omega_z, const double* s, const uint8_t* active, int64_t n,
+                   const vpm_fmm_params* prm, double u_inf, double v_inf, double w_inf, double* u, double* v,
+                   double* w, vpm_fmm_stats* stats);
+
+/*
+ * Octree only (FMMCell::generateTree), for the parity dumps: counts, then
+ * per cell in this library's order (level-major, parents in order, octants
+ * 0..7 under a parent): ints6 = nPar, chdFlag, parent index, isActive,
+ * level, max_level (cell 0 only); geom4 = xc, yc, zc, size; and for every
+ * leaf (cell k > 0 with chdFlag 0) its particle IDs in ascending order as
+ * CSR leaf_offs[k]..leaf_offs[k+1] (n_cells + 1 offsets). Any output may be
+ * NULL.
+ */
+int vpm_tree3d_build(vpm_ctx* ctx, const double* x, const double* y, const double* z, const uint8_t* active,
+                     int64_t n, const vpm_fmm_params* prm, vpm_fmm_stats* stats);
+int vpm_tree3d_counts(vpm_ctx* ctx, int64_t* n_cells, int64_t* n_leaves, int32_t* depth);
+int vpm_tree3d_cells(vpm_ctx* ctx, int32_t* ints6, double* geom4, int64_t* leaf_offs, int32_t* pids);
 
 /*
  * FMA-throughput microbenchmark of the device (TFLOP/s of dependent FMA

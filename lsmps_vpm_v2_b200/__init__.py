@@ -6,9 +6,9 @@ reference's operator interface for the path.
 """
 from ._lib import (BINOM_EXACT, BINOM_REFERENCE, PREC_FP64, PREC_MIXED, Params, Stats, VpmError,
                    default_params, lib)
-from .fmm import Context, Particle, TreeCell, VelocityCalc, default_context, fmm2D
+from .fmm import Context, Particle, TreeCell, VelocityCalc, default_context, fmm2D, fmm3D
 
 __all__ = [
-    "BINOM_EXACT", "BINOM_REFERENCE", "PREC_FP64", "PREC_MIXED", "Params", "Stats", "VpmError",
+    "BINOM_EXACT", "BINOM_REFERENCE", "PREC_FP64", "PREC_MIXED", "Params", "Stats", "VpmError", "fmm3D",
     "default_params", "lib", "Context", "Particle", "TreeCell", "VelocityCalc", "default_context", "fmm2D",
 ]

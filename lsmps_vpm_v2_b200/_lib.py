@@ -38,6 +38,7 @@ class Params(C.Structure):
         ("binom", C.c_int32),
         ("max_depth", C.c_int32),
         ("use_graph", C.c_int32),
+        ("center_3d", C.c_double * 3),
     ]
 
 
@@ -99,6 +100,15 @@ SIGNATURES = {
     "vpm_tree2d_list": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp]),
     "vpm_measure_fma_peaks": (C.c_int, [_vp, _dp, _dp]),
     "vpm_stage_history": (C.c_int, [_vp, C.c_int32, C.c_int32, _vp, C.POINTER(C.c_int32)]),
+    "vpm_fmm3d_velocity": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int64, C.POINTER(Params),
+                                     _vp, _vp, _vp, C.POINTER(Stats)]),
+    "vpm_fmm3d_velocity_device": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int64, C.POINTER(Params),
+                                            _vp, _vp, _vp]),
+    "vpm_velocity3d": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int64, C.POINTER(Params),
+                                 C.c_double, C.c_double, C.c_double, _vp, _vp, _vp, C.POINTER(Stats)]),
+    "vpm_tree3d_build": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int64, C.POINTER(Params), C.POINTER(Stats)]),
+    "vpm_tree3d_counts": (C.c_int, [_vp, _i64p, _i64p, _i32p]),
+    "vpm_tree3d_cells": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "vpm_fmm2d_field_device_static": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int64, C.POINTER(Params), _vp, _vp, _vp,
                                                 C.c_char_p, C.c_size_t]),
 }

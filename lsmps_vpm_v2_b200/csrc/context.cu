@@ -37,6 +37,7 @@ Ctx::~Ctx() {
     if (device >= 0) cudaSetDevice(device);
     drop_graph();
     if (arena2d) cudaFree(arena2d);
+    if (arena3d) cudaFree(arena3d);
     if (d_err) cudaFree(d_err);
     for (auto& e : ev)
         if (e) cudaEventDestroy(e);

@@ -6,12 +6,17 @@
 #include <vector>
 
 #include "fmm2d.cuh"
+#include "fmm3d.cuh"
 
 namespace vpm {
 
 // Stage marks of one evaluation: 0 start, 1 keys+sort, 2 tree levels,
 // 3 lists, 4 P2M+M2M, 5 M2L, 6 L2L, 7 M2P+L2P, 8 P2P (end).
 constexpr int kStageEvents = 9;
+
+struct Caps3D {
+    int n = 0, cells = 0;
+};
 
 struct Caps2D {
     int n = 0, cells = 0, P = 0;
@@ -78,6 +83,20 @@ struct Ctx {
     bool last_was_graph = false;
     int graph_launches = 0;
 
+    // 3D arena
+    void* arena3d = nullptr;
+    Caps3D cap3;
+    double* in3[7] = {};          // x, y, z, alpha_x, alpha_y, alpha_z (or vorticity), s
+    uint8_t* in3_act = nullptr;
+    double* out3[3] = {};
+    Tree3D tree3{};
+    Scratch3D s3{};
+    double* bbox3 = nullptr;
+    bool have_tree3 = false;
+    int last_n3 = 0;
+    float last_ms3 = 0.f;
+    int last_launches3 = 0;
+
     // last evaluation
     bool have_tree = false;
     int last_n = 0;
@@ -105,6 +124,14 @@ struct Ctx {
     int fetch_tree(HostTree2D& h);
     int launch2d(const double* x, const double* y, const double* q, const uint8_t* act, int n,
                  const vpm_fmm_params& p, int K, double* o0, double* o1, int velocity, double uinf, double vinf);
+    int reserve3d(int n, int cap_cells);
+    int enqueue3d(const double* x, const double* y, const double* z, const double* ax, const double* ay,
+                  const double* az, const uint8_t* act, int n, const vpm_fmm_params& p, double* u, double* v,
+                  double* w, double uinf, double vinf, double winf, bool tree_only);
+    int run3d_host(const double* x, const double* y, const double* z, const double* a0, const double* a1,
+                   const double* a2, const double* s, const uint8_t* act, int64_t n, const vpm_fmm_params* prm,
+                   double* u, double* v, double* w, double uinf, double vinf, double winf, vpm_fmm_stats* stats,
+                   bool tree_only);
     void drop_graph();
     void begin_ring();
     void end_ring();

@@ -106,46 +106,68 @@ p2m2d(Tree2D t, double2* __restrict__ a, int P, unsigned* err) {
     }
 }
 
-// M2M into the active non-leaf cells of level L (fmm2D.cpp:309-379), one warp
-// per cell, lane p computing a_p by Horner's rule in t = z_child - z_parent:
+// M2M into the active non-leaf cells of level L (fmm2D.cpp:309-379). A warp
+// holds G = 32/(P+1) cells, lane (g, p) computing a_p of cell g by Horner's
+// rule in t = z_child - z_parent for all children at once (independent
+// chains), then summing the children in order:
 //   a_p += a0 t^p + sum_{k=1..p} m2m[p][k] a_k t^(p-k).
-//
 // Child expansions are read through L2 (ld.cg): in the cooperative kernel the
 // level below was written by other blocks of the same launch.
 __device__ __forceinline__ void m2m_level_body(const Tree2D& t, double2* __restrict__ a,
                                                const double* __restrict__ coef, int P, int L) {
-    __shared__ double2 s_child[4][W];
+    __shared__ double2 s_child[4][4][32];  // [warp][child][g * (P+1) + k]
+    __shared__ double2 s_tt[4][4][16];     // [warp][child][g]
     const double* g_m2m = coef + kCoefM2M;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int Q = P + 1, G = 32 / Q, g = lane / Q, k = lane - g * Q;
     const int c0 = t.info->level_start[L], c1 = t.info->level_start[L + 1];
     const int warps = gridDim.x * (blockDim.x >> 5);
-    for (int c = c0 + blockIdx.x * (blockDim.x >> 5) + wib; c < c1; c += warps) {
-        const uint8_t f = t.c_flags[c];
-        if ((f & CELL_LEAF) || !(f & CELL_ACTIVE)) continue;
-        const double px = t.c_cx[c], py = t.c_cy[c];
-        const unsigned m = t.c_chmask[c];
-        const int ch0 = t.c_child0[c];
-        if (ch0 < 0) continue;
-        double2 acc = make_double2(0.0, 0.0);
-        for (int r = 0; r < __popc(m); ++r) {
-            const int ch = ch0 + r;
-            if (lane <= P) s_child[wib][lane] = __ldcg(&a[(size_t)ch * (P + 1) + lane]);
-            __syncwarp();
-            const double2 tt = make_double2(t.c_cx[ch] - px, t.c_cy[ch] - py);
-            if (lane == 0) {
-                acc = cadd(acc, s_child[wib][0]);
-            } else if (lane <= P) {
-                const int p = lane;
-                double2 S = s_child[wib][0];
-                for (int j = p - 1; j >= 0; --j) {
-                    const int k = p - j;
-                    S = cfma(S, tt, cscale(s_child[wib][k], g_m2m[p * W + k]));
-                }
-                acc = cadd(acc, S);
-            }
-            __syncwarp();
+    const int gw = blockIdx.x * (blockDim.x >> 5) + wib;
+    for (int cb = c0 + gw * G; cb < c1; cb += warps * G) {
+        const int c = cb + g;
+        bool ok = g < G && c < c1;
+        if (ok) {
+            const uint8_t f = t.c_flags[c];
+            ok = !(f & CELL_LEAF) && (f & CELL_ACTIVE);
         }
-        if (lane <= P) a[(size_t)c * (P + 1) + lane] = acc;
+        unsigned m = 0;
+        int ch0 = -1;
+        if (ok) {
+            m = t.c_chmask[c];
+            ch0 = t.c_child0[c];
+            ok = ch0 >= 0;
+        }
+        const int nch = ok ? __popc(m) : 0;
+        #pragma unroll
+        for (int r = 0; r < 4; ++r)
+            if (r < nch) s_child[wib][r][lane] = __ldcg(&a[(size_t)(ch0 + r) * Q + k]);
+        if (k < nch) s_tt[wib][k][g] = make_double2(t.c_cx[ch0 + k] - t.c_cx[c], t.c_cy[ch0 + k] - t.c_cy[c]);
+        __syncwarp();
+        if (ok) {
+            double2 acc = make_double2(0.0, 0.0);
+            if (k == 0) {
+                for (int r = 0; r < nch; ++r) acc = cadd(acc, s_child[wib][r][g * Q]);
+            } else {
+                double2 S[4], tt[4];
+                #pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    S[r] = s_child[wib][r][g * Q];
+                    tt[r] = s_tt[wib][r][g];
+                }
+                for (int j = k - 1; j >= 0; --j) {
+                    const int kk = k - j;
+                    const double cf = g_m2m[k * W + kk];
+                    #pragma unroll
+                    for (int r = 0; r < 4; ++r)
+                        if (r < nch) S[r] = cfma(S[r], tt[r], cscale(s_child[wib][r][g * Q + kk], cf));
+                }
+                #pragma unroll
+                for (int r = 0; r < 4; ++r)
+                    if (r < nch) acc = cadd(acc, S[r]);
+            }
+            a[(size_t)c * Q + k] = acc;
+        }
+        __syncwarp();
     }
 }
 
@@ -170,26 +192,32 @@ m2m_levels_coop(Tree2D t, double2* __restrict__ a, const double* __restrict__ co
 // L2L pull into every cell of level L >= 3 from its parent (fmm2D.cpp:587-651,
 // where each non-leaf parent at levels 2..max-1 pushes into its children):
 //   b_p(c) += sum_{k=p..P} l2l[p][k] b_k(parent) t^(k-p),  t = z_c - z_parent.
-// The parent's expansion is final because level L-1 ran in the previous launch.
-// Parent expansions are read through L2 (ld.cg) for the cooperative kernel.
+// A warp holds G = 32/(P+1) cells, lane (g, p) computing b_p of cell g. The
+// parent's expansion is final because level L-1 is complete (previous launch,
+// or before the grid barrier in the cooperative kernel); it is read through
+// L2 (ld.cg).
 __device__ __forceinline__ void l2l_level_body(const Tree2D& t, double2* __restrict__ b,
                                                const double* __restrict__ coef, int P, int L) {
-    __shared__ double2 s_par[4][W];
+    __shared__ double2 s_par[4][32];
     const double* g_l2l = coef + kCoefL2L;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int Q = P + 1, G = 32 / Q, g = lane / Q, k = lane - g * Q;
     const int c0 = t.info->level_start[L], c1 = t.info->level_start[L + 1];
     const int warps = gridDim.x * (blockDim.x >> 5);
-    for (int c = c0 + blockIdx.x * (blockDim.x >> 5) + wib; c < c1; c += warps) {
-        const int par = t.c_parent[c];
-        if (lane <= P) s_par[wib][lane] = __ldcg(&b[(size_t)par * (P + 1) + lane]);
+    const int gw = blockIdx.x * (blockDim.x >> 5) + wib;
+    for (int cb = c0 + gw * G; cb < c1; cb += warps * G) {
+        const int c = cb + g;
+        const bool ok = g < G && c < c1;
+        const int par = ok ? t.c_parent[c] : 0;
+        if (ok) s_par[wib][lane] = __ldcg(&b[(size_t)par * Q + k]);
         __syncwarp();
-        if (lane <= P) {
+        if (ok) {
             const double2 tt = make_double2(t.c_cx[c] - t.c_cx[par], t.c_cy[c] - t.c_cy[par]);
-            const int pp = lane;
-            const double* cf = g_l2l + pp * W;
-            double2 S = cscale(s_par[wib][P], cf[P]);
-            for (int kk = P - 1; kk >= pp; --kk) S = cfma(S, tt, cscale(s_par[wib][kk], cf[kk]));
-            double2* bc = &b[(size_t)c * (P + 1) + pp];
+            const double* cf = g_l2l + k * W;
+            const double2* sp = &s_par[wib][g * Q];
+            double2 S = cscale(sp[P], cf[P]);
+            for (int kk = P - 1; kk >= k; --kk) S = cfma(S, tt, cscale(sp[kk], cf[kk]));
+            double2* bc = &b[(size_t)c * Q + k];
             *bc = cadd(__ldcg(bc), S);
         }
         __syncwarp();

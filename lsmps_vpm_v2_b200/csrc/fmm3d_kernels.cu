@@ -1,0 +1,280 @@
+// 3D treecode evaluation (fastFMM3Dutils::evaluateFMM, src/FMM/fast3DFMM.cpp:318-472):
+// every particle is a target; from the root's children down, each active
+// child k of a cell on the target's list is
+//   far   if R^2 > (2 size_k)^2   -> M2P with the derivative multipliers of
+//                                    fmm3D::M2P_mul_calc (fmm3D.cpp:147-200)
+//   else a non-leaf               -> onto the target's list for the next level
+//   else a leaf                   -> P2P  u += (alpha_j x r) / |r|^3, j != i,
+//                                    active j only (fast3DFMM.cpp:440-460)
+// (level-1 cells themselves are never evaluated, as in the reference).
+//
+// One warp per leaf, one lane per target particle of the leaf. The warp
+// walks the union of its targets' lists level by level, each entry carrying
+// the mask of the lanes whose own list holds it; every lane therefore makes
+// exactly its own reference decisions, in its own order. The far/near test
+// uses separately rounded IEEE operations (no contraction) so it decides as
+// the reference does.
+#include "fmm3d.cuh"
+
+#include <algorithm>
+
+namespace vpm {
+
+namespace {
+
+struct Src3 {
+    const double *px, *py, *pz, *ax, *ay, *az;
+    const uint8_t* act;
+};
+
+// M2P of one far cell, FP64: multipliers g of r / |r|^3 and its first two
+// derivatives paired with the ten moments of each source component, then
+// u += M_y g_z - M_z g_y etc. (fast3DFMM.cpp:395-425).
+__device__ __forceinline__ void m2p64(const double* __restrict__ M, double R2, double dx, double dy, double dz,
+                                      double& vx, double& vy, double& vz) {
+    const double R = sqrt(R2);
+    const double i2 = 1.0 / R2;
+    const double i3 = 1.0 / (R * R2);
+    const double i5 = i3 * i2, i7 = i5 * i2;
+    double gx[10], gy[10], gz[10];
+    gx[0] = dx * i3;
+    gx[1] = -(3 * dx * dx * i5) + i3;
+    gx[2] = -(3 * dx * dy * i5);
+    gx[3] = -(3 * dx * dz * i5);
+    gx[4] = (15 * dx * dx * dx * i7) - (9 * dx * i5);
+    gx[5] = (15 * dx * dy * dy * i7) - (3 * dx * i5);
+    gx[6] = (15 * dx * dz * dz * i7) - (3 * dx * i5);
+    gx[7] = (15 * dx * dx * dy * i7) - (3 * dy * i5);
+    gx[8] = (15 * dx * dy * dz * i7);
+    gx[9] = (15 * dx * dx * dz * i7) - (3 * dz * i5);
+    gy[0] = dy * i3;
+    gy[1] = -(3 * dy * dx * i5);
+    gy[2] = -(3 * dy * dy * i5) + i3;
+    gy[3] = -(3 * dy * dz * i5);
+    gy[4] = (15 * dy * dx * dx * i7) - (3 * dy * i5);
+    gy[5] = (15 * dy * dy * dy * i7) - (9 * dy * i5);
+    gy[6] = (15 * dy * dz * dz * i7) - (3 * dy * i5);
+    gy[7] = (15 * dy * dx * dy * i7) - (3 * dx * i5);
+    gy[8] = (15 * dy * dy * dz * i7) - (3 * dz * i5);
+    gy[9] = (15 * dy * dx * dz * i7);
+    gz[0] = dz * i3;
+    gz[1] = -(3 * dz * dx * i5);
+    gz[2] = -(3 * dz * dy * i5);
+    gz[3] = -(3 * dz * dz * i5) + i3;
+    gz[4] = (15 * dz * dx * dx * i7) - (3 * dz * i5);
+    gz[5] = (15 * dz * dy * dy * i7) - (3 * dz * i5);
+    gz[6] = (15 * dz * dz * dz * i7) - (9 * dz * i5);
+    gz[7] = (15 * dz * dx * dy * i7);
+    gz[8] = (15 * dz * dy * dz * i7) - (3 * dy * i5);
+    gz[9] = (15 * dz * dx * dz * i7) - (3 * dx * i5);
+    const double* Mx = M;
+    const double* My = M + 10;
+    const double* Mz = M + 20;
+    #pragma unroll
+    for (int m = 0; m < 10; ++m) {
+        const double mx = Mx[m], my = My[m], mz = Mz[m];
+        vx += my * gz[m] - mz * gy[m];
+        vy += mz * gx[m] - mx * gz[m];
+        vz += mx * gy[m] - my * gx[m];
+    }
+}
+
+// The same in FP32 (mixed form): offsets rounded to float after the FP64
+// subtraction, the cell's sum formed in FP32 and added to the FP64 total.
+__device__ __forceinline__ void m2p32(const double* __restrict__ M, double dxd, double dyd, double dzd,
+                                      double& vx, double& vy, double& vz) {
+    const float dx = (float)dxd, dy = (float)dyd, dz = (float)dzd;
+    const float R2 = dx * dx + dy * dy + dz * dz;
+    const float iR = rsqrtf(R2);
+    const float i2 = iR * iR;
+    const float i3 = i2 * iR;
+    const float i5 = i3 * i2, i7 = i5 * i2;
+    const float a5x = 3.f * i5 * dx, a5y = 3.f * i5 * dy, a5z = 3.f * i5 * dz;
+    const float b7 = 15.f * i7;
+    float gx[10], gy[10], gz[10];
+    gx[0] = dx * i3;
+    gx[1] = -(a5x * dx) + i3;
+    gx[2] = -(a5x * dy);
+    gx[3] = -(a5x * dz);
+    gx[4] = (b7 * dx * dx * dx) - 3.f * a5x;
+    gx[5] = (b7 * dx * dy * dy) - a5x;
+    gx[6] = (b7 * dx * dz * dz) - a5x;
+    gx[7] = (b7 * dx * dx * dy) - a5y;
+    gx[8] = (b7 * dx * dy * dz);
+    gx[9] = (b7 * dx * dx * dz) - a5z;
+    gy[0] = dy * i3;
+    gy[1] = -(a5y * dx);
+    gy[2] = -(a5y * dy) + i3;
+    gy[3] = -(a5y * dz);
+    gy[4] = (b7 * dy * dx * dx) - a5y;
+    gy[5] = (b7 * dy * dy * dy) - 3.f * a5y;
+    gy[6] = (b7 * dy * dz * dz) - a5y;
+    gy[7] = (b7 * dy * dx * dy) - a5x;
+    gy[8] = (b7 * dy * dy * dz) - a5z;
+    gy[9] = (b7 * dy * dx * dz);
+    gz[0] = dz * i3;
+    gz[1] = -(a5z * dx);
+    gz[2] = -(a5z * dy);
+    gz[3] = -(a5z * dz) + i3;
+    gz[4] = (b7 * dz * dx * dx) - a5z;
+    gz[5] = (b7 * dz * dy * dy) - a5z;
+    gz[6] = (b7 * dz * dz * dz) - 3.f * a5z;
+    gz[7] = (b7 * dz * dx * dy);
+    gz[8] = (b7 * dz * dy * dz) - a5y;
+    gz[9] = (b7 * dz * dx * dz) - a5x;
+    float sx = 0.f, sy = 0.f, sz = 0.f;
+    #pragma unroll
+    for (int m = 0; m < 10; ++m) {
+        const float mx = (float)M[m], my = (float)M[10 + m], mz = (float)M[20 + m];
+        sx += my * gz[m] - mz * gy[m];
+        sy += mz * gx[m] - mx * gz[m];
+        sz += mx * gy[m] - my * gx[m];
+    }
+    vx += sx;
+    vy += sy;
+    vz += sz;
+}
+
+// P2P of one near leaf [lo, hi) onto target slot `self` at (xp, yp, zp).
+template <bool F32>
+__device__ __forceinline__ void p2p3(const Src3& s, int lo, int hi, int self, double xp, double yp, double zp,
+                                     double& vx, double& vy, double& vz) {
+    if (F32) {
+        float sx = 0.f, sy = 0.f, sz = 0.f;
+        for (int j = lo; j < hi; ++j) {
+            if (!s.act[j] || j == self) continue;
+            const float ex = (float)(xp - s.px[j]), ey = (float)(yp - s.py[j]), ez = (float)(zp - s.pz[j]);
+            const float r2 = ex * ex + ey * ey + ez * ez;
+            const float ir = rsqrtf(r2);
+            const float ir3 = ir * ir * ir;
+            const float ax = (float)s.ax[j], ay = (float)s.ay[j], az = (float)s.az[j];
+            sx += (ay * ez - az * ey) * ir3;
+            sy += (az * ex - ax * ez) * ir3;
+            sz += (ax * ey - ay * ex) * ir3;
+        }
+        vx += sx;
+        vy += sy;
+        vz += sz;
+    } else {
+        for (int j = lo; j < hi; ++j) {
+            if (!s.act[j] || j == self) continue;
+            const double ex = xp - s.px[j], ey = yp - s.py[j], ez = zp - s.pz[j];
+            const double r2 = ex * ex + ey * ey + ez * ez;
+            const double ir3 = 1.0 / (sqrt(r2) * r2);
+            vx += (s.ay[j] * ez - s.az[j] * ey) * ir3;
+            vy += (s.az[j] * ex - s.ax[j] * ez) * ir3;
+            vz += (s.ax[j] * ey - s.ay[j] * ex) * ir3;
+        }
+    }
+}
+
+template <bool F32>
+__global__ void __launch_bounds__(32 * kEval3DWarps)
+eval3d_kernel(Tree3D t, double* __restrict__ u, double* __restrict__ v, double* __restrict__ w, double uinf,
+              double vinf, double winf, unsigned* ticket, unsigned* err) {
+    __shared__ int s_cell[kEval3DWarps][2][kWork3DCap];
+    __shared__ unsigned s_mask[kEval3DWarps][2][kWork3DCap];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    int stop = 0;
+    if (lane == 0) stop = fatal(err);
+    if (__shfl_sync(0xffffffffu, stop, 0)) return;  // warp-uniform
+    const int nc = t.info->n_cells, depth = t.info->depth;
+    const Src3 src{t.px, t.py, t.pz, t.ax, t.ay, t.az, t.pact};
+    const unsigned rm = t.c_chmask[0];
+    const int r0 = t.c_child0[0];
+    for (;;) {
+        int c = 0;
+        if (lane == 0) c = (int)atomicAdd(ticket, 1u);
+        c = __shfl_sync(0xffffffffu, c, 0);
+        if (c >= nc) break;
+        if (t.c_chmask[c] != 0) continue;  // leaves only
+        const int lo = t.c_lo[c], hi = t.c_hi[c];
+        for (int tb = lo; tb < hi; tb += 32) {
+            const int slot = tb + lane;
+            const bool has = slot < hi;
+            const double xp = has ? t.px[slot] : 0.0, yp = has ? t.py[slot] : 0.0, zp = has ? t.pz[slot] : 0.0;
+            const unsigned full = __ballot_sync(0xffffffffu, has);
+            double vx = 0.0, vy = 0.0, vz = 0.0;
+            int which = 0;
+            int ncur = __popc(rm);
+            if (lane < ncur) {
+                s_cell[wib][0][lane] = r0 + lane;
+                s_mask[wib][0][lane] = full;
+            }
+            __syncwarp();
+            for (int lv = 1; lv < depth && ncur > 0; ++lv) {
+                const int* cur_c = s_cell[wib][which];
+                const unsigned* cur_m = s_mask[wib][which];
+                int* nxt_c = s_cell[wib][which ^ 1];
+                unsigned* nxt_m = s_mask[wib][which ^ 1];
+                int nn = 0;
+                for (int e = 0; e < ncur; ++e) {
+                    const int cc = cur_c[e];
+                    const bool mine = (cur_m[e] >> lane) & 1u;
+                    const unsigned cm = t.c_chmask[cc];
+                    const int k0 = t.c_child0[cc];
+                    int r = 0;
+                    for (int o = 0; o < 8; ++o) {
+                        if (!((cm >> o) & 1u)) continue;
+                        const int k = k0 + r++;
+                        if (!t.c_active[k]) continue;
+                        bool far = false;
+                        double dx = 0.0, dy = 0.0, dz = 0.0, R2 = 0.0;
+                        if (mine) {
+                            dx = xsub(xp, t.c_x[k]);
+                            dy = xsub(yp, t.c_y[k]);
+                            dz = xsub(zp, t.c_z[k]);
+                            R2 = xadd(xadd(xmul(dx, dx), xmul(dy, dy)), xmul(dz, dz));
+                            const double Rc = xmul(t.c_size[k], 2.0);
+                            far = R2 > xmul(Rc, Rc);
+                            if (far) {
+                                if (F32) m2p32(&t.mom[(size_t)k * 30], dx, dy, dz, vx, vy, vz);
+                                else m2p64(&t.mom[(size_t)k * 30], R2, dx, dy, dz, vx, vy, vz);
+                            }
+                        }
+                        const unsigned near = __ballot_sync(0xffffffffu, mine && !far);
+                        if (!near) continue;
+                        if (t.c_chmask[k] != 0) {
+                            if (nn < kWork3DCap) {
+                                if (lane == 0) {
+                                    nxt_c[nn] = k;
+                                    nxt_m[nn] = near;
+                                }
+                            } else if (lane == 0) {
+                                set_err(err, ERR_QUEUE);
+                            }
+                            ++nn;
+                        } else if ((near >> lane) & 1u) {
+                            p2p3<F32>(src, t.c_lo[k], t.c_hi[k], slot, xp, yp, zp, vx, vy, vz);
+                        }
+                    }
+                }
+                __syncwarp();
+                which ^= 1;
+                ncur = min(nn, kWork3DCap);
+            }
+            if (has) {
+                const uint32_t i = t.perm[slot];
+                u[i] = vx + uinf;
+                v[i] = vy + vinf;
+                w[i] = vz + winf;
+            }
+            __syncwarp();
+        }
+    }
+}
+
+}  // namespace
+
+cudaError_t eval3d(const Tree3D& t, bool mixed, double* u, double* v, double* w, double uinf, double vinf,
+                   double winf, unsigned* err, cudaStream_t st, int* launches) {
+    unsigned* ticket = t.gbar + 4;
+    cudaError_t e = cudaMemsetAsync(ticket, 0, sizeof(unsigned), st);
+    if (e != cudaSuccess) return e;
+    if (mixed) eval3d_kernel<true><<<148 * 8, 32 * kEval3DWarps, 0, st>>>(t, u, v, w, uinf, vinf, winf, ticket, err);
+    else eval3d_kernel<false><<<148 * 8, 32 * kEval3DWarps, 0, st>>>(t, u, v, w, uinf, vinf, winf, ticket, err);
+    *launches += 1;
+    return cudaGetLastError();
+}
+
+}  // namespace vpm

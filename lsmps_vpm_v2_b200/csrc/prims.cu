@@ -76,29 +76,20 @@ scan_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, int n, 
     }
     uint64_t agg;
     uint64_t excl = block_excl_scan(sum, warp_sums, &agg);
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 32) {
         uint64_t prefix = 0;
         if (tile == 0) {
-            store_volatile(&status[0], kFlagP | agg);
+            if (threadIdx.x == 0) store_volatile(&status[0], kFlagP | agg);
         } else {
-            store_volatile(&status[tile], kFlagA | agg);
-            int k = tile - 1;
-            long long spins = 0;
-            while (k >= 0) {
-                uint64_t w = load_volatile(&status[k]);
-                if ((w & ~kValMask) == 0) {
-                    if (++spins > kSpinLimit) { set_err(err, ERR_TIMEOUT); break; }
-                    continue;
-                }
-                prefix += w & kValMask;
-                if ((w & ~kValMask) == kFlagP) break;
-                --k;
-            }
-            store_volatile(&status[tile], kFlagP | (prefix + agg));
+            if (threadIdx.x == 0) store_volatile(&status[tile], kFlagA | agg);
+            prefix = warp_lookback<kFlagP, kValMask>(status, tile, err);
+            if (threadIdx.x == 0) store_volatile(&status[tile], kFlagP | (prefix + agg));
         }
-        s_prefix = prefix;
-        int ntiles = scan_tiles(n);
-        if (total && tile == ntiles - 1) *total = (uint32_t)(prefix + agg);
+        if (threadIdx.x == 0) {
+            s_prefix = prefix;
+            int ntiles = scan_tiles(n);
+            if (total && tile == ntiles - 1) *total = (uint32_t)(prefix + agg);
+        }
     }
     __syncthreads();
     uint64_t run = s_prefix + excl;
@@ -116,13 +107,14 @@ constexpr uint32_t kRsA = 1u << 30;
 constexpr uint32_t kRsP = 2u << 30;
 constexpr uint32_t kRsMask = (1u << 30) - 1;
 
+template <typename K>
 __global__ void __launch_bounds__(256)
-rs_histogram(const uint64_t* __restrict__ keys, int n, int passes, uint32_t* hist) {
+rs_histogram(const K* __restrict__ keys, int n, int passes, uint32_t* hist) {
     __shared__ uint32_t h[8][256];
     for (int i = threadIdx.x; i < 8 * 256; i += blockDim.x) (&h[0][0])[i] = 0;
     __syncthreads();
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        uint64_t k = keys[i];
+        const K k = keys[i];
         for (int p = 0; p < passes; ++p) atomicAdd(&h[p][(k >> (8 * p)) & 255], 1u);
     }
     __syncthreads();
@@ -147,21 +139,31 @@ __global__ void rs_hist_scan(uint32_t* hist, int passes) {
 
 // One 8-bit digit pass. Items are arranged warp-striped: item j of lane l in
 // warp w is tile_base + w*256 + j*32 + l, so processing j in order ranks keys
-// in index order (stability).
+// in index order (stability). The tile is first reordered by digit in shared
+// memory, then written out so that consecutive threads store consecutive
+// addresses within each digit's run.
+template <typename K>
 __global__ void __launch_bounds__(kSortThreads)
-rs_pass(const uint64_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint64_t* __restrict__ kout,
+rs_pass(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* __restrict__ kout,
         uint32_t* __restrict__ vout, int n, int shift, const uint32_t* __restrict__ digit_offset,
         uint32_t* status, unsigned* ticket, unsigned* err) {
+    constexpr int kSortItems = SortItems<K>::value;
+    constexpr int kSortTile = kSortThreads * kSortItems;
     __shared__ uint32_t s_wh[kSortThreads / 32][256];  // per-warp digit counts, then warp prefixes
-    __shared__ uint32_t s_base[256];
+    __shared__ uint32_t s_local[256];                   // tile-local start of each digit
+    __shared__ uint32_t s_base[256];                    // global start minus tile-local start
+    __shared__ K s_key[kSortTile];
+    __shared__ uint32_t s_val[kSortTile];
+    __shared__ uint64_t s_warp_sums[kSortThreads / 32];
     __shared__ unsigned s_tile;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
     for (int i = threadIdx.x; i < (kSortThreads / 32) * 256; i += blockDim.x) (&s_wh[0][0])[i] = 0;
     __syncthreads();
     const int tile = (int)s_tile;
-    const long long tbase = (long long)tile * kSortTile + warp * (32 * kSortItems);
-    uint64_t key[kSortItems];
+    const long long tile0 = (long long)tile * kSortTile;
+    const long long tbase = tile0 + warp * (32 * kSortItems);
+    K key[kSortItems];
     uint32_t val[kSortItems];
     uint32_t rank[kSortItems];
     int dig[kSortItems];
@@ -170,9 +172,13 @@ rs_pass(const uint64_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint
     for (int j = 0; j < kSortItems; ++j) {
         long long i = tbase + j * 32 + lane;
         bool ok = i < n;
-        key[j] = ok ? kin[i] : 0ull;
+        key[j] = ok ? kin[i] : (K)0;
         val[j] = ok ? vin[i] : 0u;
         dig[j] = ok ? (int)((key[j] >> shift) & 255) : 256;
+    }
+    #pragma unroll
+    for (int j = 0; j < kSortItems; ++j) {
+        const bool ok = dig[j] < 256;
         unsigned m = __match_any_sync(0xffffffffu, dig[j]);
         uint32_t prior = 0;
         if (ok) prior = s_wh[warp][dig[j]];
@@ -191,41 +197,95 @@ rs_pass(const uint64_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint
         s_wh[w][d] = run;
         run += c;
     }
+    uint64_t agg;
+    const uint32_t local = (uint32_t)block_excl_scan(run, s_warp_sums, &agg);
+    s_local[d] = local;
     uint32_t* st = status + (size_t)tile * 256;
+    uint32_t prefix = 0;
     if (tile == 0) {
         store_volatile32(&st[d], kRsP | run);
-        s_base[d] = digit_offset[d];
     } else {
         store_volatile32(&st[d], kRsA | run);
-        uint32_t prefix = 0;
+        // Look-back for digit d, reading 16 predecessors per round (independent
+        // loads) and consuming them in order up to the first one not yet
+        // published or the first inclusive prefix.
         int k = tile - 1;
         long long spins = 0;
-        while (k >= 0) {
-            uint32_t w = load_volatile32(&status[(size_t)k * 256 + d]);
-            if ((w & ~kRsMask) == 0) {
-                if (++spins > kSpinLimit) { set_err(err, ERR_TIMEOUT); break; }
-                continue;
+        bool done = false;
+        while (!done && k >= 0) {
+            uint32_t w[16];
+            #pragma unroll
+            for (int j = 0; j < 16; ++j) w[j] = k - j >= 0 ? load_volatile32(&status[(size_t)(k - j) * 256 + d]) : kRsP;
+            bool stalled = false;
+            #pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                if (done || stalled) continue;
+                const uint32_t f = w[j] & ~kRsMask;
+                if (f == 0) { stalled = true; continue; }
+                prefix += w[j] & kRsMask;
+                --k;
+                if (f == kRsP) done = true;
             }
-            prefix += w & kRsMask;
-            if ((w & ~kRsMask) == kRsP) break;
-            --k;
+            if (stalled && ++spins > kSpinLimit) { set_err(err, ERR_TIMEOUT); break; }
         }
         store_volatile32(&st[d], kRsP | (prefix + run));
-        s_base[d] = digit_offset[d] + prefix;
     }
+    s_base[d] = digit_offset[d] + prefix - local;  // modulo 2^32; adding a tile-local index gives the output index
     __syncthreads();
     #pragma unroll
     for (int j = 0; j < kSortItems; ++j) {
         if (dig[j] < 256) {
-            uint32_t pos = s_base[dig[j]] + s_wh[warp][dig[j]] + rank[j];
-            if (pos < (uint32_t)n) {
-                kout[pos] = key[j];
-                vout[pos] = val[j];
-            } else {
-                set_err(err, ERR_INDEX);
-            }
+            const uint32_t lp = s_local[dig[j]] + s_wh[warp][dig[j]] + rank[j];
+            s_key[lp] = key[j];
+            s_val[lp] = val[j];
         }
     }
+    __syncthreads();
+    const int cnt = (int)min((long long)kSortTile, (long long)n - tile0);
+    for (int i = threadIdx.x; i < cnt; i += kSortThreads) {
+        const K k = s_key[i];
+        const uint32_t pos = s_base[(int)((k >> shift) & 255)] + (uint32_t)i;
+        if (pos < (uint32_t)n) {
+            kout[pos] = k;
+            vout[pos] = s_val[i];
+        } else {
+            set_err(err, ERR_INDEX);
+        }
+    }
+}
+
+template <typename K>
+cudaError_t sort_pairs(K** keys, uint32_t** vals, K* keys_alt, uint32_t* vals_alt, int n, int bits,
+                       const SortScratch& s, unsigned* err, cudaStream_t st, int* launches) {
+    int passes = (bits + 7) / 8;
+    if (passes < 1 || passes > (int)sizeof(K)) return cudaErrorInvalidValue;
+    const int tiles = ceil_div(n > 0 ? n : 1, kSortThreads * SortItems<K>::value);
+    if (tiles > s.max_tiles) return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemsetAsync(s.status, 0, sizeof(uint32_t) * (size_t)passes * tiles * 256, st);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(s.tickets, 0, sizeof(unsigned) * 8, st);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(s.hist, 0, sizeof(uint32_t) * 8 * 256, st);
+    if (e != cudaSuccess) return e;
+    int hblocks = std::min(1184, ceil_div(n, 256 * 8));
+    if (hblocks < 1) hblocks = 1;
+    rs_histogram<K><<<hblocks, 256, 0, st>>>(*keys, n, passes, s.hist);
+    rs_hist_scan<<<1, 256, 0, st>>>(s.hist, passes);
+    if (launches) *launches += 2;
+    K* ka = *keys;
+    uint32_t* va = *vals;
+    K* kb = keys_alt;
+    uint32_t* vb = vals_alt;
+    for (int p = 0; p < passes; ++p) {
+        rs_pass<K><<<tiles, kSortThreads, 0, st>>>(ka, va, kb, vb, n, 8 * p, s.hist + 256 * p,
+                                                   s.status + (size_t)p * tiles * 256, s.tickets + p, err);
+        if (launches) *launches += 1;
+        std::swap(ka, kb);
+        std::swap(va, vb);
+    }
+    *keys = ka;
+    *vals = va;
+    return cudaGetLastError();
 }
 
 }  // namespace
@@ -245,35 +305,13 @@ cudaError_t scan_exclusive(const uint32_t* in, uint32_t* out, int n, uint32_t* t
 cudaError_t radix_sort_pairs(uint64_t** keys, uint32_t** vals, uint64_t* keys_alt, uint32_t* vals_alt,
                              int n, int bits, const SortScratch& s, unsigned* err, cudaStream_t st,
                              int* launches) {
-    int passes = (bits + 7) / 8;
-    if (passes < 1 || passes > 8) return cudaErrorInvalidValue;
-    int tiles = sort_tiles(n);
-    if (tiles > s.max_tiles) return cudaErrorInvalidValue;
-    cudaError_t e = cudaMemsetAsync(s.status, 0, sizeof(uint32_t) * (size_t)passes * tiles * 256, st);
-    if (e != cudaSuccess) return e;
-    e = cudaMemsetAsync(s.tickets, 0, sizeof(unsigned) * 8, st);
-    if (e != cudaSuccess) return e;
-    e = cudaMemsetAsync(s.hist, 0, sizeof(uint32_t) * 8 * 256, st);
-    if (e != cudaSuccess) return e;
-    int hblocks = std::min(1184, ceil_div(n, 256 * 8));
-    if (hblocks < 1) hblocks = 1;
-    rs_histogram<<<hblocks, 256, 0, st>>>(*keys, n, passes, s.hist);
-    rs_hist_scan<<<1, 256, 0, st>>>(s.hist, passes);
-    if (launches) *launches += 2;
-    uint64_t* ka = *keys;
-    uint32_t* va = *vals;
-    uint64_t* kb = keys_alt;
-    uint32_t* vb = vals_alt;
-    for (int p = 0; p < passes; ++p) {
-        rs_pass<<<tiles, kSortThreads, 0, st>>>(ka, va, kb, vb, n, 8 * p, s.hist + 256 * p,
-                                                s.status + (size_t)p * tiles * 256, s.tickets + p, err);
-        if (launches) *launches += 1;
-        std::swap(ka, kb);
-        std::swap(va, vb);
-    }
-    *keys = ka;
-    *vals = va;
-    return cudaGetLastError();
+    return sort_pairs<uint64_t>(keys, vals, keys_alt, vals_alt, n, bits, s, err, st, launches);
+}
+
+cudaError_t radix_sort_pairs(uint32_t** keys, uint32_t** vals, uint32_t* keys_alt, uint32_t* vals_alt,
+                             int n, int bits, const SortScratch& s, unsigned* err, cudaStream_t st,
+                             int* launches) {
+    return sort_pairs<uint32_t>(keys, vals, keys_alt, vals_alt, n, bits, s, err, st, launches);
 }
 
 }  // namespace vpm

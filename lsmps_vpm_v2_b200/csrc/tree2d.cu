@@ -110,8 +110,10 @@ bbox2d(const double* __restrict__ x, const double* __restrict__ y, int n, double
 }
 
 // Morton key of each particle at the key level (treeCell.cpp:290-303).
+// Key type KT: 32-bit when 2 * key_levels <= 32 (halves the sort's traffic).
+template <typename KT>
 __global__ void keys2d(const double* __restrict__ x, const double* __restrict__ y, int n, const Geom2D* g,
-                       int key_levels, uint64_t* key, uint32_t* idx, unsigned* err) {
+                       int key_levels, KT* key, uint32_t* idx, unsigned* err) {
     const double pivx = g->pivx, pivy = g->pivy, s = g->size_k;
     const double lim = ldexp(1.0, key_levels);
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
@@ -124,17 +126,23 @@ __global__ void keys2d(const double* __restrict__ x, const double* __restrict__ 
         } else {
             set_err(err, ERR_RANGE);
         }
-        key[i] = morton2(ix, iy);
+        key[i] = (KT)morton2(ix, iy);
         idx[i] = (uint32_t)i;
     }
 }
 
-// Sorted copies of the particle data and the active flags as 0/1 words.
+// Sorted copies of the particle data and the active flags as 0/1 words; the
+// sorted keys (from whichever buffer the sort ended in, 32- or 64-bit) and
+// permutation land in the tree's own arrays.
+template <typename KT>
 __global__ void gather2d(const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ q,
-                         const uint8_t* __restrict__ act, const uint32_t* __restrict__ perm, int n, double* px,
+                         const uint8_t* __restrict__ act, const KT* __restrict__ skey,
+                         const uint32_t* __restrict__ sperm, int n, uint64_t* key, uint32_t* perm, double* px,
                          double* py, double* pq, uint8_t* pact, uint32_t* act_u32, unsigned* err) {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        uint32_t j = perm[i];
+        const uint32_t j = sperm[i];
+        if ((const void*)skey != (const void*)key) key[i] = (uint64_t)skey[i];
+        if (sperm != perm) perm[i] = j;
         if (j >= (uint32_t)n) {
             set_err(err, ERR_INDEX);
             continue;
@@ -324,26 +332,15 @@ __device__ void level_step(const Tree2D& t, int L, int max_src, int max_par, int
             if (lane < kLvlWarps) { s_xc[lane] = ic - c; s_xl[lane] = il - lf; }
             const uint64_t agg = (uint64_t)__shfl_sync(0xffffffffu, ic, 31) |
                                  ((uint64_t)__shfl_sync(0xffffffffu, il, 31) << 31);
+            uint64_t prefix = 0;
+            if (tile == 0) {
+                if (lane == 0) st_relaxed(&status[0], kLvP | agg);
+            } else {
+                if (lane == 0) st_relaxed(&status[tile], kLvA | agg);
+                prefix = warp_lookback<kLvP, kLvMask>(status, tile, err);
+                if (lane == 0) st_relaxed(&status[tile], kLvP | (prefix + agg));
+            }
             if (lane == 0) {
-                uint64_t prefix = 0;
-                if (tile == 0) {
-                    st_relaxed(&status[0], kLvP | agg);
-                } else {
-                    st_relaxed(&status[tile], kLvA | agg);
-                    int k = tile - 1;
-                    long long spins = 0;
-                    while (k >= 0) {
-                        uint64_t w = ld_relaxed(&status[k]);
-                        if ((w & ~kLvMask) == 0) {
-                            if (++spins > kSpinLimit) { set_err(err, ERR_TIMEOUT); break; }
-                            continue;
-                        }
-                        prefix += w & kLvMask;
-                        if ((w & ~kLvMask) == kLvP) break;
-                        --k;
-                    }
-                    st_relaxed(&status[tile], kLvP | (prefix + agg));
-                }
                 s_prefix = prefix;
                 if (tile == ntiles - 1) {
                     const uint64_t tot = prefix + agg;
@@ -450,19 +447,24 @@ cudaError_t keys_sort2d(const double* x, const double* y, const double* q, const
     cudaError_t e = cudaMemsetAsync(s.lvl_ticket, 0, sizeof(unsigned) * kTicketWords, st);
     if (e != cudaSuccess) return e;
     bbox2d<<<bb_blocks, 256, 0, st>>>(x, y, n, exp_pct, K, t.geom, s.bbox_partial, done, err);
-    keys2d<<<gridN, 256, 0, st>>>(x, y, n, t.geom, K, t.key, t.perm, err);
     *launches += 2;
-    uint64_t* keys = t.key;
     uint32_t* vals = t.perm;
-    e = radix_sort_pairs(&keys, &vals, s.key_alt, s.val_alt, n, 2 * K, s.sort, err, st, launches);
-    if (e != cudaSuccess) return e;
-    if (keys != t.key) {
-        e = cudaMemcpyAsync(t.key, keys, sizeof(uint64_t) * n, cudaMemcpyDeviceToDevice, st);
+    if (2 * K <= 32) {
+        // 32-bit keys in the two halves of key_alt
+        uint32_t* k32 = reinterpret_cast<uint32_t*>(s.key_alt);
+        keys2d<uint32_t><<<gridN, 256, 0, st>>>(x, y, n, t.geom, K, k32, t.perm, err);
+        e = radix_sort_pairs(&k32, &vals, k32 + n, s.val_alt, n, 2 * K, s.sort, err, st, launches);
         if (e != cudaSuccess) return e;
-        e = cudaMemcpyAsync(t.perm, vals, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st);
+        gather2d<uint32_t><<<gridN, 256, 0, st>>>(x, y, q, act, k32, vals, n, t.key, t.perm, t.px, t.py, t.pq,
+                                                  t.pact, s.act_u32, err);
+    } else {
+        uint64_t* keys = t.key;
+        keys2d<uint64_t><<<gridN, 256, 0, st>>>(x, y, n, t.geom, K, t.key, t.perm, err);
+        e = radix_sort_pairs(&keys, &vals, s.key_alt, s.val_alt, n, 2 * K, s.sort, err, st, launches);
         if (e != cudaSuccess) return e;
+        gather2d<uint64_t><<<gridN, 256, 0, st>>>(x, y, q, act, keys, vals, n, t.key, t.perm, t.px, t.py, t.pq,
+                                                  t.pact, s.act_u32, err);
     }
-    gather2d<<<gridN, 256, 0, st>>>(x, y, q, act, t.perm, n, t.px, t.py, t.pq, t.pact, s.act_u32, err);
     *launches += 1;
     e = scan_exclusive(s.act_u32, t.actscan, n, t.actscan + n, s.scan, err, st);
     if (e != cudaSuccess) return e;

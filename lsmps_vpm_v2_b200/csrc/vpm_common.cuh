@@ -46,6 +46,55 @@ __device__ __forceinline__ bool fatal(const unsigned* err) {
 // kSpinLimit times (then ERR_TIMEOUT and continue). bar[0] must be zero at
 // launch. Every block must call it the same number of times.
 // ---------------------------------------------------------------------------
+// Device-scope relaxed accesses for look-back status words, which carry their
+// flag and value in one word.
+__device__ __forceinline__ uint64_t ld_relaxed64(const uint64_t* p) {
+    uint64_t v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed64(uint64_t* p, uint64_t v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Decoupled look-back by one warp: the sum of the values published by tiles
+// tile-1, tile-2, ... down to and including the nearest inclusive prefix.
+// Status words are FLAG_A | aggregate or FLAG_P | inclusive prefix in the
+// bits above VMASK (0: not yet published). Each round reads 32 predecessors
+// at once, so a chain of published aggregates costs one load round per 32
+// tiles. Call with the whole warp; the result is in every lane. A wait that
+// exceeds kSpinLimit rounds sets ERR_TIMEOUT and returns the partial sum.
+template <uint64_t FLAG_P, uint64_t VMASK>
+__device__ __forceinline__ uint64_t warp_lookback(const uint64_t* status, int tile, unsigned* err) {
+    const int lane = threadIdx.x & 31;
+    uint64_t prefix = 0;
+    int k = tile - 1;
+    long long spins = 0;
+    while (k >= 0) {
+        const int idx = k - lane;
+        const uint64_t w = idx >= 0 ? ld_relaxed64(&status[idx]) : FLAG_P;  // before tile 0: empty prefix
+        const uint64_t f = w & ~VMASK;
+        const unsigned notready = __ballot_sync(0xffffffffu, f == 0);
+        const unsigned incl = __ballot_sync(0xffffffffu, f == FLAG_P);
+        // lanes 0 .. first inclusive prefix (all 32 when there is none)
+        const unsigned upto = ((incl & (0u - incl)) << 1) - 1u;
+        if (notready & upto) {
+            if (++spins > kSpinLimit) {
+                if (lane == 0) set_err(err, ERR_TIMEOUT);
+                break;
+            }
+            continue;
+        }
+        uint64_t v = ((upto >> lane) & 1u) ? (w & VMASK) : 0;
+        #pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        prefix += v;
+        if (incl) break;
+        k -= 32;
+    }
+    return prefix;
+}
+
 // The error word's fatal bits, read once per block so that every thread of
 // the block takes the same branch (safe around __syncthreads).
 __device__ __forceinline__ bool block_fatal(const unsigned* err) {

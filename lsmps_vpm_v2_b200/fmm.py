@@ -113,6 +113,64 @@ class Context:
                                          C.byref(st) if stats else None))
         return (u, v, st) if stats else (u, v)
 
+    def velocity3d_alpha(self, x, y, z, ax, ay, az, active, params: Params | None = None, stats: bool = False):
+        """u = sum_j alpha_j x r / |r|^3 by the octree treecode (host arrays)."""
+        x, y, z = _f64(x), _f64(y), _f64(z)
+        ax, ay, az, a = _f64(ax), _f64(ay), _f64(az), _u8(active)
+        n = x.size
+        u, v, w = np.empty(n), np.empty(n), np.empty(n)
+        p = params or default_params()
+        st = Stats()
+        self._check(lib().vpm_fmm3d_velocity(self._h, _ptr(x), _ptr(y), _ptr(z), _ptr(ax), _ptr(ay), _ptr(az),
+                                             _ptr(a), None, n, C.byref(p), _ptr(u), _ptr(v), _ptr(w),
+                                             C.byref(st) if stats else None))
+        return (u, v, w, st) if stats else (u, v, w)
+
+    def velocity3d(self, x, y, z, wx, wy, wz, s, active, u_inf=0.0, v_inf=0.0, w_inf=0.0,
+                   params: Params | None = None, stats: bool = False):
+        """alpha = omega s^3 / (4 pi), then the treecode velocity plus the free stream."""
+        x, y, z = _f64(x), _f64(y), _f64(z)
+        wx, wy, wz, sz, a = _f64(wx), _f64(wy), _f64(wz), _f64(s), _u8(active)
+        n = x.size
+        u, v, w = np.empty(n), np.empty(n), np.empty(n)
+        p = params or default_params()
+        st = Stats()
+        self._check(lib().vpm_velocity3d(self._h, _ptr(x), _ptr(y), _ptr(z), _ptr(wx), _ptr(wy), _ptr(wz), _ptr(sz),
+                                         _ptr(a), n, C.byref(p), float(u_inf), float(v_inf), float(w_inf), _ptr(u),
+                                         _ptr(v), _ptr(w), C.byref(st) if stats else None))
+        return (u, v, w, st) if stats else (u, v, w)
+
+    def velocity3d_device(self, n, x, y, z, ax, ay, az, active, u, v, w, params: Params | None = None):
+        """Device-pointer form with an explicit particle count, asynchronous."""
+        p = params or default_params()
+        self._check(lib().vpm_fmm3d_velocity_device(self._h, x, y, z, ax, ay, az, active, int(n), C.byref(p),
+                                                    u, v, w))
+
+    def build_tree3d(self, x, y, z, active, params: Params | None = None) -> Stats:
+        x, y, z, a = _f64(x), _f64(y), _f64(z), _u8(active)
+        p = params or default_params()
+        s = Stats()
+        self._check(lib().vpm_tree3d_build(self._h, _ptr(x), _ptr(y), _ptr(z), _ptr(a), x.size, C.byref(p),
+                                           C.byref(s)))
+        return s
+
+    def dump_tree3d(self):
+        """The last octree: per cell (library order) nPar, chdFlag, parent,
+        isActive, level and geometry (xc, yc, zc, size), plus each leaf's
+        particle IDs (CSR over cells)."""
+        nc, nl, depth = C.c_int64(), C.c_int64(), C.c_int32()
+        self._check(lib().vpm_tree3d_counts(self._h, C.byref(nc), C.byref(nl), C.byref(depth)))
+        nc = nc.value
+        ints = np.zeros((nc, 6), np.int32)
+        geom = np.zeros((nc, 4))
+        offs = np.zeros(nc + 1, np.int64)
+        self._check(lib().vpm_tree3d_cells(self._h, _ptr(ints), _ptr(geom), _ptr(offs), None))
+        pids = np.zeros(max(int(offs[-1]), 1), np.int32)
+        self._check(lib().vpm_tree3d_cells(self._h, None, None, _ptr(offs), _ptr(pids)))
+        return dict(npar=ints[:, 0], chd=ints[:, 1], parent=ints[:, 2], active=ints[:, 3].astype(bool),
+                    level=ints[:, 4], depth=int(depth.value), n_leaves=int(nl.value), geom=geom, leaf_offs=offs,
+                    leaf_pids=pids[: int(offs[-1])])
+
     def fma_peaks(self):
         """(FP64, FP32) FMA throughput of the device in TFLOP/s."""
         a, b = C.c_double(), C.c_double()
@@ -236,6 +294,32 @@ class fmm2D:
         return self._ey
 
 
+class fmm3D:
+    """Mirror of fmm3D's fast path (src/FMM/fmm3D.hpp:106-138:
+    calcVelocityFast + get_Field_x/y/z) on the GPU treecode."""
+
+    def __init__(self, ctx: Context | None = None, params: Params | None = None):
+        self.ctx = ctx or default_context()
+        self.params = params or default_params()
+        self._u = self._v = self._w = None
+        self.stats: Stats | None = None
+
+    def calcVelocityFast(self, _parPos, _activeFlag, _targetFlag, _alphaX, _alphaY, _alphaZ):
+        """The target flags are accepted and ignored, as the reference ignores them."""
+        pos = np.asarray(_parPos, dtype=np.float64)
+        self._u, self._v, self._w, self.stats = self.ctx.velocity3d_alpha(
+            pos[:, 0], pos[:, 1], pos[:, 2], _alphaX, _alphaY, _alphaZ, _activeFlag, self.params, stats=True)
+
+    def get_Field_x(self):
+        return self._u
+
+    def get_Field_y(self):
+        return self._v
+
+    def get_Field_z(self):
+        return self._w
+
+
 @dataclass
 class Particle:
     """The fields of the reference's Particle (Utils.hpp:77-159) that the
@@ -246,6 +330,9 @@ class Particle:
     vorticity: np.ndarray
     isActive: np.ndarray
     z: np.ndarray | None = None
+    vortx: np.ndarray | None = None
+    vorty: np.ndarray | None = None
+    vortz: np.ndarray | None = None
     u: np.ndarray = field(default_factory=lambda: np.zeros(0))
     v: np.ndarray = field(default_factory=lambda: np.zeros(0))
     w: np.ndarray = field(default_factory=lambda: np.zeros(0))
@@ -257,16 +344,23 @@ class Particle:
 
 class VelocityCalc:
     """Mirror of VelocityCalc::get_velocity (velocity_calc.cpp:48-139) for the
-    FMM branch (VELOCITY_2D_TYPE 2): u = Ey + u_inf, v = -Ex + v_inf."""
+    FMM branches: 2D (VELOCITY_2D_TYPE 2) u = Ey + u_inf, v = -Ex + v_inf;
+    3D (VELOCITY_3D_TYPE 1, velocity_fmm_3d_fast) when the particles carry z,
+    u = treecode velocity of alpha = omega s^3 / (4 pi) plus the free stream."""
 
     def __init__(self, ctx: Context | None = None, params: Params | None = None, u_inf: float = 0.0,
-                 v_inf: float = 0.0):
+                 v_inf: float = 0.0, w_inf: float = 0.0):
         self.ctx = ctx or default_context()
         self.params = params or default_params()
-        self.u_inf, self.v_inf = u_inf, v_inf
+        self.u_inf, self.v_inf, self.w_inf = u_inf, v_inf, w_inf
         self.stats: Stats | None = None
 
     def get_velocity(self, p: Particle, step: int = 0) -> None:
+        if p.z is not None:
+            u, v, w, self.stats = self.ctx.velocity3d(p.x, p.y, p.z, p.vortx, p.vorty, p.vortz, p.s, p.isActive,
+                                                      self.u_inf, self.v_inf, self.w_inf, self.params, stats=True)
+            p.u, p.v, p.w = u, v, w
+            return
         u, v, self.stats = self.ctx.velocity2d(p.x, p.y, p.vorticity, p.s, p.isActive, self.u_inf, self.v_inf,
                                                self.params, stats=True)
         p.u, p.v = u, v
