@@ -36,7 +36,9 @@ extern "C" {
 
 /* Arithmetic of the evaluation. */
 #define VPM_PREC_FP64 0    /* plain form: FP64 everywhere                           */
-#define VPM_PREC_MIXED 1   /* chosen form: FP32 near field, split-precision M2L      */
+#define VPM_PREC_MIXED 1   /* chosen form: FP32 near field, list-2 M2L on the tensor
+                              cores as 3xTF32 products (orders 1..20; FP64 above) */
+#define VPM_PREC_MIXED_FP64_M2L 2 /* FP32 near field, FP64 M2L (for comparisons)  */
 
 /* Binomial coefficients of the translations. */
 #define VPM_BINOM_REFERENCE 0 /* as the reference's binComb computes them in 32-bit
@@ -126,6 +128,18 @@ const char* vpm_last_error(vpm_ctx* ctx);
 int vpm_fmm2d_field(vpm_ctx* ctx, const double* x, const double* y, const double* q,
                     const uint8_t* active, int64_t n, const vpm_fmm_params* prm,
                     double* ex, double* ey, vpm_fmm_stats* stats);
+
+/*
+ * 2D potential of the same sources by the same FMM:
+ *   phi(x_i) = sum_j q_j log|x_i - x_j|
+ * Replaces fmm2D::calcPotential (src/FMM/fmm2D.cpp:681-896) and
+ * fmm2D::get_Potential (fmm2D.hpp:65), as called by the pressure Poisson
+ * solver (src/pressure_poisson/pressure_poisson.cpp:216-219). FP64 in either
+ * precision setting. Host buffers; stats may be NULL.
+ */
+int vpm_fmm2d_potential(vpm_ctx* ctx, const double* x, const double* y, const double* q,
+                        const uint8_t* active, int64_t n, const vpm_fmm_params* prm, double* phi,
+                        vpm_fmm_stats* stats);
 
 /* Same with device pointers, asynchronous on the context's stream. */
 int vpm_fmm2d_field_device(vpm_ctx* ctx, const double* x, const double* y, const double* q,

@@ -21,6 +21,7 @@ VPM_ETIMEDOUT = 110
 
 PREC_FP64 = 0
 PREC_MIXED = 1
+PREC_MIXED_FP64_M2L = 2
 BINOM_REFERENCE = 0
 BINOM_EXACT = 1
 
@@ -89,6 +90,8 @@ SIGNATURES = {
     "vpm_last_error": (C.c_char_p, [_vp]),
     "vpm_fmm2d_field": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int64, C.POINTER(Params), _vp, _vp,
                                   C.POINTER(Stats)]),
+    "vpm_fmm2d_potential": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int64, C.POINTER(Params), _vp,
+                                      C.POINTER(Stats)]),
     "vpm_fmm2d_field_device": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int64, C.POINTER(Params), _vp, _vp]),
     "vpm_velocity2d": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, C.c_int64, C.POINTER(Params), C.c_double,
                                  C.c_double, _vp, _vp, C.POINTER(Stats)]),

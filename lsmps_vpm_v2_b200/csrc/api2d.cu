@@ -151,6 +151,11 @@ int Ctx::reserve2d(int n, int cap_cells, int P, long long cap_l1, long long cap_
     ex2.op = (double2*)P_(o_op);
     coef_P = -1;  // the new arena holds no coefficients yet
     mixed_base = P_(o_mixed);
+    {
+        const size_t r0 = ((sizeof(double4) * (size_t)n + 1023) & ~(size_t)1023);
+        tc_rows = (float*)((char*)mixed_base + r0);
+        tc_ops = (float*)((char*)tc_rows + ((m2l_tc_rows_bytes(cap_cells) + 1023) & ~(size_t)1023));
+    }
     cap.n = n; cap.cells = cap_cells; cap.P = P; cap.l1 = cap_l1; cap.l3 = cap_l3;
     return VPM_OK;
 }
@@ -173,7 +178,8 @@ int Ctx::check_params(const vpm_fmm_params* prm, vpm_fmm_params& out) {
     if (out.max_src < 0 || out.max_par < 1) return fail(VPM_EINVAL, "leaf caps must be max_src >= 0, max_par >= 1");
     if (out.max_depth != 16 && out.max_depth != 31) out.max_depth = 16;
     if (!(out.exp_tree_pct >= 0.0) || !std::isfinite(out.exp_tree_pct)) return fail(VPM_EINVAL, "exp_tree_pct");
-    if (out.precision != VPM_PREC_FP64 && out.precision != VPM_PREC_MIXED) return fail(VPM_EINVAL, "precision");
+    if (out.precision != VPM_PREC_FP64 && out.precision != VPM_PREC_MIXED && out.precision != VPM_PREC_MIXED_FP64_M2L)
+        return fail(VPM_EINVAL, "precision");
     return VPM_OK;
 }
 
@@ -200,6 +206,7 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
     if (coef_P != p.p || coef_binom != p.binom) {
         VPM_CUDA_TRY(set_coefficients2d(p.p, p.binom == VPM_BINOM_EXACT, ex2.coef, st));
         VPM_CUDA_TRY(set_m2l_operators2d(p.p, p.binom == VPM_BINOM_EXACT, ex2.op, st));
+        if (m2l_tc_supported(p.p)) VPM_CUDA_TRY(set_m2l_tc_operators(p.p, ex2.op, tc_ops, st));
         coef_P = p.p;
         coef_binom = p.binom;
     }
@@ -216,13 +223,24 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
     } else {
         VPM_CUDA_TRY(fmm2d_upward(tree, ex2, p.p, d_err, st, &launches));
         if (int r = record(4)) return r;
-        VPM_CUDA_TRY(fmm2d_m2l_only(tree, lists, ex2, p.p, d_err, st, &launches));
+        if (p.precision == VPM_PREC_MIXED && velocity != kModePotential && m2l_tc_supported(p.p))
+            VPM_CUDA_TRY(fmm2d_m2l_tc(tree, lists, ex2, p.p, tc_rows, tc_ops, d_err, st, &launches));
+        else
+            VPM_CUDA_TRY(fmm2d_m2l_only(tree, lists, ex2, p.p, d_err, st, &launches));
+        if (velocity == kModePotential) VPM_CUDA_TRY(fmm2d_m2l_b0(tree, lists, ex2, p.p, d_err, st, &launches));
         if (int r = record(5)) return r;
         VPM_CUDA_TRY(fmm2d_l2l(tree, ex2, p.p, d_err, st, &launches));
         if (int r = record(6)) return r;
-        VPM_CUDA_TRY(fmm2d_eval(tree, lists, ex2, p.p, d_err, st, &launches));
-        if (int r = record(7)) return r;
-        if (p.precision == VPM_PREC_MIXED) {
+        if (velocity == kModePotential) {
+            // far field and near field in one stage pair: the events keep their slots
+            VPM_CUDA_TRY(fmm2d_potential_eval(tree, lists, ex2, p.p, o0, d_err, st, &launches));
+            if (int r = record(7)) return r;
+        } else {
+            VPM_CUDA_TRY(fmm2d_eval(tree, lists, ex2, p.p, d_err, st, &launches));
+            if (int r = record(7)) return r;
+        }
+        if (velocity == kModePotential) {
+        } else if (p.precision == VPM_PREC_MIXED || p.precision == VPM_PREC_MIXED_FP64_M2L) {
             float4* rel = (float4*)mixed_base;
             VPM_CUDA_TRY(fmm2d_p2p_f32(tree, lists, ex2, rel, o0, o1, velocity, uinf, vinf, d_err, st, &launches,
                                        p.max_par));
@@ -405,7 +423,8 @@ int Ctx::run2d_host(const double* x, const double* y, const double* q_or_omega, 
     int r = check_params(prm, p);
     if (r) return r;
     if (n64 < 0 || n64 >= (1ll << 30)) return fail(VPM_EINVAL, "n out of range");
-    if (!x || !y || !act || (!tree_only && (!q_or_omega || !o0 || !o1)) || (velocity && !s))
+    if (!x || !y || !act || (!tree_only && (!q_or_omega || !o0 || (!o1 && velocity != kModePotential))) ||
+        (velocity == 1 && !s))
         return fail(VPM_EINVAL, "null buffer");
     const int n = (int)n64;
     if (n == 0) return VPM_OK;
@@ -430,7 +449,7 @@ int Ctx::run2d_host(const double* x, const double* y, const double* q_or_omega, 
         VPM_CUDA_TRY(cudaMemcpyAsync(in_act, act, n, cudaMemcpyHostToDevice, stream));
         if (tree_only) {
             VPM_CUDA_TRY(cudaMemsetAsync(in_q, 0, sizeof(double) * n, stream));
-        } else if (velocity) {
+        } else if (velocity == 1) {
             VPM_CUDA_TRY(cudaMemcpyAsync(in_q, q_or_omega, sizeof(double) * n, cudaMemcpyHostToDevice, stream));
             VPM_CUDA_TRY(cudaMemcpyAsync(out0, s, sizeof(double) * n, cudaMemcpyHostToDevice, stream));
             source_from_vorticity<<<std::min(1184, ceil_div(n, 256)), 256, 0, stream>>>(in_q, out0, n, in_q);
@@ -454,7 +473,7 @@ int Ctx::run2d_host(const double* x, const double* y, const double* q_or_omega, 
         if (bits) return map_err(bits);
         if (tree_only) return stats ? collect_stats(stats) : VPM_OK;
         VPM_CUDA_TRY(cudaMemcpyAsync(o0, out0, sizeof(double) * n, cudaMemcpyDeviceToHost, stream));
-        VPM_CUDA_TRY(cudaMemcpyAsync(o1, out1, sizeof(double) * n, cudaMemcpyDeviceToHost, stream));
+        if (o1) VPM_CUDA_TRY(cudaMemcpyAsync(o1, out1, sizeof(double) * n, cudaMemcpyDeviceToHost, stream));
         VPM_CUDA_TRY(cudaStreamSynchronize(stream));
         if (stats) return collect_stats(stats);
         return VPM_OK;
@@ -602,6 +621,15 @@ int vpm_velocity2d(vpm_ctx* ctx, const double* x, const double* y, const double*
     cudaError_t e = cudaSetDevice(c->device);
     if (e != cudaSuccess) return c->fail_cuda(e, "cudaSetDevice");
     return c->run2d_host(x, y, omega, s, active, n, prm, u, v, 1, u_inf, v_inf, stats, false);
+}
+
+int vpm_fmm2d_potential(vpm_ctx* ctx, const double* x, const double* y, const double* q, const uint8_t* active,
+                        int64_t n, const vpm_fmm_params* prm, double* phi, vpm_fmm_stats* stats) {
+    if (!ctx) return VPM_EINVAL;
+    Ctx* c = (Ctx*)ctx;
+    cudaError_t e = cudaSetDevice(c->device);
+    if (e != cudaSuccess) return c->fail_cuda(e, "cudaSetDevice");
+    return c->run2d_host(x, y, q, nullptr, active, n, prm, phi, nullptr, vpm::kModePotential, 0.0, 0.0, stats, false);
 }
 
 int vpm_fmm2d_field_device(vpm_ctx* ctx, const double* x, const double* y, const double* q, const uint8_t* active,

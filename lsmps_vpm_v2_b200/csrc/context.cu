@@ -79,9 +79,12 @@ int Ctx::count_interactions(vpm_fmm_stats* s) {
     return VPM_OK;
 }
 
-// Near-field work area: leaf-relative FP32 particles (float4 per particle,
-// mixed form) or the AoS FP64 copy (double4 per particle, plain form).
-size_t mixed_bytes(int n, int cap_cells, int P) { return sizeof(double4) * (size_t)n + 256; }
+// Mixed/near-field work area: leaf-relative FP32 particles (float4 per
+// particle, mixed form) or the AoS FP64 copy (double4 per particle, plain
+// form), then the tensor-core M2L rows and operators.
+size_t mixed_bytes(int n, int cap_cells, int P) {
+    return sizeof(double4) * (size_t)n + 1024 + m2l_tc_rows_bytes(cap_cells) + 1024 + m2l_tc_ops_bytes() + 1024;
+}
 
 
 

@@ -14,6 +14,10 @@ namespace vpm {
 // 3 lists, 4 P2M+M2M, 5 M2L, 6 L2L, 7 M2P+L2P, 8 P2P (end).
 constexpr int kStageEvents = 9;
 
+// Output mode of a 2D evaluation (the `velocity` argument below): 0 field
+// (Ex, Ey), 1 velocity (u, v), kModePotential the potential (one output).
+constexpr int kModePotential = 2;
+
 struct Caps3D {
     int n = 0, cells = 0;
 };
@@ -57,6 +61,8 @@ struct Ctx {
     Lists2D lists{};
     Expansions2D ex2{};
     void* mixed_base = nullptr;
+    float* tc_rows = nullptr;   // tensor-core M2L: scaled TF32 multipole rows
+    float* tc_ops = nullptr;    //                  list-2 operators (hi, lo)
     int coef_P = -1, coef_binom = -1;
 
     // CUDA graph of the device entry point (capture once, replay)

@@ -159,6 +159,19 @@ struct Expansions2D {
 cudaError_t fmm2d_upward(const Tree2D& t, Expansions2D& e, int P, unsigned* err, cudaStream_t st, int* launches);
 cudaError_t fmm2d_m2l(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, unsigned* err, cudaStream_t st,
                       int* launches);  // M2L followed by the L2L levels
+// Potential (fmm2D::calcPotential): b_0 of the M2L after fmm2d_m2l_only, then
+// after the L2L levels the far-field and list-1 potential into out (caller order).
+cudaError_t fmm2d_m2l_b0(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, unsigned* err, cudaStream_t st,
+                         int* launches);
+cudaError_t fmm2d_potential_eval(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, double* out,
+                                 unsigned* err, cudaStream_t st, int* launches);
+// Tensor-core list-2 M2L of the mixed form (m2l_tc.cu): orders 1..20.
+bool m2l_tc_supported(int P);
+size_t m2l_tc_rows_bytes(int cap_cells);
+size_t m2l_tc_ops_bytes();
+cudaError_t set_m2l_tc_operators(int P, const double2* op_dev, float* dst, cudaStream_t st);
+cudaError_t fmm2d_m2l_tc(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, float* rows, const float* ops,
+                         unsigned* err, cudaStream_t st, int* launches);
 cudaError_t fmm2d_m2l_only(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, unsigned* err,
                            cudaStream_t st, int* launches);
 cudaError_t fmm2d_l2l(const Tree2D& t, Expansions2D& e, int P, unsigned* err, cudaStream_t st, int* launches);

@@ -77,6 +77,16 @@ class Context:
                                           _ptr(ex), _ptr(ey), C.byref(s) if stats else None))
         return (ex, ey, s) if stats else (ex, ey)
 
+    def potential2d(self, x, y, q, active, params: Params | None = None, stats: bool = False):
+        """phi_i = sum_j q_j log|x_i - x_j| by the 2D FMM (host arrays)."""
+        x, y, q, a = _f64(x), _f64(y), _f64(q), _u8(active)
+        phi = np.empty(x.size)
+        p = params or default_params()
+        st = Stats()
+        self._check(lib().vpm_fmm2d_potential(self._h, _ptr(x), _ptr(y), _ptr(q), _ptr(a), x.size, C.byref(p),
+                                              _ptr(phi), C.byref(st) if stats else None))
+        return (phi, st) if stats else phi
+
     def field2d_device(self, x, y, q, active, ex, ey, params: Params | None = None):
         """Asynchronous field on device buffers (objects with .data_ptr(), e.g. torch CUDA tensors)."""
         p = params or default_params()
@@ -276,7 +286,7 @@ class fmm2D:
     def __init__(self, ctx: Context | None = None, params: Params | None = None):
         self.ctx = ctx or default_context()
         self.params = params or default_params()
-        self._ex = self._ey = None
+        self._ex = self._ey = self._phi = None
         self.stats: Stats | None = None
 
     def calcField(self, _cellTree, parPos, activeFlag, srcVal):
@@ -292,6 +302,15 @@ class fmm2D:
 
     def get_Field_y(self):
         return self._ey
+
+    def calcPotential(self, _cellTree, parPos, activeMark, srcVal):
+        """fmm2D::calcPotential (fmm2D.cpp:681-896) on the GPU FMM."""
+        pos = np.asarray(parPos, dtype=np.float64)
+        self._phi, self.stats = self.ctx.potential2d(pos[:, 0], pos[:, 1], srcVal, activeMark, self.params,
+                                                     stats=True)
+
+    def get_Potential(self):
+        return self._phi
 
 
 class fmm3D:

@@ -28,7 +28,7 @@ def test_mixed_vs_direct(ctx, port, name):
     if err_fp64 <= 1e-4:
         assert err_mixed <= 1e-4
     assert err_mixed <= err_fp64 * 1.05 + 1e-6
-    assert rel_l2((ex, ey), (fx, fy)) <= 2e-6   # only the near field changed precision
+    assert rel_l2((ex, ey), (fx, fy)) <= 1e-5   # FP32 near field, 3xTF32 tensor-core M2L
 
 
 def test_mixed_full_size(ctx, port):
