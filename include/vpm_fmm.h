@@ -221,6 +221,25 @@ int vpm_fmm2d_field_device_static(const double* x, const double* y, const double
                                   size_t errlen);
 
 /*
+ * Batched independent 2D solves (no counterpart in the reference, which
+ * evaluates one particle set per call): solve i is the particle range
+ * offsets[i] .. offsets[i+1]-1 of the concatenated arrays (offsets: host
+ * array of n_solves + 1 entries, offsets[0] = 0; each solve holds 0 or >= 2
+ * particles). Each solve is exactly vpm_fmm2d_field on its range. Solves run
+ * concurrently on up to 8 streams of sub-contexts forked from the context's
+ * stream; with prm->use_graph the whole batch is captured as one CUDA graph
+ * and replayed while offsets, buffers and parameters are unchanged.
+ * The _device form takes device pointers and returns without synchronising
+ * (vpm_ctx_sync reports the batch's errors); the host form copies in and out.
+ */
+int vpm_fmm2d_field_batched(vpm_ctx* ctx, int32_t n_solves, const int64_t* offsets, const double* x,
+                            const double* y, const double* q, const uint8_t* active, const vpm_fmm_params* prm,
+                            double* ex, double* ey);
+int vpm_fmm2d_field_batched_device(vpm_ctx* ctx, int32_t n_solves, const int64_t* offsets, const double* x,
+                                   const double* y, const double* q, const uint8_t* active,
+                                   const vpm_fmm_params* prm, double* ex, double* ey);
+
+/*
  * 3D velocity of the vortex particles (x_j, alpha_j) by the octree treecode
  * of the reference's default 3D path (VELOCITY_3D_TYPE 1):
  *   u(x_i) = sum_j alpha_j x (x_i - x_j) / |x_i - x_j|^3

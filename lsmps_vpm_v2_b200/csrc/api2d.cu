@@ -203,13 +203,7 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
     tree.n = n;
     tree.key_levels = K;
     VPM_CUDA_TRY(cudaMemsetAsync(d_err, 0, sizeof(unsigned), st));
-    if (coef_P != p.p || coef_binom != p.binom) {
-        VPM_CUDA_TRY(set_coefficients2d(p.p, p.binom == VPM_BINOM_EXACT, ex2.coef, st));
-        VPM_CUDA_TRY(set_m2l_operators2d(p.p, p.binom == VPM_BINOM_EXACT, ex2.op, st));
-        if (m2l_tc_supported(p.p)) VPM_CUDA_TRY(set_m2l_tc_operators(p.p, ex2.op, tc_ops, st));
-        coef_P = p.p;
-        coef_binom = p.binom;
-    }
+    if (int r = ensure_coefs(p)) return r;
     if (int r = record(0)) return r;
     VPM_CUDA_TRY(keys_sort2d(x, y, q, act, tree, ts, p.exp_tree_pct, d_err, st, &launches));
     if (int r = record(1)) return r;
@@ -254,6 +248,21 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
     last_params = p;
     last_n = n;
     have_tree = true;
+    return VPM_OK;
+}
+
+// Translation coefficients, list-2 operators (FP64 and tensor-core forms) of
+// order p.p on this context's arena; uploaded when the order, the binomials
+// or the arena changed. The uploads synchronise the stream, so callers that
+// capture graphs call this before the capture begins.
+int Ctx::ensure_coefs(const vpm_fmm_params& p) {
+    if (coef_P == p.p && coef_binom == p.binom) return VPM_OK;
+    if (capturing) return fail(VPM_EINVAL, "coefficient upload inside a graph capture");
+    VPM_CUDA_TRY(set_coefficients2d(p.p, p.binom == VPM_BINOM_EXACT, ex2.coef, stream));
+    VPM_CUDA_TRY(set_m2l_operators2d(p.p, p.binom == VPM_BINOM_EXACT, ex2.op, stream));
+    if (m2l_tc_supported(p.p)) VPM_CUDA_TRY(set_m2l_tc_operators(p.p, ex2.op, tc_ops, stream));
+    coef_P = p.p;
+    coef_binom = p.binom;
     return VPM_OK;
 }
 
@@ -343,12 +352,7 @@ int Ctx::launch2d(const double* x, const double* y, const double* q, const uint8
         return VPM_OK;
     }
     drop_graph();
-    if (coef_P != p.p || coef_binom != p.binom) {
-        VPM_CUDA_TRY(set_coefficients2d(p.p, p.binom == VPM_BINOM_EXACT, ex2.coef, stream));
-        VPM_CUDA_TRY(set_m2l_operators2d(p.p, p.binom == VPM_BINOM_EXACT, ex2.op, stream));
-        coef_P = p.p;
-        coef_binom = p.binom;
-    }
+    if (int r = ensure_coefs(p)) return r;  // uploads synchronise: never inside a capture
     VPM_CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     capturing = true;
     split_capture = split;
@@ -587,6 +591,13 @@ int vpm_ctx_sync(vpm_ctx* ctx) {
     e = cudaMemcpyAsync(&bits, c->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return c->fail_cuda(e, "vpm_ctx_sync");
+    if (c->batch_subs > 0) {  // errors of the sub-contexts of the last batch
+        unsigned b = 0;
+        int r = c->batch_errors(&b);
+        if (r) return r;
+        bits |= b;
+        c->batch_subs = 0;
+    }
     return c->map_err(bits);
 }
 

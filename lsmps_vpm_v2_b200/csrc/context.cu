@@ -35,6 +35,7 @@ __global__ void count2d(Tree2D t, Lists2D l, unsigned long long* out, const unsi
 
 Ctx::~Ctx() {
     if (device >= 0) cudaSetDevice(device);
+    drop_batch();
     drop_graph();
     if (arena2d) cudaFree(arena2d);
     if (arena3d) cudaFree(arena3d);

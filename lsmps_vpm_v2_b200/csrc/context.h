@@ -103,6 +103,16 @@ struct Ctx {
     float last_ms3 = 0.f;
     int last_launches3 = 0;
 
+    // batched solves (batch2d.cu)
+    std::vector<Ctx*> subs;
+    std::vector<cudaEvent_t> join_ev;
+    cudaEvent_t fork_ev = nullptr;
+    cudaGraphExec_t batch_exec = nullptr;
+    std::vector<int64_t> batch_key;
+    int batch_subs = 0;
+    void* batch_in = nullptr;
+    size_t batch_in_bytes = 0;
+
     // last evaluation
     bool have_tree = false;
     int last_n = 0;
@@ -128,6 +138,7 @@ struct Ctx {
     int collect_stats(vpm_fmm_stats* s);
     int count_interactions(vpm_fmm_stats* s);
     int fetch_tree(HostTree2D& h);
+    int ensure_coefs(const vpm_fmm_params& p);
     int launch2d(const double* x, const double* y, const double* q, const uint8_t* act, int n,
                  const vpm_fmm_params& p, int K, double* o0, double* o1, int velocity, double uinf, double vinf);
     int reserve3d(int n, int cap_cells);
@@ -138,6 +149,10 @@ struct Ctx {
                    const double* a2, const double* s, const uint8_t* act, int64_t n, const vpm_fmm_params* prm,
                    double* u, double* v, double* w, double uinf, double vinf, double winf, vpm_fmm_stats* stats,
                    bool tree_only);
+    int batch2d(int ns, const int64_t* offs, const double* x, const double* y, const double* q, const uint8_t* act,
+                const vpm_fmm_params& p, double* ex, double* ey);
+    int batch_errors(unsigned* bits);
+    void drop_batch();
     void drop_graph();
     void begin_ring();
     void end_ring();

@@ -77,6 +77,29 @@ class Context:
                                           _ptr(ex), _ptr(ey), C.byref(s) if stats else None))
         return (ex, ey, s) if stats else (ex, ey)
 
+    def field2d_batched(self, solves, params: Params | None = None):
+        """Independent 2D solves in one call. `solves` is a list of (x, y, q,
+        active) tuples; returns a list of (ex, ey)."""
+        sizes = [np.asarray(s[0]).size for s in solves]
+        offs = np.zeros(len(solves) + 1, np.int64)
+        offs[1:] = np.cumsum(sizes)
+        cat = [np.ascontiguousarray(np.concatenate([np.asarray(s[k], dtype=np.float64) for s in solves]))
+               for k in range(3)]
+        act = np.ascontiguousarray(np.concatenate([np.asarray(s[3], dtype=np.uint8) for s in solves]))
+        ex, ey = np.empty(int(offs[-1])), np.empty(int(offs[-1]))
+        p = params or default_params()
+        self._check(lib().vpm_fmm2d_field_batched(self._h, len(solves), _ptr(offs), _ptr(cat[0]), _ptr(cat[1]),
+                                                  _ptr(cat[2]), _ptr(act), C.byref(p), _ptr(ex), _ptr(ey)))
+        return [(ex[offs[i]:offs[i + 1]], ey[offs[i]:offs[i + 1]]) for i in range(len(solves))]
+
+    def field2d_batched_device(self, offsets, x, y, q, active, ex, ey, params: Params | None = None):
+        """Device-pointer batch (integers such as torch data_ptr()); offsets is
+        a host int64 array of n_solves + 1 entries. Asynchronous."""
+        offs = np.ascontiguousarray(offsets, dtype=np.int64)
+        p = params or default_params()
+        self._check(lib().vpm_fmm2d_field_batched_device(self._h, offs.size - 1, _ptr(offs), x, y, q, active,
+                                                         C.byref(p), ex, ey))
+
     def potential2d(self, x, y, q, active, params: Params | None = None, stats: bool = False):
         """phi_i = sum_j q_j log|x_i - x_j| by the 2D FMM (host arrays)."""
         x, y, q, a = _f64(x), _f64(y), _f64(q), _u8(active)
