@@ -290,6 +290,61 @@ int vpm_tree3d_counts(vpm_ctx* ctx, int64_t* n_cells, int64_t* n_leaves, int32_t
 int vpm_tree3d_cells(vpm_ctx* ctx, int32_t* ints6, double* geom4, int64_t* leaf_offs, int32_t* pids);
 
 /*
+ * Learned (leaf caps, p) selector of the mixed 2D form. No counterpart in the
+ * reference, which always uses caps 50/75 and p = 10 (global.cpp:311-313);
+ * that pair is the selector's fallback.
+ *
+ * Candidates: 35 pairs (cap, p), cap in {25, 50, 100, 200, 400} (max_src =
+ * cap, max_par = 3 cap / 2) times p in {4, 6, 8, 10, 12, 16, 20}, in the
+ * order vpm_selector_candidates lists them.
+ * Features (228 floats): log10 N, log10 root length, log10 max|q|, log10
+ * target error, then for grid levels 3..9 of the root box a 32-bin histogram
+ * (fractions of occupied cells) of floor(log2 particles per cell).
+ * Network: 228 -> 64 -> 64 -> 64 -> 70 (GELU), FP32 parameters stored per
+ * layer as W [out x in] then b [out]; outputs are the standardised log10
+ * relative L2 error and log10 time of each candidate. Training (minibatch
+ * Adam, masked MSE) and inference (BF16 weights) are CUDA kernels of this
+ * library; the inputs and targets given to vpm_mlp_* are already normalised,
+ * vpm_select2d normalises with the statistics of vpm_mlp_set_norm.
+ */
+int64_t vpm_mlp_param_count(void);
+int vpm_selector_candidates(int32_t* caps, int32_t* ps, int32_t count);
+int vpm_mlp_init(vpm_ctx* ctx, uint64_t seed);
+int vpm_mlp_set_params(vpm_ctx* ctx, const float* params, int64_t count);
+int vpm_mlp_get_params(vpm_ctx* ctx, float* params, int64_t count);
+int vpm_mlp_set_norm(vpm_ctx* ctx, const float* in_mean, const float* in_std, const float* out_mean,
+                     const float* out_std);
+/* B rows of normalised inputs -> outputs (host arrays); bf16 selects the BF16 inference kernel. */
+int vpm_mlp_forward(vpm_ctx* ctx, const float* X, int32_t B, float* Y, int32_t bf16);
+/* Gradient (param_count floats) and value of the masked MSE over B rows; mask may be NULL. */
+int vpm_mlp_grads(vpm_ctx* ctx, const float* X, const float* Y, const float* mask, int32_t B, float* grads,
+                  float* loss);
+/* `steps` Adam steps of `batch` rows drawn per epoch without replacement (seeded). */
+int vpm_mlp_train(vpm_ctx* ctx, const float* X, const float* Y, const float* mask, int64_t rows, int32_t batch,
+                  int32_t steps, float lr, uint64_t seed, float* loss_hist);
+/* The 228 features of a particle set (host or device arrays); synchronises. */
+int vpm_selector_features2d(vpm_ctx* ctx, const double* x, const double* y, const double* q,
+                            const uint8_t* active, int64_t n, double target_err, float* feat);
+int vpm_selector_features2d_device(vpm_ctx* ctx, const double* x, const double* y, const double* q,
+                                   const uint8_t* active, int64_t n, double target_err, float* feat);
+/* The cheapest candidate predicted to meet target_err with margin_decades to
+ * spare (fallback 50/75, p = 10); pred (may be NULL) gets the 70 predictions
+ * (log10 error, then log10 ms). */
+int vpm_select2d(vpm_ctx* ctx, const float* feat, double target_err, double margin_decades, int32_t* max_src,
+                 int32_t* max_par, int32_t* p, float* pred);
+
+/*
+ * FP64 direct sum of the 2D field at m sampled targets (device pointers,
+ * int64 target indices on the device): E_t = sum over active j != t of
+ * q_j (x_t - x_j) / |x_t - x_j|^2, the judge of the FMM's error (the
+ * reference's own direct form, fmm2D::fieldDirSum, fmm2D.cpp:135-179, over
+ * all sources). Asynchronous on the context's stream.
+ */
+int vpm_direct2d_field_device(vpm_ctx* ctx, const double* x, const double* y, const double* q,
+                              const uint8_t* active, int64_t n, const int64_t* targets, int64_t m, double* ex,
+                              double* ey);
+
+/*
  * FMA-throughput microbenchmark of the device (TFLOP/s of dependent FMA
  * chains in FP64 and FP32): the pipe peaks the near-field roofline fractions
  * are quoted against. No counterpart in the reference (measurement utility).

@@ -106,6 +106,20 @@ SIGNATURES = {
     "vpm_fmm2d_field_batched": (C.c_int, [_vp, C.c_int32, _vp, _vp, _vp, _vp, _vp, C.POINTER(Params), _vp, _vp]),
     "vpm_fmm2d_field_batched_device": (C.c_int, [_vp, C.c_int32, _vp, _vp, _vp, _vp, _vp, C.POINTER(Params), _vp,
                                                  _vp]),
+    "vpm_mlp_param_count": (C.c_int64, []),
+    "vpm_selector_candidates": (C.c_int, [_vp, _vp, C.c_int32]),
+    "vpm_mlp_init": (C.c_int, [_vp, C.c_uint64]),
+    "vpm_mlp_set_params": (C.c_int, [_vp, _vp, C.c_int64]),
+    "vpm_mlp_get_params": (C.c_int, [_vp, _vp, C.c_int64]),
+    "vpm_mlp_set_norm": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "vpm_mlp_forward": (C.c_int, [_vp, _vp, C.c_int32, _vp, C.c_int32]),
+    "vpm_mlp_grads": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int32, _vp, C.POINTER(C.c_float)]),
+    "vpm_mlp_train": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int64, C.c_int32, C.c_int32, C.c_float, C.c_uint64, _vp]),
+    "vpm_selector_features2d": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int64, C.c_double, _vp]),
+    "vpm_selector_features2d_device": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int64, C.c_double, _vp]),
+    "vpm_select2d": (C.c_int, [_vp, _vp, C.c_double, C.c_double, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                               C.POINTER(C.c_int32), _vp]),
+    "vpm_direct2d_field_device": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int64, _vp, C.c_int64, _vp, _vp]),
     "vpm_fmm3d_velocity": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int64, C.POINTER(Params),
                                      _vp, _vp, _vp, C.POINTER(Stats)]),
     "vpm_fmm3d_velocity_device": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int64, C.POINTER(Params),

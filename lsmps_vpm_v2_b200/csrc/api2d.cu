@@ -97,6 +97,7 @@ int Ctx::reserve2d(int n, int cap_cells, int P, long long cap_l1, long long cap_
     size_t o_l3c = L.take<uint32_t>(C), o_l3o = L.take<uint32_t>(C + 1), o_l3s = L.take<int32_t>(cap_l3);
     size_t o_a = L.take<double2>(C * (P + 1)), o_b = L.take<double2>(C * (P + 1)), o_cnt = L.take<unsigned>(C);
     size_t o_fx = L.take<double>(n), o_fy = L.take<double>(n);
+    size_t o_nx = L.take<double>(n), o_ny = L.take<double>(n);
     size_t o_geom = L.take<Geom2D>(1), o_info = L.take<TreeInfo2D>(1);
     size_t o_coef = L.take<double>(3 * kCoefTable);
     size_t o_op = L.take<double2>((size_t)49 * (P + 1) * P);
@@ -147,6 +148,7 @@ int Ctx::reserve2d(int n, int cap_cells, int P, long long cap_l1, long long cap_
     lists.cap_l3 = cap_l3;
     ex2.a = (double2*)P_(o_a); ex2.b = (double2*)P_(o_b); ex2.up_count = (unsigned*)P_(o_cnt);
     ex2.fx = (double*)P_(o_fx); ex2.fy = (double*)P_(o_fy);
+    near_x = (double*)P_(o_nx); near_y = (double*)P_(o_ny);
     ex2.coef = (double*)P_(o_coef);
     ex2.op = (double2*)P_(o_op);
     coef_P = -1;  // the new arena holds no coefficients yet
@@ -209,6 +211,36 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
     if (int r = record(1)) return r;
     VPM_CUDA_TRY(levels2d(tree, ts, p.max_src, p.max_par, d_err, st, &launches));
     if (int r = record(2)) return r;
+    if (capturing && !split_capture && !tree_only && velocity != kModePotential) {
+        // One captured graph: the near field (lists 1/3, P2P) runs on the side
+        // stream concurrently with lists 2/4 and the far field (P2M, M2M, M2L,
+        // L2L); M2P + L2P then add the near field and write the output.
+        VPM_CUDA_TRY(cudaEventRecord(fork2, st));
+        VPM_CUDA_TRY(cudaStreamWaitEvent(side, fork2, 0));
+        VPM_CUDA_TRY(build_int_lists2d(tree, lists, ts.scan, p.eps, d_err, side, &launches));
+        if (p.precision == VPM_PREC_MIXED || p.precision == VPM_PREC_MIXED_FP64_M2L)
+            VPM_CUDA_TRY(fmm2d_p2p_f32(tree, lists, ex2, (float4*)mixed_base, near_x, near_y, 0, 0.0, 0.0, d_err, side,
+                                       &launches, p.max_par, true));
+        else
+            VPM_CUDA_TRY(fmm2d_p2p_f64_tma(tree, lists, ex2, (double4*)mixed_base, near_x, near_y, 0, 0.0, 0.0, d_err,
+                                           side, &launches, p.max_par, true));
+        VPM_CUDA_TRY(cudaEventRecord(join2, side));
+        VPM_CUDA_TRY(build_ext_lists2d(tree, lists, p.eps, d_err, st, &launches));
+        VPM_CUDA_TRY(fmm2d_upward(tree, ex2, p.p, d_err, st, &launches));
+        if (p.precision == VPM_PREC_MIXED && m2l_tc_supported(p.p))
+            VPM_CUDA_TRY(fmm2d_m2l_tc(tree, lists, ex2, p.p, tc_rows, tc_ops, d_err, st, &launches));
+        else
+            VPM_CUDA_TRY(fmm2d_m2l_only(tree, lists, ex2, p.p, d_err, st, &launches));
+        VPM_CUDA_TRY(fmm2d_l2l(tree, ex2, p.p, d_err, st, &launches));
+        VPM_CUDA_TRY(cudaStreamWaitEvent(st, join2, 0));
+        VPM_CUDA_TRY(fmm2d_eval_combine(tree, lists, ex2, p.p, near_x, near_y, o0, o1, velocity, uinf, vinf, d_err, st,
+                                        &launches));
+        last_launches = launches;
+        last_params = p;
+        last_n = n;
+        have_tree = true;
+        return VPM_OK;
+    }
     VPM_CUDA_TRY(build_lists2d(tree, lists, ts.scan, p.eps, d_err, st, &launches));
     if (int r = record(3)) return r;
     if (tree_only) {

@@ -36,6 +36,8 @@ __global__ void count2d(Tree2D t, Lists2D l, unsigned long long* out, const unsi
 Ctx::~Ctx() {
     if (device >= 0) cudaSetDevice(device);
     drop_batch();
+    drop_selector(selector);
+    selector = nullptr;
     drop_graph();
     if (arena2d) cudaFree(arena2d);
     if (arena3d) cudaFree(arena3d);
@@ -43,6 +45,9 @@ Ctx::~Ctx() {
     for (auto& e : ev)
         if (e) cudaEventDestroy(e);
     if (own_stream) cudaStreamDestroy(own_stream);
+    if (side) cudaStreamDestroy(side);
+    if (fork2) cudaEventDestroy(fork2);
+    if (join2) cudaEventDestroy(join2);
 }
 
 int Ctx::init(int dev) {
@@ -54,6 +59,11 @@ int Ctx::init(int dev) {
     e = cudaStreamCreate(&own_stream);
     if (e != cudaSuccess) return fail_cuda(e, "cudaStreamCreate");
     stream = own_stream;
+    e = cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaStreamCreate");
+    e = cudaEventCreateWithFlags(&fork2, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&join2, cudaEventDisableTiming);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaEventCreate");
     e = cudaMalloc(&d_err, 64);
     if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc");
     e = cudaMemset(d_err, 0, 64);

@@ -10,6 +10,9 @@
 
 namespace vpm {
 
+struct Selector;  // learned (caps, p) selector state (selector.cu)
+void drop_selector(Selector* s);
+
 // Stage marks of one evaluation: 0 start, 1 keys+sort, 2 tree levels,
 // 3 lists, 4 P2M+M2M, 5 M2L, 6 L2L, 7 M2P+L2P, 8 P2P (end).
 constexpr int kStageEvents = 9;
@@ -45,6 +48,11 @@ struct Ctx {
     int device = 0;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
+    // Second stream of a captured evaluation: lists 1/3 and the near field run
+    // on it while the main stream builds lists 2/4 and the far field.
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork2 = nullptr, join2 = nullptr;
+    double *near_x = nullptr, *near_y = nullptr;
     std::string last_error;
     unsigned* d_err = nullptr;
     cudaEvent_t ev[kStageEvents] = {};
@@ -102,6 +110,8 @@ struct Ctx {
     int last_n3 = 0;
     float last_ms3 = 0.f;
     int last_launches3 = 0;
+
+    Selector* selector = nullptr;
 
     // batched solves (batch2d.cu)
     std::vector<Ctx*> subs;
@@ -164,12 +174,17 @@ struct Ctx {
 // (max_par < 0).
 cudaError_t fmm2d_p2p_f32(const Tree2D& t, const Lists2D& l, const Expansions2D& e, float4* rel, double* out0,
                           double* out1, int velocity, double u_inf, double v_inf, unsigned* err, cudaStream_t st,
-                          int* launches, int max_par);
+                          int* launches, int max_par, bool near_only = false);
 // FP64 P2P on an AoS copy of the particles (`aos`, n entries); kernel choice as
 // for fmm2d_p2p_f32.
 cudaError_t fmm2d_p2p_f64_tma(const Tree2D& t, const Lists2D& l, const Expansions2D& e, double4* aos, double* out0,
                               double* out1, int velocity, double u_inf, double v_inf, unsigned* err, cudaStream_t st,
-                              int* launches, int max_par);
+                              int* launches, int max_par, bool near_only = false);
+// Far field (M2P + L2P) plus the near field nx/ny (tree order), written in the
+// caller's order (field or velocity).
+cudaError_t fmm2d_eval_combine(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, const double* nx,
+                               const double* ny, double* out0, double* out1, int velocity, double u_inf, double v_inf,
+                               unsigned* err, cudaStream_t st, int* launches);
 cudaError_t fmm2d_p2p_out(const Tree2D& t, const Lists2D& l, const Expansions2D& e, double* out0, double* out1,
                           int velocity, double u_inf, double v_inf, unsigned* err, cudaStream_t st, int* launches);
 

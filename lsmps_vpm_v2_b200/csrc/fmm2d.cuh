@@ -128,6 +128,12 @@ cudaError_t keys_sort2d(const double* x, const double* y, const double* q, const
 cudaError_t levels2d(Tree2D& t, TreeScratch2D& s, int max_src, int max_par, unsigned* err, cudaStream_t st,
                      int* launches);
 
+// Lists 2 and 4 (fixed width), and lists 1 and 3 (count, scan, fill); the two
+// are independent of each other.
+cudaError_t build_ext_lists2d(const Tree2D& t, Lists2D& l, double eps, unsigned* err, cudaStream_t st,
+                              int* launches);
+cudaError_t build_int_lists2d(const Tree2D& t, Lists2D& l, ScanScratch& scan, double eps, unsigned* err,
+                              cudaStream_t st, int* launches);
 // Lists 1-4 (count, scan, fill). Requires the tree on `st`.
 cudaError_t build_lists2d(const Tree2D& t, Lists2D& l, ScanScratch& scan, double eps, unsigned* err,
                           cudaStream_t st, int* launches);

@@ -419,7 +419,9 @@ constexpr int kEvalThreads = 64;
 // above level 2 carry no local expansion (M2L starts at level 2).
 __global__ void __launch_bounds__(kEvalThreads)
 eval2d(Tree2D t, Lists2D l, const double2* __restrict__ a, const double2* __restrict__ b, double* __restrict__ fx,
-       double* __restrict__ fy, int P, unsigned* err) {
+       double* __restrict__ fy, int P, const double* __restrict__ nx, const double* __restrict__ ny,
+       double* __restrict__ out0, double* __restrict__ out1, int velocity, double u_inf, double v_inf,
+       unsigned* err) {
     __shared__ double2 s_b[W];
     if (fatal(err)) return;
     const int nl = t.info->n_leaves;
@@ -450,8 +452,24 @@ eval2d(Tree2D t, Lists2D l, const double2* __restrict__ a, const double2* __rest
             for (int pp = P - 1; pp >= 1; --pp) S = cfma(S, w, cscale(s_b[pp], (double)pp));
             ex += S.x;
             ey -= S.y;
-            fx[i] = ex;
-            fy[i] = ey;
+            if (nx) {
+                // near field already computed: write the total in the caller's order
+                ex = nx[i] + ex;
+                ey = ny[i] + ey;
+                const uint32_t orig = t.perm[i];
+                if (orig >= (uint32_t)t.n) {
+                    set_err(err, ERR_INDEX);
+                } else if (velocity) {
+                    out0[orig] = ey + u_inf;
+                    out1[orig] = -ex + v_inf;
+                } else {
+                    out0[orig] = ex;
+                    out1[orig] = ey;
+                }
+            } else {
+                fx[i] = ex;
+                fy[i] = ey;
+            }
         }
         __syncthreads();
     }
@@ -461,10 +479,17 @@ eval2d(Tree2D t, Lists2D l, const double2* __restrict__ a, const double2* __rest
 
 constexpr int kP2PThreads = 128;
 
-// Writes one target's total field (near + far) in the caller's order.
+// Writes one target's total field (near + far) in the caller's order; with
+// fx == nullptr (near field computed concurrently with the far field) the
+// near field alone, in tree order, into out0/out1.
 __device__ __forceinline__ void p2p_store(const Tree2D& t, int ti, double ex, double ey, const double* fx,
                                           const double* fy, double* out0, double* out1, int velocity, double u_inf,
                                           double v_inf, unsigned* err) {
+    if (!fx) {
+        out0[ti] = ex;
+        out1[ti] = ey;
+        return;
+    }
     ex += fx[ti];
     ey += fy[ti];
     const uint32_t orig = t.perm[ti];
@@ -1204,7 +1229,17 @@ cudaError_t fmm2d_m2l(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P,
 
 cudaError_t fmm2d_eval(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, unsigned* err, cudaStream_t st,
                        int* launches) {
-    eval2d<<<148 * 16, kEvalThreads, 0, st>>>(t, l, e.a, e.b, e.fx, e.fy, P, err);
+    eval2d<<<148 * 16, kEvalThreads, 0, st>>>(t, l, e.a, e.b, e.fx, e.fy, P, nullptr, nullptr, nullptr, nullptr, 0,
+                                              0.0, 0.0, err);
+    *launches += 1;
+    return cudaGetLastError();
+}
+
+cudaError_t fmm2d_eval_combine(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, const double* nx,
+                               const double* ny, double* out0, double* out1, int velocity, double u_inf, double v_inf,
+                               unsigned* err, cudaStream_t st, int* launches) {
+    eval2d<<<148 * 16, kEvalThreads, 0, st>>>(t, l, e.a, e.b, e.fx, e.fy, P, nx, ny, out0, out1, velocity, u_inf,
+                                              v_inf, err);
     *launches += 1;
     return cudaGetLastError();
 }
@@ -1218,22 +1253,26 @@ cudaError_t fmm2d_p2p_out(const Tree2D& t, const Lists2D& l, const Expansions2D&
 
 cudaError_t fmm2d_p2p_f32(const Tree2D& t, const Lists2D& l, const Expansions2D& e, float4* rel, double* out0,
                           double* out1, int velocity, double u_inf, double v_inf, unsigned* err, cudaStream_t st,
-                          int* launches, int max_par) {
+                          int* launches, int max_par, bool near_only) {
     leaf_relative_f32<<<148 * 8, 128, 0, st>>>(t, rel, err);
     *launches += 2;
-    if (max_par < 0) return launch_p2p_tma<P2PF32>(t, l, rel, e, out0, out1, velocity, u_inf, v_inf, err, st, -max_par);
-    p2p2d_warp<P2PF32><<<148 * 16, 32 * kWarpP2PWarps, 0, st>>>(t, l, rel, e.fx, e.fy, out0, out1, velocity, u_inf,
+    Expansions2D en = e;
+    if (near_only) en.fx = en.fy = nullptr;
+    if (max_par < 0) return launch_p2p_tma<P2PF32>(t, l, rel, en, out0, out1, velocity, u_inf, v_inf, err, st, -max_par);
+    p2p2d_warp<P2PF32><<<148 * 16, 32 * kWarpP2PWarps, 0, st>>>(t, l, rel, en.fx, en.fy, out0, out1, velocity, u_inf,
                                                                v_inf, err);
     return cudaGetLastError();
 }
 
 cudaError_t fmm2d_p2p_f64_tma(const Tree2D& t, const Lists2D& l, const Expansions2D& e, double4* aos, double* out0,
                               double* out1, int velocity, double u_inf, double v_inf, unsigned* err, cudaStream_t st,
-                              int* launches, int max_par) {
+                              int* launches, int max_par, bool near_only) {
     particles_aos<<<148 * 8, 256, 0, st>>>(t, aos, err);
     *launches += 2;
-    if (max_par < 0) return launch_p2p_tma<P2PF64>(t, l, aos, e, out0, out1, velocity, u_inf, v_inf, err, st, -max_par);
-    p2p2d_warp<P2PF64><<<148 * 16, 32 * kWarpP2PWarps, 0, st>>>(t, l, aos, e.fx, e.fy, out0, out1, velocity, u_inf,
+    Expansions2D en = e;
+    if (near_only) en.fx = en.fy = nullptr;
+    if (max_par < 0) return launch_p2p_tma<P2PF64>(t, l, aos, en, out0, out1, velocity, u_inf, v_inf, err, st, -max_par);
+    p2p2d_warp<P2PF64><<<148 * 16, 32 * kWarpP2PWarps, 0, st>>>(t, l, aos, en.fx, en.fy, out0, out1, velocity, u_inf,
                                                                v_inf, err);
     return cudaGetLastError();
 }

@@ -236,13 +236,26 @@ __global__ void list_totals(Tree2D t, Lists2D l, unsigned* err) {
 
 }  // namespace
 
-cudaError_t build_lists2d(const Tree2D& t, Lists2D& l, ScanScratch& scan, double eps, unsigned* err,
-                          cudaStream_t st, int* launches) {
-    const int gl = std::max(1, std::min(148 * 4, ceil_div(l.cap_leaves, 128)));
+cudaError_t build_ext_lists2d(const Tree2D& t, Lists2D& l, double eps, unsigned* err, cudaStream_t st,
+                              int* launches) {
     const int gc = std::max(1, std::min(148 * 4, ceil_div(t.cap_cells, 128)));
     ext_list_kernel<<<gc, 128, 0, st>>>(t, eps, l, err);
+    *launches += 1;
+    return cudaGetLastError();
+}
+
+cudaError_t build_lists2d(const Tree2D& t, Lists2D& l, ScanScratch& scan, double eps, unsigned* err,
+                          cudaStream_t st, int* launches) {
+    cudaError_t e = build_ext_lists2d(t, l, eps, err, st, launches);
+    if (e != cudaSuccess) return e;
+    return build_int_lists2d(t, l, scan, eps, err, st, launches);
+}
+
+cudaError_t build_int_lists2d(const Tree2D& t, Lists2D& l, ScanScratch& scan, double eps, unsigned* err,
+                              cudaStream_t st, int* launches) {
+    const int gl = std::max(1, std::min(148 * 4, ceil_div(l.cap_leaves, 128)));
     int_list_kernel<<<gl, 128, 0, st>>>(t, eps, 0, l, err);
-    *launches += 2;
+    *launches += 1;
     cudaError_t e = scan_exclusive(l.l1_cnt, l.l1_off, l.cap_leaves, l.l1_off + l.cap_leaves, scan, err, st);
     if (e != cudaSuccess) return e;
     e = scan_exclusive(l.l3_cnt, l.l3_off, l.cap_leaves, l.l3_off + l.cap_leaves, scan, err, st);
