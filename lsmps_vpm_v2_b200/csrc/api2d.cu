@@ -81,6 +81,9 @@ int Ctx::reserve2d(int n, int cap_cells, int P, long long cap_l1, long long cap_
     size_t o_keyalt = L.take<uint64_t>(n), o_valalt = L.take<uint32_t>(n), o_actu = L.take<uint32_t>(n);
     size_t o_bbox = L.take<double>(kBBoxBlocks * 4);
     size_t o_lstat = L.take<uint64_t>((size_t)(K + 1) * lvl_tiles), o_ltick = L.take<unsigned>(kTicketWords);
+    const int flat_tiles = ceil_div(n, kFlatTile);
+    size_t o_pinfo = L.take<uint32_t>(n), o_tcnt = L.take<uint32_t>((size_t)2 * (K + 1) * flat_tiles),
+           o_ltot = L.take<uint32_t>(2 * (K + 1));
     size_t o_sstat = L.take<uint32_t>((size_t)8 * s_tiles * 256), o_stick = L.take<unsigned>(8),
            o_hist = L.take<uint32_t>(8 * 256);
     size_t o_scstat = L.take<uint64_t>(sc_tiles), o_sctick = L.take<unsigned>(1);
@@ -95,6 +98,7 @@ int Ctx::reserve2d(int n, int cap_cells, int P, long long cap_l1, long long cap_
     size_t o_l4 = L.take<int32_t>(C * kList4Cap), o_l4n = L.take<uint8_t>(C);
     size_t o_l1c = L.take<uint32_t>(C), o_l1o = L.take<uint32_t>(C + 1), o_l1s = L.take<int32_t>(cap_l1);
     size_t o_l3c = L.take<uint32_t>(C), o_l3o = L.take<uint32_t>(C + 1), o_l3s = L.take<int32_t>(cap_l3);
+    size_t o_l1slot = L.take<int32_t>(C * kListSlot1), o_l3slot = L.take<int32_t>(C * kListSlot3);
     size_t o_a = L.take<double2>(C * (P + 1)), o_b = L.take<double2>(C * (P + 1)), o_cnt = L.take<unsigned>(C);
     size_t o_fx = L.take<double>(n), o_fy = L.take<double>(n);
     size_t o_nx = L.take<double>(n), o_ny = L.take<double>(n);
@@ -125,6 +129,8 @@ int Ctx::reserve2d(int n, int cap_cells, int P, long long cap_l1, long long cap_
     ts.key_alt = (uint64_t*)P_(o_keyalt); ts.val_alt = (uint32_t*)P_(o_valalt); ts.act_u32 = (uint32_t*)P_(o_actu);
     ts.bbox_partial = (double*)P_(o_bbox);
     ts.lvl_status = (uint64_t*)P_(o_lstat); ts.lvl_ticket = (unsigned*)P_(o_ltick); ts.lvl_max_tiles = lvl_tiles;
+    ts.pinfo = (uint32_t*)P_(o_pinfo); ts.tile_cnt = (uint32_t*)P_(o_tcnt); ts.level_tot = (uint32_t*)P_(o_ltot);
+    ts.flat_tiles = flat_tiles;
     ts.sort.status = (uint32_t*)P_(o_sstat); ts.sort.tickets = (unsigned*)P_(o_stick);
     ts.sort.hist = (uint32_t*)P_(o_hist); ts.sort.max_tiles = s_tiles;
     ts.scan.status = (uint64_t*)P_(o_scstat); ts.scan.ticket = (unsigned*)P_(o_sctick); ts.scan.max_tiles = sc_tiles;
@@ -143,6 +149,7 @@ int Ctx::reserve2d(int n, int cap_cells, int P, long long cap_l1, long long cap_
     lists.l4_src = (int32_t*)P_(o_l4); lists.l4_n = (uint8_t*)P_(o_l4n);
     lists.l1_cnt = (uint32_t*)P_(o_l1c); lists.l1_off = (uint32_t*)P_(o_l1o); lists.l1_src = (int32_t*)P_(o_l1s);
     lists.l3_cnt = (uint32_t*)P_(o_l3c); lists.l3_off = (uint32_t*)P_(o_l3o); lists.l3_src = (int32_t*)P_(o_l3s);
+    lists.l1_slot = (int32_t*)P_(o_l1slot); lists.l3_slot = (int32_t*)P_(o_l3slot);
     lists.cap_leaves = cap_cells;
     lists.cap_l1 = cap_l1;
     lists.cap_l3 = cap_l3;
@@ -225,8 +232,11 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
             VPM_CUDA_TRY(fmm2d_p2p_f64_tma(tree, lists, ex2, (double4*)mixed_base, near_x, near_y, 0, 0.0, 0.0, d_err,
                                            side, &launches, p.max_par, true));
         VPM_CUDA_TRY(cudaEventRecord(join2, side));
-        VPM_CUDA_TRY(build_ext_lists2d(tree, lists, p.eps, d_err, st, &launches));
+        VPM_CUDA_TRY(cudaStreamWaitEvent(side2, fork2, 0));
+        VPM_CUDA_TRY(build_ext_lists2d(tree, lists, p.eps, d_err, side2, &launches));
+        VPM_CUDA_TRY(cudaEventRecord(join3, side2));
         VPM_CUDA_TRY(fmm2d_upward(tree, ex2, p.p, d_err, st, &launches));
+        VPM_CUDA_TRY(cudaStreamWaitEvent(st, join3, 0));
         if (p.precision == VPM_PREC_MIXED && m2l_tc_supported(p.p))
             VPM_CUDA_TRY(fmm2d_m2l_tc(tree, lists, ex2, p.p, tc_rows, tc_ops, d_err, st, &launches));
         else

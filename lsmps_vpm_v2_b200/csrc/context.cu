@@ -46,6 +46,8 @@ Ctx::~Ctx() {
         if (e) cudaEventDestroy(e);
     if (own_stream) cudaStreamDestroy(own_stream);
     if (side) cudaStreamDestroy(side);
+    if (side2) cudaStreamDestroy(side2);
+    if (join3) cudaEventDestroy(join3);
     if (fork2) cudaEventDestroy(fork2);
     if (join2) cudaEventDestroy(join2);
 }
@@ -60,9 +62,11 @@ int Ctx::init(int dev) {
     if (e != cudaSuccess) return fail_cuda(e, "cudaStreamCreate");
     stream = own_stream;
     e = cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&side2, cudaStreamNonBlocking);
     if (e != cudaSuccess) return fail_cuda(e, "cudaStreamCreate");
     e = cudaEventCreateWithFlags(&fork2, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&join2, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&join3, cudaEventDisableTiming);
     if (e != cudaSuccess) return fail_cuda(e, "cudaEventCreate");
     e = cudaMalloc(&d_err, 64);
     if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc");

@@ -51,7 +51,8 @@ struct Ctx {
     // Second stream of a captured evaluation: lists 1/3 and the near field run
     // on it while the main stream builds lists 2/4 and the far field.
     cudaStream_t side = nullptr;
-    cudaEvent_t fork2 = nullptr, join2 = nullptr;
+    cudaStream_t side2 = nullptr;   // lists 2/4 while the main stream runs P2M + M2M
+    cudaEvent_t fork2 = nullptr, join2 = nullptr, join3 = nullptr;
     double *near_x = nullptr, *near_y = nullptr;
     std::string last_error;
     unsigned* d_err = nullptr;

@@ -16,6 +16,8 @@ constexpr int kMaxLevels2D = 31;   // key resolution limit (2 bits per level, 62
 constexpr int kList2Cap = 27;      // list 2 of a cell has at most 27 members
 constexpr int kList4Cap = 16;      // list 4 (coarser leaves next to the parent) slots
 constexpr int kQueueCap = 160;     // BFS queue of TreeCell::intList / extList
+constexpr int kListSlot1 = 32;     // fixed slots of list 1 / list 3 per leaf in the one-pass build
+constexpr int kListSlot3 = 32;
 constexpr int kMaxP = 30;          // largest expansion order
 
 enum CellFlags : uint8_t { CELL_LEAF = 1, CELL_ACTIVE = 2 };
@@ -94,12 +96,15 @@ struct Lists2D {
     uint32_t* l3_cnt;
     uint32_t* l3_off;
     int32_t* l3_src;     // [cap_l3]
+    int32_t* l1_slot;    // [cap_leaves][kListSlot1] one-pass staging of list 1 (nullptr: two passes)
+    int32_t* l3_slot;    // [cap_leaves][kListSlot3]
     int cap_leaves;
     long long cap_l1, cap_l3;
 };
 
 // Scratch of the tree build.
 constexpr int kBBoxBlocks = 296;
+constexpr int kFlatTile = 256;   // particles per block of the flat tree build
 constexpr int kTicketWords = kMaxLevels2D + 2 + 8;  // level tickets, bbox counter, 3 x 2 barrier words
 constexpr int kBarrierWordsAt = kMaxLevels2D + 2;
 
@@ -111,6 +116,10 @@ struct TreeScratch2D {
     uint64_t* lvl_status;   // [kMaxLevels2D + 1][max_tiles]
     unsigned* lvl_ticket;   // [kTicketWords]: level tickets, bbox counter, then the grid-barrier words
     int lvl_max_tiles;      // in tiles of 8 parents
+    uint32_t* pinfo;        // [n] per sorted particle: level it starts a group at, big-level + 1, cell levels
+    uint32_t* tile_cnt;     // [2][kMaxLevels2D + 1][flat_tiles] cells / leaves per tile and level, then offsets
+    uint32_t* level_tot;    // [2][kMaxLevels2D + 1] cells / leaves per level
+    int flat_tiles;         // tiles of kFlatTile particles
     SortScratch sort;
     ScanScratch scan;
 };

@@ -90,6 +90,8 @@ __device__ void int_list(const TreeView& v, int c, double eps, int mode, uint32_
             if (mode == 1) {
                 if ((long long)off1 + k1 < cap1) out1[off1 + k1] = e;
                 else set_err(err, ERR_LIST_CAP);
+            } else if (mode == 2 && (long long)k1 < cap1) {
+                out1[k1] = e;
             }
             ++k1;
             continue;
@@ -111,6 +113,8 @@ __device__ void int_list(const TreeView& v, int c, double eps, int mode, uint32_
                 if (mode == 1) {
                     if ((long long)off3 + k3 < cap3) out3[off3 + k3] = ch;
                     else set_err(err, ERR_LIST_CAP);
+                } else if (mode == 2 && (long long)k3 < cap3) {
+                    out3[k3] = ch;
                 }
                 ++k3;
             }
@@ -118,6 +122,60 @@ __device__ void int_list(const TreeView& v, int c, double eps, int mode, uint32_
     }
     *n1 = k1;
     *n3 = k3;
+}
+
+// Counts and the first kListSlot1 / kListSlot3 entries of lists 1 and 3 of
+// every leaf into fixed slots, in one pass.
+__global__ void int_list_slots(Tree2D t, double eps, Lists2D l, unsigned* err) {
+    if (fatal(err)) return;
+    TreeView v(t);
+    const int nl = t.info->n_leaves;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < l.cap_leaves; i += gridDim.x * blockDim.x) {
+        if (i >= nl) {
+            l.l1_cnt[i] = 0;
+            l.l3_cnt[i] = 0;
+            continue;
+        }
+        uint32_t n1, n3;
+        int_list(v, t.leaf_cells[i], eps, 2, &n1, &n3, l.l1_slot + (size_t)i * kListSlot1,
+                 l.l3_slot + (size_t)i * kListSlot3, kListSlot1, kListSlot3, 0, 0, err);
+        l.l1_cnt[i] = n1;
+        l.l3_cnt[i] = n3;
+    }
+}
+
+// Slots to CSR, one warp per leaf; a leaf whose list outgrew its slots is
+// filled again by int_list_overflow.
+__global__ void int_list_compact(Tree2D t, Lists2D l, unsigned* err) {
+    if (fatal(err)) return;
+    const int nl = t.info->n_leaves;
+    const int lane = threadIdx.x & 31;
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < nl; i += warps) {
+        const uint32_t n1 = l.l1_cnt[i], n3 = l.l3_cnt[i];
+        const uint32_t o1 = l.l1_off[i], o3 = l.l3_off[i];
+        if (n1 <= kListSlot1 && (long long)o1 + n1 <= l.cap_l1) {
+            for (uint32_t k = lane; k < n1; k += 32) l.l1_src[o1 + k] = l.l1_slot[(size_t)i * kListSlot1 + k];
+        }
+        if (n3 <= kListSlot3 && (long long)o3 + n3 <= l.cap_l3) {
+            for (uint32_t k = lane; k < n3; k += 32) l.l3_src[o3 + k] = l.l3_slot[(size_t)i * kListSlot3 + k];
+        }
+    }
+}
+
+__global__ void int_list_overflow(Tree2D t, double eps, Lists2D l, unsigned* err) {
+    if (fatal(err)) return;
+    TreeView v(t);
+    const int nl = t.info->n_leaves;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nl; i += gridDim.x * blockDim.x) {
+        const uint32_t n1 = l.l1_cnt[i], n3 = l.l3_cnt[i];
+        const bool big1 = n1 > kListSlot1 || (long long)l.l1_off[i] + n1 > l.cap_l1;
+        const bool big3 = n3 > kListSlot3 || (long long)l.l3_off[i] + n3 > l.cap_l3;
+        if (!big1 && !big3) continue;
+        uint32_t m1, m3;
+        int_list(v, t.leaf_cells[i], eps, 1, &m1, &m3, l.l1_src, l.l3_src, l.cap_l1, l.cap_l3, l.l1_off[i],
+                 l.l3_off[i], err);
+    }
 }
 
 __global__ void int_list_kernel(Tree2D t, double eps, int mode, Lists2D l, unsigned* err) {
@@ -254,6 +312,18 @@ cudaError_t build_lists2d(const Tree2D& t, Lists2D& l, ScanScratch& scan, double
 cudaError_t build_int_lists2d(const Tree2D& t, Lists2D& l, ScanScratch& scan, double eps, unsigned* err,
                               cudaStream_t st, int* launches) {
     const int gl = std::max(1, std::min(148 * 4, ceil_div(l.cap_leaves, 128)));
+    if (l.l1_slot && l.l3_slot) {
+        int_list_slots<<<gl, 128, 0, st>>>(t, eps, l, err);
+        cudaError_t e = scan_exclusive(l.l1_cnt, l.l1_off, l.cap_leaves, l.l1_off + l.cap_leaves, scan, err, st);
+        if (e != cudaSuccess) return e;
+        e = scan_exclusive(l.l3_cnt, l.l3_off, l.cap_leaves, l.l3_off + l.cap_leaves, scan, err, st);
+        if (e != cudaSuccess) return e;
+        int_list_compact<<<148 * 8, 256, 0, st>>>(t, l, err);
+        int_list_overflow<<<gl, 128, 0, st>>>(t, eps, l, err);
+        list_totals<<<1, 32, 0, st>>>(t, l, err);
+        *launches += 6;
+        return cudaGetLastError();
+    }
     int_list_kernel<<<gl, 128, 0, st>>>(t, eps, 0, l, err);
     *launches += 1;
     cudaError_t e = scan_exclusive(l.l1_cnt, l.l1_off, l.cap_leaves, l.l1_off + l.cap_leaves, scan, err, st);

@@ -155,6 +155,10 @@ extern "C" int vpm_fmm2d_field_device_static(const double* x, const double* y, c
     ts.lvl_status = cv.take<uint64_t>(base, (size_t)(kMaxLevels2D + 1) * lvl_tiles);
     ts.lvl_ticket = cv.take<unsigned>(base, kTicketWords);
     ts.lvl_max_tiles = lvl_tiles;
+    ts.flat_tiles = ceil_div(kStaticMaxN, kFlatTile);
+    ts.pinfo = cv.take<uint32_t>(base, kStaticMaxN);
+    ts.tile_cnt = cv.take<uint32_t>(base, (size_t)2 * (kMaxLevels2D + 1) * ts.flat_tiles);
+    ts.level_tot = cv.take<uint32_t>(base, 2 * (kMaxLevels2D + 1));
     ts.sort.status = cv.take<uint32_t>(base, (size_t)8 * s_tiles * 256);
     ts.sort.tickets = cv.take<unsigned>(base, 8);
     ts.sort.hist = cv.take<uint32_t>(base, 8 * 256);

@@ -422,6 +422,362 @@ tree_levels_coop(Tree2D t, int max_src, int max_par, int* dense, int dense_level
     }
 }
 
+// ---- flat build: every level at once ------------------------------------------
+//
+// With the particles sorted by their level-K Morton key, the cells of level L
+// are the runs ("groups") of equal level-L key prefixes whose parent group is
+// split, and a group is split ("big") when it holds more than max_par
+// particles or more than max_src active ones (treeCell.cpp:1170-1215). A big
+// group's parent is big too (it contains it), so a group is a cell exactly
+// when its parent is big, which needs no level-by-level sweep:
+//   lvl(i)   the first level at which particle i starts a group
+//            (1 + shared leading key digits of particles i-1 and i);
+//   bigL(i)  the deepest level at which the group starting at i is big: the
+//            group holds particle i + max_par, or the (max_src+1)-th active
+//            particle from i, iff the keys share that many leading digits;
+//   cells    particle i starts the cells at levels lvl(i) .. min(K,
+//            max(lvl(i), bigL(i) + 1)) when the parent group of its first
+//            one (the level lvl(i)-1 group containing i, found by search) is
+//            big; the deepest of them is a leaf unless it is big.
+// Cell and leaf indices then come from per-tile, per-level counts (scan over
+// tiles, in tile order = Morton order within each level).
+
+__device__ __forceinline__ int lcp_levels(uint64_t a, uint64_t b, int K) {
+    const uint64_t x = a ^ b;
+    if (x == 0) return K;
+    const int m = 63 - __clzll((long long)x);
+    return (2 * K - 1 - m) >> 1;
+}
+
+// Smallest m in [lo, hi] with a[m] >= target, or hi + 1 (a nondecreasing):
+// galloping from lo, then bisection.
+__device__ __forceinline__ int gallop_ge(const uint32_t* __restrict__ a, int lo, int hi, uint32_t target) {
+    if (lo > hi) return hi + 1;
+    if (a[lo] >= target) return lo;
+    int prev = lo, step = 1;
+    int cur = lo + 1;
+    while (cur <= hi && a[cur] < target) {
+        prev = cur;
+        step <<= 1;
+        cur = lo + step;
+    }
+    int L = prev + 1, R = min(cur, hi + 1);  // answer in [L, R]
+    while (L < R) {
+        const int mid = (L + R) >> 1;
+        if (a[mid] >= target) R = mid;
+        else L = mid + 1;
+    }
+    return L;
+}
+
+// First j in (i, lim] with key prefix (>> sh) different from particle i's,
+// or lim (the group is known to end at or before lim; bisection).
+__device__ __forceinline__ int group_end(const uint64_t* __restrict__ key, int i, int lim, int sh) {
+    const uint64_t v = key[i] >> sh;
+    int L = i + 1, R = lim;
+    while (L < R) {
+        const int mid = (L + R) >> 1;
+        if ((key[mid] >> sh) == v) L = mid + 1;
+        else R = mid;
+    }
+    return L;
+}
+
+// First j <= i with the same key prefix (>> sh) as particle i (bisection).
+__device__ __forceinline__ int group_start(const uint64_t* __restrict__ key, int i, int sh) {
+    const uint64_t v = key[i] >> sh;
+    int L = 0, R = i;
+    while (L < R) {
+        const int mid = (L + R) >> 1;
+        if ((key[mid] >> sh) == v) R = mid;
+        else L = mid + 1;
+    }
+    return L;
+}
+
+__device__ __forceinline__ uint32_t compact2(uint64_t x) {
+    x &= 0x5555555555555555ull;
+    x = (x | (x >> 1)) & 0x3333333333333333ull;
+    x = (x | (x >> 2)) & 0x0F0F0F0F0F0F0F0Full;
+    x = (x | (x >> 4)) & 0x00FF00FF00FF00FFull;
+    x = (x | (x >> 8)) & 0x0000FFFF0000FFFFull;
+    x = (x | (x >> 16)) & 0x00000000FFFFFFFFull;
+    return (uint32_t)x;
+}
+
+// pinfo[i] = lvl | (bigL + 1) << 8
+__global__ void __launch_bounds__(kFlatTile)
+flat_bigl(Tree2D t, int max_src, int max_par, uint32_t* __restrict__ pinfo, unsigned* err) {
+    const int n = t.n, K = t.key_levels;
+    const uint64_t* __restrict__ key = t.key;
+    const uint32_t* __restrict__ as = t.actscan;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint64_t ki = key[i];
+        const int lvl = i == 0 ? 1 : lcp_levels(key[i - 1], ki, K) + 1;   // K + 1: equal keys
+        int big = -1;
+        if (i + max_par < n) big = lcp_levels(ki, key[i + max_par], K);
+        const uint32_t target = as[i] + (uint32_t)max_src + 1u;
+        if (as[n] >= target) {
+            // as[m] - as[i] <= m - i, so m >= i + max_src + 1: start the search there
+            const int m = gallop_ge(as, min(n, i + max_src + 1), n, target);  // particle m-1 is that active one
+            big = max(big, lcp_levels(ki, key[m - 1], K));
+        }
+        pinfo[i] = (uint32_t)lvl | ((uint32_t)(big + 1) << 8);
+    }
+}
+
+// The cell levels of every particle (pinfo bits 16..23 first, 24..31 last; 0 =
+// none) and the per-tile counts of cells and leaves of every level.
+__global__ void __launch_bounds__(kFlatTile)
+flat_cells(Tree2D t, uint32_t* __restrict__ pinfo, uint32_t* __restrict__ tile_cnt, int tiles, unsigned* err) {
+    __shared__ unsigned s_c[kMaxLevels2D + 1], s_l[kMaxLevels2D + 1];
+    const int n = t.n, K = t.key_levels;
+    const uint64_t* __restrict__ key = t.key;
+    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        for (int k = threadIdx.x; k <= K; k += blockDim.x) s_c[k] = s_l[k] = 0;
+        __syncthreads();
+        const int i = tile * kFlatTile + threadIdx.x;
+        if (i < n) {
+            const uint32_t w = pinfo[i];
+            const int lvl = (int)(w & 0xff), big = (int)((w >> 8) & 0xff) - 1;
+            int first = 0, last = 0;
+            if (lvl <= K) {
+                bool exists = lvl == 1;
+                if (!exists) {
+                    const int sp = group_start(key, i, 2 * (K - (lvl - 1)));
+                    const int bigp = (int)((pinfo[sp] >> 8) & 0xff) - 1;
+                    exists = bigp >= lvl - 1;
+                }
+                if (exists) {
+                    first = lvl;
+                    last = min(K, max(lvl, big + 1));
+                    if (big >= K) set_err(err, ERR_DEPTH);  // a group of level K cannot be split
+                    for (int L = first; L <= last; ++L) atomicAdd(&s_c[L], 1u);
+                    if (big < last) atomicAdd(&s_l[last], 1u);
+                }
+            }
+            pinfo[i] = (w & 0xffffu) | ((uint32_t)first << 16) | ((uint32_t)last << 24);
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k <= K; k += blockDim.x) {
+            tile_cnt[(size_t)k * tiles + tile] = s_c[k];
+            tile_cnt[(size_t)(kMaxLevels2D + 1 + k) * tiles + tile] = s_l[k];
+        }
+        __syncthreads();
+    }
+}
+
+// One block per (kind, level) row: exclusive scan of the tile counts in place
+// and the row total.
+__global__ void __launch_bounds__(1024)
+flat_scan(uint32_t* __restrict__ tile_cnt, int tiles, uint32_t* __restrict__ level_tot) {
+    __shared__ uint32_t s_w[32];
+    __shared__ uint32_t s_carry;
+    uint32_t* row = tile_cnt + (size_t)blockIdx.x * tiles;
+    if (threadIdx.x == 0) s_carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int b = 0; b < tiles; b += blockDim.x) {
+        const int k = b + threadIdx.x;
+        const uint32_t v = k < tiles ? row[k] : 0u;
+        uint32_t x = v;
+        #pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) s_w[warp] = x;
+        __syncthreads();
+        uint32_t base = 0, tot = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            if (w < warp) base += s_w[w];
+            tot += s_w[w];
+        }
+        const uint32_t carry = s_carry;
+        if (k < tiles) row[k] = carry + base + x - v;
+        __syncthreads();
+        if (threadIdx.x == 0) s_carry = carry + tot;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) level_tot[blockIdx.x] = s_carry;
+}
+
+// Level starts, totals and the root cell (treeCell.cpp:1117-1133).
+__global__ void flat_totals(Tree2D t, const uint32_t* __restrict__ level_tot, unsigned* err) {
+    const int K = t.key_levels;
+    TreeInfo2D* info = t.info;
+    int cells = 1, leaves = 0, depth = 0;
+    info->level_start[0] = 0;
+    info->leaf_start[0] = 0;
+    for (int L = 1; L < kMaxLevels2D + 3; ++L) {
+        info->level_start[L] = cells;
+        info->leaf_start[L] = leaves;
+        if (L <= K) {
+            const int c = (int)level_tot[L], lf = (int)level_tot[kMaxLevels2D + 1 + L];
+            if (c > 0) depth = L;
+            cells += c;
+            leaves += lf;
+        }
+    }
+    info->n_cells = cells;
+    info->n_leaves = leaves;
+    info->depth = depth;
+    if (cells > t.cap_cells) set_err(err, ERR_CELL_CAP);
+    const Geom2D* g = t.geom;
+    t.c_lo[0] = 0;
+    t.c_hi[0] = t.n;
+    const int src = (int)t.actscan[t.n];
+    t.c_src[0] = src;
+    t.c_flags[0] = src != 0 ? CELL_ACTIVE : 0;
+    t.c_parent[0] = -1;
+    t.c_child0[0] = 0x7fffffff;
+    t.c_chmask[0] = 0;
+    t.c_level[0] = 0;
+    t.c_ix[0] = 0;
+    t.c_iy[0] = 0;
+    t.c_code[0] = 0;
+    t.c_leafidx[0] = -1;
+    t.c_cx[0] = xadd(g->pivx, xmul(0.5, g->root));
+    t.c_cy[0] = xadd(g->pivy, xmul(0.5, g->root));
+    if (t.dense) t.dense[0] = 0;
+}
+
+// Cell records (and leaf entries) of every particle's cell levels, indices
+// from the scanned tile counts plus the rank inside the tile.
+__global__ void __launch_bounds__(kFlatTile)
+flat_emit(Tree2D t, const uint32_t* __restrict__ pinfo, const uint32_t* __restrict__ tile_cnt, int tiles,
+          int max_par, unsigned* err) {
+    __shared__ int s_wc[kMaxLevels2D + 1][kFlatTile / 32], s_wl[kMaxLevels2D + 1][kFlatTile / 32];
+    __shared__ int s_lo, s_hi;
+    if (block_fatal(err)) return;
+    const int n = t.n, K = t.key_levels;
+    const TreeInfo2D* info = t.info;
+    const double root = t.geom->root, pivx = t.geom->pivx, pivy = t.geom->pivy;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned below = (1u << lane) - 1u;
+    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const int i = tile * kFlatTile + threadIdx.x;
+        const uint32_t w = i < n ? pinfo[i] : 0u;
+        const int first = (int)((w >> 16) & 0xff), last = (int)(w >> 24), big = (int)((w >> 8) & 0xff) - 1;
+        if (threadIdx.x == 0) {
+            s_lo = kMaxLevels2D + 1;
+            s_hi = 0;
+        }
+        __syncthreads();
+        if (first) {
+            atomicMin(&s_lo, first);
+            atomicMax(&s_hi, last);
+        }
+        __syncthreads();
+        const int Llo = s_lo, Lhi = s_hi;
+        // per-warp counts of every level, then one barrier
+        for (int L = Llo; L <= Lhi; ++L) {
+            const bool has = first && first <= L && L <= last;
+            const bool lf = has && L == last && big < last;
+            const unsigned mc = __ballot_sync(0xffffffffu, has), ml = __ballot_sync(0xffffffffu, lf);
+            if (lane == 0) {
+                s_wc[L][warp] = __popc(mc);
+                s_wl[L][warp] = __popc(ml);
+            }
+        }
+        __syncthreads();
+        for (int L = Llo; L <= Lhi; ++L) {
+            const bool has = first && first <= L && L <= last;
+            const bool lf = has && L == last && big < last;
+            const unsigned mc = __ballot_sync(0xffffffffu, has), ml = __ballot_sync(0xffffffffu, lf);
+            if (!has) continue;
+            int bc = 0, bl = 0;
+            for (int k = 0; k < warp; ++k) {
+                bc += s_wc[L][k];
+                bl += s_wl[L][k];
+            }
+            const int ci = info->level_start[L] + (int)tile_cnt[(size_t)L * tiles + tile] + bc + __popc(mc & below);
+            if (ci >= t.cap_cells) {
+                set_err(err, ERR_CELL_CAP);
+                continue;
+            }
+            const int sh = 2 * (K - L);
+            const uint64_t code = t.key[i] >> sh;
+            const int ix = (int)compact2(code), iy = (int)compact2(code >> 1);
+            const double len = xdiv(root, ldexp(1.0, L));
+            t.c_lo[ci] = i;
+            t.c_flags[ci] = lf ? CELL_LEAF : 0;   // range end, counts and activity: flat_link
+            t.c_child0[ci] = 0x7fffffff;
+            t.c_chmask[ci] = 0;
+            t.c_level[ci] = (uint8_t)L;
+            t.c_ix[ci] = ix;
+            t.c_iy[ci] = iy;
+            t.c_code[ci] = code;
+            t.c_cx[ci] = xadd(pivx, xmul(xadd(0.5, (double)ix), len));
+            t.c_cy[ci] = xadd(pivy, xmul(xadd(0.5, (double)iy), len));
+            if (t.dense && L <= t.dense_levels) t.dense[start_id2(L) + ix + ((int64_t)iy << L)] = ci;
+            if (lf) {
+                const int li = info->leaf_start[L] + (int)tile_cnt[(size_t)(kMaxLevels2D + 1 + L) * tiles + tile] + bl +
+                               __popc(ml & below);
+                t.c_leafidx[ci] = li;
+                t.leaf_cells[li] = ci;
+            } else {
+                t.c_leafidx[ci] = -1;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Range end, source count and activity of every cell (one search per cell,
+// all in parallel; a leaf holds at most max_par particles), then the parent
+// (level L-1 cell holding its prefix), the parent's child mask and first
+// child.
+__global__ void flat_link(Tree2D t, int max_par, unsigned* err) {
+    if (fatal(err)) return;
+    const int nc = t.info->n_cells, n = t.n, K = t.key_levels;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x + 1; c < nc; c += gridDim.x * blockDim.x) {
+        const int L = t.c_level[c];
+        const uint64_t code = t.c_code[c];
+        {
+            const int lo = t.c_lo[c];
+            const bool leaf = t.c_flags[c] & CELL_LEAF;
+            const int hi = group_end(t.key, lo, leaf ? min(n, lo + max_par) : n, 2 * (K - L));
+            const int src = (int)(t.actscan[hi] - t.actscan[lo]);
+            t.c_hi[c] = hi;
+            t.c_src[c] = src;
+            if (src != 0) t.c_flags[c] = (leaf ? CELL_LEAF : 0) | CELL_ACTIVE;
+        }
+        int p = 0;
+        if (L >= 2) {
+            const int px = t.c_ix[c] >> 1, py = t.c_iy[c] >> 1;
+            p = -1;
+            if (t.dense && L - 1 <= t.dense_levels) {
+                p = t.dense[start_id2(L - 1) + px + ((int64_t)py << (L - 1))];
+            } else {
+                int lo = t.info->level_start[L - 1], hi = t.info->level_start[L];
+                const uint64_t pc = code >> 2;
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (t.c_code[mid] < pc) lo = mid + 1;
+                    else hi = mid;
+                }
+                p = lo;
+            }
+            if (p < 0 || p >= nc || t.c_level[p] != L - 1 || t.c_code[p] != (code >> 2)) {
+                set_err(err, ERR_INDEX);
+                continue;
+            }
+        }
+        t.c_parent[c] = p;
+        unsigned* word = reinterpret_cast<unsigned*>(reinterpret_cast<uintptr_t>(&t.c_chmask[p]) & ~(uintptr_t)3);
+        const unsigned shift = 8u * (unsigned)(reinterpret_cast<uintptr_t>(&t.c_chmask[p]) & 3);
+        atomicOr(word, (1u << (unsigned)(code & 3)) << shift);
+        atomicMin(&t.c_child0[p], c);
+    }
+}
+
+__global__ void flat_fix(Tree2D t) {
+    const int nc = t.info->n_cells;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x)
+        if (t.c_child0[c] == 0x7fffffff) t.c_child0[c] = -1;
+}
+
 // Leaf level range (TreeCell::min_level / max_level, treeCell.cpp:1236-1240).
 __global__ void tree_finish2d(TreeInfo2D* info) {
     int mn = -1, mx = -1;
@@ -472,8 +828,32 @@ cudaError_t keys_sort2d(const double* x, const double* y, const double* q, const
     return cudaGetLastError();
 }
 
+cudaError_t levels2d_flat(Tree2D& t, TreeScratch2D& s, int max_src, int max_par, unsigned* err, cudaStream_t st,
+                          int* launches) {
+    const int n = t.n;
+    const int tiles = ceil_div(n, kFlatTile);
+    if (tiles > s.flat_tiles) return cudaErrorInvalidValue;
+    const int grid = std::max(1, std::min(tiles, 148 * 8));
+    flat_bigl<<<grid, kFlatTile, 0, st>>>(t, max_src, max_par, s.pinfo, err);
+    flat_cells<<<grid, kFlatTile, 0, st>>>(t, s.pinfo, s.tile_cnt, tiles, err);
+    flat_scan<<<2 * (kMaxLevels2D + 1), 1024, 0, st>>>(s.tile_cnt, tiles, s.level_tot);
+    flat_totals<<<1, 1, 0, st>>>(t, s.level_tot, err);
+    flat_emit<<<grid, kFlatTile, 0, st>>>(t, s.pinfo, s.tile_cnt, tiles, max_par, err);
+    const int gc = std::max(1, std::min(148 * 8, ceil_div(t.cap_cells, 256)));
+    flat_link<<<gc, 256, 0, st>>>(t, max_par, err);
+    flat_fix<<<gc, 256, 0, st>>>(t);
+    tree_finish2d<<<1, 1, 0, st>>>(t.info);
+    *launches += 8;
+    return cudaGetLastError();
+}
+
 cudaError_t levels2d(Tree2D& t, TreeScratch2D& s, int max_src, int max_par, unsigned* err, cudaStream_t st,
                      int* launches) {
+    return levels2d_flat(t, s, max_src, max_par, err, st, launches);
+}
+
+cudaError_t levels2d_by_level(Tree2D& t, TreeScratch2D& s, int max_src, int max_par, unsigned* err, cudaStream_t st,
+                              int* launches) {
     const int K = t.key_levels;
     cudaError_t e = cudaMemsetAsync(s.lvl_status, 0, sizeof(uint64_t) * (size_t)(K + 1) * s.lvl_max_tiles, st);
     if (e != cudaSuccess) return e;
