@@ -5,9 +5,13 @@ p = 10, leaf caps 50/75).
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--form mixed|fp64]
 
-Prints one JSON line (rank 0). Our arm: `value` is particle velocities per
-second of device-resident evaluations (inputs in HBM, CUDA events on the
-launching stream, L2 flushed by a 256 MiB write between steps); `e2e` is the
+Prints one JSON line (rank 0). Our arm measures both forms - the plain FP64
+form (the reference's caps 50/75 and p = 10) and the mixed form (FP32 near
+field, tensor-core M2L, caps and p from the learned selector for a 1e-4
+target) - with their errors against the FP64 direct sum on 4,096 targets, and
+reports the --form one (default mixed) as the headline: `value` is particle
+velocities per second of device-resident evaluations (inputs in HBM, CUDA
+events on the launching stream, L2 flushed by a 256 MiB write between steps); `e2e` is the
 same metric through the public host API (pinned host buffers, H2D + D2H
 inside the timed region); `roofline` covers the dominant kernel; and
 `cpu_baseline` is the reference's own FMM compiled from its sources
@@ -146,8 +150,8 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"boundary_layer_2d N={x.size} p=10 caps 50/75", "n": int(x.size), "p": 10,
-                   "max_src": 50, "max_par": 75, "parallelism": "replicas"},
+        "config": {"workload": f"boundary_layer_2d N={x.size}", "n": int(x.size), "form": "reference CPU FP64",
+                   "p": 10, "max_src": 50, "max_par": 75, "parallelism": "replicas"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
                          "sample": f"{args.steps} full evaluations (TreeCell::initializeTree + fmm2D::calcField)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -156,11 +160,39 @@ def run_reference(args):
     return 0
 
 
+def max_over_ranks(value: float, world: int, device) -> float:
+    """The maximum of a per-rank float over all ranks (all_reduce MAX)."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def time_steps(ctx, stream, flush, args_fn, steps):
+    """Mean CUDA-event time (ms) of `steps` evaluations, L2 flushed between."""
+    import torch
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    for k in range(steps):
+        flush.fill_(k)
+        starts[k].record(stream)
+        args_fn()
+        ends[k].record(stream)
+    torch.cuda.synchronize()
+    ctx.sync()
+    return float(np.mean([s.elapsed_time(e) for s, e in zip(starts, ends)]))
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
 
     from lsmps_vpm_v2_b200 import Context, default_params, PREC_FP64, PREC_MIXED
+    from lsmps_vpm_v2_b200._lib import lib
+    from lsmps_vpm_v2_b200.selector import Selector
 
     world, rank, local = _dist_env()
     torch.cuda.set_device(local)
@@ -175,8 +207,7 @@ def run_ours(args):
     torch.cuda.set_stream(stream)
     ctx = Context(local)
     ctx.set_stream(stream.cuda_stream)
-    form = args.form
-    prm = default_params(precision=PREC_MIXED if form == "mixed" else PREC_FP64, use_graph=0 if args.no_graph else 1)
+    graph = 0 if args.no_graph else 1
 
     x = torch.from_numpy(wl["x"]).to(dev)
     y = torch.from_numpy(wl["y"]).to(dev)
@@ -186,42 +217,63 @@ def run_ours(args):
     ey = torch.empty(n, dtype=torch.float64, device=dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
 
-    for _ in range(max(args.warmup, 3)):
-        ctx.field2d_device(x, y, q, act, ex, ey, prm)
-    ctx.sync()
+    # ---- the two forms: plain FP64 (reference caps and order) and the mixed
+    # form with the learned (caps, p) for a 1e-4 target (reference pair when
+    # no trained network is present) ----
+    p64 = default_params(precision=PREC_FP64, use_graph=graph)
+    sel = Selector(ctx)
+    t0 = time.perf_counter()
+    have_net = sel.load()
+    feat = sel.features(wl["x"], wl["y"], wl["q"], wl["active"], 1e-4)
+    (ms_, mp_, pp_), _ = sel.choose(feat, 1e-4)
+    t_sel = (time.perf_counter() - t0) * 1e3
+    pmx = default_params(precision=PREC_MIXED, binom=1, max_src=ms_, max_par=mp_, p=pp_, use_graph=graph)
+    forms = {"fp64": p64, "mixed": pmx}
+    headline = args.form
+    prm = forms[headline]
 
-    # ---- timed region: device-resident evaluations ----
+    # ---- accuracy of both forms against the FP64 direct sum (4,096 targets) ----
+    tg = torch.from_numpy(workloads.sample_targets(n, 4096)).to(dev)
+    dx = torch.empty(tg.numel(), dtype=torch.float64, device=dev)
+    dy = torch.empty_like(dx)
+    ctx._check(lib().vpm_direct2d_field_device(ctx._h, x.data_ptr(), y.data_ptr(), q.data_ptr(), act.data_ptr(), n,
+                                               tg.data_ptr(), tg.numel(), dx.data_ptr(), dy.data_ptr()))
+    err = {}
+    for name, p_ in forms.items():
+        ctx.field2d_device(x, y, q, act, ex, ey, p_)
+        ctx.sync()
+        num = torch.sqrt(((ex[tg] - dx) ** 2).sum() + ((ey[tg] - dy) ** 2).sum())
+        den = torch.sqrt((dx * dx).sum() + (dy * dy).sum())
+        err[name] = float((num / den).item())
+
+    # ---- timed regions: device-resident evaluations of both forms ----
     clocks = ClockSampler(local)
     clocks.start()
     time.sleep(0.3)
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    for k in range(args.steps):
-        flush.fill_(k)
-        starts[k].record(stream)
-        ctx.field2d_device(x, y, q, act, ex, ey, prm)
-        ends[k].record(stream)
-    torch.cuda.synchronize()
-    ctx.sync()
-    if world > 1:
-        dist.barrier()
+    ms = {}
+    for name in (["fp64", "mixed"] if headline == "mixed" else ["mixed", "fp64"]):
+        p_ = forms[name]
+        for _ in range(max(args.warmup, 3)):
+            ctx.field2d_device(x, y, q, act, ex, ey, p_)
+        ctx.sync()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ms[name] = time_steps(ctx, stream, flush, lambda: ctx.field2d_device(x, y, q, act, ex, ey, p_), args.steps)
+        if world > 1:
+            dist.barrier()
+        ms[name] = max_over_ranks(ms[name], world, dev)
     clk = clocks.stop()
-    ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    ms_step = float(np.mean(ms))
-    if world > 1:
-        t = torch.tensor([ms_step], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_step = float(t.item())
+    ms_step = ms[headline]
     value = world * n / (ms_step * 1e-3)
+    ctx.field2d_device(x, y, q, act, ex, ey, prm)
+    ctx.sync()
     st = ctx.last_stats()
     launches_per_step = int(st.kernels)
 
-    # ---- stage profile (same workload, per-stage CUDA events) ----
-    # one graph per stage, events between them, evaluations back to back
-    prm_stage = default_params(precision=prm.precision, use_graph=0 if args.no_graph else 2)
+    # ---- stage profile of the headline form (one graph per stage, events between) ----
+    prm_stage = default_params(precision=prm.precision, binom=prm.binom, max_src=prm.max_src, max_par=prm.max_par,
+                               p=prm.p, use_graph=0 if args.no_graph else 2)
     ctx.field2d_device(x, y, q, act, ex, ey, prm_stage)   # capture
     ctx.stage_history(enable=True)
     nprof = max(3, min(args.steps, 40))
@@ -232,6 +284,8 @@ def run_ours(args):
     stage = {f"ms_{nm}": float(np.mean(hist[:, i])) for i, nm in enumerate(ctx.STAGES)}
     stage["ms_total"] = float(np.mean(hist.sum(axis=1)))
     ctx.field2d_device(x, y, q, act, ex, ey, prm)
+    ctx.sync()
+    st = ctx.last_stats()
 
     # ---- end to end through the public host API (pinned buffers) ----
     hx = torch.from_numpy(wl["x"]).pin_memory().numpy()
@@ -250,14 +304,11 @@ def run_ours(args):
         t1 = time.perf_counter()
         if k >= 2:
             e2e_ms.append((t1 - t0) * 1e3)
-    e2e_step = float(np.mean(e2e_ms))
-    if world > 1:
-        t = torch.tensor([e2e_step], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_step = float(t.item())
+    e2e_step = max_over_ranks(float(np.mean(e2e_ms)), world, dev)
 
     # ---- roofline of the dominant kernel (near-field P2P) ----
     fp64_peak, fp32_peak = ctx.fma_peaks()
+    form = headline
     pairs = int(st.p2p_pairs)
     flops = P2P_FLOPS_PER_PAIR * pairs
     p2p_ms = stage["ms_p2p"]
@@ -276,11 +327,22 @@ def run_ours(args):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64" if form == "fp64" else "f32+f64", "data": "synthetic",
-        "config": {"workload": f"boundary_layer_2d N={n} p=10 caps 50/75", "n": n, "p": 10, "max_src": 50,
-                   "max_par": 75, "form": form, "parallelism": "replicas" if world > 1 else "single",
+        "vs_baseline": None, "dtype": "f64" if form == "fp64" else "f32+tf32+f64", "data": "synthetic",
+        "config": {"workload": f"boundary_layer_2d N={n}", "n": n, "form": form,
+                   "p": int(prm.p), "max_src": int(prm.max_src), "max_par": int(prm.max_par),
+                   "binomials": "reference 32-bit binComb" if prm.binom == 0 else "exact",
+                   "parallelism": "replicas" if world > 1 else "single",
                    "l2": "256 MiB write between steps (outside the per-step events)",
-                   "launch": "CUDA graph replay" if prm.use_graph else "eager"},
+                   "launch": "CUDA graph replay" if prm.use_graph else "eager",
+                   "mixed_params": "learned selector, target 1e-4" if have_net else "reference pair (no network)",
+                   "selector_ms": t_sel},
+        "forms": {"fp64": {"value": world * n / (ms["fp64"] * 1e-3), "ms_per_step": ms["fp64"],
+                           "rel_l2_vs_direct": err["fp64"], "p": int(p64.p), "caps": [50, 75]},
+                  "mixed": {"value": world * n / (ms["mixed"] * 1e-3), "ms_per_step": ms["mixed"],
+                            "rel_l2_vs_direct": err["mixed"], "p": int(pmx.p),
+                            "caps": [int(pmx.max_src), int(pmx.max_par)]},
+                  "mixed_over_fp64": ms["fp64"] / ms["mixed"],
+                  "direct_sum": "FP64 direct sum on 4,096 sampled targets (vpm_direct2d_field_device)"},
         "e2e": {"value": world * n / (e2e_step * 1e-3), "unit": UNIT, "ms_per_step": e2e_step,
                 "h2d_bytes_per_step": n * (8 * 4 + 1), "d2h_bytes_per_step": n * 16,
                 "api": "vpm_velocity2d (host buffers)"},
@@ -309,7 +371,8 @@ def main():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--form", choices=["mixed", "fp64"], default="fp64")
+    ap.add_argument("--form", choices=["mixed", "fp64"], default="mixed",
+                    help="headline form (both are measured; mixed = learned caps/p, FP32 near field, TC M2L)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-graph", action="store_true", help="launch stage by stage instead of replaying a CUDA graph")
     args = ap.parse_args()
