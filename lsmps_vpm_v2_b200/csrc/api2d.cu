@@ -69,7 +69,6 @@ int Ctx::reserve2d(int n, int cap_cells, int P, long long cap_l1, long long cap_
     cap_l1 = std::max(cap_l1, cap.l1);
     cap_l3 = std::max(cap_l3, cap.l3);
     const int K = kMaxLevels2D;
-    const int lvl_tiles = ceil_div(cap_cells, 8) + 1;   // tiles of 8 parents
     const int s_tiles = sort_tiles(n);
     const int sc_tiles = scan_tiles(std::max(n, cap_cells) + 1);
     Layout2D L;
@@ -80,7 +79,7 @@ int Ctx::reserve2d(int n, int cap_cells, int P, long long cap_l1, long long cap_
     size_t o_actscan = L.take<uint32_t>((size_t)n + 1);
     size_t o_keyalt = L.take<uint64_t>(n), o_valalt = L.take<uint32_t>(n), o_actu = L.take<uint32_t>(n);
     size_t o_bbox = L.take<double>(kBBoxBlocks * 4);
-    size_t o_lstat = L.take<uint64_t>((size_t)(K + 1) * lvl_tiles), o_ltick = L.take<unsigned>(kTicketWords);
+    size_t o_ltick = L.take<unsigned>(kTicketWords);
     const int flat_tiles = ceil_div(n, kFlatTile);
     size_t o_pinfo = L.take<uint32_t>(n), o_tcnt = L.take<uint32_t>((size_t)2 * (K + 1) * flat_tiles),
            o_ltot = L.take<uint32_t>(2 * (K + 1));
@@ -128,7 +127,7 @@ int Ctx::reserve2d(int n, int cap_cells, int P, long long cap_l1, long long cap_
     tree.pact = (uint8_t*)P_(o_pact); tree.actscan = (uint32_t*)P_(o_actscan);
     ts.key_alt = (uint64_t*)P_(o_keyalt); ts.val_alt = (uint32_t*)P_(o_valalt); ts.act_u32 = (uint32_t*)P_(o_actu);
     ts.bbox_partial = (double*)P_(o_bbox);
-    ts.lvl_status = (uint64_t*)P_(o_lstat); ts.lvl_ticket = (unsigned*)P_(o_ltick); ts.lvl_max_tiles = lvl_tiles;
+    ts.lvl_ticket = (unsigned*)P_(o_ltick);
     ts.pinfo = (uint32_t*)P_(o_pinfo); ts.tile_cnt = (uint32_t*)P_(o_tcnt); ts.level_tot = (uint32_t*)P_(o_ltot);
     ts.flat_tiles = flat_tiles;
     ts.sort.status = (uint32_t*)P_(o_sstat); ts.sort.tickets = (unsigned*)P_(o_stick);

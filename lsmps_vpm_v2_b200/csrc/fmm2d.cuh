@@ -113,9 +113,7 @@ struct TreeScratch2D {
     uint64_t* key_alt;
     uint32_t* val_alt;
     uint32_t* act_u32;
-    uint64_t* lvl_status;   // [kMaxLevels2D + 1][max_tiles]
-    unsigned* lvl_ticket;   // [kTicketWords]: level tickets, bbox counter, then the grid-barrier words
-    int lvl_max_tiles;      // in tiles of 8 parents
+    unsigned* lvl_ticket;   // [kTicketWords]: bbox counter at kMaxLevels2D + 1, then the grid-barrier words
     uint32_t* pinfo;        // [n] per sorted particle: level it starts a group at, big-level + 1, cell levels
     uint32_t* tile_cnt;     // [2][kMaxLevels2D + 1][flat_tiles] cells / leaves per tile and level, then offsets
     uint32_t* level_tot;    // [2][kMaxLevels2D + 1] cells / leaves per level

@@ -53,16 +53,6 @@ __device__ __forceinline__ double rcp_nr(double a) {
     return y;
 }
 
-__device__ __forceinline__ double2 ldcg2(const double2* p) { return __ldcg(p); }
-
-__device__ __forceinline__ double2 warp_sum2(double2 v) {
-    #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
-        v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
-    }
-    return v;
-}
 
 // ---- upward pass -----------------------------------------------------------
 
@@ -106,6 +96,10 @@ p2m2d(Tree2D t, double2* __restrict__ a, int P, unsigned* err) {
     }
 }
 
+// Warps per block of the level kernels (M2M, L2L): the cooperative loops run
+// one 256-thread block per SM, so a grid barrier has 148 arrivals.
+constexpr int kLevelWarps = 8;
+
 // M2M into the active non-leaf cells of level L (fmm2D.cpp:309-379). A warp
 // holds G = 32/(P+1) cells, lane (g, p) computing a_p of cell g by Horner's
 // rule in t = z_child - z_parent for all children at once (independent
@@ -115,8 +109,8 @@ p2m2d(Tree2D t, double2* __restrict__ a, int P, unsigned* err) {
 // level below was written by other blocks of the same launch.
 __device__ __forceinline__ void m2m_level_body(const Tree2D& t, double2* __restrict__ a,
                                                const double* __restrict__ coef, int P, int L) {
-    __shared__ double2 s_child[4][4][32];  // [warp][child][g * (P+1) + k]
-    __shared__ double2 s_tt[4][4][16];     // [warp][child][g]
+    __shared__ double2 s_child[kLevelWarps][4][32];  // [warp][child][g * (P+1) + k]
+    __shared__ double2 s_tt[kLevelWarps][4][16];     // [warp][child][g]
     const double* g_m2m = coef + kCoefM2M;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int Q = P + 1, G = 32 / Q, g = lane / Q, k = lane - g * Q;
@@ -179,7 +173,7 @@ m2m_level2d(Tree2D t, double2* __restrict__ a, const double* __restrict__ coef, 
 
 // All M2M levels (depth-1 down to 1) in one cooperative launch, a grid
 // barrier between levels.
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(32 * kLevelWarps)
 m2m_levels_coop(Tree2D t, double2* __restrict__ a, const double* __restrict__ coef, int P, unsigned* bar,
                 unsigned* err) {
     const int depth = t.info->depth;
@@ -198,7 +192,7 @@ m2m_levels_coop(Tree2D t, double2* __restrict__ a, const double* __restrict__ co
 // L2 (ld.cg).
 __device__ __forceinline__ void l2l_level_body(const Tree2D& t, double2* __restrict__ b,
                                                const double* __restrict__ coef, int P, int L) {
-    __shared__ double2 s_par[4][32];
+    __shared__ double2 s_par[kLevelWarps][32];
     const double* g_l2l = coef + kCoefL2L;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int Q = P + 1, G = 32 / Q, g = lane / Q, k = lane - g * Q;
@@ -231,7 +225,7 @@ l2l_level2d(Tree2D t, double2* __restrict__ b, const double* __restrict__ coef, 
 }
 
 // All L2L levels (3 down to the depth) in one cooperative launch.
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(32 * kLevelWarps)
 l2l_levels_coop(Tree2D t, double2* __restrict__ b, const double* __restrict__ coef, int P, unsigned* bar,
                 unsigned* err) {
     const int depth = t.info->depth;
@@ -412,7 +406,8 @@ m2l2d_op(Tree2D t, Lists2D l, const double2* __restrict__ a, double2* __restrict
 
 // ---- leaf evaluation: M2P (list 3), L2P --------------------------------------
 
-constexpr int kEvalThreads = 64;
+constexpr int kEvalWarps = 4;   // one warp per leaf
+constexpr int kEvalThreads = 32 * kEvalWarps;
 
 // Far field of every particle of a leaf: M2P over list 3 (fmm2D.cpp:1040-1066)
 // and L2P of the leaf's complete local expansion (fmm2D.cpp:1076-1093). Cells
@@ -422,19 +417,20 @@ eval2d(Tree2D t, Lists2D l, const double2* __restrict__ a, const double2* __rest
        double* __restrict__ fy, int P, const double* __restrict__ nx, const double* __restrict__ ny,
        double* __restrict__ out0, double* __restrict__ out1, int velocity, double u_inf, double v_inf,
        unsigned* err) {
-    __shared__ double2 s_b[W];
+    __shared__ double2 s_bw[kEvalWarps][W];
     if (fatal(err)) return;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    double2* s_b = s_bw[wib];
     const int nl = t.info->n_leaves;
-    for (int li = blockIdx.x; li < nl; li += gridDim.x) {
+    for (int li = blockIdx.x * kEvalWarps + wib; li < nl; li += gridDim.x * kEvalWarps) {
         const int c = t.leaf_cells[li];
         const int L = t.c_level[c];
-        if (threadIdx.x <= P)
-            s_b[threadIdx.x] = L >= 2 ? b[(size_t)c * (P + 1) + threadIdx.x] : make_double2(0.0, 0.0);
-        __syncthreads();
+        for (int k = lane; k <= P; k += 32) s_b[k] = L >= 2 ? b[(size_t)c * (P + 1) + k] : make_double2(0.0, 0.0);
+        __syncwarp();
         const int lo = t.c_lo[c], hi = t.c_hi[c];
         const double zx = t.c_cx[c], zy = t.c_cy[c];
         const uint32_t o3 = l.l3_off[li], e3 = l.l3_off[li + 1];
-        for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+        for (int i = lo + lane; i < hi; i += 32) {
             const double x = t.px[i], y = t.py[i];
             double ex = 0.0, ey = 0.0;
             for (uint32_t k = o3; k < e3; ++k) {
@@ -471,7 +467,7 @@ eval2d(Tree2D t, Lists2D l, const double2* __restrict__ a, const double2* __rest
                 fy[i] = ey;
             }
         }
-        __syncthreads();
+        __syncwarp();
     }
 }
 
@@ -596,93 +592,17 @@ __global__ void leaf_relative_f32(Tree2D t, float4* __restrict__ rel, unsigned* 
     }
 }
 
-// FP32 P2P over list 1. Targets and sources are expressed relative to the
-// target leaf's centre: source = (c_src - c_tgt) [FP64 difference, rounded
-// once per source cell] + (x - c_src) [FP32, precomputed], so every pair
-// offset keeps ~1e-7 relative accuracy. Each thread sums one source cell's
-// contributions in FP32 and adds that block sum into an FP64 accumulator
-// (compensated per-target summation). Same mapping as p2p2d (two targets
-// per thread).
+// FP32 reciprocal (hardware approximation, ~1 ulp) of the mixed near field.
+// Targets and sources there are expressed relative to the target leaf's
+// centre: source = (c_src - c_tgt) [FP64 difference, rounded once per source
+// cell] + (x - c_src) [FP32, precomputed], so every pair offset keeps ~1e-7
+// relative accuracy; per-cell FP32 sums go into FP64 per-target accumulators.
 __device__ __forceinline__ float rcp_approx(float a) {
     float r;
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
     return r;
 }
 
-__global__ void __launch_bounds__(kP2PThreads)
-p2p2d_f32(Tree2D t, Lists2D l, const float4* __restrict__ rel, const double* __restrict__ fx,
-          const double* __restrict__ fy, double* __restrict__ out0, double* __restrict__ out1, int velocity,
-          double u_inf, double v_inf, unsigned* err) {
-    __shared__ double s_px[2][kP2PThreads], s_py[2][kP2PThreads];
-    if (fatal(err)) return;
-    const int nl = t.info->n_leaves;
-    for (int li = blockIdx.x; li < nl; li += gridDim.x) {
-        const int c = t.leaf_cells[li];
-        const int lo = t.c_lo[c], hi = t.c_hi[c];
-        const double ccx = t.c_cx[c], ccy = t.c_cy[c];
-        const uint32_t o1 = l.l1_off[li], e1 = l.l1_off[li + 1];
-        for (int tb = lo; tb < hi; tb += 2 * kP2PThreads) {
-            const int T = min(2 * kP2PThreads, hi - tb);
-            const int H = (T + 1) >> 1;
-            const int ns = kP2PThreads / H;
-            const int tt = threadIdx.x % H, split = threadIdx.x / H;
-            const bool on = split < ns;
-            const int ta = tb + tt, tbb = tb + tt + H;
-            const bool hasb = tt + H < T;
-            const float4 ga = rel[ta];
-            const float4 gb = hasb ? rel[tbb] : ga;
-            double exa = 0.0, eya = 0.0, exb = 0.0, eyb = 0.0;
-            if (on) {
-                for (uint32_t k = o1; k < e1; ++k) {
-                    const int sc = l.l1_src[k];
-                    const int s_hi = t.c_hi[sc];
-                    const float ox = (float)(t.c_cx[sc] - ccx), oy = (float)(t.c_cy[sc] - ccy);
-                    const float ax = ga.x - ox, ay = ga.y - oy, bx = gb.x - ox, by = gb.y - oy;
-                    float pxa = 0.f, pya = 0.f, pxb = 0.f, pyb = 0.f;
-                    if (sc != c) {
-                        for (int j = t.c_lo[sc] + split; j < s_hi; j += ns) {
-                            const float4 sv = __ldg(rel + j);
-                            const float dxa = ax - sv.x, dya = ay - sv.y, dxb = bx - sv.x, dyb = by - sv.y;
-                            const float fa = sv.z * rcp_approx(fmaf(dxa, dxa, dya * dya));
-                            const float fb = sv.z * rcp_approx(fmaf(dxb, dxb, dyb * dyb));
-                            pxa = fmaf(fa, dxa, pxa);
-                            pya = fmaf(fa, dya, pya);
-                            pxb = fmaf(fb, dxb, pxb);
-                            pyb = fmaf(fb, dyb, pyb);
-                        }
-                    } else {
-                        for (int j = t.c_lo[sc] + split; j < s_hi; j += ns) {
-                            const float4 sv = __ldg(rel + j);
-                            const float dxa = ax - sv.x, dya = ay - sv.y, dxb = bx - sv.x, dyb = by - sv.y;
-                            const float fa = (j == ta) ? 0.f : sv.z * rcp_approx(fmaf(dxa, dxa, dya * dya));
-                            const float fb = (j == tbb) ? 0.f : sv.z * rcp_approx(fmaf(dxb, dxb, dyb * dyb));
-                            pxa = fmaf(fa, dxa, pxa);
-                            pya = fmaf(fa, dya, pya);
-                            pxb = fmaf(fb, dxb, pxb);
-                            pyb = fmaf(fb, dyb, pyb);
-                        }
-                    }
-                    exa += (double)pxa; eya += (double)pya;
-                    exb += (double)pxb; eyb += (double)pyb;
-                }
-            }
-            if (on && split > 0) {
-                s_px[0][threadIdx.x] = exa; s_py[0][threadIdx.x] = eya;
-                s_px[1][threadIdx.x] = exb; s_py[1][threadIdx.x] = eyb;
-            }
-            __syncthreads();
-            if (split == 0) {
-                for (int s2 = 1; s2 < ns; ++s2) {
-                    exa += s_px[0][s2 * H + tt]; eya += s_py[0][s2 * H + tt];
-                    exb += s_px[1][s2 * H + tt]; eyb += s_py[1][s2 * H + tt];
-                }
-                p2p_store(t, ta, exa, eya, fx, fy, out0, out1, velocity, u_inf, v_inf, err);
-                if (hasb) p2p_store(t, tbb, exb, eyb, fx, fy, out0, out1, velocity, u_inf, v_inf, err);
-            }
-            __syncthreads();
-        }
-    }
-}
 
 // ---- TMA-staged FP32 P2P ------------------------------------------------------
 
@@ -766,12 +686,14 @@ struct P2PF32 {
     using Acc = float;
     static __device__ __forceinline__ void shift(Elem& e, float ox, float oy) { e.x += ox; e.y += oy; }
     static __device__ __forceinline__ float inv(float r2) { return rcp_approx(r2); }
+    static constexpr int kMinBlocks = 8;   // <= 64 registers: 32 warps per SM
 };
 struct P2PF64 {
     using Elem = double4;  // (x, y, q, -) in FP64, absolute coordinates
     using Acc = double;
     static __device__ __forceinline__ void shift(Elem&, float, float) {}
     static __device__ __forceinline__ double inv(double r2) { return rcp_nr(r2); }
+    static constexpr int kMinBlocks = 5;   // <= 102 registers
 };
 
 // Stage the list-1 sources of leaf `li` into `buf` with one bulk copy per
@@ -831,8 +753,11 @@ __device__ __forceinline__ void pair_loop4(const typename Tr::Elem* __restrict__
         #pragma unroll
         for (int k = 0; k < kTPT; ++k) { px[k] = 0; py[k] = 0; }
         if (!has_self) {
+            // the next source is loaded while this one is computed
+            typename Tr::Elem nv = jb < je ? buf[jb] : typename Tr::Elem{};
             for (int j = jb; j < je; j += ns) {
-                const typename Tr::Elem sv = buf[j];
+                const typename Tr::Elem sv = nv;
+                if (j + ns < je) nv = buf[j + ns];
                 const A sx = (A)sv.x, sy = (A)sv.y, sq = (A)sv.z;
                 #pragma unroll
                 for (int k = 0; k < kTPT; ++k) {
@@ -1010,14 +935,18 @@ p2p2d_tma(Tree2D t, Lists2D l, const typename Tr::Elem* __restrict__ src, const 
 // a per-warp shared-memory tile. FP32 form: coordinates relative to the
 // target leaf (source-cell offset rounded once per cell).
 constexpr int kWarpP2PWarps = 4;
+constexpr int kP2PMeta = 64;   // list-1 cells staged per leaf (longer lists read them directly)
 
 template <class Tr>
-__global__ void __launch_bounds__(32 * kWarpP2PWarps)
+__global__ void __launch_bounds__(32 * kWarpP2PWarps, Tr::kMinBlocks)
 p2p2d_warp(Tree2D t, Lists2D l, const typename Tr::Elem* __restrict__ src, const double* __restrict__ fx,
            const double* __restrict__ fy, double* __restrict__ out0, double* __restrict__ out1, int velocity,
            double u_inf, double v_inf, unsigned* err) {
     using Elem = typename Tr::Elem;
     __shared__ double s_red[kWarpP2PWarps][2 * kTPT][32];
+    // list-1 cells of the warp's leaf: first/last slot, FP32-rounded centre
+    // offset, loaded by the whole warp at once (one round of latency)
+    __shared__ int4 s_meta[kWarpP2PWarps][kP2PMeta];
     if (fatal(err)) return;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int nl = t.info->n_leaves;
@@ -1027,6 +956,21 @@ p2p2d_warp(Tree2D t, Lists2D l, const typename Tr::Elem* __restrict__ src, const
         const int lo = t.c_lo[c], hi = t.c_hi[c];
         const double ccx = t.c_cx[c], ccy = t.c_cy[c];
         const uint32_t o1 = l.l1_off[li], e1 = l.l1_off[li + 1];
+        const int n1 = (int)(e1 - o1);
+        const bool meta = n1 <= kP2PMeta;
+        if (meta) {
+            for (int k = lane; k < n1; k += 32) {
+                const int sc = l.l1_src[o1 + k];
+                float ox = 0.f, oy = 0.f;
+                if (rel) {
+                    ox = (float)(t.c_cx[sc] - ccx);
+                    oy = (float)(t.c_cy[sc] - ccy);
+                }
+                s_meta[wib][k] = make_int4(t.c_lo[sc], sc == c ? -t.c_hi[sc] - 1 : t.c_hi[sc], __float_as_int(ox),
+                                           __float_as_int(oy));
+            }
+            __syncwarp();
+        }
         for (int tb = lo; tb < hi; tb += kTPT * 32) {
             const int T = min(kTPT * 32, hi - tb);
             const int H = (T + kTPT - 1) / kTPT;
@@ -1047,12 +991,25 @@ p2p2d_warp(Tree2D t, Lists2D l, const typename Tr::Elem* __restrict__ src, const
             }
             if (on) {
                 for (uint32_t kk = o1; kk < e1; ++kk) {
-                    const int sc = l.l1_src[kk];
-                    const int slo = t.c_lo[sc], shi = t.c_hi[sc];
+                    int slo, shi;
+                    bool own;
                     double sx = 0.0, sy = 0.0;
-                    if (rel) {
-                        sx = (double)(float)(t.c_cx[sc] - ccx);
-                        sy = (double)(float)(t.c_cy[sc] - ccy);
+                    if (meta) {
+                        const int4 m = s_meta[wib][kk - o1];
+                        slo = m.x;
+                        own = m.y < 0;
+                        shi = own ? -m.y - 1 : m.y;
+                        sx = (double)__int_as_float(m.z);
+                        sy = (double)__int_as_float(m.w);
+                    } else {
+                        const int sc = l.l1_src[kk];
+                        slo = t.c_lo[sc];
+                        shi = t.c_hi[sc];
+                        own = sc == c;
+                        if (rel) {
+                            sx = (double)(float)(t.c_cx[sc] - ccx);
+                            sy = (double)(float)(t.c_cy[sc] - ccy);
+                        }
                     }
                     double tx2[kTPT], ty2[kTPT];
                     int self[kTPT];
@@ -1060,7 +1017,7 @@ p2p2d_warp(Tree2D t, Lists2D l, const typename Tr::Elem* __restrict__ src, const
                     for (int k = 0; k < kTPT; ++k) {
                         tx2[k] = tx[k] - sx;
                         ty2[k] = ty[k] - sy;
-                        self[k] = (sc == c) ? ti[k] : -1;
+                        self[k] = own ? ti[k] : -1;
                     }
                     pair_loop4<Tr>(src, slo + split, shi, ns, tx2, ty2, self, ex, ey);
                 }
@@ -1114,10 +1071,6 @@ cudaError_t launch_p2p_tma(const Tree2D& t, const Lists2D& l, const typename Tr:
     return cudaGetLastError();
 }
 
-__global__ void zero_u32(unsigned* p, int n) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = 0;
-}
-
 }  // namespace
 
 cudaError_t set_coefficients2d(int P, bool exact, double* dst, cudaStream_t st) {
@@ -1149,7 +1102,8 @@ cudaError_t fmm2d_upward(const Tree2D& t, Expansions2D& e, int P, unsigned* err,
     *launches += 1;
     if (t.gbar) {
         int grid = 0;
-        r = launch_coop(m2m_levels_coop, 128, 0, st, 4, &grid, t, e.a, (const double*)e.coef, P, t.gbar + 2, err);
+        r = launch_coop(m2m_levels_coop, 32 * kLevelWarps, 0, st, 1, &grid, t, e.a, (const double*)e.coef, P,
+                        t.gbar + 2, err);
         if (r == cudaSuccess) {
             *launches += 1;
             return cudaGetLastError();
@@ -1205,8 +1159,8 @@ cudaError_t fmm2d_m2l_only(const Tree2D& t, const Lists2D& l, Expansions2D& e, i
 cudaError_t fmm2d_l2l(const Tree2D& t, Expansions2D& e, int P, unsigned* err, cudaStream_t st, int* launches) {
     if (t.gbar) {
         int grid = 0;
-        cudaError_t r = launch_coop(l2l_levels_coop, 128, 0, st, 4, &grid, t, e.b, (const double*)e.coef, P,
-                                    t.gbar + 4, err);
+        cudaError_t r = launch_coop(l2l_levels_coop, 32 * kLevelWarps, 0, st, 1, &grid, t, e.b,
+                                    (const double*)e.coef, P, t.gbar + 4, err);
         if (r == cudaSuccess) {
             *launches += 1;
             return cudaGetLastError();

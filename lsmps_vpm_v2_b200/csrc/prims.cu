@@ -124,19 +124,6 @@ rs_histogram(const K* __restrict__ keys, int n, int passes, uint32_t* hist) {
     }
 }
 
-// hist[p][d] -> exclusive offsets within pass p (one block of 256 threads).
-__global__ void rs_hist_scan(uint32_t* hist, int passes) {
-    __shared__ uint64_t warp_sums[8];
-    for (int p = 0; p < passes; ++p) {
-        uint64_t agg;
-        uint64_t v = hist[p * 256 + threadIdx.x];
-        uint64_t e = block_excl_scan(v, warp_sums, &agg);
-        __syncthreads();
-        hist[p * 256 + threadIdx.x] = (uint32_t)e;
-        __syncthreads();
-    }
-}
-
 // One 8-bit digit pass. Items are arranged warp-striped: item j of lane l in
 // warp w is tile_base + w*256 + j*32 + l, so processing j in order ranks keys
 // in index order (stability). The tile is first reordered by digit in shared
@@ -145,7 +132,7 @@ __global__ void rs_hist_scan(uint32_t* hist, int passes) {
 template <typename K>
 __global__ void __launch_bounds__(kSortThreads)
 rs_pass(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* __restrict__ kout,
-        uint32_t* __restrict__ vout, int n, int shift, const uint32_t* __restrict__ digit_offset,
+        uint32_t* __restrict__ vout, int n, int shift, const uint32_t* __restrict__ digit_hist,
         uint32_t* status, unsigned* ticket, unsigned* err) {
     constexpr int kSortItems = SortItems<K>::value;
     constexpr int kSortTile = kSortThreads * kSortItems;
@@ -230,7 +217,11 @@ rs_pass(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* __restri
         }
         store_volatile32(&st[d], kRsP | (prefix + run));
     }
-    s_base[d] = digit_offset[d] + prefix - local;  // modulo 2^32; adding a tile-local index gives the output index
+    // exclusive scan of the pass's global digit histogram (every block: 256 values)
+    __syncthreads();   // s_warp_sums is reused
+    uint64_t agg2;
+    const uint32_t dig_off = (uint32_t)block_excl_scan(digit_hist[d], s_warp_sums, &agg2);
+    s_base[d] = dig_off + prefix - local;  // modulo 2^32; adding a tile-local index gives the output index
     __syncthreads();
     #pragma unroll
     for (int j = 0; j < kSortItems; ++j) {
@@ -270,8 +261,7 @@ cudaError_t sort_pairs(K** keys, uint32_t** vals, K* keys_alt, uint32_t* vals_al
     int hblocks = std::min(1184, ceil_div(n, 256 * 8));
     if (hblocks < 1) hblocks = 1;
     rs_histogram<K><<<hblocks, 256, 0, st>>>(*keys, n, passes, s.hist);
-    rs_hist_scan<<<1, 256, 0, st>>>(s.hist, passes);
-    if (launches) *launches += 2;
+    if (launches) *launches += 1;
     K* ka = *keys;
     uint32_t* va = *vals;
     K* kb = keys_alt;

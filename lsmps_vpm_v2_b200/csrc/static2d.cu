@@ -132,7 +132,6 @@ extern "C" int vpm_fmm2d_field_device_static(const double* x, const double* y, c
     // Carve the static array (same buffers as the context arena).
     char* base = (char*)base_ptr;
     const size_t C = kStaticMaxCells;
-    const int lvl_tiles = ceil_div(kStaticMaxCells, 8) + 1;
     const int s_tiles = sort_tiles(kStaticMaxN);
     const int sc_tiles = scan_tiles(kStaticMaxCells + 1);
     Carve cv;
@@ -152,9 +151,7 @@ extern "C" int vpm_fmm2d_field_device_static(const double* x, const double* y, c
     ts.val_alt = cv.take<uint32_t>(base, kStaticMaxN);
     ts.act_u32 = cv.take<uint32_t>(base, kStaticMaxN);
     ts.bbox_partial = cv.take<double>(base, kBBoxBlocks * 4);
-    ts.lvl_status = cv.take<uint64_t>(base, (size_t)(kMaxLevels2D + 1) * lvl_tiles);
     ts.lvl_ticket = cv.take<unsigned>(base, kTicketWords);
-    ts.lvl_max_tiles = lvl_tiles;
     ts.flat_tiles = ceil_div(kStaticMaxN, kFlatTile);
     ts.pinfo = cv.take<uint32_t>(base, kStaticMaxN);
     ts.tile_cnt = cv.take<uint32_t>(base, (size_t)2 * (kMaxLevels2D + 1) * ts.flat_tiles);

@@ -20,21 +20,6 @@ namespace vpm {
 
 namespace {
 
-constexpr int kLvlWarps = 8;                 // parents per tile, one warp each
-constexpr int kLvlThreads = 32 * kLvlWarps;
-constexpr uint64_t kLvA = 1ull << 62;
-constexpr uint64_t kLvP = 2ull << 62;
-constexpr uint64_t kLvMask = (1ull << 62) - 1;
-
-__device__ __forceinline__ uint64_t ld_relaxed(const uint64_t* p) {
-    uint64_t v;
-    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ void st_relaxed(uint64_t* p, uint64_t v) {
-    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-
 // Bounding box and root geometry (treeCell.cpp:1061-1092).
 __global__ void __launch_bounds__(256)
 bbox2d(const double* __restrict__ x, const double* __restrict__ y, int n, double exp_pct, int key_levels,
@@ -153,272 +138,6 @@ __global__ void gather2d(const double* __restrict__ x, const double* __restrict_
         uint8_t a = act[j] ? 1 : 0;
         pact[i] = a;
         act_u32[i] = a;
-    }
-}
-
-// Root cell (treeCell.cpp:1117-1133): never a leaf.
-__global__ void tree_root2d(Tree2D t) {
-    const Geom2D* g = t.geom;
-    TreeInfo2D* info = t.info;
-    t.c_lo[0] = 0;
-    t.c_hi[0] = t.n;
-    int src = (int)t.actscan[t.n];
-    t.c_src[0] = src;
-    t.c_flags[0] = src != 0 ? CELL_ACTIVE : 0;
-    t.c_parent[0] = -1;
-    t.c_child0[0] = -1;
-    t.c_chmask[0] = 0;
-    t.c_level[0] = 0;
-    t.c_ix[0] = 0;
-    t.c_iy[0] = 0;
-    t.c_code[0] = 0;
-    t.c_leafidx[0] = -1;
-    t.c_cx[0] = xadd(g->pivx, xmul(0.5, g->root));
-    t.c_cy[0] = xadd(g->pivy, xmul(0.5, g->root));
-    if (t.dense) t.dense[0] = 0;
-    for (int L = 0; L < kMaxLevels2D + 3; ++L) {
-        info->level_start[L] = L == 0 ? 0 : 1;
-        info->leaf_start[L] = 0;
-    }
-    info->n_cells = 1;
-    info->n_leaves = 0;
-    info->depth = 0;
-}
-
-// The three inner child boundaries of a parent range [lo, hi): the first
-// index whose level code (key >> shift) is >= v+1, v+2 and v+3. The three
-// 33-ary searches run interleaved, each lane issuing up to three independent
-// loads per round, so the warp waits on one chain of dependent loads instead
-// of three; the first round's probes are shared. Results are warp-uniform.
-__device__ __forceinline__ void warp_split3(const uint64_t* __restrict__ key, int lo, int hi, int shift, uint64_t v,
-                                            int lane, int& r1, int& r2, int& r3) {
-    int a[3] = {lo, lo, lo}, b[3] = {hi, hi, hi};
-    if (hi - lo > 32) {
-        const long long len = hi - lo;
-        const uint64_t kv = key[lo + (int)(((long long)(lane + 1) * len) / 33)] >> shift;
-        #pragma unroll
-        for (int t = 0; t < 3; ++t) {
-            const unsigned m = __ballot_sync(0xffffffffu, kv >= v + 1 + t);
-            if (m == 0) {
-                a[t] = lo + (int)((32ll * len) / 33) + 1;
-            } else {
-                const int f = __ffs(m) - 1;
-                b[t] = lo + (int)(((long long)(f + 1) * len) / 33);
-                if (f > 0) a[t] = lo + (int)(((long long)f * len) / 33) + 1;
-            }
-        }
-    }
-    for (;;) {
-        bool more = false;
-        uint64_t kv[3];
-        #pragma unroll
-        for (int t = 0; t < 3; ++t) {
-            const long long len = b[t] - a[t];
-            kv[t] = 0;
-            if (len > 32) {
-                more = true;
-                kv[t] = key[a[t] + (int)(((long long)(lane + 1) * len) / 33)] >> shift;
-            }
-        }
-        if (!more) break;
-        #pragma unroll
-        for (int t = 0; t < 3; ++t) {
-            const long long len = b[t] - a[t];
-            if (len <= 32) continue;
-            const unsigned m = __ballot_sync(0xffffffffu, kv[t] >= v + 1 + t);
-            const int a0 = a[t];
-            if (m == 0) {
-                a[t] = a0 + (int)((32ll * len) / 33) + 1;
-            } else {
-                const int f = __ffs(m) - 1;
-                b[t] = a0 + (int)(((long long)(f + 1) * len) / 33);
-                if (f > 0) a[t] = a0 + (int)(((long long)f * len) / 33) + 1;
-            }
-        }
-    }
-    int r[3];
-    uint64_t kv[3];
-    #pragma unroll
-    for (int t = 0; t < 3; ++t) {
-        const int pos = a[t] + lane;
-        kv[t] = pos < b[t] ? key[pos] >> shift : 0;
-    }
-    #pragma unroll
-    for (int t = 0; t < 3; ++t) {
-        const int pos = a[t] + lane;
-        const unsigned m = __ballot_sync(0xffffffffu, pos < b[t] && kv[t] >= v + 1 + t);
-        r[t] = m ? a[t] + __ffs(m) - 1 : b[t];
-    }
-    r1 = r[0];
-    r2 = r[1];
-    r3 = r[2];
-}
-
-__device__ __forceinline__ int sel4(int i, int v0, int v1, int v2, int v3) {
-    return i == 0 ? v0 : i == 1 ? v1 : i == 2 ? v2 : v3;
-}
-
-// Cells of level L from the non-leaf cells of level L-1, one warp per parent,
-// kLvlWarps parents per tile. Tiles take ordered tickets and combine their
-// packed (cells, leaves) counts by decoupled look-back, so children are
-// emitted in parent order, i.e. Morton order within the level. Each new cell
-// also lands in the dense lookup grid (indexed by the reference's cell ID)
-// when its level is covered by it.
-//
-// Everything this step reads that an earlier level wrote (level starts,
-// parent cells) is loaded through L2 (ld.cg): in the cooperative kernel all
-// levels run in one launch and L1 is not coherent across blocks.
-__device__ void level_step(const Tree2D& t, int L, int max_src, int max_par, int* dense, int dense_levels,
-                           uint64_t* status, unsigned* ticket, unsigned* err) {
-    __shared__ unsigned s_tile;
-    __shared__ uint64_t s_prefix;
-    __shared__ int s_cnt[kLvlWarps], s_lf[kLvlWarps], s_xc[kLvlWarps], s_xl[kLvlWarps];
-    __shared__ unsigned s_stop;
-    TreeInfo2D* info = t.info;
-    // One read of the error word per block, so the whole block takes the same exit.
-    if (threadIdx.x == 0) s_stop = *(volatile const unsigned*)err & (ERR_CELL_CAP | ERR_TIMEOUT | ERR_NONFINITE);
-    __syncthreads();
-    if (s_stop) return;
-    const int p0 = __ldcg(&info->level_start[L - 1]);
-    const int np = __ldcg(&info->level_start[L]) - p0;
-    const int ntiles = np > 0 ? ceil_div(np, kLvlWarps) : 1;
-    const int base_cell = __ldcg(&info->level_start[L]);
-    const int base_leaf = __ldcg(&info->leaf_start[L]);
-    const int shift = 2 * (t.key_levels - L);
-    const double len = xdiv(t.geom->root, ldexp(1.0, L));
-    const double pivx = t.geom->pivx, pivy = t.geom->pivy;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-
-    for (;;) {
-        if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
-        __syncthreads();
-        const int tile = (int)s_tile;
-        if (tile >= ntiles) return;
-        const int pi = tile * kLvlWarps + warp;
-        const int p = p0 + pi;
-        const bool nonleaf = pi < np && !(__ldcg(&t.c_flags[p]) & CELL_LEAF);   // warp-uniform
-        int b0 = 0, b1 = 0, b2 = 0, b3 = 0, b4 = 0;
-        bool has = false, leaf = false;
-        unsigned mask = 0, lmask = 0;
-        int clo = 0, chi = 0, src = 0;
-        if (nonleaf) {
-            b0 = __ldcg(&t.c_lo[p]);
-            b4 = __ldcg(&t.c_hi[p]);
-            const uint64_t pc = __ldcg(&t.c_code[p]) << 2;
-            warp_split3(t.key, b0, b4, shift, pc, lane, b1, b2, b3);
-            clo = sel4(lane, b0, b1, b2, b3);
-            chi = sel4(lane, b1, b2, b3, b4);
-            has = lane < 4 && chi > clo;
-            if (has) {
-                src = (int)(t.actscan[chi] - t.actscan[clo]);
-                leaf = src <= max_src && (chi - clo) <= max_par;
-            }
-            mask = __ballot_sync(0xffffffffu, has);
-            lmask = __ballot_sync(0xffffffffu, leaf);
-        }
-        if (lane == 0) {
-            s_cnt[warp] = __popc(mask);
-            s_lf[warp] = __popc(lmask);
-        }
-        __syncthreads();
-        if (warp == 0) {
-            int c = lane < kLvlWarps ? s_cnt[lane] : 0, lf = lane < kLvlWarps ? s_lf[lane] : 0;
-            int ic = c, il = lf;
-            #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                int yc = __shfl_up_sync(0xffffffffu, ic, o), yl = __shfl_up_sync(0xffffffffu, il, o);
-                if (lane >= o) { ic += yc; il += yl; }
-            }
-            if (lane < kLvlWarps) { s_xc[lane] = ic - c; s_xl[lane] = il - lf; }
-            const uint64_t agg = (uint64_t)__shfl_sync(0xffffffffu, ic, 31) |
-                                 ((uint64_t)__shfl_sync(0xffffffffu, il, 31) << 31);
-            uint64_t prefix = 0;
-            if (tile == 0) {
-                if (lane == 0) st_relaxed(&status[0], kLvP | agg);
-            } else {
-                if (lane == 0) st_relaxed(&status[tile], kLvA | agg);
-                prefix = warp_lookback<kLvP, kLvMask>(status, tile, err);
-                if (lane == 0) st_relaxed(&status[tile], kLvP | (prefix + agg));
-            }
-            if (lane == 0) {
-                s_prefix = prefix;
-                if (tile == ntiles - 1) {
-                    const uint64_t tot = prefix + agg;
-                    const int ncell = (int)(tot & 0x7FFFFFFFull), nlf = (int)(tot >> 31);
-                    for (int k2 = L + 1; k2 < kMaxLevels2D + 3; ++k2) {
-                        info->level_start[k2] = base_cell + ncell;
-                        info->leaf_start[k2] = base_leaf + nlf;
-                    }
-                    info->n_cells = base_cell + ncell;
-                    info->n_leaves = base_leaf + nlf;
-                    if (ncell > 0) info->depth = L;
-                    if (base_cell + ncell > t.cap_cells) set_err(err, ERR_CELL_CAP);
-                }
-            }
-        }
-        __syncthreads();
-        if (nonleaf) {
-            const int nchild = __popc(mask);
-            const int ci0 = base_cell + (int)(s_prefix & 0x7FFFFFFFull) + s_xc[warp];
-            const int li0 = base_leaf + (int)(s_prefix >> 31) + s_xl[warp];
-            if (lane == 0) {
-                const bool fits = ci0 + nchild <= t.cap_cells;
-                t.c_child0[p] = fits ? ci0 : -1;
-                t.c_chmask[p] = fits ? (uint8_t)mask : 0;
-            }
-            if (has) {
-                const unsigned below = (1u << lane) - 1u;
-                const int ci = ci0 + __popc(mask & below);
-                if (ci >= t.cap_cells) {
-                    set_err(err, ERR_CELL_CAP);
-                } else {
-                    const int ix = 2 * __ldcg(&t.c_ix[p]) + (lane & 1), iy = 2 * __ldcg(&t.c_iy[p]) + (lane >> 1);
-                    t.c_lo[ci] = clo;
-                    t.c_hi[ci] = chi;
-                    t.c_src[ci] = src;
-                    t.c_flags[ci] = (leaf ? CELL_LEAF : 0) | (src != 0 ? CELL_ACTIVE : 0);
-                    t.c_parent[ci] = p;
-                    t.c_child0[ci] = -1;
-                    t.c_chmask[ci] = 0;
-                    t.c_level[ci] = (uint8_t)L;
-                    t.c_ix[ci] = ix;
-                    t.c_iy[ci] = iy;
-                    t.c_code[ci] = (__ldcg(&t.c_code[p]) << 2) + lane;
-                    t.c_cx[ci] = xadd(pivx, xmul(xadd(0.5, (double)ix), len));
-                    t.c_cy[ci] = xadd(pivy, xmul(xadd(0.5, (double)iy), len));
-                    if (dense && L <= dense_levels) dense[start_id2(L) + ix + ((int64_t)iy << L)] = ci;
-                    if (leaf) {
-                        const int li = li0 + __popc(lmask & below);
-                        t.c_leafidx[ci] = li;
-                        t.leaf_cells[li] = ci;
-                    } else {
-                        t.c_leafidx[ci] = -1;
-                        if (L == t.key_levels) set_err(err, ERR_DEPTH);
-                    }
-                }
-            }
-        }
-        __syncthreads();
-    }
-}
-
-__global__ void __launch_bounds__(kLvlThreads)
-tree_level2d(Tree2D t, int L, int max_src, int max_par, int* dense, int dense_levels, uint64_t* status,
-             unsigned* ticket, unsigned* err) {
-    level_step(t, L, max_src, max_par, dense, dense_levels, status, ticket, err);
-}
-
-// All levels in one cooperative launch: a grid barrier between levels, and a
-// stop as soon as a level creates no cells (that test reads a value written
-// before the barrier, so every block takes the same decision).
-__global__ void __launch_bounds__(kLvlThreads)
-tree_levels_coop(Tree2D t, int max_src, int max_par, int* dense, int dense_levels, uint64_t* status, int stride,
-                 unsigned* tickets, unsigned* bar, unsigned* err) {
-    for (int L = 1; L <= t.key_levels; ++L) {
-        level_step(t, L, max_src, max_par, dense, dense_levels, status + (size_t)L * stride, tickets + L, err);
-        grid_sync(bar, err);
-        const int created = __ldcg(&t.info->level_start[L + 1]) - __ldcg(&t.info->level_start[L]);
-        if (created == 0) break;
     }
 }
 
@@ -622,6 +341,16 @@ __global__ void flat_totals(Tree2D t, const uint32_t* __restrict__ level_tot, un
     info->n_cells = cells;
     info->n_leaves = leaves;
     info->depth = depth;
+    // leaf level range (TreeCell::min_level / max_level, treeCell.cpp:1236-1240)
+    int mn = -1, mx = -1;
+    for (int L = 1; L <= K; ++L) {
+        if (level_tot[kMaxLevels2D + 1 + L] > 0) {
+            if (mn < 0) mn = L;
+            mx = L;
+        }
+    }
+    info->min_leaf_level = mn;
+    info->max_leaf_level = mx;
     if (cells > t.cap_cells) set_err(err, ERR_CELL_CAP);
     const Geom2D* g = t.geom;
     t.c_lo[0] = 0;
@@ -630,7 +359,7 @@ __global__ void flat_totals(Tree2D t, const uint32_t* __restrict__ level_tot, un
     t.c_src[0] = src;
     t.c_flags[0] = src != 0 ? CELL_ACTIVE : 0;
     t.c_parent[0] = -1;
-    t.c_child0[0] = 0x7fffffff;
+    t.c_child0[0] = -1;   // lowered by flat_link (unsigned minimum, so -1 = none)
     t.c_chmask[0] = 0;
     t.c_level[0] = 0;
     t.c_ix[0] = 0;
@@ -702,7 +431,7 @@ flat_emit(Tree2D t, const uint32_t* __restrict__ pinfo, const uint32_t* __restri
             const double len = xdiv(root, ldexp(1.0, L));
             t.c_lo[ci] = i;
             t.c_flags[ci] = lf ? CELL_LEAF : 0;   // range end, counts and activity: flat_link
-            t.c_child0[ci] = 0x7fffffff;
+            t.c_child0[ci] = -1;
             t.c_chmask[ci] = 0;
             t.c_level[ci] = (uint8_t)L;
             t.c_ix[ci] = ix;
@@ -768,27 +497,8 @@ __global__ void flat_link(Tree2D t, int max_par, unsigned* err) {
         unsigned* word = reinterpret_cast<unsigned*>(reinterpret_cast<uintptr_t>(&t.c_chmask[p]) & ~(uintptr_t)3);
         const unsigned shift = 8u * (unsigned)(reinterpret_cast<uintptr_t>(&t.c_chmask[p]) & 3);
         atomicOr(word, (1u << (unsigned)(code & 3)) << shift);
-        atomicMin(&t.c_child0[p], c);
+        atomicMin(reinterpret_cast<unsigned*>(&t.c_child0[p]), (unsigned)c);   // -1 is the largest unsigned
     }
-}
-
-__global__ void flat_fix(Tree2D t) {
-    const int nc = t.info->n_cells;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x)
-        if (t.c_child0[c] == 0x7fffffff) t.c_child0[c] = -1;
-}
-
-// Leaf level range (TreeCell::min_level / max_level, treeCell.cpp:1236-1240).
-__global__ void tree_finish2d(TreeInfo2D* info) {
-    int mn = -1, mx = -1;
-    for (int L = 0; L <= kMaxLevels2D; ++L) {
-        if (info->leaf_start[L + 1] > info->leaf_start[L]) {
-            if (mn < 0) mn = L;
-            mx = L;
-        }
-    }
-    info->min_leaf_level = mn;
-    info->max_leaf_level = mx;
 }
 
 }  // namespace
@@ -841,9 +551,7 @@ cudaError_t levels2d_flat(Tree2D& t, TreeScratch2D& s, int max_src, int max_par,
     flat_emit<<<grid, kFlatTile, 0, st>>>(t, s.pinfo, s.tile_cnt, tiles, max_par, err);
     const int gc = std::max(1, std::min(148 * 8, ceil_div(t.cap_cells, 256)));
     flat_link<<<gc, 256, 0, st>>>(t, max_par, err);
-    flat_fix<<<gc, 256, 0, st>>>(t);
-    tree_finish2d<<<1, 1, 0, st>>>(t.info);
-    *launches += 8;
+    *launches += 6;
     return cudaGetLastError();
 }
 
@@ -852,38 +560,6 @@ cudaError_t levels2d(Tree2D& t, TreeScratch2D& s, int max_src, int max_par, unsi
     return levels2d_flat(t, s, max_src, max_par, err, st, launches);
 }
 
-cudaError_t levels2d_by_level(Tree2D& t, TreeScratch2D& s, int max_src, int max_par, unsigned* err, cudaStream_t st,
-                              int* launches) {
-    const int K = t.key_levels;
-    cudaError_t e = cudaMemsetAsync(s.lvl_status, 0, sizeof(uint64_t) * (size_t)(K + 1) * s.lvl_max_tiles, st);
-    if (e != cudaSuccess) return e;
-    tree_root2d<<<1, 1, 0, st>>>(t);
-    *launches += 1;
-    if (t.gbar) {
-        int grid = 0;
-        e = launch_coop(tree_levels_coop, kLvlThreads, 0, st, 8, &grid, t, max_src, max_par, t.dense, t.dense_levels,
-                        s.lvl_status, s.lvl_max_tiles, s.lvl_ticket, t.gbar, err);
-        if (e == cudaSuccess) {
-            *launches += 1;
-            tree_finish2d<<<1, 1, 0, st>>>(t.info);
-            *launches += 1;
-            return cudaGetLastError();
-        }
-        (void)cudaGetLastError();  // cooperative launch refused: one launch per level instead
-    }
-    for (int L = 1; L <= K; ++L) {
-        long long bound = std::min<long long>(t.cap_cells, 1ll << std::min(2 * (L - 1), 40));
-        int tiles = std::max(1, ceil_div(bound, kLvlWarps));
-        if (tiles > s.lvl_max_tiles) return cudaErrorInvalidValue;
-        int grid = std::min(tiles, 148 * 8);
-        tree_level2d<<<grid, kLvlThreads, 0, st>>>(t, L, max_src, max_par, t.dense, t.dense_levels,
-                                                   s.lvl_status + (size_t)L * s.lvl_max_tiles, s.lvl_ticket + L, err);
-        *launches += 1;
-    }
-    tree_finish2d<<<1, 1, 0, st>>>(t.info);
-    *launches += 1;
-    return cudaGetLastError();
-}
 
 cudaError_t build_tree2d(const double* x, const double* y, const double* q, const uint8_t* act, Tree2D& t,
                          TreeScratch2D& s, int max_src, int max_par, double exp_pct, unsigned* err, cudaStream_t st,
