@@ -240,7 +240,10 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
             VPM_CUDA_TRY(fmm2d_m2l_tc(tree, lists, ex2, p.p, tc_rows, tc_ops, d_err, st, &launches));
         else
             VPM_CUDA_TRY(fmm2d_m2l_only(tree, lists, ex2, p.p, d_err, st, &launches));
-        VPM_CUDA_TRY(fmm2d_l2l(tree, ex2, p.p, d_err, st, &launches));
+        if (l2l_direct_ok(p.p, p.binom == VPM_BINOM_EXACT))
+            VPM_CUDA_TRY(fmm2d_l2l_leaves(tree, ex2, p.p, d_err, st, &launches));
+        else
+            VPM_CUDA_TRY(fmm2d_l2l(tree, ex2, p.p, d_err, st, &launches));
         VPM_CUDA_TRY(cudaStreamWaitEvent(st, join2, 0));
         VPM_CUDA_TRY(fmm2d_eval_combine(tree, lists, ex2, p.p, near_x, near_y, o0, o1, velocity, uinf, vinf, d_err, st,
                                         &launches));
@@ -264,7 +267,10 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
             VPM_CUDA_TRY(fmm2d_m2l_only(tree, lists, ex2, p.p, d_err, st, &launches));
         if (velocity == kModePotential) VPM_CUDA_TRY(fmm2d_m2l_b0(tree, lists, ex2, p.p, d_err, st, &launches));
         if (int r = record(5)) return r;
-        VPM_CUDA_TRY(fmm2d_l2l(tree, ex2, p.p, d_err, st, &launches));
+        if (l2l_direct_ok(p.p, p.binom == VPM_BINOM_EXACT))
+            VPM_CUDA_TRY(fmm2d_l2l_leaves(tree, ex2, p.p, d_err, st, &launches));
+        else
+            VPM_CUDA_TRY(fmm2d_l2l(tree, ex2, p.p, d_err, st, &launches));
         if (int r = record(6)) return r;
         if (velocity == kModePotential) {
             // far field and near field in one stage pair: the events keep their slots

@@ -178,6 +178,11 @@ cudaError_t fmm2d_m2l_b0(const Tree2D& t, const Lists2D& l, Expansions2D& e, int
                          int* launches);
 cudaError_t fmm2d_potential_eval(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, double* out,
                                  unsigned* err, cudaStream_t st, int* launches);
+// Leaves' full local expansions straight from their ancestors' M2L parts
+// (replaces the level-by-level L2L when l2l_direct_ok: exact binomials up to
+// order P).
+bool l2l_direct_ok(int P, bool exact);
+cudaError_t fmm2d_l2l_leaves(const Tree2D& t, Expansions2D& e, int P, unsigned* err, cudaStream_t st, int* launches);
 // Tensor-core list-2 M2L of the mixed form (m2l_tc.cu): orders 1..20.
 bool m2l_tc_supported(int P);
 size_t m2l_tc_rows_bytes(int cap_cells);

@@ -1174,6 +1174,111 @@ cudaError_t fmm2d_l2l(const Tree2D& t, Expansions2D& e, int P, unsigned* err, cu
     return cudaGetLastError();
 }
 
+// Full local expansion of every leaf straight from the M2L parts of its
+// ancestors: b(leaf) = b_M2L(leaf) + sum over ancestors a at levels 2..L-1 of
+// the L2L shift of b_M2L(a) by z_leaf - z_a. Shifts of a degree-P polynomial
+// compose exactly (shift by t1 then t2 = shift by t1 + t2) when the binomials
+// C(k, p) are exact, which the reference's 32-bit binComb gives for k <= 17;
+// the result then equals the level-by-level pull of fmm2D.cpp:587-651 up to
+// rounding, without a level loop or grid barrier. G = 32/(P+1) leaves per
+// warp, lane k of group g holds coefficient k of leaf g. Ancestors come from
+// the dense grid (written for every cell of levels <= dense_levels by the
+// tree build, so an ancestor's entry is always current) and the parent chain
+// below it; their centres and coefficients are staged in shared memory in
+// chunks of kL2LChunk levels.
+constexpr int kL2LChunk = 4;
+constexpr int kL2LWarps = 4;
+constexpr int kL2LGroups = 16;   // leaves per warp at most (P >= 1)
+
+__global__ void __launch_bounds__(32 * kL2LWarps)
+l2l_leaves2d(Tree2D t, double2* __restrict__ b, const double* __restrict__ coef, int P) {
+    __shared__ int s_anc[kL2LWarps][kL2LGroups][kMaxLevels2D + 1];  // [warp][group][level]
+    __shared__ int s_lev[kL2LWarps][kL2LGroups];                    // leaf level per group
+    __shared__ double2 s_ctr[kL2LWarps][kL2LGroups][kL2LChunk];     // ancestor centres
+    __shared__ double2 s_cf[kL2LWarps][kL2LChunk * 32];             // chunk coefficients, all groups
+    const double* g_l2l = coef + kCoefL2L;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int Q = P + 1, G = 32 / Q, g = lane / Q, k = lane - g * Q;
+    const bool in_grp = g < G;
+    const int nl = t.info->n_leaves, nc = t.info->n_cells;
+    const int dlev = t.dense ? t.dense_levels : 1;
+    const int warps = gridDim.x * kL2LWarps;
+    for (int lb = (blockIdx.x * kL2LWarps + wib) * G; lb < nl; lb += warps * G) {
+        const int li = lb + g;
+        const bool has = in_grp && li < nl;
+        const int c = has ? t.leaf_cells[li] : 0;
+        const int L = has ? (int)t.c_level[c] : 0;
+        const int na = L > 2 ? L - 2 : 0;   // ancestors at levels 2..L-1
+        int ix = 0, iy = 0;
+        double zx = 0.0, zy = 0.0;
+        double2 acc = make_double2(0.0, 0.0);
+        if (in_grp && k == 0) s_lev[wib][g] = L;
+        if (na) {
+            ix = t.c_ix[c];
+            iy = t.c_iy[c];
+            zx = t.c_cx[c];
+            zy = t.c_cy[c];
+            acc = b[(size_t)c * Q + k];
+            // dense-grid ancestors, one level per lane of the group
+            for (int m = 2 + k; m < L && m <= dlev; m += Q) {
+                const int sh = L - m;
+                const int a = t.dense[start_id2(m) + (ix >> sh) + ((int64_t)(iy >> sh) << m)];
+                s_anc[wib][g][m] = (a >= 0 && a < nc) ? a : -1;
+            }
+            // deeper ancestors by the parent chain
+            if (k == 0) {
+                int a = t.c_parent[c];
+                for (int m = L - 1; m > dlev && m >= 2; --m) {
+                    s_anc[wib][g][m] = a;
+                    a = t.c_parent[a];
+                }
+            }
+        }
+        __syncwarp();
+        const int na_max = __reduce_max_sync(0xffffffffu, na);
+        for (int m0 = 0; m0 < na_max; m0 += kL2LChunk) {
+            const int mc = min(kL2LChunk, na_max - m0);
+            // stage: centres (one ancestor per lane of the group), then coefficients of all groups
+            if (k < mc && 2 + m0 + k < L) {
+                const int a = s_anc[wib][g][2 + m0 + k];
+                s_ctr[wib][g][k] = a >= 0 ? make_double2(t.c_cx[a], t.c_cy[a]) : make_double2(zx, zy);
+            }
+            for (int j = lane; j < G * mc * Q; j += 32) {
+                const int gj = j / (mc * Q), r = j - gj * (mc * Q), mj = r / Q, kj = r - mj * Q;
+                double2 v = make_double2(0.0, 0.0);
+                if (2 + m0 + mj < s_lev[wib][gj]) {
+                    const int a = s_anc[wib][gj][2 + m0 + mj];
+                    if (a >= 0) v = b[(size_t)a * Q + kj];
+                }
+                s_cf[wib][(gj * kL2LChunk + mj) * Q + kj] = v;
+            }
+            __syncwarp();
+            if (has) {
+                const double* cf = g_l2l + k * W;
+                for (int mj = 0; mj < mc && m0 + mj < na; ++mj) {
+                    const double2 ctr = s_ctr[wib][g][mj];
+                    const double2 tt = make_double2(zx - ctr.x, zy - ctr.y);
+                    const double2* par = &s_cf[wib][(g * kL2LChunk + mj) * Q];
+                    double2 S = cscale(par[P], cf[P]);
+                    for (int kk = P - 1; kk >= k; --kk) S = cfma(S, tt, cscale(par[kk], cf[kk]));
+                    acc = cadd(acc, S);
+                }
+            }
+            __syncwarp();
+        }
+        if (na) b[(size_t)c * Q + k] = acc;
+    }
+}
+
+bool l2l_direct_ok(int P, bool exact) { return P >= 1 && (exact || P <= 17); }
+
+cudaError_t fmm2d_l2l_leaves(const Tree2D& t, Expansions2D& e, int P, unsigned* err, cudaStream_t st, int* launches) {
+    (void)err;
+    l2l_leaves2d<<<148 * 8, 32 * kL2LWarps, 0, st>>>(t, e.b, e.coef, P);
+    *launches += 1;
+    return cudaGetLastError();
+}
+
 cudaError_t fmm2d_m2l(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, unsigned* err, cudaStream_t st,
                       int* launches) {
     cudaError_t r = fmm2d_m2l_only(t, l, e, P, err, st, launches);
