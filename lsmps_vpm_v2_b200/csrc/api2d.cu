@@ -78,7 +78,7 @@ int Ctx::reserve2d(int n, int cap_cells, int P, long long cap_l1, long long cap_
     size_t o_px = L.take<double>(n), o_py = L.take<double>(n), o_pq = L.take<double>(n), o_pact = L.take<uint8_t>(n);
     size_t o_actscan = L.take<uint32_t>((size_t)n + 1);
     size_t o_keyalt = L.take<uint64_t>(n), o_valalt = L.take<uint32_t>(n), o_actu = L.take<uint32_t>(n);
-    size_t o_bbox = L.take<double>(kBBoxBlocks * 4);
+    size_t o_bbox = L.take<double>(kBBoxBlocks * 4), o_coop = L.take<uint32_t>(kCoopSortWords);
     size_t o_ltick = L.take<unsigned>(kTicketWords);
     const int flat_tiles = ceil_div(n, kFlatTile);
     size_t o_pinfo = L.take<uint32_t>(n), o_tcnt = L.take<uint32_t>((size_t)2 * (K + 1) * flat_tiles),
@@ -126,7 +126,7 @@ int Ctx::reserve2d(int n, int cap_cells, int P, long long cap_l1, long long cap_
     tree.px = (double*)P_(o_px); tree.py = (double*)P_(o_py); tree.pq = (double*)P_(o_pq);
     tree.pact = (uint8_t*)P_(o_pact); tree.actscan = (uint32_t*)P_(o_actscan);
     ts.key_alt = (uint64_t*)P_(o_keyalt); ts.val_alt = (uint32_t*)P_(o_valalt); ts.act_u32 = (uint32_t*)P_(o_actu);
-    ts.bbox_partial = (double*)P_(o_bbox);
+    ts.bbox_partial = (double*)P_(o_bbox); ts.coop_words = (uint32_t*)P_(o_coop);
     ts.lvl_ticket = (unsigned*)P_(o_ltick);
     ts.pinfo = (uint32_t*)P_(o_pinfo); ts.tile_cnt = (uint32_t*)P_(o_tcnt); ts.level_tot = (uint32_t*)P_(o_ltot);
     ts.flat_tiles = flat_tiles;
@@ -159,6 +159,7 @@ int Ctx::reserve2d(int n, int cap_cells, int P, long long cap_l1, long long cap_
     ex2.op = (double2*)P_(o_op);
     coef_P = -1;  // the new arena holds no coefficients yet
     mixed_base = P_(o_mixed);
+    ts.sort_aos = mixed_base;   // the near-field work area is free while the tree is built
     {
         const size_t r0 = ((sizeof(double4) * (size_t)n + 1023) & ~(size_t)1023);
         tc_rows = (float*)((char*)mixed_base + r0);

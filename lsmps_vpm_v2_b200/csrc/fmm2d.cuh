@@ -108,6 +108,13 @@ constexpr int kFlatTile = 256;   // particles per block of the flat tree build
 constexpr int kTicketWords = kMaxLevels2D + 2 + 8;  // level tickets, bbox counter, 3 x 2 barrier words
 constexpr int kBarrierWordsAt = kMaxLevels2D + 2;
 
+// Cooperative sort (one launch for bounding box, keys, radix passes, gather
+// and active scan): at most kCoopSortGridMax blocks of kCoopSortMaxChunk
+// particles; larger inputs take the multi-kernel path.
+constexpr int kCoopSortGridMax = 160;
+constexpr int kCoopSortMaxChunk = 16384;
+constexpr int kCoopSortWords = 1024 * kCoopSortGridMax + 512;
+
 struct TreeScratch2D {
     double* bbox_partial;   // [kBBoxBlocks * 4]
     uint64_t* key_alt;
@@ -118,6 +125,8 @@ struct TreeScratch2D {
     uint32_t* tile_cnt;     // [2][kMaxLevels2D + 1][flat_tiles] cells / leaves per tile and level, then offsets
     uint32_t* level_tot;    // [2][kMaxLevels2D + 1] cells / leaves per level
     int flat_tiles;         // tiles of kFlatTile particles
+    uint32_t* coop_words;   // [kCoopSortWords] count tables of the cooperative sort (nullptr: multi-kernel sort)
+    void* sort_aos;         // [n] double4 staging of the cooperative sort (free again once the tree is built)
     SortScratch sort;
     ScanScratch scan;
 };

@@ -20,6 +20,38 @@ namespace vpm {
 
 namespace {
 
+// Root cell of the box [mnx, mxx] x [mny, mxy] (treeCell.cpp:1061-1092).
+__device__ void root_geometry(double mnx, double mxx, double mny, double mxy, double exp_pct, int key_levels,
+                              Geom2D& g, unsigned* err) {
+    double root = 0.0;
+    double ex = fabs(xsub(mxx, mnx)), ey = fabs(xsub(mxy, mny));
+    if (ex > root) root = ex;
+    if (ey > root) root = ey;
+    double expansion = xadd(1.0, xdiv(exp_pct, 100.0));
+    root = xmul(root, expansion);
+    g.minx = mnx; g.maxx = mxx; g.miny = mny; g.maxy = mxy;
+    g.root = root;
+    g.pivx = xdiv(xsub(xadd(mxx, mnx), root), 2.0);
+    g.pivy = xdiv(xsub(xadd(mxy, mny), root), 2.0);
+    g.size_k = xdiv(root, ldexp(1.0, key_levels));
+    if (err && (!(root > 0.0) || !isfinite(root))) set_err(err, ERR_NONFINITE);
+}
+
+// Morton key of one particle at the key level (treeCell.cpp:290-303).
+__device__ __forceinline__ uint64_t particle_key(double x, double y, double pivx, double pivy, double s, double lim,
+                                                 unsigned* err) {
+    double tx = xdiv(xsub(x, pivx), s);
+    double ty = xdiv(xsub(y, pivy), s);
+    uint32_t ix = 0, iy = 0;
+    if (tx >= 0.0 && tx < lim && ty >= 0.0 && ty < lim) {
+        ix = (uint32_t)__double2ull_rz(tx);
+        iy = (uint32_t)__double2ull_rz(ty);
+    } else {
+        set_err(err, ERR_RANGE);
+    }
+    return morton2(ix, iy);
+}
+
 // Bounding box and root geometry (treeCell.cpp:1061-1092).
 __global__ void __launch_bounds__(256)
 bbox2d(const double* __restrict__ x, const double* __restrict__ y, int n, double exp_pct, int key_levels,
@@ -79,18 +111,9 @@ bbox2d(const double* __restrict__ x, const double* __restrict__ y, int n, double
         mnx = fmin(mnx, sh[0][w]); mxx = fmax(mxx, sh[1][w]);
         mny = fmin(mny, sh[2][w]); mxy = fmax(mxy, sh[3][w]);
     }
-    double root = 0.0;
-    double ex = fabs(xsub(mxx, mnx)), ey = fabs(xsub(mxy, mny));
-    if (ex > root) root = ex;
-    if (ey > root) root = ey;
-    double expansion = xadd(1.0, xdiv(exp_pct, 100.0));
-    root = xmul(root, expansion);
-    g->minx = mnx; g->maxx = mxx; g->miny = mny; g->maxy = mxy;
-    g->root = root;
-    g->pivx = xdiv(xsub(xadd(mxx, mnx), root), 2.0);
-    g->pivy = xdiv(xsub(xadd(mxy, mny), root), 2.0);
-    g->size_k = xdiv(root, ldexp(1.0, key_levels));
-    if (!(root > 0.0) || !isfinite(root)) set_err(err, ERR_NONFINITE);
+    Geom2D gg;
+    root_geometry(mnx, mxx, mny, mxy, exp_pct, key_levels, gg, err);
+    *g = gg;
     *done = 0;
 }
 
@@ -102,16 +125,7 @@ __global__ void keys2d(const double* __restrict__ x, const double* __restrict__ 
     const double pivx = g->pivx, pivy = g->pivy, s = g->size_k;
     const double lim = ldexp(1.0, key_levels);
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        double tx = xdiv(xsub(x[i], pivx), s);
-        double ty = xdiv(xsub(y[i], pivy), s);
-        uint32_t ix = 0, iy = 0;
-        if (tx >= 0.0 && tx < lim && ty >= 0.0 && ty < lim) {
-            ix = (uint32_t)__double2ull_rz(tx);
-            iy = (uint32_t)__double2ull_rz(ty);
-        } else {
-            set_err(err, ERR_RANGE);
-        }
-        key[i] = (KT)morton2(ix, iy);
+        key[i] = (KT)particle_key(x[i], y[i], pivx, pivy, s, lim, err);
         idx[i] = (uint32_t)i;
     }
 }
@@ -138,6 +152,359 @@ __global__ void gather2d(const double* __restrict__ x, const double* __restrict_
         uint8_t a = act[j] ? 1 : 0;
         pact[i] = a;
         act_u32[i] = a;
+    }
+}
+
+// ---- the sorted particle order in one cooperative launch ------------------------
+//
+// With 32-bit keys and at most kCoopSortMaxChunk particles per block, one
+// launch of one 1024-thread block per SM replaces bbox2d, keys2d, the radix
+// sort, gather2d and the active-count scan (ten launches, most of them
+// latency-bound at these sizes). Block b owns the contiguous range
+// [b C, (b+1) C) of every pass's input. A pass ranks the block's items by
+// digit warp by warp in index order (so the sort is stable), publishes the
+// block's 256 digit counts, meets the grid at a barrier, takes each digit's
+// output base from the column sums of the count table (the blocks before it
+// plus the digit's global start), reorders its items by digit in shared
+// memory and writes each digit's run contiguously. Results are identical to
+// the multi-kernel path: the same keys, the same stable order.
+constexpr int kCoopSortThreads = 1024;
+constexpr int kCoopSortWarps = kCoopSortThreads / 32;
+constexpr int kCoopBarrierWord = 6;
+constexpr int kCoopRounds = 6;        // rounds of 32 items per warp loaded together
+constexpr int kCoopActRun = 16;       // sorted flags per thread in the active scan (kCoopSortMaxChunk / 1024)   // grid-barrier words 6, 7 of Tree2D::gbar
+
+// Exclusive scan over the 1024 threads of the block; *total = the block sum.
+// Every thread must call it (it holds three block barriers).
+__device__ __forceinline__ uint32_t coop_block_scan(uint32_t v, uint32_t* s_ws, uint32_t* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+    #pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_ws[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = s_ws[lane];
+        #pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        s_ws[lane] = w;
+    }
+    __syncthreads();
+    const uint32_t base = warp ? s_ws[warp - 1] : 0u;
+    *total = s_ws[kCoopSortWarps - 1];
+    __syncthreads();
+    return base + x - v;
+}
+
+// Word offsets in the count tables of sort2d_coop (GM = kCoopSortGridMax):
+// per-block digit counts [256][GM] and active counts [256][GM] (column d
+// holds the blocks' counts of digit d), their exclusive prefixes over blocks
+// [GM][256] (row b is what block b reads) and the per-digit totals.
+constexpr int kCwCount = 0;
+constexpr int kCwActCount = 256 * kCoopSortGridMax;
+constexpr int kCwPrefix = 512 * kCoopSortGridMax;
+constexpr int kCwActPrefix = 768 * kCoopSortGridMax;
+constexpr int kCwTotal = 1024 * kCoopSortGridMax;
+constexpr int kCwActTotal = kCwTotal + 256;
+static_assert(kCwActTotal + 256 <= kCoopSortWords, "count tables of the cooperative sort");
+
+// kb0/kb1: 32-bit key ping-pong buffers (pass 0's keys are computed into
+// kb0); vb0/vb1: index ping-pong buffers, vb1 may alias t.perm (the last
+// pass reads vb0). An index carries its particle's active flag in bit 31.
+// aos: n entries of (x, y, q, active) in input order, written while the
+// bounding box is read, so that the last pass fetches one 32-byte sector per
+// particle. The last pass also produces the active-count scan: a block's
+// sorted items form one run per digit, so the count before an item is the
+// digit's global start, the runs of that digit in earlier blocks, and the
+// item's place in its own run.
+__global__ void __launch_bounds__(kCoopSortThreads, 1)
+sort2d_coop(const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ q,
+            const uint8_t* __restrict__ act, double exp_pct, int passes, Tree2D t, double* partial, double4* aos,
+            uint32_t* kb0, uint32_t* kb1, uint32_t* vb0, uint32_t* vb1, uint32_t* words, int chunk_cap,
+            unsigned* err) {
+    extern __shared__ __align__(16) unsigned char cs_sm[];
+    __shared__ uint32_t s_wh[kCoopSortWarps][256];   // per-warp digit counts, then warp-exclusive prefixes
+    __shared__ uint32_t s_local[256];                // tile-local start of each digit
+    __shared__ uint32_t s_base[256];                 // output index minus tile-local index, per digit
+    __shared__ uint32_t s_wa[256];                   // last pass: the block's active count per digit
+    __shared__ uint32_t s_abase[256];                // last pass: active count before the digit's run, minus local
+    __shared__ uint32_t s_ws[32];
+    __shared__ double s_red[4][kCoopSortWarps];
+    __shared__ double s_geo[3];
+    const int n = t.n;
+    const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int chunk = (n + G - 1) / G;
+    if (chunk > chunk_cap || G > kCoopSortGridMax) {   // uniform over the grid: no block reaches a barrier
+        if (b == 0 && tid == 0) set_err(err, ERR_INDEX);
+        return;
+    }
+    unsigned* bar = t.gbar + kCoopBarrierWord;
+    uint32_t* s_key = (uint32_t*)cs_sm;                  // [chunk_cap]
+    uint32_t* s_val = s_key + chunk_cap;                 // [chunk_cap]
+    uint16_t* s_rank = (uint16_t*)(s_val + chunk_cap);   // [chunk_cap]
+    const int c0 = min(n, b * chunk), c1 = min(n, c0 + chunk);
+    const int S = (chunk + kCoopSortWarps - 1) / kCoopSortWarps;   // items per warp
+    const int w0 = min(c1, c0 + warp * S), w1 = min(c1, w0 + S);
+
+    // 1. bounding box (block partials, barrier, every block reduces all of
+    //    them) and the AoS copy of the particles
+    {
+        double mnx = x[0], mxx = x[0], mny = y[0], mxy = y[0];
+        bool bad = false;
+        #pragma unroll 6
+        for (int i = c0 + tid; i < c1; i += kCoopSortThreads) {
+            const double a = x[i], c = y[i];
+            aos[i] = make_double4(a, c, q[i], act[i] ? 1.0 : 0.0);
+            bad |= !isfinite(a) || !isfinite(c);
+            mnx = fmin(mnx, a); mxx = fmax(mxx, a);
+            mny = fmin(mny, c); mxy = fmax(mxy, c);
+        }
+        if (bad) set_err(err, ERR_NONFINITE);
+        #pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            mnx = fmin(mnx, __shfl_xor_sync(0xffffffffu, mnx, o));
+            mxx = fmax(mxx, __shfl_xor_sync(0xffffffffu, mxx, o));
+            mny = fmin(mny, __shfl_xor_sync(0xffffffffu, mny, o));
+            mxy = fmax(mxy, __shfl_xor_sync(0xffffffffu, mxy, o));
+        }
+        if (lane == 0) { s_red[0][warp] = mnx; s_red[1][warp] = mxx; s_red[2][warp] = mny; s_red[3][warp] = mxy; }
+        __syncthreads();
+        if (tid == 0) {
+            for (int w = 1; w < kCoopSortWarps; ++w) {
+                mnx = fmin(mnx, s_red[0][w]); mxx = fmax(mxx, s_red[1][w]);
+                mny = fmin(mny, s_red[2][w]); mxy = fmax(mxy, s_red[3][w]);
+            }
+            double* pp = partial + 4 * b;
+            pp[0] = mnx; pp[1] = mxx; pp[2] = mny; pp[3] = mxy;
+        }
+        grid_sync_counter(bar, err);
+        if (warp == 0) {
+            mnx = __ldcg(partial); mxx = __ldcg(partial + 1); mny = __ldcg(partial + 2); mxy = __ldcg(partial + 3);
+            #pragma unroll 5
+            for (int bb = lane; bb < G; bb += 32) {
+                const double* pp = partial + 4 * bb;
+                mnx = fmin(mnx, __ldcg(pp)); mxx = fmax(mxx, __ldcg(pp + 1));
+                mny = fmin(mny, __ldcg(pp + 2)); mxy = fmax(mxy, __ldcg(pp + 3));
+            }
+            #pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                mnx = fmin(mnx, __shfl_xor_sync(0xffffffffu, mnx, o));
+                mxx = fmax(mxx, __shfl_xor_sync(0xffffffffu, mxx, o));
+                mny = fmin(mny, __shfl_xor_sync(0xffffffffu, mny, o));
+                mxy = fmax(mxy, __shfl_xor_sync(0xffffffffu, mxy, o));
+            }
+            if (lane == 0) {
+                Geom2D gg;
+                root_geometry(mnx, mxx, mny, mxy, exp_pct, t.key_levels, gg, b == 0 ? err : nullptr);
+                s_geo[0] = gg.pivx;
+                s_geo[1] = gg.pivy;
+                s_geo[2] = gg.size_k;
+                if (b == 0) *t.geom = gg;
+            }
+        }
+        __syncthreads();
+    }
+    const double pivx = s_geo[0], pivy = s_geo[1], size_k = s_geo[2];
+    const double lim = ldexp(1.0, t.key_levels);
+
+    // 2. LSD passes of 8 bits
+    const unsigned lt = (1u << lane) - 1u;
+    for (int p = 0; p < passes; ++p) {
+        const int shift = 8 * p;
+        const bool last = p == passes - 1;
+        const uint32_t* kin = (p & 1) ? kb1 : kb0;
+        uint32_t* kout = (p & 1) ? kb0 : kb1;
+        const uint32_t* vin = ((passes - 1 - p) & 1) ? vb1 : vb0;
+        uint32_t* vout = ((passes - 2 - p) & 1) ? vb1 : vb0;
+        for (int i = tid; i < kCoopSortWarps * 256; i += kCoopSortThreads) (&s_wh[0][0])[i] = 0u;
+        if (tid < 256) s_wa[tid] = 0u;
+        __syncthreads();
+        // rank of each item among the warp's items of its digit, in index order
+        for (int i0 = w0; i0 < w1; i0 += 32 * kCoopRounds) {
+            // kCoopRounds rounds of 32 items: loads first (independent), then the ranking
+            uint32_t kr[kCoopRounds], fr[kCoopRounds];
+            #pragma unroll
+            for (int r = 0; r < kCoopRounds; ++r) {
+                const int i = i0 + r * 32 + lane;
+                kr[r] = 0u;
+                fr[r] = 0u;
+                if (i < w1) {
+                    if (p == 0) {
+                        kr[r] = (uint32_t)particle_key(x[i], y[i], pivx, pivy, size_k, lim, err);
+                        kb0[i] = kr[r];
+                        if (last) fr[r] = act[i] ? 1u : 0u;
+                    } else {
+                        kr[r] = __ldcg(kin + i);
+                        if (last) fr[r] = __ldcg(vin + i) >> 31;
+                    }
+                }
+            }
+            #pragma unroll
+            for (int r = 0; r < kCoopRounds; ++r) {
+                const int i = i0 + r * 32 + lane;
+                const bool ok = i < w1;
+                const int d = (int)((kr[r] >> shift) & 255u);
+                // lanes holding the same digit: one ballot per digit bit
+                unsigned m = __ballot_sync(0xffffffffu, ok);
+                #pragma unroll
+                for (int bit = 0; bit < 8; ++bit) {
+                    const bool bs = (d >> bit) & 1;
+                    const unsigned bv = __ballot_sync(0xffffffffu, bs);
+                    m &= bs ? bv : ~bv;
+                }
+                uint32_t prior = 0;
+                if (ok) prior = s_wh[warp][d];
+                __syncwarp();
+                if (ok && (m & lt) == 0) s_wh[warp][d] = prior + __popc(m);
+                __syncwarp();
+                if (ok) {
+                    s_rank[i - c0] = (uint16_t)(prior + __popc(m & lt));
+                    if (fr[r]) atomicAdd(&s_wa[d], 1u);
+                }
+            }
+        }
+        __syncthreads();
+        uint32_t run = 0, tot = 0;
+        if (tid < 256) {
+            for (int w = 0; w < kCoopSortWarps; ++w) {
+                const uint32_t c = s_wh[w][tid];
+                s_wh[w][tid] = run;
+                run += c;
+            }
+            words[kCwCount + (size_t)tid * kCoopSortGridMax + b] = run;
+            if (last) words[kCwActCount + (size_t)tid * kCoopSortGridMax + b] = s_wa[tid];
+        }
+        const uint32_t loc = coop_block_scan(tid < 256 ? run : 0u, s_ws, &tot);
+        if (tid < 256) s_local[tid] = loc;
+        uint32_t aloc = 0;
+        if (last) aloc = coop_block_scan(tid < 256 ? s_wa[tid] : 0u, s_ws, &tot);
+        grid_sync_counter(bar, err);
+        // prefixes over blocks, one digit column per warp: block b takes
+        // digits b + (warp + 32 m) G; lane l holds blocks 5l .. 5l+4
+        for (int d = b + warp * G; d < 256; d += kCoopSortWarps * G) {
+            #pragma unroll 1
+            for (int tb = 0; tb < (last ? 2 : 1); ++tb) {
+                const uint32_t* col = words + (tb ? kCwActCount : kCwCount) + (size_t)d * kCoopSortGridMax;
+                uint32_t v[5], sum = 0;
+                #pragma unroll
+                for (int u = 0; u < 5; ++u) {
+                    const int bb = 5 * lane + u;
+                    v[u] = bb < G ? __ldcg(col + bb) : 0u;
+                    sum += v[u];
+                }
+                uint32_t incl = sum;
+                #pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t yv = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += yv;
+                }
+                uint32_t ex = incl - sum;
+                uint32_t* pre = words + (tb ? kCwActPrefix : kCwPrefix);
+                #pragma unroll
+                for (int u = 0; u < 5; ++u) {
+                    const int bb = 5 * lane + u;
+                    if (bb < G) pre[(size_t)bb * 256 + d] = ex;
+                    ex += v[u];
+                }
+                if (lane == 31) words[(tb ? kCwActTotal : kCwTotal) + d] = incl;
+            }
+        }
+        grid_sync_counter(bar, err);
+        {
+            const uint32_t before = tid < 256 ? __ldcg(words + kCwPrefix + (size_t)b * 256 + tid) : 0u;
+            const uint32_t all = tid < 256 ? __ldcg(words + kCwTotal + tid) : 0u;
+            const uint32_t start = coop_block_scan(all, s_ws, &tot);
+            if (tid < 256) s_base[tid] = start + before - s_local[tid];   // modulo 2^32
+            if (last) {
+                const uint32_t abefore = tid < 256 ? __ldcg(words + kCwActPrefix + (size_t)b * 256 + tid) : 0u;
+                const uint32_t aall = tid < 256 ? __ldcg(words + kCwActTotal + tid) : 0u;
+                uint32_t atot = 0;
+                const uint32_t astart = coop_block_scan(aall, s_ws, &atot);
+                if (tid < 256) s_abase[tid] = astart + abefore - aloc;
+                if (b == 0 && tid == 0) t.actscan[n] = atot;
+            }
+        }
+        __syncthreads();
+        // reorder by digit in shared memory
+        for (int i0 = w0; i0 < w1; i0 += 32 * kCoopRounds) {
+            uint32_t kr[kCoopRounds], vr[kCoopRounds];
+            #pragma unroll
+            for (int r = 0; r < kCoopRounds; ++r) {
+                const int i = i0 + r * 32 + lane;
+                kr[r] = 0u;
+                vr[r] = 0u;
+                if (i < w1) {
+                    if (p == 0) {
+                        kr[r] = kb0[i];
+                        vr[r] = (uint32_t)i | (act[i] ? 0x80000000u : 0u);
+                    } else {
+                        kr[r] = __ldcg(kin + i);
+                        vr[r] = __ldcg(vin + i);
+                    }
+                }
+            }
+            #pragma unroll
+            for (int r = 0; r < kCoopRounds; ++r) {
+                const int i = i0 + r * 32 + lane;
+                if (i < w1) {
+                    const int d = (int)((kr[r] >> shift) & 255u);
+                    const uint32_t lp = s_local[d] + s_wh[warp][d] + s_rank[i - c0];
+                    s_key[lp] = kr[r];
+                    s_val[lp] = vr[r];
+                }
+            }
+        }
+        __syncthreads();
+        const int cnt = c1 - c0;
+        if (last) {
+            // active flags before each staged item (thread tid: a contiguous run), into s_rank
+            const int a0 = tid * kCoopActRun;
+            uint32_t fl[kCoopActRun], na = 0;
+            #pragma unroll
+            for (int u = 0; u < kCoopActRun; ++u) {
+                fl[u] = a0 + u < cnt ? s_val[a0 + u] >> 31 : 0u;
+                na += fl[u];
+            }
+            uint32_t ra = coop_block_scan(na, s_ws, &tot);
+            #pragma unroll
+            for (int u = 0; u < kCoopActRun; ++u) {
+                if (a0 + u < cnt) s_rank[a0 + u] = (uint16_t)ra;
+                ra += fl[u];
+            }
+            __syncthreads();
+        }
+        #pragma unroll 4
+        for (int j = tid; j < cnt; j += kCoopSortThreads) {
+            const uint32_t key = s_key[j], vf = s_val[j];
+            const uint32_t val = vf & 0x7fffffffu;
+            const uint32_t d = (key >> shift) & 255u;
+            const uint32_t pos = s_base[d] + (uint32_t)j;
+            if (pos >= (uint32_t)n || val >= (uint32_t)n) {
+                set_err(err, ERR_INDEX);
+                continue;
+            }
+            if (!last) {
+                kout[pos] = key;
+                vout[pos] = vf;
+            } else {
+                const double4 e = aos[val];
+                t.key[pos] = key;
+                t.perm[pos] = val;
+                t.px[pos] = e.x;
+                t.py[pos] = e.y;
+                t.pq[pos] = e.z;
+                t.pact[pos] = (uint8_t)(vf >> 31);
+                t.actscan[pos] = s_abase[d] + s_rank[j];
+            }
+        }
+        if (!last) grid_sync_counter(bar, err);
     }
 }
 
@@ -503,6 +870,35 @@ __global__ void flat_link(Tree2D t, int max_par, unsigned* err) {
 
 }  // namespace
 
+// Grid and per-block share of the cooperative sort for n particles, or false
+// when it does not apply (share above kCoopSortMaxChunk, or fewer than one
+// resident block per SM).
+bool coop_sort_shape(int n, int* grid, int* chunk) {
+    static int sms = 0, smem_set = 0;
+    if (sms == 0) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess) return false;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return false;
+    }
+    const int g = std::max(1, std::min(std::min(sms, kCoopSortGridMax), ceil_div(n, 2048)));
+    const int c = ceil_div(n, g);
+    if (c > kCoopSortMaxChunk) return false;
+    if (smem_set == 0) {
+        if (cudaFuncSetAttribute(sort2d_coop, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 kCoopSortMaxChunk * 10) != cudaSuccess)
+            return false;
+        smem_set = 1;
+    }
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, sort2d_coop, kCoopSortThreads, (size_t)c * 10) !=
+            cudaSuccess ||
+        occ < 1)
+        return false;
+    *grid = g;
+    *chunk = c;
+    return true;
+}
+
 cudaError_t keys_sort2d(const double* x, const double* y, const double* q, const uint8_t* act, Tree2D& t,
                         TreeScratch2D& s, double exp_pct, unsigned* err, cudaStream_t st, int* launches) {
     const int n = t.n;
@@ -512,8 +908,30 @@ cudaError_t keys_sort2d(const double* x, const double* y, const double* q, const
     const int bb_blocks = std::max(1, std::min(kBBoxBlocks, ceil_div(n, 256)));
     cudaError_t e = cudaMemsetAsync(s.lvl_ticket, 0, sizeof(unsigned) * kTicketWords, st);
     if (e != cudaSuccess) return e;
+    *launches += 1;
+    int coop_grid = 0, coop_chunk = 0;
+    if (2 * K <= 32 && s.coop_words && s.sort_aos && coop_sort_shape(n, &coop_grid, &coop_chunk)) {
+        uint32_t* k32 = reinterpret_cast<uint32_t*>(s.key_alt);
+        const size_t smem = (size_t)coop_chunk * 10;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(coop_grid);
+        cfg.blockDim = dim3(kCoopSortThreads);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        e = cudaLaunchKernelEx(&cfg, sort2d_coop, x, y, q, act, exp_pct, (2 * K + 7) / 8, t, s.bbox_partial,
+                               (double4*)s.sort_aos, k32, k32 + n, s.val_alt, t.perm, s.coop_words, coop_chunk,
+                               err);
+        if (e != cudaSuccess) return e;
+        *launches += 1;
+        return cudaGetLastError();
+    }
     bbox2d<<<bb_blocks, 256, 0, st>>>(x, y, n, exp_pct, K, t.geom, s.bbox_partial, done, err);
-    *launches += 2;
+    *launches += 1;
     uint32_t* vals = t.perm;
     if (2 * K <= 32) {
         // 32-bit keys in the two halves of key_alt

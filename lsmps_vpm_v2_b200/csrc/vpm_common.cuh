@@ -105,6 +105,34 @@ __device__ __forceinline__ bool block_fatal(const unsigned* err) {
     return s_fatal != 0;
 }
 
+// Grid barrier on a counter that only grows: the G blocks of barrier i take
+// it from i G to (i + 1) G, and a block waits until it reaches the next
+// multiple of G above the value its own arrival saw. One atomic per block and
+// no reset step, so the wait ends one memory round trip after the last
+// arrival. The counter must be zero at launch and used by one kernel only
+// (a word of its own, zeroed before every evaluation).
+__device__ __forceinline__ void grid_sync_counter(unsigned* bar, unsigned* err) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned old = atomicAdd(bar, 1u);
+        const unsigned target = (old / gridDim.x + 1u) * gridDim.x;
+        long long spins = 0;
+        for (;;) {
+            unsigned v;
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(bar) : "memory");
+            if ((int)(v - target) >= 0) break;
+            if (++spins > kSpinLimit) {
+                set_err(err, ERR_TIMEOUT);
+                break;
+            }
+            __nanosleep(16);
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
 __device__ __forceinline__ void grid_sync(unsigned* bar, unsigned* err) {
     __syncthreads();
     if (threadIdx.x == 0) {
