@@ -68,9 +68,10 @@ struct Tree2D {
     // accepts an entry only if that cell has the queried level and index.
     int32_t* dense;
     int dense_levels;
-    // Grid-barrier words of the cooperative level loops (tree levels at 0,
-    // M2M at 2, L2L at 4), zeroed with the tickets at the start of every
-    // evaluation; nullptr: launch level by level.
+    // Grid-barrier counters of the cooperative kernels (M2M levels at 2, L2L
+    // levels at 4, particle sort at 6), zeroed with the tickets at the start
+    // of every evaluation, each used by one kernel; nullptr: launch level by
+    // level.
     unsigned* gbar;
 };
 

@@ -172,14 +172,15 @@ m2m_level2d(Tree2D t, double2* __restrict__ a, const double* __restrict__ coef, 
 }
 
 // All M2M levels (depth-1 down to 1) in one cooperative launch, a grid
-// barrier between levels.
+// barrier between levels (barrier word: zeroed before every evaluation, used
+// by this kernel only).
 __global__ void __launch_bounds__(32 * kLevelWarps)
 m2m_levels_coop(Tree2D t, double2* __restrict__ a, const double* __restrict__ coef, int P, unsigned* bar,
                 unsigned* err) {
     const int depth = t.info->depth;
     for (int L = depth - 1; L >= 1; --L) {
         if (!block_fatal(err)) m2m_level_body(t, a, coef, P, L);
-        grid_sync(bar, err);
+        grid_sync_counter(bar, err);
     }
 }
 
@@ -231,7 +232,7 @@ l2l_levels_coop(Tree2D t, double2* __restrict__ b, const double* __restrict__ co
     const int depth = t.info->depth;
     for (int L = 3; L <= depth; ++L) {
         if (!block_fatal(err)) l2l_level_body(t, b, coef, P, L);
-        grid_sync(bar, err);
+        grid_sync_counter(bar, err);
     }
 }
 
