@@ -687,13 +687,15 @@ struct P2PF32 {
     using Acc = float;
     static __device__ __forceinline__ void shift(Elem& e, float ox, float oy) { e.x += ox; e.y += oy; }
     static __device__ __forceinline__ float inv(float r2) { return rcp_approx(r2); }
-    static constexpr int kMinBlocks = 8;   // <= 64 registers: 32 warps per SM
+    static constexpr int kWarps = 4;
+    static constexpr int kMinBlocks = 8;
 };
 struct P2PF64 {
     using Elem = double4;  // (x, y, q, -) in FP64, absolute coordinates
     using Acc = double;
     static __device__ __forceinline__ void shift(Elem&, float, float) {}
     static __device__ __forceinline__ double inv(double r2) { return rcp_nr(r2); }
+    static constexpr int kWarps = 4;
     static constexpr int kMinBlocks = 5;   // <= 102 registers
 };
 
@@ -927,32 +929,31 @@ p2p2d_tma(Tree2D t, Lists2D l, const typename Tr::Elem* __restrict__ src, const 
     }
 }
 
-// Warp-per-leaf P2P (the default near field). Each warp owns one leaf at a
-// time (grid-stride over leaves), so no block-wide barrier sits in the loop.
+// Warp-per-leaf P2P (the plain FP64 form's near field). Each warp owns one
+// leaf at a time (grid-stride over leaves), so no block-wide barrier sits in
+// the loop.
 // With H = ceil(T/4) lanes per split, lane (t, split) owns targets t, t+H,
 // t+2H, t+3H and the sources split, split + ns, ... (ns = 32/H) of every
 // list-1 cell, read straight from global memory (nearly warp-uniform
 // addresses, L1-resident). Split partials are summed in a fixed order through
-// a per-warp shared-memory tile. FP32 form: coordinates relative to the
-// target leaf (source-cell offset rounded once per cell).
-constexpr int kWarpP2PWarps = 4;
+// a per-warp shared-memory tile.
 constexpr int kP2PMeta = 64;   // list-1 cells staged per leaf (longer lists read them directly)
 
 template <class Tr>
-__global__ void __launch_bounds__(32 * kWarpP2PWarps, Tr::kMinBlocks)
+__global__ void __launch_bounds__(32 * Tr::kWarps, Tr::kMinBlocks)
 p2p2d_warp(Tree2D t, Lists2D l, const typename Tr::Elem* __restrict__ src, const double* __restrict__ fx,
            const double* __restrict__ fy, double* __restrict__ out0, double* __restrict__ out1, int velocity,
            double u_inf, double v_inf, unsigned* err) {
     using Elem = typename Tr::Elem;
-    __shared__ double s_red[kWarpP2PWarps][2 * kTPT][32];
+    __shared__ double s_red[Tr::kWarps][2 * kTPT][32];
     // list-1 cells of the warp's leaf: first/last slot, FP32-rounded centre
     // offset, loaded by the whole warp at once (one round of latency)
-    __shared__ int4 s_meta[kWarpP2PWarps][kP2PMeta];
+    __shared__ int4 s_meta[Tr::kWarps][kP2PMeta];
     if (fatal(err)) return;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int nl = t.info->n_leaves;
     const bool rel = sizeof(Elem) == sizeof(float4);
-    for (int li = blockIdx.x * kWarpP2PWarps + wib; li < nl; li += gridDim.x * kWarpP2PWarps) {
+    for (int li = blockIdx.x * Tr::kWarps + wib; li < nl; li += gridDim.x * Tr::kWarps) {
         const int c = t.leaf_cells[li];
         const int lo = t.c_lo[c], hi = t.c_hi[c];
         const double ccx = t.c_cx[c], ccy = t.c_cy[c];
@@ -1042,6 +1043,252 @@ p2p2d_warp(Tree2D t, Lists2D l, const typename Tr::Elem* __restrict__ src, const
                 }
             }
             __syncwarp();
+        }
+    }
+}
+
+// Warp-per-leaf FP32 near field (the mixed form's default). A chunk of
+// T <= 192 targets of the warp's leaf is spread over H lanes (the smallest
+// power of two with M = ceil(T/H) <= 12 targets per lane), so all 32 lanes
+// are busy and at most H - 1 target slots idle. The leaf's list-1 cells form
+// one flat sequence of sources; every step the warp stages the next 32 of
+// them in shared memory (one load per lane, issued a step ahead, moved into
+// the target leaf's frame by the FP32 cell offset and stored with x, y and q
+// duplicated so that they feed packed FP32x2 instructions directly), and
+// lane group ("split") s of the ns = 32/H groups applies staged sources
+// s, s + ns, ... to its M targets. Only a step that holds particles of the
+// leaf itself runs the variant that skips i == j. Every kTileFlush sources
+// the per-lane FP32 sums are reduced over the splits with shuffles into FP64
+// accumulators in shared memory (target k is kept by split k mod ns).
+constexpr int kTileWarps = 8;
+constexpr int kTileFlush = 64;
+constexpr int kTileMaxM = 12;
+constexpr int kTileChunk = 16 * kTileMaxM;      // targets per chunk (H <= 16, so ns >= 2)
+constexpr int kTileSlots = kTileMaxM / 2;       // FP64 target slots per lane (ns >= 2)
+
+struct TileShared {
+    float4 xy[kTileWarps][32];                     // (x, x, y, y) of the staged sources
+    float2 qq[kTileWarps][32];                     // (q, q)
+    int4 meta[kTileWarps][kP2PMeta];               // (lo, size, ox, oy) per list-1 cell
+    int cs[kTileWarps][kP2PMeta + 1];              // flat start of each cell, then the total
+    double acc[kTileWarps][2 * kTileSlots][32];    // FP64 accumulators: row 2i x, 2i+1 y of slot i
+};
+
+// Staged sources j0, j0 + ns, ... < cnt applied to the lane's M targets.
+// SELF: staged source j is particle e0 + j - (this lane's first target) of the
+// leaf, and adds nothing to target k when that equals k H.
+template <int M, bool SELF>
+__device__ __forceinline__ void tile_pairs(const float4* xy, const float2* qq, int j0, int cnt, int ns, int hs, int e0,
+                                           const float2* nx, const float2* ny, float nxo, float nyo, float2* px,
+                                           float2* py, float& pxo, float& pyo) {
+    constexpr int MP = M / 2;
+    constexpr bool ODD = (M & 1) != 0;
+    for (int j = j0; j < cnt; j += ns) {
+        const float4 sv = xy[j];
+        const float2 sq = qq[j];
+        const float2 sx = make_float2(sv.x, sv.y), sy = make_float2(sv.z, sv.w);
+        const int e = e0 + j;
+        #pragma unroll
+        for (int h = 0; h < MP; ++h) {
+            const float2 dx = __fadd2_rn(nx[h], sx), dy = __fadd2_rn(ny[h], sy);
+            const float2 r2 = __ffma2_rn(dy, dy, __fmul2_rn(dx, dx));
+            float2 fq = __fmul2_rn(sq, make_float2(rcp_approx(r2.x), rcp_approx(r2.y)));
+            if (SELF) {
+                if (e == ((2 * h) << hs)) fq.x = 0.f;
+                if (e == ((2 * h + 1) << hs)) fq.y = 0.f;
+            }
+            px[h] = __ffma2_rn(fq, dx, px[h]);
+            py[h] = __ffma2_rn(fq, dy, py[h]);
+        }
+        if (ODD) {
+            const float dx = nxo + sv.x, dy = nyo + sv.z;
+            float fq = sq.x * rcp_approx(fmaf(dy, dy, dx * dx));
+            if (SELF && e == ((M - 1) << hs)) fq = 0.f;
+            pxo = fmaf(fq, dx, pxo);
+            pyo = fmaf(fq, dy, pyo);
+        }
+    }
+}
+
+template <int M>
+__device__ __forceinline__ void tile_chunk(TileShared& sm, const Tree2D& t, const Lists2D& l,
+                                           const float4* __restrict__ src, int c, int lo, double ccx, double ccy,
+                                           uint32_t o1, int n1, int tb, int T, int hs, const double* fx,
+                                           const double* fy, double* out0, double* out1, int velocity, double u_inf,
+                                           double v_inf, unsigned* err) {
+    constexpr int MP = M / 2;
+    constexpr int NP = MP > 0 ? MP : 1;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int H = 1 << hs, ns = 32 >> hs;
+    const int tt = lane & (H - 1), split = lane >> hs;
+    // negated target coordinates (leaf frame); target k of this lane is chunk slot tt + k H
+    float2 nx[NP], ny[NP], px[NP], py[NP];
+    float nxo = 0.f, nyo = 0.f, pxo = 0.f, pyo = 0.f;
+    #pragma unroll
+    for (int h = 0; h < MP; ++h) {
+        const int i0 = tt + ((2 * h) << hs), i1 = tt + ((2 * h + 1) << hs);
+        const float4 g0 = src[tb + (i0 < T ? i0 : 0)], g1 = src[tb + (i1 < T ? i1 : 0)];
+        nx[h] = make_float2(-g0.x, -g1.x);
+        ny[h] = make_float2(-g0.y, -g1.y);
+        px[h] = py[h] = make_float2(0.f, 0.f);
+    }
+    if (M & 1) {
+        const int i0 = tt + ((M - 1) << hs);
+        const float4 g0 = src[tb + (i0 < T ? i0 : 0)];
+        nxo = -g0.x;
+        nyo = -g0.y;
+    }
+    double* acc = &sm.acc[wib][0][lane];
+    #pragma unroll
+    for (int i = 0; i < 2 * kTileSlots; ++i) acc[32 * i] = 0.0;
+    // reduce the FP32 partials over the splits into the FP64 slots
+    auto flush = [&]() {
+        #pragma unroll
+        for (int k = 0; k < M; ++k) {
+            float vx = (k < 2 * MP) ? ((k & 1) ? px[k >> 1].y : px[k >> 1].x) : pxo;
+            float vy = (k < 2 * MP) ? ((k & 1) ? py[k >> 1].y : py[k >> 1].x) : pyo;
+            for (int o = H; o < 32; o <<= 1) {
+                vx += __shfl_xor_sync(0xffffffffu, vx, o);
+                vy += __shfl_xor_sync(0xffffffffu, vy, o);
+            }
+            if ((k & (ns - 1)) == split) {
+                const int slot = k >> (5 - hs);
+                acc[32 * (2 * slot)] -= (double)vx;
+                acc[32 * (2 * slot + 1)] -= (double)vy;
+            }
+        }
+        #pragma unroll
+        for (int h = 0; h < MP; ++h) px[h] = py[h] = make_float2(0.f, 0.f);
+        pxo = pyo = 0.f;
+    };
+    int steps = 0;   // staged sources applied by this lane since the last flush, times ns
+    for (int seg = 0; seg < n1; seg += kP2PMeta) {
+        const int nseg = min(kP2PMeta, n1 - seg);
+        __syncwarp();
+        // metadata and flat prefix of the segment; the own cell's flat range
+        int own = -1;
+        {
+            int sz[2] = {0, 0};
+            #pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int k = lane + 32 * h;
+                if (k < nseg) {
+                    const int sc = l.l1_src[o1 + seg + k];
+                    const int slo = t.c_lo[sc];
+                    sz[h] = t.c_hi[sc] - slo;
+                    const float ox = (float)(t.c_cx[sc] - ccx), oy = (float)(t.c_cy[sc] - ccy);
+                    sm.meta[wib][k] = make_int4(slo, sz[h], __float_as_int(ox), __float_as_int(oy));
+                    if (sc == c) own = k;
+                }
+            }
+            own = __reduce_max_sync(0xffffffffu, own);
+            int inc0 = sz[0], inc1 = sz[1];
+            #pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int a0 = __shfl_up_sync(0xffffffffu, inc0, o), a1 = __shfl_up_sync(0xffffffffu, inc1, o);
+                if (lane >= o) {
+                    inc0 += a0;
+                    inc1 += a1;
+                }
+            }
+            const int tot0 = __shfl_sync(0xffffffffu, inc0, 31);
+            const int tot1 = __shfl_sync(0xffffffffu, inc1, 31);
+            if (lane < nseg) sm.cs[wib][lane] = inc0 - sz[0];
+            if (lane + 32 < nseg) sm.cs[wib][lane + 32] = tot0 + inc1 - sz[1];
+            if (lane == 0) sm.cs[wib][nseg] = tot0 + tot1;
+        }
+        __syncwarp();
+        const int total = sm.cs[wib][nseg];
+        const int own0 = own >= 0 ? sm.cs[wib][own] : -1;
+        const int own1 = own >= 0 ? sm.cs[wib][own + 1] : -1;
+        // staged source j of step cb is flat source cb + j; within the own cell
+        // that is particle lo + (cb + j - own0); minus this lane's first target tb + tt
+        const int e_base = lo - own0 - tb - tt;
+        // per-lane walker over the flat sequence: lane stages flat source m = cb + lane
+        int k = 0, o = lane;
+        while (k < nseg && o >= sm.meta[wib][k].y) {
+            o -= sm.meta[wib][k].y;
+            ++k;
+        }
+        auto fetch = [&]() -> float4 {
+            if (k >= nseg) return make_float4(0.f, 0.f, 0.f, 0.f);
+            const int4 mt = sm.meta[wib][k];
+            float4 v = src[mt.x + o];
+            v.x += __int_as_float(mt.z);
+            v.y += __int_as_float(mt.w);
+            return v;
+        };
+        float4 pv = fetch();
+        for (int cb = 0; cb < total; cb += 32) {
+            sm.xy[wib][lane] = make_float4(pv.x, pv.x, pv.y, pv.y);
+            sm.qq[wib][lane] = make_float2(pv.z, pv.z);
+            __syncwarp();
+            // advance the walker by 32 and prefetch the next step's source
+            o += 32;
+            while (k < nseg && o >= sm.meta[wib][k].y) {
+                o -= sm.meta[wib][k].y;
+                ++k;
+            }
+            pv = fetch();
+            const int cnt = min(32, total - cb);
+            if (own0 >= 0 && cb < own1 && cb + cnt > own0)
+                tile_pairs<M, true>(sm.xy[wib], sm.qq[wib], split, cnt, ns, hs, e_base + cb, nx, ny, nxo, nyo, px, py,
+                                    pxo, pyo);
+            else
+                tile_pairs<M, false>(sm.xy[wib], sm.qq[wib], split, cnt, ns, hs, 0, nx, ny, nxo, nyo, px, py, pxo,
+                                     pyo);
+            __syncwarp();
+            steps += 32;
+            if (steps >= kTileFlush * ns) {
+                flush();
+                steps = 0;
+            }
+        }
+    }
+    flush();
+    __syncwarp();
+    #pragma unroll
+    for (int i = 0; i < kTileSlots; ++i) {
+        const int kk = split + (i << (5 - hs));
+        const int ti = tt + (kk << hs);
+        if (kk < M && ti < T)
+            p2p_store(t, tb + ti, acc[32 * (2 * i)], acc[32 * (2 * i + 1)], fx, fy, out0, out1, velocity, u_inf, v_inf,
+                      err);
+    }
+    __syncwarp();
+}
+
+__global__ void __launch_bounds__(32 * kTileWarps, 2)
+p2p2d_tile_f32(Tree2D t, Lists2D l, const float4* __restrict__ src, const double* __restrict__ fx,
+               const double* __restrict__ fy, double* __restrict__ out0, double* __restrict__ out1, int velocity,
+               double u_inf, double v_inf, unsigned* err) {
+    __shared__ TileShared sm;
+    if (fatal(err)) return;
+    const int wib = threadIdx.x >> 5;
+    const int nl = t.info->n_leaves;
+    for (int li = blockIdx.x * kTileWarps + wib; li < nl; li += gridDim.x * kTileWarps) {
+        const int c = t.leaf_cells[li];
+        const int lo = t.c_lo[c], hi = t.c_hi[c];
+        const double ccx = t.c_cx[c], ccy = t.c_cy[c];
+        const uint32_t o1 = l.l1_off[li];
+        const int n1 = (int)(l.l1_off[li + 1] - o1);
+        for (int tb = lo; tb < hi; tb += kTileChunk) {
+            const int T = min(kTileChunk, hi - tb);
+            int hs = 0;   // the smallest H = 2^hs with ceil(T / H) <= kTileMaxM (H <= 16)
+            while (((T + (1 << hs) - 1) >> hs) > kTileMaxM) ++hs;
+            const int M = (T + (1 << hs) - 1) >> hs;
+            switch (M) {
+#define VPM_TILE_CASE(MM)                                                                                           \
+    case MM:                                                                                                        \
+        tile_chunk<MM>(sm, t, l, src, c, lo, ccx, ccy, o1, n1, tb, T, hs, fx, fy, out0, out1, velocity, u_inf, v_inf, \
+                       err);                                                                                        \
+        break;
+                VPM_TILE_CASE(1) VPM_TILE_CASE(2) VPM_TILE_CASE(3) VPM_TILE_CASE(4) VPM_TILE_CASE(5) VPM_TILE_CASE(6)
+                VPM_TILE_CASE(7) VPM_TILE_CASE(8) VPM_TILE_CASE(9) VPM_TILE_CASE(10) VPM_TILE_CASE(11)
+                VPM_TILE_CASE(12)
+#undef VPM_TILE_CASE
+                default: break;
+            }
         }
     }
 }
@@ -1319,8 +1566,7 @@ cudaError_t fmm2d_p2p_f32(const Tree2D& t, const Lists2D& l, const Expansions2D&
     Expansions2D en = e;
     if (near_only) en.fx = en.fy = nullptr;
     if (max_par < 0) return launch_p2p_tma<P2PF32>(t, l, rel, en, out0, out1, velocity, u_inf, v_inf, err, st, -max_par);
-    p2p2d_warp<P2PF32><<<148 * 16, 32 * kWarpP2PWarps, 0, st>>>(t, l, rel, en.fx, en.fy, out0, out1, velocity, u_inf,
-                                                               v_inf, err);
+    p2p2d_tile_f32<<<148 * 2, 32 * kTileWarps, 0, st>>>(t, l, rel, en.fx, en.fy, out0, out1, velocity, u_inf, v_inf, err);
     return cudaGetLastError();
 }
 
@@ -1332,8 +1578,8 @@ cudaError_t fmm2d_p2p_f64_tma(const Tree2D& t, const Lists2D& l, const Expansion
     Expansions2D en = e;
     if (near_only) en.fx = en.fy = nullptr;
     if (max_par < 0) return launch_p2p_tma<P2PF64>(t, l, aos, en, out0, out1, velocity, u_inf, v_inf, err, st, -max_par);
-    p2p2d_warp<P2PF64><<<148 * 16, 32 * kWarpP2PWarps, 0, st>>>(t, l, aos, en.fx, en.fy, out0, out1, velocity, u_inf,
-                                                               v_inf, err);
+    p2p2d_warp<P2PF64><<<148 * 64 / P2PF64::kWarps, 32 * P2PF64::kWarps, 0, st>>>(
+        t, l, aos, en.fx, en.fy, out0, out1, velocity, u_inf, v_inf, err);
     return cudaGetLastError();
 }
 
