@@ -687,8 +687,6 @@ struct P2PF32 {
     using Acc = float;
     static __device__ __forceinline__ void shift(Elem& e, float ox, float oy) { e.x += ox; e.y += oy; }
     static __device__ __forceinline__ float inv(float r2) { return rcp_approx(r2); }
-    static constexpr int kWarps = 4;
-    static constexpr int kMinBlocks = 8;
 };
 struct P2PF64 {
     using Elem = double4;  // (x, y, q, -) in FP64, absolute coordinates
@@ -1051,59 +1049,82 @@ p2p2d_warp(Tree2D t, Lists2D l, const typename Tr::Elem* __restrict__ src, const
 // T <= 192 targets of the warp's leaf is spread over H lanes (the smallest
 // power of two with M = ceil(T/H) <= 12 targets per lane), so all 32 lanes
 // are busy and at most H - 1 target slots idle. The leaf's list-1 cells form
-// one flat sequence of sources; every step the warp stages the next 32 of
-// them in shared memory (one load per lane, issued a step ahead, moved into
+// one flat sequence of sources; every step the warp stages the next
+// kTileStage of them in shared memory (loads issued a step ahead, moved into
 // the target leaf's frame by the FP32 cell offset and stored with x, y and q
 // duplicated so that they feed packed FP32x2 instructions directly), and
 // lane group ("split") s of the ns = 32/H groups applies staged sources
-// s, s + ns, ... to its M targets. Only a step that holds particles of the
-// leaf itself runs the variant that skips i == j. Every kTileFlush sources
-// the per-lane FP32 sums are reduced over the splits with shuffles into FP64
-// accumulators in shared memory (target k is kept by split k mod ns).
+// s, s + ns, ... to its M targets. Every kTileFlush sources the per-lane FP32
+// sums are reduced over the splits with shuffles into FP64 accumulators in
+// shared memory (target k is kept by split k mod ns).
+//
+// i == j needs no test: r^2 is formed as dx dx + dy dy + kTileEps, and a
+// particle of the leaf meets itself at dx = dy = 0 exactly (the own cell's
+// offset is zero), so q / kTileEps multiplies zero offsets. kTileEps is far
+// below the square of the smallest non-zero FP32 offset in leaf-relative
+// coordinates and keeps q / kTileEps finite for |q| < 3e8.
 constexpr int kTileWarps = 8;
 constexpr int kTileFlush = 64;
-constexpr int kTileMaxM = 12;
+constexpr int kTileMaxM = 6;
 constexpr int kTileChunk = 16 * kTileMaxM;      // targets per chunk (H <= 16, so ns >= 2)
 constexpr int kTileSlots = kTileMaxM / 2;       // FP64 target slots per lane (ns >= 2)
+constexpr int kTileStage = 64;                  // sources staged per step (two per lane)
+constexpr float kTileEps = 1e-30f;
 
 struct TileShared {
-    float4 xy[kTileWarps][32];                     // (x, x, y, y) of the staged sources
-    float2 qq[kTileWarps][32];                     // (q, q)
+    float4 xy[kTileWarps][kTileStage];             // (x, x, y, y) of the staged sources
+    float2 qq[kTileWarps][kTileStage];             // (q, q)
     int4 meta[kTileWarps][kP2PMeta];               // (lo, size, ox, oy) per list-1 cell
     int cs[kTileWarps][kP2PMeta + 1];              // flat start of each cell, then the total
     double acc[kTileWarps][2 * kTileSlots][32];    // FP64 accumulators: row 2i x, 2i+1 y of slot i
 };
 
+// Two targets (packed: low half the first) against one source, on the
+// packed FP32x2 instructions: d = -t + s, r2 = d.d + eps, f = q rcp(r2),
+// p += f d.
+__device__ __forceinline__ void tile_pair2(uint64_t nx, uint64_t ny, uint64_t sx, uint64_t sy, uint64_t sq,
+                                           uint64_t eps, uint64_t& px, uint64_t& py) {
+    asm("{\n\t"
+        ".reg .b64 dx, dy, r2, rr, fq;\n\t"
+        ".reg .f32 a, b;\n\t"
+        "add.rn.f32x2 dx, %2, %4;\n\t"
+        "add.rn.f32x2 dy, %3, %5;\n\t"
+        "fma.rn.f32x2 r2, dx, dx, %7;\n\t"
+        "fma.rn.f32x2 r2, dy, dy, r2;\n\t"
+        "mov.b64 {a, b}, r2;\n\t"
+        "rcp.approx.ftz.f32 a, a;\n\t"
+        "rcp.approx.ftz.f32 b, b;\n\t"
+        "mov.b64 rr, {a, b};\n\t"
+        "mul.rn.f32x2 fq, %6, rr;\n\t"
+        "fma.rn.f32x2 %0, fq, dx, %0;\n\t"
+        "fma.rn.f32x2 %1, fq, dy, %1;\n\t"
+        "}"
+        : "+l"(px), "+l"(py)
+        : "l"(nx), "l"(ny), "l"(sx), "l"(sy), "l"(sq), "l"(eps));
+}
+
+__device__ __forceinline__ uint64_t pack2(float lo, float hi) {
+    return ((uint64_t)__float_as_uint(hi) << 32) | (uint64_t)__float_as_uint(lo);
+}
+__device__ __forceinline__ float lo2(uint64_t v) { return __uint_as_float((uint32_t)v); }
+__device__ __forceinline__ float hi2(uint64_t v) { return __uint_as_float((uint32_t)(v >> 32)); }
+
 // Staged sources j0, j0 + ns, ... < cnt applied to the lane's M targets.
-// SELF: staged source j is particle e0 + j - (this lane's first target) of the
-// leaf, and adds nothing to target k when that equals k H.
-template <int M, bool SELF>
-__device__ __forceinline__ void tile_pairs(const float4* xy, const float2* qq, int j0, int cnt, int ns, int hs, int e0,
-                                           const float2* nx, const float2* ny, float nxo, float nyo, float2* px,
-                                           float2* py, float& pxo, float& pyo) {
+template <int M>
+__device__ __forceinline__ void tile_pairs(const ulonglong2* xy, const uint64_t* qq, int j0, int cnt, int ns,
+                                           const uint64_t* nx, const uint64_t* ny, float nxo, float nyo, uint64_t* px,
+                                           uint64_t* py, float& pxo, float& pyo) {
     constexpr int MP = M / 2;
     constexpr bool ODD = (M & 1) != 0;
+    const uint64_t eps = pack2(kTileEps, kTileEps);
     for (int j = j0; j < cnt; j += ns) {
-        const float4 sv = xy[j];
-        const float2 sq = qq[j];
-        const float2 sx = make_float2(sv.x, sv.y), sy = make_float2(sv.z, sv.w);
-        const int e = e0 + j;
+        const ulonglong2 sv = xy[j];   // (x, x), (y, y)
+        const uint64_t sq = qq[j];     // (q, q)
         #pragma unroll
-        for (int h = 0; h < MP; ++h) {
-            const float2 dx = __fadd2_rn(nx[h], sx), dy = __fadd2_rn(ny[h], sy);
-            const float2 r2 = __ffma2_rn(dy, dy, __fmul2_rn(dx, dx));
-            float2 fq = __fmul2_rn(sq, make_float2(rcp_approx(r2.x), rcp_approx(r2.y)));
-            if (SELF) {
-                if (e == ((2 * h) << hs)) fq.x = 0.f;
-                if (e == ((2 * h + 1) << hs)) fq.y = 0.f;
-            }
-            px[h] = __ffma2_rn(fq, dx, px[h]);
-            py[h] = __ffma2_rn(fq, dy, py[h]);
-        }
+        for (int h = 0; h < MP; ++h) tile_pair2(nx[h], ny[h], sv.x, sv.y, sq, eps, px[h], py[h]);
         if (ODD) {
-            const float dx = nxo + sv.x, dy = nyo + sv.z;
-            float fq = sq.x * rcp_approx(fmaf(dy, dy, dx * dx));
-            if (SELF && e == ((M - 1) << hs)) fq = 0.f;
+            const float dx = nxo + lo2(sv.x), dy = nyo + lo2(sv.y);
+            const float fq = lo2(sq) * rcp_approx(fmaf(dy, dy, fmaf(dx, dx, kTileEps)));
             pxo = fmaf(fq, dx, pxo);
             pyo = fmaf(fq, dy, pyo);
         }
@@ -1112,25 +1133,25 @@ __device__ __forceinline__ void tile_pairs(const float4* xy, const float2* qq, i
 
 template <int M>
 __device__ __forceinline__ void tile_chunk(TileShared& sm, const Tree2D& t, const Lists2D& l,
-                                           const float4* __restrict__ src, int c, int lo, double ccx, double ccy,
-                                           uint32_t o1, int n1, int tb, int T, int hs, const double* fx,
-                                           const double* fy, double* out0, double* out1, int velocity, double u_inf,
-                                           double v_inf, unsigned* err) {
+                                           const float4* __restrict__ src, int c, double ccx, double ccy, uint32_t o1,
+                                           int n1, int tb, int T, int hs, const double* fx, const double* fy,
+                                           double* out0, double* out1, int velocity, double u_inf, double v_inf,
+                                           unsigned* err) {
     constexpr int MP = M / 2;
     constexpr int NP = MP > 0 ? MP : 1;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int H = 1 << hs, ns = 32 >> hs;
     const int tt = lane & (H - 1), split = lane >> hs;
     // negated target coordinates (leaf frame); target k of this lane is chunk slot tt + k H
-    float2 nx[NP], ny[NP], px[NP], py[NP];
+    uint64_t nx[NP], ny[NP], px[NP], py[NP];
     float nxo = 0.f, nyo = 0.f, pxo = 0.f, pyo = 0.f;
     #pragma unroll
     for (int h = 0; h < MP; ++h) {
         const int i0 = tt + ((2 * h) << hs), i1 = tt + ((2 * h + 1) << hs);
         const float4 g0 = src[tb + (i0 < T ? i0 : 0)], g1 = src[tb + (i1 < T ? i1 : 0)];
-        nx[h] = make_float2(-g0.x, -g1.x);
-        ny[h] = make_float2(-g0.y, -g1.y);
-        px[h] = py[h] = make_float2(0.f, 0.f);
+        nx[h] = pack2(-g0.x, -g1.x);
+        ny[h] = pack2(-g0.y, -g1.y);
+        px[h] = py[h] = 0ull;
     }
     if (M & 1) {
         const int i0 = tt + ((M - 1) << hs);
@@ -1145,8 +1166,8 @@ __device__ __forceinline__ void tile_chunk(TileShared& sm, const Tree2D& t, cons
     auto flush = [&]() {
         #pragma unroll
         for (int k = 0; k < M; ++k) {
-            float vx = (k < 2 * MP) ? ((k & 1) ? px[k >> 1].y : px[k >> 1].x) : pxo;
-            float vy = (k < 2 * MP) ? ((k & 1) ? py[k >> 1].y : py[k >> 1].x) : pyo;
+            float vx = (k < 2 * MP) ? ((k & 1) ? hi2(px[k >> 1]) : lo2(px[k >> 1])) : pxo;
+            float vy = (k < 2 * MP) ? ((k & 1) ? hi2(py[k >> 1]) : lo2(py[k >> 1])) : pyo;
             for (int o = H; o < 32; o <<= 1) {
                 vx += __shfl_xor_sync(0xffffffffu, vx, o);
                 vy += __shfl_xor_sync(0xffffffffu, vy, o);
@@ -1158,15 +1179,14 @@ __device__ __forceinline__ void tile_chunk(TileShared& sm, const Tree2D& t, cons
             }
         }
         #pragma unroll
-        for (int h = 0; h < MP; ++h) px[h] = py[h] = make_float2(0.f, 0.f);
+        for (int h = 0; h < MP; ++h) px[h] = py[h] = 0ull;
         pxo = pyo = 0.f;
     };
-    int steps = 0;   // staged sources applied by this lane since the last flush, times ns
+    int steps = 0;   // staged sources since the last flush (each lane applied steps / ns of them)
     for (int seg = 0; seg < n1; seg += kP2PMeta) {
         const int nseg = min(kP2PMeta, n1 - seg);
         __syncwarp();
-        // metadata and flat prefix of the segment; the own cell's flat range
-        int own = -1;
+        // metadata and flat prefix of the segment
         {
             int sz[2] = {0, 0};
             #pragma unroll
@@ -1178,10 +1198,8 @@ __device__ __forceinline__ void tile_chunk(TileShared& sm, const Tree2D& t, cons
                     sz[h] = t.c_hi[sc] - slo;
                     const float ox = (float)(t.c_cx[sc] - ccx), oy = (float)(t.c_cy[sc] - ccy);
                     sm.meta[wib][k] = make_int4(slo, sz[h], __float_as_int(ox), __float_as_int(oy));
-                    if (sc == c) own = k;
                 }
             }
-            own = __reduce_max_sync(0xffffffffu, own);
             int inc0 = sz[0], inc1 = sz[1];
             #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
@@ -1199,18 +1217,18 @@ __device__ __forceinline__ void tile_chunk(TileShared& sm, const Tree2D& t, cons
         }
         __syncwarp();
         const int total = sm.cs[wib][nseg];
-        const int own0 = own >= 0 ? sm.cs[wib][own] : -1;
-        const int own1 = own >= 0 ? sm.cs[wib][own + 1] : -1;
-        // staged source j of step cb is flat source cb + j; within the own cell
-        // that is particle lo + (cb + j - own0); minus this lane's first target tb + tt
-        const int e_base = lo - own0 - tb - tt;
-        // per-lane walker over the flat sequence: lane stages flat source m = cb + lane
-        int k = 0, o = lane;
-        while (k < nseg && o >= sm.meta[wib][k].y) {
-            o -= sm.meta[wib][k].y;
-            ++k;
+        // per-lane walkers over the flat sequence: the lane stages flat sources
+        // cb + lane and cb + 32 + lane of step cb
+        int k0 = 0, q0 = lane, k1 = 0, q1 = lane + 32;
+        while (k0 < nseg && q0 >= sm.meta[wib][k0].y) {
+            q0 -= sm.meta[wib][k0].y;
+            ++k0;
         }
-        auto fetch = [&]() -> float4 {
+        while (k1 < nseg && q1 >= sm.meta[wib][k1].y) {
+            q1 -= sm.meta[wib][k1].y;
+            ++k1;
+        }
+        auto fetch = [&](int k, int o) -> float4 {
             if (k >= nseg) return make_float4(0.f, 0.f, 0.f, 0.f);
             const int4 mt = sm.meta[wib][k];
             float4 v = src[mt.x + o];
@@ -1218,27 +1236,28 @@ __device__ __forceinline__ void tile_chunk(TileShared& sm, const Tree2D& t, cons
             v.y += __int_as_float(mt.w);
             return v;
         };
-        float4 pv = fetch();
-        for (int cb = 0; cb < total; cb += 32) {
-            sm.xy[wib][lane] = make_float4(pv.x, pv.x, pv.y, pv.y);
-            sm.qq[wib][lane] = make_float2(pv.z, pv.z);
-            __syncwarp();
-            // advance the walker by 32 and prefetch the next step's source
-            o += 32;
+        auto advance = [&](int& k, int& o) {
+            o += kTileStage;
             while (k < nseg && o >= sm.meta[wib][k].y) {
                 o -= sm.meta[wib][k].y;
                 ++k;
             }
-            pv = fetch();
-            const int cnt = min(32, total - cb);
-            if (own0 >= 0 && cb < own1 && cb + cnt > own0)
-                tile_pairs<M, true>(sm.xy[wib], sm.qq[wib], split, cnt, ns, hs, e_base + cb, nx, ny, nxo, nyo, px, py,
-                                    pxo, pyo);
-            else
-                tile_pairs<M, false>(sm.xy[wib], sm.qq[wib], split, cnt, ns, hs, 0, nx, ny, nxo, nyo, px, py, pxo,
-                                     pyo);
+        };
+        float4 pv0 = fetch(k0, q0), pv1 = fetch(k1, q1);
+        for (int cb = 0; cb < total; cb += kTileStage) {
+            sm.xy[wib][lane] = make_float4(pv0.x, pv0.x, pv0.y, pv0.y);
+            sm.qq[wib][lane] = make_float2(pv0.z, pv0.z);
+            sm.xy[wib][lane + 32] = make_float4(pv1.x, pv1.x, pv1.y, pv1.y);
+            sm.qq[wib][lane + 32] = make_float2(pv1.z, pv1.z);
             __syncwarp();
-            steps += 32;
+            advance(k0, q0);
+            advance(k1, q1);
+            pv0 = fetch(k0, q0);
+            pv1 = fetch(k1, q1);
+            tile_pairs<M>(reinterpret_cast<const ulonglong2*>(sm.xy[wib]), reinterpret_cast<const uint64_t*>(sm.qq[wib]),
+                          split, min(kTileStage, total - cb), ns, nx, ny, nxo, nyo, px, py, pxo, pyo);
+            __syncwarp();
+            steps += kTileStage;
             if (steps >= kTileFlush * ns) {
                 flush();
                 steps = 0;
@@ -1258,7 +1277,7 @@ __device__ __forceinline__ void tile_chunk(TileShared& sm, const Tree2D& t, cons
     __syncwarp();
 }
 
-__global__ void __launch_bounds__(32 * kTileWarps, 2)
+__global__ void __launch_bounds__(32 * kTileWarps, 3)
 p2p2d_tile_f32(Tree2D t, Lists2D l, const float4* __restrict__ src, const double* __restrict__ fx,
                const double* __restrict__ fy, double* __restrict__ out0, double* __restrict__ out1, int velocity,
                double u_inf, double v_inf, unsigned* err) {
@@ -1280,12 +1299,10 @@ p2p2d_tile_f32(Tree2D t, Lists2D l, const float4* __restrict__ src, const double
             switch (M) {
 #define VPM_TILE_CASE(MM)                                                                                           \
     case MM:                                                                                                        \
-        tile_chunk<MM>(sm, t, l, src, c, lo, ccx, ccy, o1, n1, tb, T, hs, fx, fy, out0, out1, velocity, u_inf, v_inf, \
+        tile_chunk<MM>(sm, t, l, src, c, ccx, ccy, o1, n1, tb, T, hs, fx, fy, out0, out1, velocity, u_inf, v_inf,     \
                        err);                                                                                        \
         break;
                 VPM_TILE_CASE(1) VPM_TILE_CASE(2) VPM_TILE_CASE(3) VPM_TILE_CASE(4) VPM_TILE_CASE(5) VPM_TILE_CASE(6)
-                VPM_TILE_CASE(7) VPM_TILE_CASE(8) VPM_TILE_CASE(9) VPM_TILE_CASE(10) VPM_TILE_CASE(11)
-                VPM_TILE_CASE(12)
 #undef VPM_TILE_CASE
                 default: break;
             }
@@ -1566,7 +1583,7 @@ cudaError_t fmm2d_p2p_f32(const Tree2D& t, const Lists2D& l, const Expansions2D&
     Expansions2D en = e;
     if (near_only) en.fx = en.fy = nullptr;
     if (max_par < 0) return launch_p2p_tma<P2PF32>(t, l, rel, en, out0, out1, velocity, u_inf, v_inf, err, st, -max_par);
-    p2p2d_tile_f32<<<148 * 2, 32 * kTileWarps, 0, st>>>(t, l, rel, en.fx, en.fy, out0, out1, velocity, u_inf, v_inf, err);
+    p2p2d_tile_f32<<<148 * 3, 32 * kTileWarps, 0, st>>>(t, l, rel, en.fx, en.fy, out0, out1, velocity, u_inf, v_inf, err);
     return cudaGetLastError();
 }
 
