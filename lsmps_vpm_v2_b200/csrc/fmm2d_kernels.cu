@@ -580,16 +580,20 @@ p2p2d(Tree2D t, Lists2D l, const double* __restrict__ fx, const double* __restri
 
 // ---- mixed form: FP32 near field ---------------------------------------------
 
-// Leaf-relative FP32 coordinates and FP32 strengths: x - c_leaf is formed in
-// FP64 (exact enough: |x - c| <= cell size) and rounded once.
+// Leaf-relative FP32 coordinates in units of the leaf's size, and FP32
+// strengths: (x - c_leaf) 2^L / root is formed in FP64 and rounded once, so
+// every coordinate lies in [-1/2, 1/2] whatever the scale of the input.
 __global__ void leaf_relative_f32(Tree2D t, float4* __restrict__ rel, unsigned* err) {
     if (fatal(err)) return;
     const int nl = t.info->n_leaves;
+    const double root = t.geom->root;
     for (int li = blockIdx.x; li < nl; li += gridDim.x) {
         const int c = t.leaf_cells[li];
         const double cx = t.c_cx[c], cy = t.c_cy[c];
+        const double ih = ldexp(1.0, (int)t.c_level[c]) / root;
         for (int i = t.c_lo[c] + threadIdx.x; i < t.c_hi[c]; i += blockDim.x)
-            rel[i] = make_float4((float)(t.px[i] - cx), (float)(t.py[i] - cy), (float)t.pq[i], __int_as_float(i));
+            rel[i] = make_float4((float)((t.px[i] - cx) * ih), (float)((t.py[i] - cy) * ih), (float)t.pq[i],
+                                 __int_as_float(i));
     }
 }
 
@@ -1051,30 +1055,34 @@ p2p2d_warp(Tree2D t, Lists2D l, const typename Tr::Elem* __restrict__ src, const
 // are busy and at most H - 1 target slots idle. The leaf's list-1 cells form
 // one flat sequence of sources; every step the warp stages the next
 // kTileStage of them in shared memory (loads issued a step ahead, moved into
-// the target leaf's frame by the FP32 cell offset and stored with x, y and q
-// duplicated so that they feed packed FP32x2 instructions directly), and
+// the target leaf's frame: scaled by the exact power of two between the two
+// leaves' sizes plus the FP32 cell offset; stored with x, y and q duplicated
+// so that they feed packed FP32x2 instructions directly), and
 // lane group ("split") s of the ns = 32/H groups applies staged sources
 // s, s + ns, ... to its M targets. Every kTileFlush sources the per-lane FP32
 // sums are reduced over the splits with shuffles into FP64 accumulators in
-// shared memory (target k is kept by split k mod ns).
+// shared memory (target k is kept by split k mod ns); the sums are in units
+// of the leaf size and are scaled back on the store.
 //
 // i == j needs no test: r^2 is formed as dx dx + dy dy + kTileEps, and a
 // particle of the leaf meets itself at dx = dy = 0 exactly (the own cell's
-// offset is zero), so q / kTileEps multiplies zero offsets. kTileEps is far
-// below the square of the smallest non-zero FP32 offset in leaf-relative
-// coordinates and keeps q / kTileEps finite for |q| < 3e8.
+// offset is zero, its scale one), so q / kTileEps multiplies zero offsets.
+// In leaf units, the smallest non-zero FP32 offset squared is about 1e-15,
+// so kTileEps changes no other pair, and q / kTileEps stays finite for
+// |q| < 3e14.
 constexpr int kTileWarps = 8;
 constexpr int kTileFlush = 64;
 constexpr int kTileMaxM = 6;
 constexpr int kTileChunk = 16 * kTileMaxM;      // targets per chunk (H <= 16, so ns >= 2)
 constexpr int kTileSlots = kTileMaxM / 2;       // FP64 target slots per lane (ns >= 2)
 constexpr int kTileStage = 64;                  // sources staged per step (two per lane)
-constexpr float kTileEps = 1e-30f;
+constexpr float kTileEps = 1e-24f;
 
 struct TileShared {
     float4 xy[kTileWarps][kTileStage];             // (x, x, y, y) of the staged sources
     float2 qq[kTileWarps][kTileStage];             // (q, q)
     int4 meta[kTileWarps][kP2PMeta];               // (lo, size, ox, oy) per list-1 cell
+    float scale[kTileWarps][kP2PMeta];             // size of the cell over the size of the target leaf
     int cs[kTileWarps][kP2PMeta + 1];              // flat start of each cell, then the total
     double acc[kTileWarps][2 * kTileSlots][32];    // FP64 accumulators: row 2i x, 2i+1 y of slot i
 };
@@ -1133,10 +1141,10 @@ __device__ __forceinline__ void tile_pairs(const ulonglong2* xy, const uint64_t*
 
 template <int M>
 __device__ __forceinline__ void tile_chunk(TileShared& sm, const Tree2D& t, const Lists2D& l,
-                                           const float4* __restrict__ src, int c, double ccx, double ccy, uint32_t o1,
-                                           int n1, int tb, int T, int hs, const double* fx, const double* fy,
-                                           double* out0, double* out1, int velocity, double u_inf, double v_inf,
-                                           unsigned* err) {
+                                           const float4* __restrict__ src, int c, double ccx, double ccy, int lev,
+                                           double ih, uint32_t o1, int n1, int tb, int T, int hs, const double* fx,
+                                           const double* fy, double* out0, double* out1, int velocity, double u_inf,
+                                           double v_inf, unsigned* err) {
     constexpr int MP = M / 2;
     constexpr int NP = MP > 0 ? MP : 1;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -1196,8 +1204,9 @@ __device__ __forceinline__ void tile_chunk(TileShared& sm, const Tree2D& t, cons
                     const int sc = l.l1_src[o1 + seg + k];
                     const int slo = t.c_lo[sc];
                     sz[h] = t.c_hi[sc] - slo;
-                    const float ox = (float)(t.c_cx[sc] - ccx), oy = (float)(t.c_cy[sc] - ccy);
+                    const float ox = (float)((t.c_cx[sc] - ccx) * ih), oy = (float)((t.c_cy[sc] - ccy) * ih);
                     sm.meta[wib][k] = make_int4(slo, sz[h], __float_as_int(ox), __float_as_int(oy));
+                    sm.scale[wib][k] = ldexpf(1.f, lev - (int)t.c_level[sc]);
                 }
             }
             int inc0 = sz[0], inc1 = sz[1];
@@ -1231,9 +1240,10 @@ __device__ __forceinline__ void tile_chunk(TileShared& sm, const Tree2D& t, cons
         auto fetch = [&](int k, int o) -> float4 {
             if (k >= nseg) return make_float4(0.f, 0.f, 0.f, 0.f);
             const int4 mt = sm.meta[wib][k];
+            const float sc = sm.scale[wib][k];
             float4 v = src[mt.x + o];
-            v.x += __int_as_float(mt.z);
-            v.y += __int_as_float(mt.w);
+            v.x = fmaf(v.x, sc, __int_as_float(mt.z));
+            v.y = fmaf(v.y, sc, __int_as_float(mt.w));
             return v;
         };
         auto advance = [&](int& k, int& o) {
@@ -1271,8 +1281,8 @@ __device__ __forceinline__ void tile_chunk(TileShared& sm, const Tree2D& t, cons
         const int kk = split + (i << (5 - hs));
         const int ti = tt + (kk << hs);
         if (kk < M && ti < T)
-            p2p_store(t, tb + ti, acc[32 * (2 * i)], acc[32 * (2 * i + 1)], fx, fy, out0, out1, velocity, u_inf, v_inf,
-                      err);
+            p2p_store(t, tb + ti, acc[32 * (2 * i)] * ih, acc[32 * (2 * i + 1)] * ih, fx, fy, out0, out1, velocity, u_inf,
+                      v_inf, err);
     }
     __syncwarp();
 }
@@ -1289,6 +1299,8 @@ p2p2d_tile_f32(Tree2D t, Lists2D l, const float4* __restrict__ src, const double
         const int c = t.leaf_cells[li];
         const int lo = t.c_lo[c], hi = t.c_hi[c];
         const double ccx = t.c_cx[c], ccy = t.c_cy[c];
+        const int lev = t.c_level[c];
+        const double ih = ldexp(1.0, lev) / t.geom->root;   // 1 / leaf size
         const uint32_t o1 = l.l1_off[li];
         const int n1 = (int)(l.l1_off[li + 1] - o1);
         for (int tb = lo; tb < hi; tb += kTileChunk) {
@@ -1299,8 +1311,8 @@ p2p2d_tile_f32(Tree2D t, Lists2D l, const float4* __restrict__ src, const double
             switch (M) {
 #define VPM_TILE_CASE(MM)                                                                                           \
     case MM:                                                                                                        \
-        tile_chunk<MM>(sm, t, l, src, c, ccx, ccy, o1, n1, tb, T, hs, fx, fy, out0, out1, velocity, u_inf, v_inf,     \
-                       err);                                                                                        \
+        tile_chunk<MM>(sm, t, l, src, c, ccx, ccy, lev, ih, o1, n1, tb, T, hs, fx, fy, out0, out1, velocity, u_inf,   \
+                       v_inf, err);                                                                                 \
         break;
                 VPM_TILE_CASE(1) VPM_TILE_CASE(2) VPM_TILE_CASE(3) VPM_TILE_CASE(4) VPM_TILE_CASE(5) VPM_TILE_CASE(6)
 #undef VPM_TILE_CASE
@@ -1582,7 +1594,7 @@ cudaError_t fmm2d_p2p_f32(const Tree2D& t, const Lists2D& l, const Expansions2D&
     *launches += 2;
     Expansions2D en = e;
     if (near_only) en.fx = en.fy = nullptr;
-    if (max_par < 0) return launch_p2p_tma<P2PF32>(t, l, rel, en, out0, out1, velocity, u_inf, v_inf, err, st, -max_par);
+    (void)max_par;
     p2p2d_tile_f32<<<148 * 3, 32 * kTileWarps, 0, st>>>(t, l, rel, en.fx, en.fy, out0, out1, velocity, u_inf, v_inf, err);
     return cudaGetLastError();
 }
