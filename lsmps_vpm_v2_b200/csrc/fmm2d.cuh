@@ -75,10 +75,13 @@ struct Tree2D {
     unsigned* gbar;
 };
 
-// Dense grid levels for n particles (<= 11, i.e. <= 5.6M entries).
+// Dense grid levels for n particles: the deepest L <= 13 with 4^(L-4) < n
+// (level 13 from n > 262,144: 89.5M entries, 358 MB of the 180 GB HBM, so
+// that the cells of every level a tree of that size reaches are found with
+// one load).
 inline int dense_levels_for(int n) {
     int L = 4;
-    while (L < 11 && (1ll << (2 * (L - 2))) < (long long)n) ++L;
+    while (L < 13 && (1ll << (2 * (L - 3))) < (long long)n) ++L;
     return L;
 }
 inline long long dense_entries(int levels) { return ((1ll << (2 * (levels + 1))) - 1) / 3; }

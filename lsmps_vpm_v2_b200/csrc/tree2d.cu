@@ -557,10 +557,20 @@ __device__ __forceinline__ int gallop_ge(const uint32_t* __restrict__ a, int lo,
 }
 
 // First j in (i, lim] with key prefix (>> sh) different from particle i's,
-// or lim (the group is known to end at or before lim; bisection).
+// or lim (the group is known to end at or before lim). Galloping from i, then
+// bisection: the search costs the logarithm of the group's size, not of n.
 __device__ __forceinline__ int group_end(const uint64_t* __restrict__ key, int i, int lim, int sh) {
     const uint64_t v = key[i] >> sh;
-    int L = i + 1, R = lim;
+    int L = i + 1, R = lim;   // answer in [L, R]
+    for (int step = 1; L + step - 1 < R; step <<= 1) {
+        const int probe = L + step - 1;
+        if ((key[probe] >> sh) == v) {
+            L = probe + 1;
+        } else {
+            R = probe;
+            break;
+        }
+    }
     while (L < R) {
         const int mid = (L + R) >> 1;
         if ((key[mid] >> sh) == v) L = mid + 1;
@@ -569,10 +579,20 @@ __device__ __forceinline__ int group_end(const uint64_t* __restrict__ key, int i
     return L;
 }
 
-// First j <= i with the same key prefix (>> sh) as particle i (bisection).
+// First j <= i with the same key prefix (>> sh) as particle i: galloping
+// back from i, then bisection.
 __device__ __forceinline__ int group_start(const uint64_t* __restrict__ key, int i, int sh) {
     const uint64_t v = key[i] >> sh;
-    int L = 0, R = i;
+    int L = 0, R = i;   // answer in [L, R]
+    for (int step = 1; R - step >= L; step <<= 1) {
+        const int probe = R - step;
+        if ((key[probe] >> sh) == v) {
+            R = probe;
+        } else {
+            L = probe + 1;
+            break;
+        }
+    }
     while (L < R) {
         const int mid = (L + R) >> 1;
         if ((key[mid] >> sh) == v) R = mid;
