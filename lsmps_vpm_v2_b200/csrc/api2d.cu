@@ -214,7 +214,8 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
     VPM_CUDA_TRY(cudaMemsetAsync(d_err, 0, sizeof(unsigned), st));
     if (int r = ensure_coefs(p)) return r;
     if (int r = record(0)) return r;
-    VPM_CUDA_TRY(keys_sort2d(x, y, q, act, tree, ts, p.exp_tree_pct, d_err, st, &launches));
+    VPM_CUDA_TRY(keys_sort2d(x, y, q, act, tree, ts, p.exp_tree_pct, d_err, st, &launches,
+                             std::min(p.max_src, p.max_par)));
     if (int r = record(1)) return r;
     VPM_CUDA_TRY(levels2d(tree, ts, p.max_src, p.max_par, d_err, st, &launches));
     if (int r = record(2)) return r;

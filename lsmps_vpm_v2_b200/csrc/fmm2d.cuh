@@ -117,7 +117,7 @@ constexpr int kBarrierWordsAt = kMaxLevels2D + 2;
 // particles; larger inputs take the multi-kernel path.
 constexpr int kCoopSortGridMax = 160;
 constexpr int kCoopSortMaxChunk = 16384;
-constexpr int kCoopSortWords = 1024 * kCoopSortGridMax + 512;
+constexpr int kCoopSortWords = 1024 * kCoopSortGridMax + 544;
 
 struct TreeScratch2D {
     double* bbox_partial;   // [kBBoxBlocks * 4]
@@ -143,8 +143,11 @@ cudaError_t build_tree2d(const double* x, const double* y, const double* q, cons
 
 // The two halves of build_tree2d: bounding box, keys, sort, gather and the
 // active-count scan; then the level-by-level cell construction.
+// shallow_cap = min(max_src, max_par): lets the cooperative sort try three
+// radix passes first (see sort2d_coop); 0 always sorts the full keys.
 cudaError_t keys_sort2d(const double* x, const double* y, const double* q, const uint8_t* act, Tree2D& t,
-                        TreeScratch2D& s, double exp_pct, unsigned* err, cudaStream_t st, int* launches);
+                        TreeScratch2D& s, double exp_pct, unsigned* err, cudaStream_t st, int* launches,
+                        int shallow_cap = 0);
 cudaError_t levels2d(Tree2D& t, TreeScratch2D& s, int max_src, int max_par, unsigned* err, cudaStream_t st,
                      int* launches);
 

@@ -212,7 +212,8 @@ constexpr int kCwPrefix = 512 * kCoopSortGridMax;
 constexpr int kCwActPrefix = 768 * kCoopSortGridMax;
 constexpr int kCwTotal = 1024 * kCoopSortGridMax;
 constexpr int kCwActTotal = kCwTotal + 256;
-static_assert(kCwActTotal + 256 <= kCoopSortWords, "count tables of the cooperative sort");
+constexpr int kCwFlag = kCwActTotal + 256;   // set when the shallow attempt must be redone
+static_assert(kCwFlag + 1 <= kCoopSortWords, "count tables of the cooperative sort");
 
 // kb0/kb1: 32-bit key ping-pong buffers (pass 0's keys are computed into
 // kb0); vb0/vb1: index ping-pong buffers, vb1 may alias t.perm (the last
@@ -223,10 +224,19 @@ static_assert(kCwActTotal + 256 <= kCoopSortWords, "count tables of the cooperat
 // sorted items form one run per digit, so the count before an item is the
 // digit's global start, the runs of that digit in earlier blocks, and the
 // item's place in its own run.
+//
+// Shallow attempt (shallow_cap > 0, four passes needed): the lowest digit
+// (levels K-3 .. K) is left out and the keys are stored with it cleared, so
+// particles are ordered by their level-(K-4) cells, ties in input order. The
+// tree built from those keys is the tree of the full keys whenever no
+// level-(K-4) cell needs splitting; that holds when no shallow_cap + 1
+// consecutive particles share a cell (shallow_cap = min(max_src, max_par)),
+// which the kernel checks after the three passes. Otherwise it sorts again
+// with all four passes.
 __global__ void __launch_bounds__(kCoopSortThreads, 1)
 sort2d_coop(const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ q,
-            const uint8_t* __restrict__ act, double exp_pct, int passes, Tree2D t, double* partial, double4* aos,
-            uint32_t* kb0, uint32_t* kb1, uint32_t* vb0, uint32_t* vb1, uint32_t* words, int chunk_cap,
+            const uint8_t* __restrict__ act, double exp_pct, int passes, int shallow_cap, Tree2D t, double* partial,
+            double4* aos, uint32_t* kb0, uint32_t* kb1, uint32_t* vb0, uint32_t* vb1, uint32_t* words, int chunk_cap,
             unsigned* err) {
     extern __shared__ __align__(16) unsigned char cs_sm[];
     __shared__ uint32_t s_wh[kCoopSortWarps][256];   // per-warp digit counts, then warp-exclusive prefixes
@@ -316,13 +326,19 @@ sort2d_coop(const double* __restrict__ x, const double* __restrict__ y, const do
 
     // 2. LSD passes of 8 bits
     const unsigned lt = (1u << lane) - 1u;
-    for (int p = 0; p < passes; ++p) {
-        const int shift = 8 * p;
-        const bool last = p == passes - 1;
+    if (b == 0 && tid == 0) words[kCwFlag] = 0u;
+    const bool try_shallow = passes == 4 && shallow_cap > 0;
+    for (int attempt = try_shallow ? 0 : 1; attempt < 2; ++attempt) {
+    const int np = attempt == 0 ? 3 : passes;
+    const int skip = passes - np;                               // low digits left out
+    const uint32_t kmask = skip ? ~((1u << (8 * skip)) - 1u) : ~0u;
+    for (int p = 0; p < np; ++p) {
+        const int shift = 8 * (p + skip);
+        const bool last = p == np - 1;
         const uint32_t* kin = (p & 1) ? kb1 : kb0;
         uint32_t* kout = (p & 1) ? kb0 : kb1;
-        const uint32_t* vin = ((passes - 1 - p) & 1) ? vb1 : vb0;
-        uint32_t* vout = ((passes - 2 - p) & 1) ? vb1 : vb0;
+        const uint32_t* vin = ((np - 1 - p) & 1) ? vb1 : vb0;
+        uint32_t* vout = ((np - 2 - p) & 1) ? vb1 : vb0;
         for (int i = tid; i < kCoopSortWarps * 256; i += kCoopSortThreads) (&s_wh[0][0])[i] = 0u;
         if (tid < 256) s_wa[tid] = 0u;
         __syncthreads();
@@ -495,7 +511,7 @@ sort2d_coop(const double* __restrict__ x, const double* __restrict__ y, const do
                 vout[pos] = vf;
             } else {
                 const double4 e = aos[val];
-                t.key[pos] = key;
+                t.key[pos] = key & kmask;
                 t.perm[pos] = val;
                 t.px[pos] = e.x;
                 t.py[pos] = e.y;
@@ -505,6 +521,20 @@ sort2d_coop(const double* __restrict__ x, const double* __restrict__ y, const do
             }
         }
         if (!last) grid_sync_counter(bar, err);
+    }
+    if (attempt == 1) break;
+    // is any level-(K-4) cell holding more than shallow_cap particles?
+    grid_sync_counter(bar, err);
+    {
+        bool over = false;
+        for (int i = c0 + tid; i < c1; i += kCoopSortThreads) {
+            const int j = i + shallow_cap;
+            if (j < n && __ldcg(t.key + i) == __ldcg(t.key + j)) over = true;
+        }
+        if (__syncthreads_or(over) && tid == 0) atomicOr(&words[kCwFlag], 1u);
+    }
+    grid_sync_counter(bar, err);
+    if (__ldcg(&words[kCwFlag]) == 0u) break;
     }
 }
 
@@ -920,7 +950,8 @@ bool coop_sort_shape(int n, int* grid, int* chunk) {
 }
 
 cudaError_t keys_sort2d(const double* x, const double* y, const double* q, const uint8_t* act, Tree2D& t,
-                        TreeScratch2D& s, double exp_pct, unsigned* err, cudaStream_t st, int* launches) {
+                        TreeScratch2D& s, double exp_pct, unsigned* err, cudaStream_t st, int* launches,
+                        int shallow_cap) {
     const int n = t.n;
     const int K = t.key_levels;
     const int gridN = std::max(1, std::min(148 * 8, ceil_div(n, 256)));
@@ -943,7 +974,8 @@ cudaError_t keys_sort2d(const double* x, const double* y, const double* q, const
         attr[0].val.cooperative = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        e = cudaLaunchKernelEx(&cfg, sort2d_coop, x, y, q, act, exp_pct, (2 * K + 7) / 8, t, s.bbox_partial,
+        e = cudaLaunchKernelEx(&cfg, sort2d_coop, x, y, q, act, exp_pct, (2 * K + 7) / 8, shallow_cap, t,
+                               s.bbox_partial,
                                (double4*)s.sort_aos, k32, k32 + n, s.val_alt, t.perm, s.coop_words, coop_chunk,
                                err);
         if (e != cudaSuccess) return e;
@@ -1002,7 +1034,7 @@ cudaError_t levels2d(Tree2D& t, TreeScratch2D& s, int max_src, int max_par, unsi
 cudaError_t build_tree2d(const double* x, const double* y, const double* q, const uint8_t* act, Tree2D& t,
                          TreeScratch2D& s, int max_src, int max_par, double exp_pct, unsigned* err, cudaStream_t st,
                          int* launches) {
-    cudaError_t e = keys_sort2d(x, y, q, act, t, s, exp_pct, err, st, launches);
+    cudaError_t e = keys_sort2d(x, y, q, act, t, s, exp_pct, err, st, launches, std::min(max_src, max_par));
     if (e != cudaSuccess) return e;
     return levels2d(t, s, max_src, max_par, err, st, launches);
 }
