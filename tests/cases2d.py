@@ -38,6 +38,17 @@ def clustered():
     return _field(p[:, 0], p[:, 1], seed=11)
 
 
+def deep():
+    """A tight blob in a wide background: leaves down to level 15, below
+    the level-12 digits the cooperative sort tries first (it must detect that
+    and sort the full keys)."""
+    rng = np.random.default_rng(12)
+    a = rng.normal([0.3, -0.2], 1.5e-3, (1500, 2))
+    c = rng.uniform(-10, 10, (1500, 2))
+    p = np.concatenate([a, c])
+    return _field(p[:, 0], p[:, 1], seed=12)
+
+
 def partly_inactive():
     """A third of the particles inactive, including whole inactive regions."""
     d = w.lamb_oseen_2d(n_side=80, seed=4)
@@ -88,6 +99,7 @@ CASES = {
     "lamb_mid": lamb_mid,
     "plate_small": plate_small,
     "clustered": clustered,
+    "deep": deep,
     "partly_inactive": partly_inactive,
     "boundary_aligned": boundary_aligned,
     "aspect": aspect,
