@@ -227,8 +227,7 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
         VPM_CUDA_TRY(cudaStreamWaitEvent(side, fork2, 0));
         VPM_CUDA_TRY(build_int_lists2d(tree, lists, ts.scan, p.eps, d_err, side, &launches));
         if (p.precision == VPM_PREC_MIXED || p.precision == VPM_PREC_MIXED_FP64_M2L)
-            VPM_CUDA_TRY(fmm2d_p2p_f32(tree, lists, ex2, (float4*)mixed_base, near_x, near_y, 0, 0.0, 0.0, d_err, side,
-                                       &launches, p.max_par, true));
+            VPM_CUDA_TRY(fmm2d_p2p_f32(tree, lists, ex2, near_x, near_y, 0, 0.0, 0.0, d_err, side, &launches, true));
         else
             VPM_CUDA_TRY(fmm2d_p2p_f64_tma(tree, lists, ex2, (double4*)mixed_base, near_x, near_y, 0, 0.0, 0.0, d_err,
                                            side, &launches, p.max_par, true));
@@ -284,9 +283,7 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
         }
         if (velocity == kModePotential) {
         } else if (p.precision == VPM_PREC_MIXED || p.precision == VPM_PREC_MIXED_FP64_M2L) {
-            float4* rel = (float4*)mixed_base;
-            VPM_CUDA_TRY(fmm2d_p2p_f32(tree, lists, ex2, rel, o0, o1, velocity, uinf, vinf, d_err, st, &launches,
-                                       p.max_par));
+            VPM_CUDA_TRY(fmm2d_p2p_f32(tree, lists, ex2, o0, o1, velocity, uinf, vinf, d_err, st, &launches));
         } else {
             VPM_CUDA_TRY(fmm2d_p2p_f64_tma(tree, lists, ex2, (double4*)mixed_base, o0, o1, velocity, uinf, vinf, d_err,
                                            st, &launches, p.max_par));

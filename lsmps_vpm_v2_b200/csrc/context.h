@@ -170,12 +170,11 @@ struct Ctx {
     int record(int i);
 };
 
-// FP32 P2P of the mixed form: warp per leaf (max_par >= 0), or the block-per-
-// leaf TMA-staged kernel sized for leaves of at most -max_par particles
-// (max_par < 0).
-cudaError_t fmm2d_p2p_f32(const Tree2D& t, const Lists2D& l, const Expansions2D& e, float4* rel, double* out0,
-                          double* out1, int velocity, double u_inf, double v_inf, unsigned* err, cudaStream_t st,
-                          int* launches, int max_par, bool near_only = false);
+// FP32 P2P of the mixed form (packed FP32x2, warp per leaf); near_only: the
+// near field alone in tree order into out0/out1.
+cudaError_t fmm2d_p2p_f32(const Tree2D& t, const Lists2D& l, const Expansions2D& e, double* out0, double* out1,
+                          int velocity, double u_inf, double v_inf, unsigned* err, cudaStream_t st, int* launches,
+                          bool near_only = false);
 // FP64 P2P on an AoS copy of the particles (`aos`, n entries); kernel choice as
 // for fmm2d_p2p_f32.
 cudaError_t fmm2d_p2p_f64_tma(const Tree2D& t, const Lists2D& l, const Expansions2D& e, double4* aos, double* out0,

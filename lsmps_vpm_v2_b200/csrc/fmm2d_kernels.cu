@@ -580,28 +580,7 @@ p2p2d(Tree2D t, Lists2D l, const double* __restrict__ fx, const double* __restri
 
 // ---- mixed form: FP32 near field ---------------------------------------------
 
-// Leaf-relative FP32 coordinates in units of the leaf's size, and FP32
-// strengths: (x - c_leaf) 2^L / root is formed in FP64 and rounded once, so
-// every coordinate lies in [-1/2, 1/2] whatever the scale of the input.
-__global__ void leaf_relative_f32(Tree2D t, float4* __restrict__ rel, unsigned* err) {
-    if (fatal(err)) return;
-    const int nl = t.info->n_leaves;
-    const double root = t.geom->root;
-    for (int li = blockIdx.x; li < nl; li += gridDim.x) {
-        const int c = t.leaf_cells[li];
-        const double cx = t.c_cx[c], cy = t.c_cy[c];
-        const double ih = ldexp(1.0, (int)t.c_level[c]) / root;
-        for (int i = t.c_lo[c] + threadIdx.x; i < t.c_hi[c]; i += blockDim.x)
-            rel[i] = make_float4((float)((t.px[i] - cx) * ih), (float)((t.py[i] - cy) * ih), (float)t.pq[i],
-                                 __int_as_float(i));
-    }
-}
-
 // FP32 reciprocal (hardware approximation, ~1 ulp) of the mixed near field.
-// Targets and sources there are expressed relative to the target leaf's
-// centre: source = (c_src - c_tgt) [FP64 difference, rounded once per source
-// cell] + (x - c_src) [FP32, precomputed], so every pair offset keeps ~1e-7
-// relative accuracy; per-cell FP32 sums go into FP64 per-target accumulators.
 __device__ __forceinline__ float rcp_approx(float a) {
     float r;
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
@@ -609,7 +588,7 @@ __device__ __forceinline__ float rcp_approx(float a) {
 }
 
 
-// ---- TMA-staged FP32 P2P ------------------------------------------------------
+// ---- TMA-staged P2P (bulk copies into shared memory) ------------------------------
 
 constexpr int kStageCells = 64;  // list-1 cells of one leaf held in the stage descriptor
 
@@ -651,47 +630,7 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
         : "memory");
 }
 
-// Stage the list-1 sources of leaf `li` into buffer (buf, cells): one thread.
-// Returns the number of staged slots, or -1 when the leaf does not fit (the
-// barrier is still armed, with zero bytes, so its phase completes).
-__device__ int stage_leaf(const Tree2D& t, const Lists2D& l, const float4* rel, int li, float4* buf, int cap,
-                          StageCell* cells, uint64_t* bar) {
-    const int c = t.leaf_cells[li];
-    const double ccx = t.c_cx[c], ccy = t.c_cy[c];
-    const uint32_t o1 = l.l1_off[li], e1 = l.l1_off[li + 1];
-    int total = 0;
-    bool fits = (int)(e1 - o1) <= kStageCells;
-    if (fits) {
-        for (uint32_t k = o1; k < e1; ++k) {
-            const int sc = l.l1_src[k];
-            total += t.c_hi[sc] - t.c_lo[sc];
-        }
-        fits = total <= cap;
-    }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    mbar_arrive_expect_tx(bar, fits ? (unsigned)total * 16u : 0u);
-    if (!fits) return -1;
-    int pos = 0, kk = 0;
-    for (uint32_t k = o1; k < e1; ++k, ++kk) {
-        const int sc = l.l1_src[k];
-        const int lo = t.c_lo[sc], hi = t.c_hi[sc];
-        cells[kk].start = pos;
-        cells[kk].end = pos + (hi - lo);
-        cells[kk].ox = (float)(t.c_cx[sc] - ccx);
-        cells[kk].oy = (float)(t.c_cy[sc] - ccy);
-        bulk_g2s(buf + pos, rel + lo, (unsigned)(hi - lo) * 16u, bar);
-        pos += hi - lo;
-    }
-    return total;
-}
-
 // Per-precision pieces of the TMA-staged P2P.
-struct P2PF32 {
-    using Elem = float4;   // (x - c_leaf, y - c_leaf, q, -) in FP32
-    using Acc = float;
-    static __device__ __forceinline__ void shift(Elem& e, float ox, float oy) { e.x += ox; e.y += oy; }
-    static __device__ __forceinline__ float inv(float r2) { return rcp_approx(r2); }
-};
 struct P2PF64 {
     using Elem = double4;  // (x, y, q, -) in FP64, absolute coordinates
     using Acc = double;
@@ -1081,8 +1020,7 @@ constexpr float kTileEps = 1e-24f;
 struct TileShared {
     float4 xy[kTileWarps][kTileStage];             // (x, x, y, y) of the staged sources
     float2 qq[kTileWarps][kTileStage];             // (q, q)
-    int4 meta[kTileWarps][kP2PMeta];               // (lo, size, ox, oy) per list-1 cell
-    float scale[kTileWarps][kP2PMeta];             // size of the cell over the size of the target leaf
+    int2 meta[kTileWarps][kP2PMeta];               // (lo, size) per list-1 cell
     int cs[kTileWarps][kP2PMeta + 1];              // flat start of each cell, then the total
     double acc[kTileWarps][2 * kTileSlots][32];    // FP64 accumulators: row 2i x, 2i+1 y of slot i
 };
@@ -1139,12 +1077,16 @@ __device__ __forceinline__ void tile_pairs(const ulonglong2* xy, const uint64_t*
     }
 }
 
+// Coordinate of a particle in the target leaf's frame, in units of its size:
+// formed in FP64 and rounded once (a particle of the leaf gets the same value
+// as a target and as a source).
+__device__ __forceinline__ float leaf_unit(double x, double c, double ih) { return (float)((x - c) * ih); }
+
 template <int M>
-__device__ __forceinline__ void tile_chunk(TileShared& sm, const Tree2D& t, const Lists2D& l,
-                                           const float4* __restrict__ src, int c, double ccx, double ccy, int lev,
-                                           double ih, uint32_t o1, int n1, int tb, int T, int hs, const double* fx,
-                                           const double* fy, double* out0, double* out1, int velocity, double u_inf,
-                                           double v_inf, unsigned* err) {
+__device__ __forceinline__ void tile_chunk(TileShared& sm, const Tree2D& t, const Lists2D& l, int c, double ccx,
+                                           double ccy, double ih, uint32_t o1, int n1, int tb, int T, int hs,
+                                           const double* fx, const double* fy, double* out0, double* out1,
+                                           int velocity, double u_inf, double v_inf, unsigned* err) {
     constexpr int MP = M / 2;
     constexpr int NP = MP > 0 ? MP : 1;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -1156,16 +1098,16 @@ __device__ __forceinline__ void tile_chunk(TileShared& sm, const Tree2D& t, cons
     #pragma unroll
     for (int h = 0; h < MP; ++h) {
         const int i0 = tt + ((2 * h) << hs), i1 = tt + ((2 * h + 1) << hs);
-        const float4 g0 = src[tb + (i0 < T ? i0 : 0)], g1 = src[tb + (i1 < T ? i1 : 0)];
-        nx[h] = pack2(-g0.x, -g1.x);
-        ny[h] = pack2(-g0.y, -g1.y);
+        const int j0 = tb + (i0 < T ? i0 : 0), j1 = tb + (i1 < T ? i1 : 0);
+        nx[h] = pack2(-leaf_unit(t.px[j0], ccx, ih), -leaf_unit(t.px[j1], ccx, ih));
+        ny[h] = pack2(-leaf_unit(t.py[j0], ccy, ih), -leaf_unit(t.py[j1], ccy, ih));
         px[h] = py[h] = 0ull;
     }
     if (M & 1) {
         const int i0 = tt + ((M - 1) << hs);
-        const float4 g0 = src[tb + (i0 < T ? i0 : 0)];
-        nxo = -g0.x;
-        nyo = -g0.y;
+        const int j0 = tb + (i0 < T ? i0 : 0);
+        nxo = -leaf_unit(t.px[j0], ccx, ih);
+        nyo = -leaf_unit(t.py[j0], ccy, ih);
     }
     double* acc = &sm.acc[wib][0][lane];
     #pragma unroll
@@ -1204,9 +1146,7 @@ __device__ __forceinline__ void tile_chunk(TileShared& sm, const Tree2D& t, cons
                     const int sc = l.l1_src[o1 + seg + k];
                     const int slo = t.c_lo[sc];
                     sz[h] = t.c_hi[sc] - slo;
-                    const float ox = (float)((t.c_cx[sc] - ccx) * ih), oy = (float)((t.c_cy[sc] - ccy) * ih);
-                    sm.meta[wib][k] = make_int4(slo, sz[h], __float_as_int(ox), __float_as_int(oy));
-                    sm.scale[wib][k] = ldexpf(1.f, lev - (int)t.c_level[sc]);
+                    sm.meta[wib][k] = make_int2(slo, sz[h]);
                 }
             }
             int inc0 = sz[0], inc1 = sz[1];
@@ -1239,12 +1179,8 @@ __device__ __forceinline__ void tile_chunk(TileShared& sm, const Tree2D& t, cons
         }
         auto fetch = [&](int k, int o) -> float4 {
             if (k >= nseg) return make_float4(0.f, 0.f, 0.f, 0.f);
-            const int4 mt = sm.meta[wib][k];
-            const float sc = sm.scale[wib][k];
-            float4 v = src[mt.x + o];
-            v.x = fmaf(v.x, sc, __int_as_float(mt.z));
-            v.y = fmaf(v.y, sc, __int_as_float(mt.w));
-            return v;
+            const int j = sm.meta[wib][k].x + o;
+            return make_float4(leaf_unit(t.px[j], ccx, ih), leaf_unit(t.py[j], ccy, ih), (float)t.pq[j], 0.f);
         };
         auto advance = [&](int& k, int& o) {
             o += kTileStage;
@@ -1288,7 +1224,7 @@ __device__ __forceinline__ void tile_chunk(TileShared& sm, const Tree2D& t, cons
 }
 
 __global__ void __launch_bounds__(32 * kTileWarps, 3)
-p2p2d_tile_f32(Tree2D t, Lists2D l, const float4* __restrict__ src, const double* __restrict__ fx,
+p2p2d_tile_f32(Tree2D t, Lists2D l, const double* __restrict__ fx,
                const double* __restrict__ fy, double* __restrict__ out0, double* __restrict__ out1, int velocity,
                double u_inf, double v_inf, unsigned* err) {
     __shared__ TileShared sm;
@@ -1311,7 +1247,7 @@ p2p2d_tile_f32(Tree2D t, Lists2D l, const float4* __restrict__ src, const double
             switch (M) {
 #define VPM_TILE_CASE(MM)                                                                                           \
     case MM:                                                                                                        \
-        tile_chunk<MM>(sm, t, l, src, c, ccx, ccy, lev, ih, o1, n1, tb, T, hs, fx, fy, out0, out1, velocity, u_inf,   \
+        tile_chunk<MM>(sm, t, l, c, ccx, ccy, ih, o1, n1, tb, T, hs, fx, fy, out0, out1, velocity, u_inf,             \
                        v_inf, err);                                                                                 \
         break;
                 VPM_TILE_CASE(1) VPM_TILE_CASE(2) VPM_TILE_CASE(3) VPM_TILE_CASE(4) VPM_TILE_CASE(5) VPM_TILE_CASE(6)
@@ -1587,15 +1523,13 @@ cudaError_t fmm2d_p2p_out(const Tree2D& t, const Lists2D& l, const Expansions2D&
     return cudaGetLastError();
 }
 
-cudaError_t fmm2d_p2p_f32(const Tree2D& t, const Lists2D& l, const Expansions2D& e, float4* rel, double* out0,
-                          double* out1, int velocity, double u_inf, double v_inf, unsigned* err, cudaStream_t st,
-                          int* launches, int max_par, bool near_only) {
-    leaf_relative_f32<<<148 * 8, 128, 0, st>>>(t, rel, err);
-    *launches += 2;
+cudaError_t fmm2d_p2p_f32(const Tree2D& t, const Lists2D& l, const Expansions2D& e, double* out0, double* out1,
+                          int velocity, double u_inf, double v_inf, unsigned* err, cudaStream_t st, int* launches,
+                          bool near_only) {
     Expansions2D en = e;
     if (near_only) en.fx = en.fy = nullptr;
-    (void)max_par;
-    p2p2d_tile_f32<<<148 * 3, 32 * kTileWarps, 0, st>>>(t, l, rel, en.fx, en.fy, out0, out1, velocity, u_inf, v_inf, err);
+    p2p2d_tile_f32<<<148 * 3, 32 * kTileWarps, 0, st>>>(t, l, en.fx, en.fy, out0, out1, velocity, u_inf, v_inf, err);
+    *launches += 1;
     return cudaGetLastError();
 }
 

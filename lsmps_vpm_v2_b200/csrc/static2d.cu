@@ -193,7 +193,6 @@ extern "C" int vpm_fmm2d_field_device_static(const double* x, const double* y, c
     xe.fy = cv.take<double>(base, kStaticMaxN);
     xe.coef = cv.take<double>(base, 3 * kCoefTable);
     xe.op = nullptr;  // direct M2L formula
-    float4* rel = cv.take<float4>(base, kStaticMaxN);
     if (cv.total > kStaticBytes) {
         set_msg(errbuf, errlen, "static scratch layout exceeds its array");
         return VPM_EDEVICE;
@@ -225,7 +224,7 @@ extern "C" int vpm_fmm2d_field_device_static(const double* x, const double* y, c
     if (r == cudaSuccess) r = fmm2d_eval(t, l, xe, P, err, st, &launches);
     if (r == cudaSuccess) {
         if (p.precision == VPM_PREC_MIXED)
-            r = fmm2d_p2p_f32(t, l, xe, rel, ex, ey, 0, 0.0, 0.0, err, st, &launches, 0);
+            r = fmm2d_p2p_f32(t, l, xe, ex, ey, 0, 0.0, 0.0, err, st, &launches);
         else
             r = fmm2d_p2p(t, l, xe, ex, ey, err, st, &launches);
     }
