@@ -237,7 +237,9 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
         VPM_CUDA_TRY(cudaEventRecord(join3, side2));
         VPM_CUDA_TRY(fmm2d_upward(tree, ex2, p.p, d_err, st, &launches));
         VPM_CUDA_TRY(cudaStreamWaitEvent(st, join3, 0));
-        if (p.precision == VPM_PREC_MIXED && m2l_tc_supported(p.p))
+        if (p.precision == VPM_PREC_MIXED && m2l_f32_supported(p.p))
+            VPM_CUDA_TRY(fmm2d_m2l_f32(tree, lists, ex2, p.p, tc_rows, tc_ops, d_err, st, &launches));
+        else if (p.precision == VPM_PREC_MIXED && m2l_tc_supported(p.p))
             VPM_CUDA_TRY(fmm2d_m2l_tc(tree, lists, ex2, p.p, tc_rows, tc_ops, d_err, st, &launches));
         else
             VPM_CUDA_TRY(fmm2d_m2l_only(tree, lists, ex2, p.p, d_err, st, &launches));
@@ -262,7 +264,9 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
     } else {
         VPM_CUDA_TRY(fmm2d_upward(tree, ex2, p.p, d_err, st, &launches));
         if (int r = record(4)) return r;
-        if (p.precision == VPM_PREC_MIXED && velocity != kModePotential && m2l_tc_supported(p.p))
+        if (p.precision == VPM_PREC_MIXED && velocity != kModePotential && m2l_f32_supported(p.p))
+            VPM_CUDA_TRY(fmm2d_m2l_f32(tree, lists, ex2, p.p, tc_rows, tc_ops, d_err, st, &launches));
+        else if (p.precision == VPM_PREC_MIXED && velocity != kModePotential && m2l_tc_supported(p.p))
             VPM_CUDA_TRY(fmm2d_m2l_tc(tree, lists, ex2, p.p, tc_rows, tc_ops, d_err, st, &launches));
         else
             VPM_CUDA_TRY(fmm2d_m2l_only(tree, lists, ex2, p.p, d_err, st, &launches));
@@ -306,7 +310,8 @@ int Ctx::ensure_coefs(const vpm_fmm_params& p) {
     if (capturing) return fail(VPM_EINVAL, "coefficient upload inside a graph capture");
     VPM_CUDA_TRY(set_coefficients2d(p.p, p.binom == VPM_BINOM_EXACT, ex2.coef, stream));
     VPM_CUDA_TRY(set_m2l_operators2d(p.p, p.binom == VPM_BINOM_EXACT, ex2.op, stream));
-    if (m2l_tc_supported(p.p)) VPM_CUDA_TRY(set_m2l_tc_operators(p.p, ex2.op, tc_ops, stream));
+    if (m2l_f32_supported(p.p)) VPM_CUDA_TRY(set_m2l_f32_operators(p.p, ex2.op, tc_ops, stream));
+    else if (m2l_tc_supported(p.p)) VPM_CUDA_TRY(set_m2l_tc_operators(p.p, ex2.op, tc_ops, stream));
     coef_P = p.p;
     coef_binom = p.binom;
     return VPM_OK;
