@@ -313,14 +313,16 @@ m2l2d_tc(Tree2D t, Lists2D l, const float* __restrict__ rows, const float* __res
 
 // ---- the same scaled list-2 M2L on the FP32 pipes (orders 1..kF32MaxP) ----
 //
-// b~ = sum over offsets tau of T_tau a~ in FP32, one warp per 32 consecutive
-// target cells (lane = target). The warp walks the offsets present in its
-// targets' lists in increasing order; at offset tau every lane applies the
-// same operator (read from shared memory as a broadcast) to the scaled row
-// of its own source (zero when it has none), so the 2P outputs of a lane
-// accumulate in registers. The next offset's rows are loaded while the
-// current one is applied. FP32 products and sums carry about 24 bits, as the
-// 3xTF32 tensor-core form; the order of the sums is fixed.
+// b~ = sum over offsets tau of T_tau a~ in FP32. A warp takes 32 / NG
+// consecutive target cells, NG = (2P rounded up to 4) / 4 lanes per target,
+// each lane four of the target's 2P real outputs. The warp walks the offsets
+// present in its targets' lists in increasing order; at offset tau every
+// lane applies its four rows of the same operator (shared memory, one
+// 16-byte read per input) to the scaled row of its target's source (zero
+// when it has none), accumulating in registers. The next offset's rows are
+// loaded while the current one is applied. FP32 products and sums carry
+// about 24 bits, as the 3xTF32 tensor-core form; the order of the sums is
+// fixed.
 constexpr int kF32MaxP = 12;
 constexpr int kF32Warps = 8;
 
@@ -355,7 +357,7 @@ __global__ void __launch_bounds__(32 * kF32Warps)
 m2l2d_f32(Tree2D t, Lists2D l, const float* __restrict__ rows, const float* __restrict__ ops,
           double2* __restrict__ b, unsigned* err) {
     extern __shared__ __align__(16) float f32_smem[];
-    constexpr int NRP = f32_nrp(P), NR4 = NRP / 4;
+    constexpr int NRP = f32_nrp(P), NG = NRP / 4, TPW = 32 / NG;
     constexpr int RP = f32_rp(P), RQ = RP / 4, K2 = 2 * (P + 1);
     float* s_op = f32_smem;                                                         // [49][K2][NRP]
     int* s_src = reinterpret_cast<int*>(s_op + (size_t)49 * K2 * NRP);              // [warps][49][32]
@@ -364,32 +366,32 @@ m2l2d_f32(Tree2D t, Lists2D l, const float* __restrict__ rows, const float* __re
         reinterpret_cast<float4*>(s_op)[i] = reinterpret_cast<const float4*>(ops)[i];
     __syncthreads();
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int tl = lane / NG, g = lane - tl * NG;   // target of the lane, output group
     int* my_src = s_src + (size_t)wib * 49 * 32;
     const int c_begin = t.info->level_start[2], c_end = t.info->n_cells;
-    const int ntasks = (c_end - c_begin + 31) / 32;
+    const int ntasks = (c_end - c_begin + TPW - 1) / TPW;
     const double root = t.geom->root;
     for (int task = blockIdx.x * kF32Warps + wib; task < ntasks; task += gridDim.x * kF32Warps) {
-        const int c = c_begin + task * 32 + lane;
-        const bool valid = c < c_end;
+        const int c = c_begin + task * TPW + tl;
+        const bool valid = tl < TPW && c < c_end;
         for (int s2 = 0; s2 < 49; ++s2) my_src[s2 * 32 + lane] = -1;
-        uint32_t m_lo = 0, m_hi = 0;   // offsets present in this lane's list
-        if (valid) {
+        __syncwarp();
+        uint32_t m_lo = 0, m_hi = 0;   // offsets present in this target's list
+        if (valid && g == 0) {
             const int n2 = l.l2_n[c];
             for (int k = 0; k < n2; ++k) {
                 const int slot = l.l2_slot[(size_t)c * kList2Cap + k];
-                my_src[slot * 32 + lane] = l.l2_src[(size_t)c * kList2Cap + k];
+                my_src[slot * 32 + tl] = l.l2_src[(size_t)c * kList2Cap + k];
                 if (slot < 32) m_lo |= 1u << slot;
                 else m_hi |= 1u << (slot - 32);
             }
         }
         __syncwarp();
         uint64_t mask = ((uint64_t)__reduce_or_sync(0xffffffffu, m_hi) << 32) | __reduce_or_sync(0xffffffffu, m_lo);
-        float acc[NRP];
-        #pragma unroll
-        for (int r = 0; r < NRP; ++r) acc[r] = 0.f;
-        // row of this lane's source at offset tau (zeros when it has none)
+        float acc[4] = {0.f, 0.f, 0.f, 0.f};
+        // row of this lane's target's source at offset tau (zeros when it has none)
         auto load_row = [&](int tau, float4* dst) {
-            const int src = my_src[tau * 32 + lane];
+            const int src = valid ? my_src[tau * 32 + tl] : -1;
             const float4* row = reinterpret_cast<const float4*>(rows + (size_t)(src >= 0 ? src : 0) * RP);
             #pragma unroll
             for (int q = 0; q < RQ; ++q) dst[q] = src >= 0 ? __ldg(row + q) : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -401,7 +403,7 @@ m2l2d_f32(Tree2D t, Lists2D l, const float* __restrict__ rows, const float* __re
             mask &= mask - 1;
             const int tnext = mask ? __ffsll((long long)mask) - 1 : 49;
             if (tnext < 49) load_row(tnext, nxt);
-            const float* T = s_op + (size_t)tau * K2 * NRP;
+            const float4* T = reinterpret_cast<const float4*>(s_op + (size_t)tau * K2 * NRP) + g;
             #pragma unroll
             for (int q = 0; q < RQ; ++q) {
                 const float av[4] = {cur[q].x, cur[q].y, cur[q].z, cur[q].w};
@@ -409,15 +411,11 @@ m2l2d_f32(Tree2D t, Lists2D l, const float* __restrict__ rows, const float* __re
                 for (int u = 0; u < 4; ++u) {
                     const int k = 4 * q + u;
                     if (k >= K2) break;
-                    const float4* Tk = reinterpret_cast<const float4*>(T + (size_t)k * NRP);
-                    #pragma unroll
-                    for (int r4 = 0; r4 < NR4; ++r4) {
-                        const float4 w = Tk[r4];
-                        acc[4 * r4] = fmaf(w.x, av[u], acc[4 * r4]);
-                        acc[4 * r4 + 1] = fmaf(w.y, av[u], acc[4 * r4 + 1]);
-                        acc[4 * r4 + 2] = fmaf(w.z, av[u], acc[4 * r4 + 2]);
-                        acc[4 * r4 + 3] = fmaf(w.w, av[u], acc[4 * r4 + 3]);
-                    }
+                    const float4 w = T[k * NG];
+                    acc[0] = fmaf(w.x, av[u], acc[0]);
+                    acc[1] = fmaf(w.y, av[u], acc[1]);
+                    acc[2] = fmaf(w.z, av[u], acc[2]);
+                    acc[3] = fmaf(w.w, av[u], acc[3]);
                 }
             }
             #pragma unroll
@@ -425,21 +423,21 @@ m2l2d_f32(Tree2D t, Lists2D l, const float* __restrict__ rows, const float* __re
             tau = tnext;
         }
         if (valid) {
-            // acc[r] is Re b~_{r+1} for r < P and Im b~_{r-P+1} for P <= r < 2P;
-            // registers are indexed by constants only
+            // output r = 4 g + i is Re b~_{r+1} (r < P) or Im b~_{r-P+1} (P <= r < 2P)
             const double rinv = ldexp(1.0, (int)t.c_level[c]) / root;
             double* bc = reinterpret_cast<double*>(b + (size_t)c * (P + 1));
-            bc[0] = 0.0;
-            bc[1] = 0.0;
-            double rk = 1.0, rk2 = 1.0;
+            if (g == 0) {
+                bc[0] = 0.0;
+                bc[1] = 0.0;
+            }
             #pragma unroll
-            for (int r = 0; r < NRP; ++r) {
-                if (r < P) {
-                    rk *= rinv;
-                    bc[2 * (r + 1)] = (double)acc[r] * rk;
-                } else if (r < 2 * P) {
-                    rk2 *= rinv;
-                    bc[2 * (r - P + 1) + 1] = (double)acc[r] * rk2;
+            for (int i = 0; i < 4; ++i) {
+                const int r = 4 * g + i;
+                if (r < 2 * P) {
+                    const int pp = r < P ? r + 1 : r - P + 1;
+                    double rk = 1.0;
+                    for (int e = 0; e < pp; ++e) rk *= rinv;
+                    bc[2 * pp + (r < P ? 0 : 1)] = (double)acc[i] * rk;
                 }
             }
         }
