@@ -360,28 +360,28 @@ m2l2d_f32(Tree2D t, Lists2D l, const float* __restrict__ rows, const float* __re
     constexpr int NRP = f32_nrp(P), NG = NRP / 4, TPW = 32 / NG;
     constexpr int RP = f32_rp(P), RQ = RP / 4, K2 = 2 * (P + 1);
     float* s_op = f32_smem;                                                         // [49][K2][NRP]
-    int* s_src = reinterpret_cast<int*>(s_op + (size_t)49 * K2 * NRP);              // [warps][49][32]
+    int* s_src = reinterpret_cast<int*>(s_op + (size_t)49 * K2 * NRP);              // [warps][49][TPW]
     if (fatal(err)) return;
     for (int i = threadIdx.x; i < 49 * K2 * NRP / 4; i += blockDim.x)
         reinterpret_cast<float4*>(s_op)[i] = reinterpret_cast<const float4*>(ops)[i];
     __syncthreads();
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int tl = lane / NG, g = lane - tl * NG;   // target of the lane, output group
-    int* my_src = s_src + (size_t)wib * 49 * 32;
+    int* my_src = s_src + (size_t)wib * 49 * TPW;
     const int c_begin = t.info->level_start[2], c_end = t.info->n_cells;
     const int ntasks = (c_end - c_begin + TPW - 1) / TPW;
     const double root = t.geom->root;
     for (int task = blockIdx.x * kF32Warps + wib; task < ntasks; task += gridDim.x * kF32Warps) {
         const int c = c_begin + task * TPW + tl;
         const bool valid = tl < TPW && c < c_end;
-        for (int s2 = 0; s2 < 49; ++s2) my_src[s2 * 32 + lane] = -1;
+        for (int i = lane; i < 49 * TPW; i += 32) my_src[i] = -1;
         __syncwarp();
         uint32_t m_lo = 0, m_hi = 0;   // offsets present in this target's list
         if (valid && g == 0) {
             const int n2 = l.l2_n[c];
             for (int k = 0; k < n2; ++k) {
                 const int slot = l.l2_slot[(size_t)c * kList2Cap + k];
-                my_src[slot * 32 + tl] = l.l2_src[(size_t)c * kList2Cap + k];
+                my_src[slot * TPW + tl] = l.l2_src[(size_t)c * kList2Cap + k];
                 if (slot < 32) m_lo |= 1u << slot;
                 else m_hi |= 1u << (slot - 32);
             }
@@ -391,7 +391,7 @@ m2l2d_f32(Tree2D t, Lists2D l, const float* __restrict__ rows, const float* __re
         float acc[4] = {0.f, 0.f, 0.f, 0.f};
         // row of this lane's target's source at offset tau (zeros when it has none)
         auto load_row = [&](int tau, float4* dst) {
-            const int src = valid ? my_src[tau * 32 + tl] : -1;
+            const int src = valid ? my_src[tau * TPW + tl] : -1;
             const float4* row = reinterpret_cast<const float4*>(rows + (size_t)(src >= 0 ? src : 0) * RP);
             #pragma unroll
             for (int q = 0; q < RQ; ++q) dst[q] = src >= 0 ? __ldg(row + q) : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -586,7 +586,7 @@ cudaError_t set_m2l_f32_operators(int P, const double2* op_dev, float* dst, cuda
 template <int P>
 cudaError_t launch_m2l_f32(const Tree2D& t, const Lists2D& l, Expansions2D& e, const float* rows, const float* ops,
                            unsigned* err, cudaStream_t st) {
-    const size_t smem = sizeof(float) * (size_t)49 * 2 * (P + 1) * f32_nrp(P) + sizeof(int) * kF32Warps * 49 * 32;
+    const size_t smem = sizeof(float) * (size_t)49 * 2 * (P + 1) * f32_nrp(P) + sizeof(int) * kF32Warps * 49 * (32 / (f32_nrp(P) / 4));
     cudaError_t r = cudaFuncSetAttribute(m2l2d_f32<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (r != cudaSuccess) return r;
     int occ = 0;
