@@ -446,13 +446,18 @@ m2l2d_f32(Tree2D t, Lists2D l, const float* __restrict__ rows, const float* __re
 }
 
 // List 4 of every cell (FP64, direct formula of fmm2D.cpp:504-520), added
-// to b. One warp per cell, lane p-1 computes b_p.
+// to b. One warp per cell with list-4 sources; the warp's lanes form
+// G = 32 / P groups, group g takes sources g, g + G, ... and its lane p - 1
+// computes that part of b_p; the groups' parts are summed in group order.
 __global__ void __launch_bounds__(128)
 m2l_list4_add(Tree2D t, Lists2D l, const double2* __restrict__ a, double2* __restrict__ b,
               const double* __restrict__ coef, int P, unsigned* err) {
     if (fatal(err)) return;
     const double* g_m2l = coef + kCoefM2L;
     const int lane = threadIdx.x & 31;
+    const int G = P <= 32 ? 32 / P : 1;
+    const int grp = lane / P, p = lane - grp * P + 1;
+    const bool on = grp < G;
     const int c_begin = t.info->level_start[2], c_end = t.info->n_cells;
     const int warps = gridDim.x * (blockDim.x >> 5);
     for (int c = c_begin + blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < c_end; c += warps) {
@@ -460,11 +465,10 @@ m2l_list4_add(Tree2D t, Lists2D l, const double2* __restrict__ a, double2* __res
         if (n4 == 0) continue;
         const double zx = t.c_cx[c], zy = t.c_cy[c];
         double2 acc = make_double2(0.0, 0.0);
-        const int p = lane + 1;
-        for (int si = 0; si < n4; ++si) {
-            const int src = l.l4_src[(size_t)c * kList4Cap + si];
-            const double2 w = cinv(make_double2(t.c_cx[src] - zx, t.c_cy[src] - zy));
-            if (p <= P) {
+        if (on) {
+            for (int si = grp; si < n4; si += G) {
+                const int src = l.l4_src[(size_t)c * kList4Cap + si];
+                const double2 w = cinv(make_double2(t.c_cx[src] - zx, t.c_cy[src] - zy));
                 const double2* A = a + (size_t)src * (P + 1);
                 double2 wp = make_double2(1.0, 0.0);
                 for (int e = 0; e < p; ++e) wp = cmul(wp, w);   // w^p
@@ -478,8 +482,14 @@ m2l_list4_add(Tree2D t, Lists2D l, const double2* __restrict__ a, double2* __res
                 acc = csub(acc, sv);
             }
         }
-        if (p <= P) {
-            double2* bp = &b[(size_t)c * (P + 1) + p];
+        // lane p - 1 of group 0 adds the other groups' parts in group order
+        for (int g = 1; g < G; ++g) {
+            const int from = g * P + (lane < P ? lane : 0);
+            const double vx = __shfl_sync(0xffffffffu, acc.x, from), vy = __shfl_sync(0xffffffffu, acc.y, from);
+            if (lane < P) acc = make_double2(acc.x + vx, acc.y + vy);
+        }
+        if (lane < P) {
+            double2* bp = &b[(size_t)c * (P + 1) + lane + 1];
             *bp = cadd(*bp, acc);
         }
     }
