@@ -407,12 +407,83 @@ m2l2d_op(Tree2D t, Lists2D l, const double2* __restrict__ a, double2* __restrict
 
 // ---- leaf evaluation: M2P (list 3), L2P --------------------------------------
 
+// Far field of targets i of a leaf, lane-owned: M2P over list 3
+// (fmm2D.cpp:1040-1066) and L2P of the leaf's complete local expansion
+// (fmm2D.cpp:1076-1093). With TWO, each lane takes a second target and both
+// run through the list-3 sources together (one load of every source's
+// coefficients serves both, and the two chains are independent). Each
+// target's sums run in the same order either way.
+template <bool TWO>
+__device__ __forceinline__ void eval_targets(const Tree2D& t, const Lists2D& l, const double2* __restrict__ a,
+                                             const double2* s_b, int P, int i0, int i1, bool h0, bool h1, double zx,
+                                             double zy, uint32_t o3, uint32_t e3, double* fx, double* fy,
+                                             const double* nx, const double* ny, double* out0, double* out1,
+                                             int velocity, double u_inf, double v_inf, unsigned* err) {
+    double x[2], y[2], ex[2] = {0.0, 0.0}, ey[2] = {0.0, 0.0};
+    bool h[2] = {h0, h1};
+    const int ii[2] = {i0, i1};
+    #pragma unroll
+    for (int u = 0; u < (TWO ? 2 : 1); ++u) {
+        x[u] = h[u] ? t.px[ii[u]] : zx + 1.0;
+        y[u] = h[u] ? t.py[ii[u]] : zy;
+    }
+    for (uint32_t k = o3; k < e3; ++k) {
+        const int s = l.l3_src[k];
+        const double sx = t.c_cx[s], sy = t.c_cy[s];
+        const double2* A = a + (size_t)s * (P + 1);
+        double2 w[2], S[2];
+        #pragma unroll
+        for (int u = 0; u < (TWO ? 2 : 1); ++u) {
+            w[u] = cinv(make_double2(x[u] - sx, y[u] - sy));
+            S[u] = A[P];
+        }
+        for (int pp = P - 1; pp >= 0; --pp) {
+            const double2 Ap = A[pp];
+            #pragma unroll
+            for (int u = 0; u < (TWO ? 2 : 1); ++u) S[u] = cfma(S[u], w[u], Ap);
+        }
+        #pragma unroll
+        for (int u = 0; u < (TWO ? 2 : 1); ++u) {
+            S[u] = cmul(S[u], w[u]);
+            ex[u] += S[u].x;
+            ey[u] -= S[u].y;
+        }
+    }
+    #pragma unroll
+    for (int u = 0; u < (TWO ? 2 : 1); ++u) {
+        const double2 w = make_double2(x[u] - zx, y[u] - zy);
+        double2 S = cscale(s_b[P], (double)P);
+        for (int pp = P - 1; pp >= 1; --pp) S = cfma(S, w, cscale(s_b[pp], (double)pp));
+        double fxv = ex[u] + S.x, fyv = ey[u] - S.y;
+        if (!h[u]) continue;
+        const int i = ii[u];
+        if (nx) {
+            // near field already computed: write the total in the caller's order
+            fxv = nx[i] + fxv;
+            fyv = ny[i] + fyv;
+            const uint32_t orig = t.perm[i];
+            if (orig >= (uint32_t)t.n) {
+                set_err(err, ERR_INDEX);
+            } else if (velocity) {
+                out0[orig] = fyv + u_inf;
+                out1[orig] = -fxv + v_inf;
+            } else {
+                out0[orig] = fxv;
+                out1[orig] = fyv;
+            }
+        } else {
+            fx[i] = fxv;
+            fy[i] = fyv;
+        }
+    }
+}
+
 constexpr int kEvalWarps = 4;   // one warp per leaf
 constexpr int kEvalThreads = 32 * kEvalWarps;
 
-// Far field of every particle of a leaf: M2P over list 3 (fmm2D.cpp:1040-1066)
-// and L2P of the leaf's complete local expansion (fmm2D.cpp:1076-1093). Cells
-// above level 2 carry no local expansion (M2L starts at level 2).
+// Far field of every particle of a leaf (eval_targets), one warp per leaf,
+// 64 targets per pass (two per lane). Cells above level 2 carry no local
+// expansion (M2L starts at level 2).
 __global__ void __launch_bounds__(kEvalThreads)
 eval2d(Tree2D t, Lists2D l, const double2* __restrict__ a, const double2* __restrict__ b, double* __restrict__ fx,
        double* __restrict__ fy, int P, const double* __restrict__ nx, const double* __restrict__ ny,
@@ -431,42 +502,14 @@ eval2d(Tree2D t, Lists2D l, const double2* __restrict__ a, const double2* __rest
         const int lo = t.c_lo[c], hi = t.c_hi[c];
         const double zx = t.c_cx[c], zy = t.c_cy[c];
         const uint32_t o3 = l.l3_off[li], e3 = l.l3_off[li + 1];
-        for (int i = lo + lane; i < hi; i += 32) {
-            const double x = t.px[i], y = t.py[i];
-            double ex = 0.0, ey = 0.0;
-            for (uint32_t k = o3; k < e3; ++k) {
-                const int s = l.l3_src[k];
-                const double2 w = cinv(make_double2(x - t.c_cx[s], y - t.c_cy[s]));
-                const double2* A = a + (size_t)s * (P + 1);
-                double2 S = A[P];
-                for (int pp = P - 1; pp >= 0; --pp) S = cfma(S, w, A[pp]);
-                S = cmul(S, w);
-                ex += S.x;
-                ey -= S.y;
-            }
-            const double2 w = make_double2(x - zx, y - zy);
-            double2 S = cscale(s_b[P], (double)P);
-            for (int pp = P - 1; pp >= 1; --pp) S = cfma(S, w, cscale(s_b[pp], (double)pp));
-            ex += S.x;
-            ey -= S.y;
-            if (nx) {
-                // near field already computed: write the total in the caller's order
-                ex = nx[i] + ex;
-                ey = ny[i] + ey;
-                const uint32_t orig = t.perm[i];
-                if (orig >= (uint32_t)t.n) {
-                    set_err(err, ERR_INDEX);
-                } else if (velocity) {
-                    out0[orig] = ey + u_inf;
-                    out1[orig] = -ex + v_inf;
-                } else {
-                    out0[orig] = ex;
-                    out1[orig] = ey;
-                }
-            } else {
-                fx[i] = ex;
-                fy[i] = ey;
-            }
+        for (int i0 = lo; i0 < hi; i0 += 64) {
+            const int ia = i0 + lane, ib = i0 + 32 + lane;
+            if (i0 + 32 < hi)   // warp-uniform
+                eval_targets<true>(t, l, a, s_b, P, ia, ib, ia < hi, ib < hi, zx, zy, o3, e3, fx, fy, nx, ny, out0,
+                                   out1, velocity, u_inf, v_inf, err);
+            else
+                eval_targets<false>(t, l, a, s_b, P, ia, ib, ia < hi, false, zx, zy, o3, e3, fx, fy, nx, ny, out0,
+                                    out1, velocity, u_inf, v_inf, err);
         }
         __syncwarp();
     }
