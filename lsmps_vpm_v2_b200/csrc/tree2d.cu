@@ -794,7 +794,6 @@ __global__ void __launch_bounds__(kFlatTile)
 flat_emit(Tree2D t, const uint32_t* __restrict__ pinfo, const uint32_t* __restrict__ tile_cnt, int tiles,
           int max_par, unsigned* err) {
     __shared__ int s_wc[kMaxLevels2D + 1][kFlatTile / 32], s_wl[kMaxLevels2D + 1][kFlatTile / 32];
-    __shared__ int s_lo, s_hi;
     if (block_fatal(err)) return;
     const int n = t.n, K = t.key_levels;
     const TreeInfo2D* info = t.info;
@@ -805,18 +804,15 @@ flat_emit(Tree2D t, const uint32_t* __restrict__ pinfo, const uint32_t* __restri
         const int i = tile * kFlatTile + threadIdx.x;
         const uint32_t w = i < n ? pinfo[i] : 0u;
         const int first = (int)((w >> 16) & 0xff), last = (int)(w >> 24), big = (int)((w >> 8) & 0xff) - 1;
-        if (threadIdx.x == 0) {
-            s_lo = kMaxLevels2D + 1;
-            s_hi = 0;
+        // the levels at which this warp's particles start cells (most warps: one or two)
+        const int Llo = (int)__reduce_min_sync(0xffffffffu, first ? (unsigned)first : 255u);
+        const int Lhi = (int)__reduce_max_sync(0xffffffffu, first ? (unsigned)last : 0u);
+        // per-warp counts of every level (zero outside the warp's range), then one barrier
+        if (lane <= K) {
+            s_wc[lane][warp] = 0;
+            s_wl[lane][warp] = 0;
         }
-        __syncthreads();
-        if (first) {
-            atomicMin(&s_lo, first);
-            atomicMax(&s_hi, last);
-        }
-        __syncthreads();
-        const int Llo = s_lo, Lhi = s_hi;
-        // per-warp counts of every level, then one barrier
+        __syncwarp();
         for (int L = Llo; L <= Lhi; ++L) {
             const bool has = first && first <= L && L <= last;
             const bool lf = has && L == last && big < last;
