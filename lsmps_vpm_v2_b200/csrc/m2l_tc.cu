@@ -329,17 +329,18 @@ constexpr int kF32Warps = 8;
 __host__ __device__ constexpr int f32_rp(int P) { return ((2 * (P + 1) + 3) / 4) * 4; }   // row stride (floats)
 __host__ __device__ constexpr int f32_nrp(int P) { return ((2 * P + 3) / 4) * 4; }       // outputs, padded
 
-// Scaled multipole rows [Re a~_0..Re a~_P, Im a~_0..Im a~_P, 0..] in FP32.
+// Scaled multipole rows [Re a~_0..Re a~_P, Im a~_0..Im a~_P, 0..] in FP32, and
+// after the last cell (row n_cells) a row of zeros: the source of an empty slot.
 __global__ void m2l_rows_f32(Tree2D t, const double2* __restrict__ a, float* __restrict__ rows, int P, int RP,
                              unsigned* err) {
     if (fatal(err)) return;
     const int nc = t.info->n_cells;
     const double root = t.geom->root;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < (long long)nc * RP;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < (long long)(nc + 1) * RP;
          i += (long long)gridDim.x * blockDim.x) {
         const int c = (int)(i / RP), k = (int)(i - (long long)c * RP);
         float v = 0.f;
-        if (k < 2 * (P + 1)) {
+        if (c < nc && k < 2 * (P + 1)) {
             const int kk = k <= P ? k : k - (P + 1);
             const double rinv = ldexp(1.0, (int)t.c_level[c]) / root;
             double sc = 1.0;
@@ -374,7 +375,7 @@ m2l2d_f32(Tree2D t, Lists2D l, const float* __restrict__ rows, const float* __re
     for (int task = blockIdx.x * kF32Warps + wib; task < ntasks; task += gridDim.x * kF32Warps) {
         const int c = c_begin + task * TPW + tl;
         const bool valid = tl < TPW && c < c_end;
-        for (int i = lane; i < 49 * TPW; i += 32) my_src[i] = -1;
+        for (int i = lane; i < 49 * TPW; i += 32) my_src[i] = c_end;   // the zero row
         __syncwarp();
         uint32_t m_lo = 0, m_hi = 0;   // offsets present in this target's list
         if (valid && g == 0) {
@@ -389,24 +390,18 @@ m2l2d_f32(Tree2D t, Lists2D l, const float* __restrict__ rows, const float* __re
         __syncwarp();
         uint64_t mask = ((uint64_t)__reduce_or_sync(0xffffffffu, m_hi) << 32) | __reduce_or_sync(0xffffffffu, m_lo);
         float acc[4] = {0.f, 0.f, 0.f, 0.f};
-        // row of this lane's target's source at offset tau (zeros when it has none)
+        // row of this lane's target's source at offset tau (the zero row when it has none)
         auto load_row = [&](int tau, float4* dst) {
-            const int src = valid ? my_src[tau * TPW + tl] : -1;
-            const float4* row = reinterpret_cast<const float4*>(rows + (size_t)(src >= 0 ? src : 0) * RP);
+            const int src = valid ? my_src[tau * TPW + tl] : c_end;
+            const float4* row = reinterpret_cast<const float4*>(rows + (size_t)src * RP);
             #pragma unroll
-            for (int q = 0; q < RQ; ++q) dst[q] = src >= 0 ? __ldg(row + q) : make_float4(0.f, 0.f, 0.f, 0.f);
+            for (int q = 0; q < RQ; ++q) dst[q] = __ldg(row + q);
         };
-        float4 cur[RQ], nxt[RQ];
-        int tau = mask ? __ffsll((long long)mask) - 1 : 49;
-        if (tau < 49) load_row(tau, cur);
-        while (tau < 49) {
-            mask &= mask - 1;
-            const int tnext = mask ? __ffsll((long long)mask) - 1 : 49;
-            if (tnext < 49) load_row(tnext, nxt);
+        auto apply = [&](int tau, const float4* row) {
             const float4* T = reinterpret_cast<const float4*>(s_op + (size_t)tau * K2 * NRP) + g;
             #pragma unroll
             for (int q = 0; q < RQ; ++q) {
-                const float av[4] = {cur[q].x, cur[q].y, cur[q].z, cur[q].w};
+                const float av[4] = {row[q].x, row[q].y, row[q].z, row[q].w};
                 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     const int k = 4 * q + u;
@@ -418,9 +413,25 @@ m2l2d_f32(Tree2D t, Lists2D l, const float* __restrict__ rows, const float* __re
                     acc[3] = fmaf(w.w, av[u], acc[3]);
                 }
             }
-            #pragma unroll
-            for (int q = 0; q < RQ; ++q) cur[q] = nxt[q];
-            tau = tnext;
+        };
+        auto next_tau = [&]() {
+            const int tt = mask ? __ffsll((long long)mask) - 1 : 49;
+            mask &= mask - 1;
+            return tt;
+        };
+        // offsets in increasing order, two row buffers in turn (the next row
+        // loads while the current one is applied)
+        float4 ra[RQ], rb[RQ];
+        int ta = next_tau();
+        if (ta < 49) load_row(ta, ra);
+        while (ta < 49) {
+            const int tb = next_tau();
+            if (tb < 49) load_row(tb, rb);
+            apply(ta, ra);
+            if (tb >= 49) break;
+            ta = next_tau();
+            if (ta < 49) load_row(ta, ra);
+            apply(tb, rb);
         }
         if (valid) {
             // output r = 4 g + i is Re b~_{r+1} (r < P) or Im b~_{r-P+1} (P <= r < 2P)
