@@ -1053,7 +1053,7 @@ p2p2d_warp(Tree2D t, Lists2D l, const typename Tr::Elem* __restrict__ src, const
 // so kTileEps changes no other pair, and q / kTileEps stays finite for
 // |q| < 3e14.
 constexpr int kTileWarps = 8;
-constexpr int kTileFlush = 64;
+constexpr int kTileFlush = 128;
 constexpr int kTileMaxM = 6;
 constexpr int kTileChunk = 16 * kTileMaxM;      // targets per chunk (H <= 16, so ns >= 2)
 constexpr int kTileSlots = kTileMaxM / 2;       // FP64 target slots per lane (ns >= 2)
