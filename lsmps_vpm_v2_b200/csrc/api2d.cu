@@ -222,10 +222,13 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
     if (capturing && !split_capture && !tree_only && velocity != kModePotential) {
         // One captured graph: the near field (lists 1/3, P2P) runs on the side
         // stream concurrently with lists 2/4 and the far field (P2M, M2M, M2L,
-        // L2L); M2P + L2P then add the near field and write the output.
+        // L2L); M2P follows lists 2/4 on the third stream once the upward pass
+        // and list 3 are done; L2P then adds the M2P and near-field sums and
+        // writes the output.
         VPM_CUDA_TRY(cudaEventRecord(fork2, st));
         VPM_CUDA_TRY(cudaStreamWaitEvent(side, fork2, 0));
         VPM_CUDA_TRY(build_int_lists2d(tree, lists, ts.scan, p.eps, d_err, side, &launches));
+        VPM_CUDA_TRY(cudaEventRecord(ev_l13, side));
         if (p.precision == VPM_PREC_MIXED || p.precision == VPM_PREC_MIXED_FP64_M2L)
             VPM_CUDA_TRY(fmm2d_p2p_f32(tree, lists, ex2, near_x, near_y, 0, 0.0, 0.0, d_err, side, &launches, true));
         else
@@ -236,6 +239,11 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
         VPM_CUDA_TRY(build_ext_lists2d(tree, lists, p.eps, d_err, side2, &launches));
         VPM_CUDA_TRY(cudaEventRecord(join3, side2));
         VPM_CUDA_TRY(fmm2d_upward(tree, ex2, p.p, d_err, st, &launches));
+        VPM_CUDA_TRY(cudaEventRecord(ev_up, st));
+        VPM_CUDA_TRY(cudaStreamWaitEvent(side2, ev_up, 0));
+        VPM_CUDA_TRY(cudaStreamWaitEvent(side2, ev_l13, 0));
+        VPM_CUDA_TRY(fmm2d_m2p(tree, lists, ex2, p.p, d_err, side2, &launches));
+        VPM_CUDA_TRY(cudaEventRecord(join4, side2));
         VPM_CUDA_TRY(cudaStreamWaitEvent(st, join3, 0));
         if (p.precision == VPM_PREC_MIXED && m2l_f32_supported(p.p))
             VPM_CUDA_TRY(fmm2d_m2l_f32(tree, lists, ex2, p.p, tc_rows, tc_ops, d_err, st, &launches));
@@ -248,8 +256,9 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
         else
             VPM_CUDA_TRY(fmm2d_l2l(tree, ex2, p.p, d_err, st, &launches));
         VPM_CUDA_TRY(cudaStreamWaitEvent(st, join2, 0));
+        VPM_CUDA_TRY(cudaStreamWaitEvent(st, join4, 0));
         VPM_CUDA_TRY(fmm2d_eval_combine(tree, lists, ex2, p.p, near_x, near_y, o0, o1, velocity, uinf, vinf, d_err, st,
-                                        &launches));
+                                        &launches, true));
         last_launches = launches;
         last_params = p;
         last_n = n;

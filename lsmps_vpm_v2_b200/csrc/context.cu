@@ -50,6 +50,8 @@ Ctx::~Ctx() {
     if (join3) cudaEventDestroy(join3);
     if (fork2) cudaEventDestroy(fork2);
     if (join2) cudaEventDestroy(join2);
+    for (cudaEvent_t x : {ev_up, ev_l13, join4})
+        if (x) cudaEventDestroy(x);
 }
 
 int Ctx::init(int dev) {
@@ -67,6 +69,9 @@ int Ctx::init(int dev) {
     e = cudaEventCreateWithFlags(&fork2, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&join2, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&join3, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_up, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_l13, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&join4, cudaEventDisableTiming);
     if (e != cudaSuccess) return fail_cuda(e, "cudaEventCreate");
     e = cudaMalloc(&d_err, 64);
     if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc");

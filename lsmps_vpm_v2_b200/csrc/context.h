@@ -53,6 +53,7 @@ struct Ctx {
     cudaStream_t side = nullptr;
     cudaStream_t side2 = nullptr;   // lists 2/4 while the main stream runs P2M + M2M
     cudaEvent_t fork2 = nullptr, join2 = nullptr, join3 = nullptr;
+    cudaEvent_t ev_up = nullptr, ev_l13 = nullptr, join4 = nullptr;   // upward done, lists 1/3 done, M2P done
     double *near_x = nullptr, *near_y = nullptr;
     std::string last_error;
     unsigned* d_err = nullptr;
@@ -181,10 +182,14 @@ cudaError_t fmm2d_p2p_f64_tma(const Tree2D& t, const Lists2D& l, const Expansion
                               double* out1, int velocity, double u_inf, double v_inf, unsigned* err, cudaStream_t st,
                               int* launches, int max_par, bool near_only = false);
 // Far field (M2P + L2P) plus the near field nx/ny (tree order), written in the
-// caller's order (field or velocity).
+// caller's order (field or velocity). With m2p_done the list-3 sums are
+// already in e.fx/e.fy (fmm2d_m2p) and only L2P is added (same result).
 cudaError_t fmm2d_eval_combine(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, const double* nx,
                                const double* ny, double* out0, double* out1, int velocity, double u_inf, double v_inf,
-                               unsigned* err, cudaStream_t st, int* launches);
+                               unsigned* err, cudaStream_t st, int* launches, bool m2p_done = false);
+// M2P over list 3 of every leaf's particles into e.fx/e.fy (tree order).
+cudaError_t fmm2d_m2p(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, unsigned* err, cudaStream_t st,
+                      int* launches);
 cudaError_t fmm2d_p2p_out(const Tree2D& t, const Lists2D& l, const Expansions2D& e, double* out0, double* out1,
                           int velocity, double u_inf, double v_inf, unsigned* err, cudaStream_t st, int* launches);
 

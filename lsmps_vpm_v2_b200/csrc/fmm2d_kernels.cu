@@ -412,8 +412,12 @@ m2l2d_op(Tree2D t, Lists2D l, const double2* __restrict__ a, double2* __restrict
 // (fmm2D.cpp:1076-1093). With TWO, each lane takes a second target and both
 // run through the list-3 sources together (one load of every source's
 // coefficients serves both, and the two chains are independent). Each
-// target's sums run in the same order either way.
-template <bool TWO>
+// target's sums run in the same order either way. MODE kEvalFull does both;
+// kEvalM2P writes the list-3 sums alone to fx/fy; kEvalL2P starts from those
+// sums (the same value the full mode reaches after its list-3 loop) and adds
+// L2P, so the split gives the same bits as one pass.
+constexpr int kEvalFull = 0, kEvalM2P = 1, kEvalL2P = 2;
+template <bool TWO, int MODE>
 __device__ __forceinline__ void eval_targets(const Tree2D& t, const Lists2D& l, const double2* __restrict__ a,
                                              const double2* s_b, int P, int i0, int i1, bool h0, bool h1, double zx,
                                              double zy, uint32_t o3, uint32_t e3, double* fx, double* fy,
@@ -426,6 +430,15 @@ __device__ __forceinline__ void eval_targets(const Tree2D& t, const Lists2D& l, 
     for (int u = 0; u < (TWO ? 2 : 1); ++u) {
         x[u] = h[u] ? t.px[ii[u]] : zx + 1.0;
         y[u] = h[u] ? t.py[ii[u]] : zy;
+    }
+    if (MODE == kEvalL2P) {
+        #pragma unroll
+        for (int u = 0; u < (TWO ? 2 : 1); ++u)
+            if (h[u]) {
+                ex[u] = fx[ii[u]];
+                ey[u] = fy[ii[u]];
+            }
+        o3 = e3;
     }
     for (uint32_t k = o3; k < e3; ++k) {
         const int s = l.l3_src[k];
@@ -448,6 +461,15 @@ __device__ __forceinline__ void eval_targets(const Tree2D& t, const Lists2D& l, 
             ex[u] += S[u].x;
             ey[u] -= S[u].y;
         }
+    }
+    if (MODE == kEvalM2P) {
+        #pragma unroll
+        for (int u = 0; u < (TWO ? 2 : 1); ++u)
+            if (h[u]) {
+                fx[ii[u]] = ex[u];
+                fy[ii[u]] = ey[u];
+            }
+        return;
     }
     #pragma unroll
     for (int u = 0; u < (TWO ? 2 : 1); ++u) {
@@ -484,6 +506,7 @@ constexpr int kEvalThreads = 32 * kEvalWarps;
 // Far field of every particle of a leaf (eval_targets), one warp per leaf,
 // 64 targets per pass (two per lane). Cells above level 2 carry no local
 // expansion (M2L starts at level 2).
+template <int MODE>
 __global__ void __launch_bounds__(kEvalThreads)
 eval2d(Tree2D t, Lists2D l, const double2* __restrict__ a, const double2* __restrict__ b, double* __restrict__ fx,
        double* __restrict__ fy, int P, const double* __restrict__ nx, const double* __restrict__ ny,
@@ -497,7 +520,9 @@ eval2d(Tree2D t, Lists2D l, const double2* __restrict__ a, const double2* __rest
     for (int li = blockIdx.x * kEvalWarps + wib; li < nl; li += gridDim.x * kEvalWarps) {
         const int c = t.leaf_cells[li];
         const int L = t.c_level[c];
-        for (int k = lane; k <= P; k += 32) s_b[k] = L >= 2 ? b[(size_t)c * (P + 1) + k] : make_double2(0.0, 0.0);
+        if (MODE != kEvalM2P)
+            for (int k = lane; k <= P; k += 32)
+                s_b[k] = L >= 2 ? b[(size_t)c * (P + 1) + k] : make_double2(0.0, 0.0);
         __syncwarp();
         const int lo = t.c_lo[c], hi = t.c_hi[c];
         const double zx = t.c_cx[c], zy = t.c_cy[c];
@@ -505,11 +530,11 @@ eval2d(Tree2D t, Lists2D l, const double2* __restrict__ a, const double2* __rest
         for (int i0 = lo; i0 < hi; i0 += 64) {
             const int ia = i0 + lane, ib = i0 + 32 + lane;
             if (i0 + 32 < hi)   // warp-uniform
-                eval_targets<true>(t, l, a, s_b, P, ia, ib, ia < hi, ib < hi, zx, zy, o3, e3, fx, fy, nx, ny, out0,
-                                   out1, velocity, u_inf, v_inf, err);
+                eval_targets<true, MODE>(t, l, a, s_b, P, ia, ib, ia < hi, ib < hi, zx, zy, o3, e3, fx, fy, nx, ny,
+                                         out0, out1, velocity, u_inf, v_inf, err);
             else
-                eval_targets<false>(t, l, a, s_b, P, ia, ib, ia < hi, false, zx, zy, o3, e3, fx, fy, nx, ny, out0,
-                                    out1, velocity, u_inf, v_inf, err);
+                eval_targets<false, MODE>(t, l, a, s_b, P, ia, ib, ia < hi, false, zx, zy, o3, e3, fx, fy, nx, ny,
+                                          out0, out1, velocity, u_inf, v_inf, err);
         }
         __syncwarp();
     }
@@ -1544,17 +1569,29 @@ cudaError_t fmm2d_m2l(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P,
 
 cudaError_t fmm2d_eval(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, unsigned* err, cudaStream_t st,
                        int* launches) {
-    eval2d<<<148 * 16, kEvalThreads, 0, st>>>(t, l, e.a, e.b, e.fx, e.fy, P, nullptr, nullptr, nullptr, nullptr, 0,
-                                              0.0, 0.0, err);
+    eval2d<kEvalFull><<<148 * 16, kEvalThreads, 0, st>>>(t, l, e.a, e.b, e.fx, e.fy, P, nullptr, nullptr, nullptr,
+                                                         nullptr, 0, 0.0, 0.0, err);
+    *launches += 1;
+    return cudaGetLastError();
+}
+
+cudaError_t fmm2d_m2p(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, unsigned* err, cudaStream_t st,
+                      int* launches) {
+    eval2d<kEvalM2P><<<148 * 16, kEvalThreads, 0, st>>>(t, l, e.a, e.b, e.fx, e.fy, P, nullptr, nullptr, nullptr,
+                                                        nullptr, 0, 0.0, 0.0, err);
     *launches += 1;
     return cudaGetLastError();
 }
 
 cudaError_t fmm2d_eval_combine(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, const double* nx,
                                const double* ny, double* out0, double* out1, int velocity, double u_inf, double v_inf,
-                               unsigned* err, cudaStream_t st, int* launches) {
-    eval2d<<<148 * 16, kEvalThreads, 0, st>>>(t, l, e.a, e.b, e.fx, e.fy, P, nx, ny, out0, out1, velocity, u_inf,
-                                              v_inf, err);
+                               unsigned* err, cudaStream_t st, int* launches, bool m2p_done) {
+    if (m2p_done)
+        eval2d<kEvalL2P><<<148 * 16, kEvalThreads, 0, st>>>(t, l, e.a, e.b, e.fx, e.fy, P, nx, ny, out0, out1, velocity,
+                                                            u_inf, v_inf, err);
+    else
+        eval2d<kEvalFull><<<148 * 16, kEvalThreads, 0, st>>>(t, l, e.a, e.b, e.fx, e.fy, P, nx, ny, out0, out1,
+                                                             velocity, u_inf, v_inf, err);
     *launches += 1;
     return cudaGetLastError();
 }
