@@ -1608,7 +1608,11 @@ cudaError_t fmm2d_p2p_f32(const Tree2D& t, const Lists2D& l, const Expansions2D&
                           bool near_only) {
     Expansions2D en = e;
     if (near_only) en.fx = en.fy = nullptr;
-    p2p2d_tile_f32<<<148 * 3, 32 * kTileWarps, 0, st>>>(t, l, en.fx, en.fy, out0, out1, velocity, u_inf, v_inf, err);
+    // Many short blocks (a leaf or a few per warp) rather than one persistent
+    // wave: blocks retire all through the launch, so the far-field kernels
+    // running concurrently on the other streams get SM room as they queue.
+    p2p2d_tile_f32<<<148 * 3 * 8, 32 * kTileWarps, 0, st>>>(t, l, en.fx, en.fy, out0, out1, velocity, u_inf, v_inf,
+                                                           err);
     *launches += 1;
     return cudaGetLastError();
 }
