@@ -327,7 +327,7 @@ def run_ours(args):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64" if form == "fp64" else "f32+tf32+f64", "data": "synthetic",
+        "vs_baseline": None, "dtype": mixed_dtype(form, int(prm.p)), "data": "synthetic",
         "config": {"workload": f"boundary_layer_2d N={n}", "n": n, "form": form,
                    "p": int(prm.p), "max_src": int(prm.max_src), "max_par": int(prm.max_par),
                    "binomials": "reference 32-bit binComb" if prm.binom == 0 else "exact",
@@ -363,6 +363,15 @@ def run_ours(args):
         print(json.dumps(line), flush=True)
     ctx.close()
     return 0
+
+
+def mixed_dtype(form, p):
+    """Arithmetic types of the timed form: the plain form is FP64 throughout;
+    the mixed form runs its near field and list-2 M2L in FP32 (3xTF32 on the
+    tensor cores for orders 13-20) and everything else in FP64."""
+    if form == "fp64":
+        return "f64"
+    return "f32+tf32+f64" if p >= 13 else "f32+f64"
 
 
 def main():
