@@ -1,9 +1,14 @@
 """Seeded 2D particle sets shared by the parity tests (small enough for the
 oracle to finish in seconds), including the edge cases the reference's list
 logic is sensitive to."""
+import os
+
 import numpy as np
 
 from lsmps_vpm_v2_b200 import workloads as w
+from lsmps_vpm_v2_b200.state import read_particle_state
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
 def _field(x, y, active=None, seed=0):
@@ -89,6 +94,16 @@ def duplicates():
     return d
 
 
+def state500():
+    """Every 8th particle of the reference solver's own flow state at step 500
+    (tests/golden/particle_state_00500_sub8.csv; 2,716 particles of several
+    sizes, some inactive), with the reference's source strength -omega s^2/(2 pi)
+    (velocity_calc.cpp:477)."""
+    p = read_particle_state(os.path.join(GOLDEN, "particle_state_00500_sub8.csv"))
+    return dict(x=p["x"], y=p["y"], s=p["s"], omega=p["vorticity"], active=p["active"],
+                q=-p["vorticity"] * p["s"] * p["s"] / (2 * np.pi))
+
+
 def tiny(n, seed=8):
     rng = np.random.default_rng(seed)
     return _field(rng.uniform(-1, 1, n), rng.uniform(-1, 1, n), seed=seed)
@@ -104,6 +119,7 @@ CASES = {
     "boundary_aligned": boundary_aligned,
     "aspect": aspect,
     "duplicates": duplicates,
+    "state500": state500,
     "tiny2": lambda: tiny(2),
     "tiny17": lambda: tiny(17),
     "tiny76": lambda: tiny(76),

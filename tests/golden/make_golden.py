@@ -6,7 +6,7 @@ reference's outputs: the tree dump (cells by ID, leafList, parIDList), lists
 1-4, the field (calcField) and the potential (calcPotential) for 2D; the
 treecode velocity and octree dump for 3D.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [case ...]   (all cases when none is named)
 """
 import os
 import sys
@@ -26,12 +26,15 @@ from lsmps_vpm_v2_b200 import workloads  # noqa: E402
 
 CASES_2D = [("lamb_small", 10, 50, 75), ("clustered", 10, 50, 75), ("partly_inactive", 10, 50, 75),
             ("aspect", 10, 50, 75), ("boundary_aligned", 16, 50, 75), ("clustered", 16, 20, 30),
-            ("tiny300", 8, 50, 75)]
+            ("tiny300", 8, 50, 75), ("state500", 10, 50, 75)]
 
 
 def main():
     ref = Reference()
+    only = set(sys.argv[1:])
     for name, p, ms, mp in CASES_2D:
+        if only and name not in only:
+            continue
         d = cases2d.CASES[name]()
         x, y, q, a = d["x"], d["y"], d["q"], d["active"]
         t = ref.tree2d(x, y, a, max_src=ms, max_par=mp)
@@ -48,6 +51,8 @@ def main():
         fn = os.path.join(HERE, f"fmm2d_{name}_p{p}_{ms}_{mp}.npz")
         np.savez_compressed(fn, **out)
         print(fn, x.size, t.ids.size)
+    if only and "ring3d" not in only:
+        return
     # 3D treecode on a coarse ring.
     r = workloads.vortex_ring_3d(h=0.05)
     args = [r[k] for k in ("x", "y", "z", "ax", "ay", "az")]
