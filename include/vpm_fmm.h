@@ -336,7 +336,7 @@ int vpm_select2d(vpm_ctx* ctx, const float* feat, double target_err, double marg
 /*
  * FP64 direct sum of the 2D field at m sampled targets (device pointers,
  * int64 target indices on the device): E_t = sum over active j != t of
- * q_j (x_t - x_j) / |x_t - x_j|^2, the judge of the FMM's error (the
+ * q_j (x_t - x_j) / |x_t - x_j|^2, the yardstick of the FMM's error (the
  * reference's own direct form, fmm2D::fieldDirSum, fmm2D.cpp:135-179, over
  * all sources). Asynchronous on the context's stream.
  */

@@ -1,5 +1,5 @@
 // Learned (leaf caps, p) selector of the mixed 2D form, and the FP64 direct
-// sum that labels and judges it. No counterpart in the reference, which
+// sum that labels and checks it. No counterpart in the reference, which
 // always evaluates with its fixed caps 50/75 and p = 10 (global.cpp:311-313);
 // that pair stays the fallback.
 //

@@ -14,7 +14,7 @@
 //   * P2P/M2P/L2P field         src/FMM/fmm2D.cpp:135-179, 907-1123 (calcField)
 //   * P2P/M2P/L2P potential     src/FMM/fmm2D.cpp:77-122, 681-896 (calcPotential)
 // plus an FP64 direct O(N*M) Biot-Savart sum on sampled targets, the accuracy
-// judge for the chosen (mixed / tuned) forms.
+// yardstick for the chosen (mixed / tuned) forms.
 //
 // Every floating-point step that decides an integer (cell index, adjacency,
 // separation) is written as separate IEEE operations in the same order as the

@@ -1,5 +1,5 @@
 """The NumPy restatement of the selector network (oracle/mlp.py) checks
-itself by central finite differences, so it can judge the GPU kernels."""
+itself by central finite differences, so it can check the GPU kernels."""
 import numpy as np
 
 from mlp import DIMS, forward, loss_and_grads, param_count
