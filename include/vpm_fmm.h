@@ -57,8 +57,9 @@ typedef struct vpm_ctx vpm_ctx;
  */
 typedef struct vpm_fmm_params {
     int32_t p;            /* expansion order, 1..30                                 */
-    int32_t max_src;      /* 2D leaf cap on active (source) particles               */
-    int32_t max_par;      /* 2D leaf cap on all particles                           */
+    int32_t max_src;      /* leaf cap on active (source) particles: 2D tree and
+                             3D TreeCell                                          */
+    int32_t max_par;      /* leaf cap on all particles: 2D tree and 3D TreeCell     */
     int32_t leaf_cap_3d;  /* 3D leaf iff particle count < leaf_cap_3d               */
     double exp_tree_pct;  /* root box expansion, percent                            */
     double eps;           /* list distance tolerance                                */
@@ -288,6 +289,52 @@ int vpm_tree3d_build(vpm_ctx* ctx, const double* x, const double* y, const doubl
                      int64_t n, const vpm_fmm_params* prm, vpm_fmm_stats* stats);
 int vpm_tree3d_counts(vpm_ctx* ctx, int64_t* n_cells, int64_t* n_leaves, int32_t* depth);
 int vpm_tree3d_cells(vpm_ctx* ctx, int32_t* ints6, double* geom4, int64_t* leaf_offs, int32_t* pids);
+
+/*
+ * 3D velocity by the treecode on the shared TreeCell, the reference's
+ * alternative 3D path (VELOCITY_3D_TYPE 2 with VELOCITY_CALCULATION_TYPE 2).
+ * Replaces
+ *   TreeCell::initializeTree(pos, active) with DIM 3   src/FMM/treeCell.cpp:1043-1243
+ *   fmm3D::calcVelocity(tree, pos, active, ax, ay, az)  src/FMM/fmm3D.cpp:1064-1405
+ *   fmm3D::calcVelocityNearBody(tree, pos, active, target, ax, ay, az)
+ *                                                      src/FMM/fmm3D.cpp:1406-1606
+ *   fmm3D::get_Field_x / _y / _z                       src/FMM/fmm3D.hpp:106-138
+ * as called by VelocityCalc::velocity_fmm_3d (velocity_calc.cpp:2172-2375).
+ * The root box is the particle box alone (side = max extent * (1 +
+ * exp_tree_pct/100)); a cell is a leaf iff it holds at most prm->max_src
+ * active and at most prm->max_par particles (the reference's 3D values are
+ * 30 and 50, global.cpp:778-779; vpm_fmm_params_default gives the 2D 50/75).
+ * Far iff R^2 > (2 length)^2 (10-term moments), near leaves by direct sum over
+ * all their particles, inactive ones included. target = NULL evaluates every
+ * particle (calcVelocity); otherwise only flagged ones, the others get zero
+ * (calcVelocityNearBody). precision = VPM_PREC_MIXED as for
+ * vpm_fmm3d_velocity. Returns VPM_EINVAL when the tree would go deeper than
+ * level 10 (the reference's 32-bit cell IDs overflow there) and when a level-1
+ * cell is a leaf of a deeper tree (the reference's traversal throws there).
+ * Host buffers; stats may be NULL.
+ */
+int vpm_fmm3d_velocity_treecell(vpm_ctx* ctx, const double* x, const double* y, const double* z, const double* ax,
+                                const double* ay, const double* az, const uint8_t* active, const uint8_t* target,
+                                int64_t n, const vpm_fmm_params* prm, double* u, double* v, double* w,
+                                vpm_fmm_stats* stats);
+
+/* Same with device pointers (target may be NULL), asynchronous on the
+ * context's stream; vpm_ctx_sync reports the failures found on the device. */
+int vpm_fmm3d_velocity_treecell_device(vpm_ctx* ctx, const double* x, const double* y, const double* z,
+                                       const double* ax, const double* ay, const double* az, const uint8_t* active,
+                                       const uint8_t* target, int64_t n, const vpm_fmm_params* prm, double* u,
+                                       double* v, double* w);
+
+/*
+ * 3D TreeCell only (TreeCell::initializeTree with DIM 3,
+ * treeCell.cpp:1043-1243), for the parity dumps: vpm_tree3d_counts and
+ * vpm_tree3d_cells then describe it (cells level-major, Morton order within a
+ * level), and vpm_tree3d_cell_ids gives each cell's reference ID
+ * (8^L - 1) / 7 + ix + iy 2^L + iz 4^L (treeCell.cpp:114-148, 223-250).
+ */
+int vpm_treecell3d_build(vpm_ctx* ctx, const double* x, const double* y, const double* z, const uint8_t* active,
+                         int64_t n, const vpm_fmm_params* prm, vpm_fmm_stats* stats);
+int vpm_tree3d_cell_ids(vpm_ctx* ctx, int64_t* ids);
 
 /*
  * Learned (leaf caps, p) selector of the mixed 2D form. No counterpart in the

@@ -129,6 +129,12 @@ SIGNATURES = {
     "vpm_tree3d_build": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int64, C.POINTER(Params), C.POINTER(Stats)]),
     "vpm_tree3d_counts": (C.c_int, [_vp, _i64p, _i64p, _i32p]),
     "vpm_tree3d_cells": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "vpm_fmm3d_velocity_treecell": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int64,
+                                              C.POINTER(Params), _vp, _vp, _vp, C.POINTER(Stats)]),
+    "vpm_fmm3d_velocity_treecell_device": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int64,
+                                                     C.POINTER(Params), _vp, _vp, _vp]),
+    "vpm_treecell3d_build": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int64, C.POINTER(Params), C.POINTER(Stats)]),
+    "vpm_tree3d_cell_ids": (C.c_int, [_vp, _vp]),
     "vpm_fmm2d_field_device_static": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int64, C.POINTER(Params), _vp, _vp, _vp,
                                                 C.c_char_p, C.c_size_t]),
 }
@@ -157,6 +163,12 @@ def default_params(**over) -> Params:
     for k, v in over.items():
         setattr(p, k, v)
     return p
+
+
+def treecell3d_params(**over) -> Params:
+    """Defaults with the reference's 3D TreeCell leaf caps: at most 30 active
+    and 50 particles per leaf (global.cpp:778-779)."""
+    return default_params(max_src=30, max_par=50, **over)
 
 
 class VpmError(RuntimeError):

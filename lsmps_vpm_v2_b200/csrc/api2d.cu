@@ -177,6 +177,9 @@ int Ctx::map_err(unsigned bits) {
     if (bits & ERR_DEPTH) return fail(VPM_EOVERFLOW, "tree deeper than the key resolution (coincident particles?)");
     if (bits & (ERR_CELL_CAP | ERR_LIST_CAP)) return fail(VPM_EOVERFLOW, "cell or list capacity exceeded");
     if (bits & (ERR_QUEUE | ERR_LIST4 | ERR_LIST2)) return fail(VPM_EOVERFLOW, "interaction-list queue overflow");
+    if (bits & ERR_LEAF1)
+        return fail(VPM_EINVAL, "3D TreeCell: a level-1 cell is a leaf of a deeper tree (the reference's traversal "
+                                "throws there)");
     return fail(VPM_EDEVICE, "device index check failed");
 }
 

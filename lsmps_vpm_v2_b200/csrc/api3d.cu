@@ -67,6 +67,11 @@ int Ctx::reserve3d(int n, int cap_cells) {
            o_vb = L.take<uint32_t>(n);
     size_t o_sstat = L.take<uint32_t>((size_t)4 * s_tiles * 256), o_stick = L.take<unsigned>(8),
            o_hist = L.take<uint32_t>(8 * 256);
+    const int tc_tiles = ceil_div(n, kTcTile);
+    size_t o_tgt = L.take<uint8_t>(n), o_tcact = L.take<uint32_t>(n), o_tcscan = L.take<uint32_t>((size_t)n + 1),
+           o_tcpinfo = L.take<uint32_t>(n), o_tctile = L.take<uint32_t>((size_t)2 * (kTcLevels + 1) * tc_tiles),
+           o_tctot = L.take<uint32_t>(32), o_tccode = L.take<uint32_t>(C),
+           o_scst = L.take<uint64_t>(scan_tiles(n)), o_sctk = L.take<unsigned>(8);
 
     if (arena3d) cudaFree(arena3d);
     arena3d = nullptr;
@@ -101,6 +106,11 @@ int Ctx::reserve3d(int n, int cap_cells) {
     s3.val_a = (uint32_t*)P_(o_va); s3.val_b = (uint32_t*)P_(o_vb);
     s3.sort.status = (uint32_t*)P_(o_sstat); s3.sort.tickets = (unsigned*)P_(o_stick);
     s3.sort.hist = (uint32_t*)P_(o_hist); s3.sort.max_tiles = s_tiles;
+    in3_tgt = (uint8_t*)P_(o_tgt);
+    s3.tc_act = (uint32_t*)P_(o_tcact); s3.tc_scan = (uint32_t*)P_(o_tcscan); s3.tc_pinfo = (uint32_t*)P_(o_tcpinfo);
+    s3.tc_tile = (uint32_t*)P_(o_tctile); s3.tc_tot = (uint32_t*)P_(o_tctot); s3.tc_code = (uint32_t*)P_(o_tccode);
+    s3.scan.status = (uint64_t*)P_(o_scst); s3.scan.ticket = (unsigned*)P_(o_sctk); s3.scan.max_tiles = scan_tiles(n);
+    s3.tc_tiles = tc_tiles;
     cap3.n = n;
     cap3.cells = cap_cells;
     return VPM_OK;
@@ -108,20 +118,27 @@ int Ctx::reserve3d(int n, int cap_cells) {
 
 int Ctx::enqueue3d(const double* x, const double* y, const double* z, const double* ax, const double* ay,
                    const double* az, const uint8_t* act, int n, const vpm_fmm_params& p, double* u, double* v,
-                   double* w, double uinf, double vinf, double winf, bool tree_only) {
+                   double* w, double uinf, double vinf, double winf, bool tree_only, bool treecell,
+                   const uint8_t* target) {
     cudaStream_t st = stream;
     int launches = 0;
     tree3.n = n;
     tree3.leaf_cap = p.leaf_cap_3d;
     VPM_CUDA_TRY(cudaMemsetAsync(d_err, 0, sizeof(unsigned), st));
     VPM_CUDA_TRY(cudaEventRecord(ev[0], st));
-    VPM_CUDA_TRY(build_tree3d(x, y, z, ax, ay, az, act, p.center_3d, p.exp_tree_pct, tree3, s3, bbox3, d_err, st,
-                              &launches));
+    if (treecell)
+        VPM_CUDA_TRY(build_treecell3d(x, y, z, ax, ay, az, act, p.max_src, p.max_par, p.exp_tree_pct, tree3, s3,
+                                      bbox3, d_err, st, &launches));
+    else
+        VPM_CUDA_TRY(build_tree3d(x, y, z, ax, ay, az, act, p.center_3d, p.exp_tree_pct, tree3, s3, bbox3, d_err,
+                                  st, &launches));
     if (!tree_only)
-        VPM_CUDA_TRY(eval3d(tree3, p.precision == VPM_PREC_MIXED, u, v, w, uinf, vinf, winf, d_err, st, &launches));
+        VPM_CUDA_TRY(eval3d(tree3, p.precision == VPM_PREC_MIXED, treecell, target, u, v, w, uinf, vinf, winf, d_err,
+                            st, &launches));
     VPM_CUDA_TRY(cudaEventRecord(ev[1], st));
     last_launches3 = launches;
     have_tree3 = true;
+    last_treecell3 = treecell;
     last_n3 = n;
     return VPM_OK;
 }
@@ -129,7 +146,7 @@ int Ctx::enqueue3d(const double* x, const double* y, const double* z, const doub
 int Ctx::run3d_host(const double* x, const double* y, const double* z, const double* a0, const double* a1,
                     const double* a2, const double* s, const uint8_t* act, int64_t n64, const vpm_fmm_params* prm,
                     double* u, double* v, double* w, double uinf, double vinf, double winf, vpm_fmm_stats* stats,
-                    bool tree_only) {
+                    bool tree_only, bool treecell, const uint8_t* target) {
     vpm_fmm_params p;
     int r = check_params(prm, p);
     if (r) return r;
@@ -154,13 +171,14 @@ int Ctx::run3d_host(const double* x, const double* y, const double* z, const dou
             VPM_CUDA_TRY(cudaMemcpyAsync(in3[k], src[k], sizeof(double) * n, cudaMemcpyHostToDevice, stream));
         }
         VPM_CUDA_TRY(cudaMemcpyAsync(in3_act, act, n, cudaMemcpyHostToDevice, stream));
+        if (target) VPM_CUDA_TRY(cudaMemcpyAsync(in3_tgt, target, n, cudaMemcpyHostToDevice, stream));
         if (s && !tree_only) {
             alpha_from_vorticity<<<std::min(1184, ceil_div(n, 256)), 256, 0, stream>>>(in3[3], in3[4], in3[5],
                                                                                        in3[6], n);
             VPM_CUDA_TRY(cudaGetLastError());
         }
         r = enqueue3d(in3[0], in3[1], in3[2], in3[3], in3[4], in3[5], in3_act, n, p, out3[0], out3[1], out3[2], uinf,
-                      vinf, winf, tree_only);
+                      vinf, winf, tree_only, treecell, target ? in3_tgt : nullptr);
         if (r) return r;
         unsigned bits = 0;
         VPM_CUDA_TRY(cudaMemcpyAsync(&bits, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
@@ -169,7 +187,13 @@ int Ctx::run3d_host(const double* x, const double* y, const double* z, const dou
             cells *= 2;
             continue;
         }
+        if ((bits & ERR_DEPTH) && treecell)
+            return fail(VPM_EINVAL, "TreeCell deeper than level 10: the reference's 32-bit cell IDs overflow there");
         if (bits & ERR_DEPTH) return fail(VPM_EINVAL, "octree deeper than 60 levels (coincident particles)");
+        if ((bits & ERR_LEAF1) && !tree_only)
+            return fail(VPM_EINVAL, "a level-1 cell is a leaf: the reference's TreeCell traversal cannot take its "
+                                    "children (fmm3D.cpp:1286 throws)");
+        bits &= ~(unsigned)ERR_LEAF1;
         if (bits) return map_err(bits);
         VPM_CUDA_TRY(cudaEventElapsedTime(&last_ms3, ev[0], ev[1]));
         if (!tree_only) {
@@ -208,7 +232,8 @@ int vpm_fmm3d_velocity(vpm_ctx* ctx, const double* x, const double* y, const dou
     Ctx* c = (Ctx*)ctx;
     cudaError_t e = cudaSetDevice(c->device);
     if (e != cudaSuccess) return c->fail_cuda(e, "cudaSetDevice");
-    return c->run3d_host(x, y, z, ax, ay, az, nullptr, active, n, prm, u, v, w, 0.0, 0.0, 0.0, stats, false);
+    return c->run3d_host(x, y, z, ax, ay, az, nullptr, active, n, prm, u, v, w, 0.0, 0.0, 0.0, stats, false, false,
+                         nullptr);
 }
 
 int vpm_velocity3d(vpm_ctx* ctx, const double* x, const double* y, const double* z, const double* omega_x,
@@ -221,7 +246,7 @@ int vpm_velocity3d(vpm_ctx* ctx, const double* x, const double* y, const double*
     cudaError_t e = cudaSetDevice(c->device);
     if (e != cudaSuccess) return c->fail_cuda(e, "cudaSetDevice");
     return c->run3d_host(x, y, z, omega_x, omega_y, omega_z, s, active, n, prm, u, v, w, u_inf, v_inf, w_inf, stats,
-                         false);
+                         false, false, nullptr);
 }
 
 int vpm_fmm3d_velocity_device(vpm_ctx* ctx, const double* x, const double* y, const double* z, const double* ax,
@@ -241,7 +266,7 @@ int vpm_fmm3d_velocity_device(vpm_ctx* ctx, const double* x, const double* y, co
     if (n == 0) return VPM_OK;
     r = c->reserve3d(n, std::max(4096, 2 * n));
     if (r) return r;
-    return c->enqueue3d(x, y, z, ax, ay, az, active, n, p, u, v, w, 0.0, 0.0, 0.0, false);
+    return c->enqueue3d(x, y, z, ax, ay, az, active, n, p, u, v, w, 0.0, 0.0, 0.0, false, false, nullptr);
 }
 
 int vpm_tree3d_build(vpm_ctx* ctx, const double* x, const double* y, const double* z, const uint8_t* active,
@@ -251,7 +276,7 @@ int vpm_tree3d_build(vpm_ctx* ctx, const double* x, const double* y, const doubl
     cudaError_t e = cudaSetDevice(c->device);
     if (e != cudaSuccess) return c->fail_cuda(e, "cudaSetDevice");
     return c->run3d_host(x, y, z, nullptr, nullptr, nullptr, nullptr, active, n, prm, nullptr, nullptr, nullptr, 0.0,
-                         0.0, 0.0, stats, true);
+                         0.0, 0.0, stats, true, false, nullptr);
 }
 
 int vpm_tree3d_counts(vpm_ctx* ctx, int64_t* n_cells, int64_t* n_leaves, int32_t* depth) {
@@ -324,4 +349,81 @@ int vpm_tree3d_cells(vpm_ctx* ctx, int32_t* ints6, double* geom4, int64_t* leaf_
     return VPM_OK;
 }
 
+int vpm_fmm3d_velocity_treecell(vpm_ctx* ctx, const double* x, const double* y, const double* z, const double* ax,
+                                const double* ay, const double* az, const uint8_t* active, const uint8_t* target,
+                                int64_t n, const vpm_fmm_params* prm, double* u, double* v, double* w,
+                                vpm_fmm_stats* stats) {
+    if (!ctx) return VPM_EINVAL;
+    Ctx* c = (Ctx*)ctx;
+    cudaError_t e = cudaSetDevice(c->device);
+    if (e != cudaSuccess) return c->fail_cuda(e, "cudaSetDevice");
+    return c->run3d_host(x, y, z, ax, ay, az, nullptr, active, n, prm, u, v, w, 0.0, 0.0, 0.0, stats, false, true,
+                         target);
+}
+
+int vpm_fmm3d_velocity_treecell_device(vpm_ctx* ctx, const double* x, const double* y, const double* z,
+                                       const double* ax, const double* ay, const double* az, const uint8_t* active,
+                                       const uint8_t* target, int64_t n64, const vpm_fmm_params* prm, double* u,
+                                       double* v, double* w) {
+    if (!ctx) return VPM_EINVAL;
+    Ctx* c = (Ctx*)ctx;
+    cudaError_t e = cudaSetDevice(c->device);
+    if (e != cudaSuccess) return c->fail_cuda(e, "cudaSetDevice");
+    vpm_fmm_params p;
+    int r = c->check_params(prm, p);
+    if (r) return r;
+    if (n64 < 0 || n64 >= (1ll << 30)) return c->fail(VPM_EINVAL, "n out of range");
+    if (!x || !y || !z || !ax || !ay || !az || !active || !u || !v || !w) return c->fail(VPM_EINVAL, "null buffer");
+    const int n = (int)n64;
+    if (n == 0) return VPM_OK;
+    r = c->reserve3d(n, std::max(4096, 2 * n));
+    if (r) return r;
+    return c->enqueue3d(x, y, z, ax, ay, az, active, n, p, u, v, w, 0.0, 0.0, 0.0, false, true, target);
+}
+
+int vpm_treecell3d_build(vpm_ctx* ctx, const double* x, const double* y, const double* z, const uint8_t* active,
+                         int64_t n, const vpm_fmm_params* prm, vpm_fmm_stats* stats) {
+    if (!ctx) return VPM_EINVAL;
+    Ctx* c = (Ctx*)ctx;
+    cudaError_t e = cudaSetDevice(c->device);
+    if (e != cudaSuccess) return c->fail_cuda(e, "cudaSetDevice");
+    return c->run3d_host(x, y, z, nullptr, nullptr, nullptr, nullptr, active, n, prm, nullptr, nullptr, nullptr, 0.0,
+                         0.0, 0.0, stats, true, true, nullptr);
+}
+
+int vpm_tree3d_cell_ids(vpm_ctx* ctx, int64_t* ids) {
+    if (!ctx) return VPM_EINVAL;
+    Ctx* c = (Ctx*)ctx;
+    if (!c->have_tree3) return c->fail(VPM_EINVAL, "no 3D tree on this context yet");
+    if (!c->last_treecell3) return c->fail(VPM_EINVAL, "the octree of the default 3D path has no TreeCell IDs");
+    if (!ids) return c->fail(VPM_EINVAL, "null buffer");
+    const vpm::Tree3D& t = c->tree3;
+    vpm::TreeInfo3D info;
+    cudaStream_t st = c->stream;
+    cudaError_t e = cudaMemcpyAsync(&info, t.info, sizeof(info), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return c->fail_cuda(e, "vpm_tree3d_cell_ids");
+    const int nc = info.n_cells;
+    std::vector<uint32_t> code(nc);
+    std::vector<uint8_t> lev(nc);
+    e = cudaMemcpyAsync(code.data(), c->s3.tc_code, 4ull * nc, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(lev.data(), t.c_level, nc, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return c->fail_cuda(e, "vpm_tree3d_cell_ids");
+    ids[0] = 0;
+    for (int k = 1; k < nc; ++k) {
+        const int L = lev[k];
+        const uint32_t pre = code[k] & 0x7fffffffu;
+        int64_t ix = 0, iy = 0, iz = 0;
+        for (int b = 0; b < L; ++b) {
+            ix |= (int64_t)((pre >> (3 * b)) & 1u) << b;
+            iy |= (int64_t)((pre >> (3 * b + 1)) & 1u) << b;
+            iz |= (int64_t)((pre >> (3 * b + 2)) & 1u) << b;
+        }
+        ids[k] = ((int64_t)1 << (3 * L)) / 7 + ix + (iy << L) + (iz << (2 * L));   // treeCell.cpp:114-148, 223-250
+    }
+    return VPM_OK;
+}
+
 }  // extern "C"
+

@@ -109,6 +109,8 @@ struct Ctx {
     Scratch3D s3{};
     double* bbox3 = nullptr;
     bool have_tree3 = false;
+    bool last_treecell3 = false;   // the last 3D build was a TreeCell
+    uint8_t* in3_tgt = nullptr;
     int last_n3 = 0;
     float last_ms3 = 0.f;
     int last_launches3 = 0;
@@ -154,13 +156,16 @@ struct Ctx {
     int launch2d(const double* x, const double* y, const double* q, const uint8_t* act, int n,
                  const vpm_fmm_params& p, int K, double* o0, double* o1, int velocity, double uinf, double vinf);
     int reserve3d(int n, int cap_cells);
+    // treecell: the 3D TreeCell path instead of the octree; target (device,
+    // caller order, may be null): evaluate only flagged particles.
     int enqueue3d(const double* x, const double* y, const double* z, const double* ax, const double* ay,
                   const double* az, const uint8_t* act, int n, const vpm_fmm_params& p, double* u, double* v,
-                  double* w, double uinf, double vinf, double winf, bool tree_only);
+                  double* w, double uinf, double vinf, double winf, bool tree_only, bool treecell,
+                  const uint8_t* target);
     int run3d_host(const double* x, const double* y, const double* z, const double* a0, const double* a1,
                    const double* a2, const double* s, const uint8_t* act, int64_t n, const vpm_fmm_params* prm,
                    double* u, double* v, double* w, double uinf, double vinf, double winf, vpm_fmm_stats* stats,
-                   bool tree_only);
+                   bool tree_only, bool treecell, const uint8_t* target);
     int batch2d(int ns, const int64_t* offs, const double* x, const double* y, const double* q, const uint8_t* act,
                 const vpm_fmm_params& p, double* ex, double* ey);
     int batch_errors(unsigned* bits);

@@ -28,7 +28,14 @@ struct Geom3D {
     double mn[3], mx[3];
     double cen[3];
     double root;
+    double piv[3];        // TreeCell pivot (lower corner of the root box)
 };
+
+// Deepest level of the 3D TreeCell: its cell IDs (8^L - 1) / 7 + ix + iy 2^L +
+// iz 4^L are 32-bit ints in the reference (treeCell.cpp:223-250) and overflow
+// from level 11 on. Keys hold 3 bits per level.
+constexpr int kTcLevels = 10;
+constexpr int kTcTile = 1024;   // particles per tile of the level-count scan
 
 struct TreeInfo3D {
     int level_start[kMaxLevels3D + 2];  // first cell index of each level
@@ -66,10 +73,15 @@ struct Tree3D {
     uint32_t* blk;                    // per-block scan partials [gridDim]
 };
 
-// Scratch of the 3D build (sort of particles by leaf).
+// Scratch of the 3D build (sort of particles by leaf; the TreeCell build's
+// active-count scan, per-particle level record, per-tile level counts and
+// per-cell Morton prefixes).
 struct Scratch3D {
     uint32_t *key_a, *key_b, *val_a, *val_b;
     SortScratch sort;
+    uint32_t *tc_act, *tc_scan, *tc_pinfo, *tc_tile, *tc_tot, *tc_code;
+    ScanScratch scan;
+    int tc_tiles;
 };
 
 // Bounding box, octree, leaf order, P2M and M2M, all enqueued on `st`.
@@ -78,11 +90,28 @@ cudaError_t build_tree3d(const double* x, const double* y, const double* z, cons
                          const double* az, const uint8_t* act, const double center[3], double exp_pct, Tree3D& t,
                          Scratch3D& s, double* bbox_partial, unsigned* err, cudaStream_t st, int* launches);
 
+// The same for the reference's 3D TreeCell (TreeCell::initializeTree with DIM
+// 3, treeCell.cpp:1043-1243): the root box is the particle box alone, a cell is
+// a leaf iff it holds at most max_src active and at most max_par particles,
+// cells are the absolute-grid boxes of the pivot. The result uses the same
+// Tree3D layout (level-major, Morton order within a level = parents in order
+// and children in the reference's child order under a parent). Sets ERR_DEPTH
+// past level 10 and ERR_LEAF1 when a level-1 cell of a deeper tree is a leaf.
+cudaError_t build_treecell3d(const double* x, const double* y, const double* z, const double* ax,
+                             const double* ay, const double* az, const uint8_t* act, int max_src, int max_par,
+                             double exp_pct, Tree3D& t, Scratch3D& s, double* bbox_partial, unsigned* err,
+                             cudaStream_t st, int* launches);
+
 // Per-target traversal (M2P of far cells, P2P of near leaves) writing the
 // velocity u = sum alpha x r / |r|^3 (+ free stream) in the caller's order.
 // mixed: FP32 arithmetic for the P2P and M2P terms (FP64 geometry and
-// decisions, FP64 accumulation per target).
-cudaError_t eval3d(const Tree3D& t, bool mixed, double* u, double* v, double* w, double uinf, double vinf,
-                   double winf, unsigned* err, cudaStream_t st, int* launches);
+// decisions, FP64 accumulation per target). all_src: every particle of a near
+// leaf is a P2P source (TreeCell path, fmm3D.cpp:1337-1352) instead of the
+// active ones only (octree path). target (caller order, may be null): only
+// flagged particles are evaluated, the others get zero (the free stream is
+// not added to them).
+cudaError_t eval3d(const Tree3D& t, bool mixed, bool all_src, const uint8_t* target, double* u, double* v,
+                   double* w, double uinf, double vinf, double winf, unsigned* err, cudaStream_t st,
+                   int* launches);
 
 }  // namespace vpm

@@ -6,6 +6,9 @@
 //   else a non-leaf               -> onto the target's list for the next level
 //   else a leaf                   -> P2P  u += (alpha_j x r) / |r|^3, j != i,
 //                                    active j only (fast3DFMM.cpp:440-460)
+// The reference's TreeCell path (fmm3D::calcVelocity, VELOCITY_CALCULATION_TYPE
+// 2, fmm3D.cpp:1264-1360; calcVelocityNearBody, fmm3D.cpp:1406-1606) walks
+// its TreeCell the same way, with every particle of a near leaf a source.
 // (level-1 cells themselves are never evaluated, as in the reference).
 //
 // One warp per leaf, one lane per target particle of the leaf. The warp
@@ -135,14 +138,15 @@ __device__ __forceinline__ void m2p32(const double* __restrict__ M, double dxd, 
     vz += sz;
 }
 
-// P2P of one near leaf [lo, hi) onto target slot `self` at (xp, yp, zp).
-template <bool F32>
+// P2P of one near leaf [lo, hi) onto target slot `self` at (xp, yp, zp);
+// ALL: inactive particles are sources too (TreeCell path).
+template <bool F32, bool ALL>
 __device__ __forceinline__ void p2p3(const Src3& s, int lo, int hi, int self, double xp, double yp, double zp,
                                      double& vx, double& vy, double& vz) {
     if (F32) {
         float sx = 0.f, sy = 0.f, sz = 0.f;
         for (int j = lo; j < hi; ++j) {
-            if (!s.act[j] || j == self) continue;
+            if ((!ALL && !s.act[j]) || j == self) continue;
             const float ex = (float)(xp - s.px[j]), ey = (float)(yp - s.py[j]), ez = (float)(zp - s.pz[j]);
             const float r2 = ex * ex + ey * ey + ez * ez;
             const float ir = rsqrtf(r2);
@@ -157,7 +161,7 @@ __device__ __forceinline__ void p2p3(const Src3& s, int lo, int hi, int self, do
         vz += sz;
     } else {
         for (int j = lo; j < hi; ++j) {
-            if (!s.act[j] || j == self) continue;
+            if ((!ALL && !s.act[j]) || j == self) continue;
             const double ex = xp - s.px[j], ey = yp - s.py[j], ez = zp - s.pz[j];
             const double r2 = ex * ex + ey * ey + ez * ez;
             const double ir3 = 1.0 / (sqrt(r2) * r2);
@@ -168,10 +172,10 @@ __device__ __forceinline__ void p2p3(const Src3& s, int lo, int hi, int self, do
     }
 }
 
-template <bool F32>
+template <bool F32, bool ALL>
 __global__ void __launch_bounds__(32 * kEval3DWarps)
-eval3d_kernel(Tree3D t, double* __restrict__ u, double* __restrict__ v, double* __restrict__ w, double uinf,
-              double vinf, double winf, unsigned* ticket, unsigned* err) {
+eval3d_kernel(Tree3D t, const uint8_t* __restrict__ target, double* __restrict__ u, double* __restrict__ v,
+              double* __restrict__ w, double uinf, double vinf, double winf, unsigned* ticket, unsigned* err) {
     __shared__ int s_cell[kEval3DWarps][2][kWork3DCap];
     __shared__ unsigned s_mask[kEval3DWarps][2][kWork3DCap];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -192,8 +196,9 @@ eval3d_kernel(Tree3D t, double* __restrict__ u, double* __restrict__ v, double* 
         for (int tb = lo; tb < hi; tb += 32) {
             const int slot = tb + lane;
             const bool has = slot < hi;
+            const bool tgt = has && (target == nullptr || target[t.perm[slot]] != 0);
             const double xp = has ? t.px[slot] : 0.0, yp = has ? t.py[slot] : 0.0, zp = has ? t.pz[slot] : 0.0;
-            const unsigned full = __ballot_sync(0xffffffffu, has);
+            const unsigned full = __ballot_sync(0xffffffffu, tgt);
             double vx = 0.0, vy = 0.0, vz = 0.0;
             int which = 0;
             int ncur = __popc(rm);
@@ -245,7 +250,7 @@ eval3d_kernel(Tree3D t, double* __restrict__ u, double* __restrict__ v, double* 
                             }
                             ++nn;
                         } else if ((near >> lane) & 1u) {
-                            p2p3<F32>(src, t.c_lo[k], t.c_hi[k], slot, xp, yp, zp, vx, vy, vz);
+                            p2p3<F32, ALL>(src, t.c_lo[k], t.c_hi[k], slot, xp, yp, zp, vx, vy, vz);
                         }
                     }
                 }
@@ -255,9 +260,9 @@ eval3d_kernel(Tree3D t, double* __restrict__ u, double* __restrict__ v, double* 
             }
             if (has) {
                 const uint32_t i = t.perm[slot];
-                u[i] = vx + uinf;
-                v[i] = vy + vinf;
-                w[i] = vz + winf;
+                u[i] = tgt ? vx + uinf : 0.0;
+                v[i] = tgt ? vy + vinf : 0.0;
+                w[i] = tgt ? vz + winf : 0.0;
             }
             __syncwarp();
         }
@@ -266,13 +271,17 @@ eval3d_kernel(Tree3D t, double* __restrict__ u, double* __restrict__ v, double* 
 
 }  // namespace
 
-cudaError_t eval3d(const Tree3D& t, bool mixed, double* u, double* v, double* w, double uinf, double vinf,
-                   double winf, unsigned* err, cudaStream_t st, int* launches) {
+cudaError_t eval3d(const Tree3D& t, bool mixed, bool all_src, const uint8_t* target, double* u, double* v,
+                   double* w, double uinf, double vinf, double winf, unsigned* err, cudaStream_t st,
+                   int* launches) {
     unsigned* ticket = t.gbar + 4;
     cudaError_t e = cudaMemsetAsync(ticket, 0, sizeof(unsigned), st);
     if (e != cudaSuccess) return e;
-    if (mixed) eval3d_kernel<true><<<148 * 8, 32 * kEval3DWarps, 0, st>>>(t, u, v, w, uinf, vinf, winf, ticket, err);
-    else eval3d_kernel<false><<<148 * 8, 32 * kEval3DWarps, 0, st>>>(t, u, v, w, uinf, vinf, winf, ticket, err);
+    const dim3 g(148 * 8), b(32 * kEval3DWarps);
+    if (mixed && all_src) eval3d_kernel<true, true><<<g, b, 0, st>>>(t, target, u, v, w, uinf, vinf, winf, ticket, err);
+    else if (mixed) eval3d_kernel<true, false><<<g, b, 0, st>>>(t, target, u, v, w, uinf, vinf, winf, ticket, err);
+    else if (all_src) eval3d_kernel<false, true><<<g, b, 0, st>>>(t, target, u, v, w, uinf, vinf, winf, ticket, err);
+    else eval3d_kernel<false, false><<<g, b, 0, st>>>(t, target, u, v, w, uinf, vinf, winf, ticket, err);
     *launches += 1;
     return cudaGetLastError();
 }

@@ -20,13 +20,17 @@ constexpr int kBBox3Blocks = 296;
 // Min/max of the particle box joined with the domain centre, root length and
 // centre (fast3DFMM.cpp:506-528). Each block reduces its share; the last
 // block to finish combines the partials and writes the geometry.
+// treecell: the particle box alone (start from the empty box), then the
+// TreeCell root length and pivot (treeCell.cpp:1058-1090).
 __global__ void __launch_bounds__(256)
 bbox3d(const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ z, int n,
-       double cx0, double cy0, double cz0, double exp_pct, Geom3D* g, double* partial, unsigned* done,
-       unsigned* err) {
+       double cx0, double cy0, double cz0, double exp_pct, bool treecell, Geom3D* g, double* partial,
+       unsigned* done, unsigned* err) {
     __shared__ double s_v[6][256];
     __shared__ bool s_last;
-    double mn[3] = {cx0, cy0, cz0}, mx[3] = {cx0, cy0, cz0};
+    const double lo0[3] = {treecell ? HUGE_VAL : cx0, treecell ? HUGE_VAL : cy0, treecell ? HUGE_VAL : cz0};
+    const double hi0[3] = {treecell ? -HUGE_VAL : cx0, treecell ? -HUGE_VAL : cy0, treecell ? -HUGE_VAL : cz0};
+    double mn[3] = {lo0[0], lo0[1], lo0[2]}, mx[3] = {hi0[0], hi0[1], hi0[2]};
     const double* p[3] = {x, y, z};
     bool bad = false;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -63,7 +67,7 @@ bbox3d(const double* __restrict__ x, const double* __restrict__ y, const double*
     if (!s_last) return;
     __threadfence();
     // last block: combine the partials
-    double a[6] = {cx0, cy0, cz0, cx0, cy0, cz0};
+    double a[6] = {lo0[0], lo0[1], lo0[2], hi0[0], hi0[1], hi0[2]};
     for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
         #pragma unroll
         for (int d = 0; d < 3; ++d) {
@@ -95,6 +99,7 @@ bbox3d(const double* __restrict__ x, const double* __restrict__ y, const double*
         }
         g->root = xmul(root, xadd(1.0, xdiv(exp_pct, 100.0)));
         if (!(g->root > 0.0)) set_err(err, ERR_RANGE);   // all particles at the domain centre
+        for (int d = 0; d < 3; ++d) g->piv[d] = xdiv(xsub(xadd(g->mx[d], g->mn[d]), g->root), 2.0);
         *done = 0;
     }
 }
@@ -443,7 +448,365 @@ __global__ void count_leaves3d(Tree3D t) {
     if (threadIdx.x == 0 && k) atomicAdd(&t.info->n_leaves, k);
 }
 
+// ---------------------------------------------------------------------------
+// 3D TreeCell (TreeCell::initializeTree with DIM 3, treeCell.cpp:1043-1243).
+//
+// The reference bins every unsettled particle at level L by
+// index = (int)((c - pivot) / size_L), size_L = root / 2^L (treeCell.cpp:101-105,
+// 290-300). size_L is root / 2^L exactly, and rounding commutes with scaling
+// by a power of two, so RN(d / size_L) = RN(d / size_10) / 2^(10-L) and the
+// level-L index is the level-10 index shifted right by 10 - L. Particles are
+// therefore sorted once by their level-10 Morton key (x in bit 0 of every
+// 3-bit digit, the reference's child order ix + ((i >> 0) & 1), iy + ((i >> 1)
+// & 1), iz + ((i >> 2) & 1), treeCell.cpp:395-417), and the cells of level L
+// are the runs of equal level-L prefixes whose parent run is split. A run is
+// split when it holds more than max_par particles or more than max_src active
+// ones (treeCell.cpp:1170-1215); a split run's parent is split too, so a run is
+// a cell exactly when its parent run is split, and every level is built at
+// once from per-particle records.
+// ---------------------------------------------------------------------------
+
+// Equal leading 3-bit digits (levels) of two level-10 keys (30 bits).
+__device__ __forceinline__ int tc_lcp(uint32_t a, uint32_t b) {
+    const uint32_t d = a ^ b;
+    return d == 0 ? kTcLevels : (__clz(d) - 2) / 3;
+}
+
+__device__ __forceinline__ uint32_t tc_spread(uint32_t v) {   // 10 bits -> every third bit
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000FFu;
+    v = (v | (v << 8)) & 0x0300F00Fu;
+    v = (v | (v << 4)) & 0x030C30C3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+
+__device__ __forceinline__ int tc_compact(uint32_t v) {       // inverse of tc_spread
+    v &= 0x09249249u;
+    v = (v | (v >> 2)) & 0x030C30C3u;
+    v = (v | (v >> 4)) & 0x0300F00Fu;
+    v = (v | (v >> 8)) & 0x030000FFu;
+    v = (v | (v >> 16)) & 0x3ffu;
+    return (int)v;
+}
+
+// Level-10 key and index of every particle; the grid index of an axis is
+// (int)((c - pivot) / (root / 1024)), which must lie in [0, 1024).
+__global__ void tc_keys3d(const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ z,
+                          int n, const Geom3D* __restrict__ g, uint32_t* __restrict__ key, uint32_t* __restrict__ idx,
+                          unsigned* err) {
+    const double size = xdiv(g->root, 1024.0);
+    const double pv[3] = {g->piv[0], g->piv[1], g->piv[2]};
+    const double* p[3] = {x, y, z};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t k = 0;
+        bool bad = false;
+        #pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const double q = xdiv(xsub(p[d][i], pv[d]), size);
+            bad |= !(q > -1.0 && q < 1024.0);
+            const int ix = bad ? 0 : (int)q;
+            k |= tc_spread((uint32_t)ix) << d;
+        }
+        if (bad) set_err(err, ERR_RANGE);
+        key[i] = k;
+        idx[i] = (uint32_t)i;
+    }
+}
+
+// Active flags in key order, for the active-count scan.
+__global__ void tc_act3d(const uint8_t* __restrict__ act, const uint32_t* __restrict__ idx, int n,
+                         uint32_t* __restrict__ out) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) out[j] = act[idx[j]] ? 1u : 0u;
+}
+
+// First m in [lo, hi) with as[m] >= target (as non-decreasing), galloping up from lo.
+__device__ __forceinline__ int tc_gallop_ge(const uint32_t* __restrict__ as, int lo, int hi, uint32_t target) {
+    int L = lo, R = hi, step = 1;
+    while (L + step < R && as[L + step] < target) {
+        L += step;
+        step <<= 1;
+    }
+    R = min(R, L + step);
+    while (L < R) {
+        const int mid = (L + R) >> 1;
+        if (as[mid] < target) L = mid + 1;
+        else R = mid;
+    }
+    return L;
+}
+
+// First j' <= j whose key has the same prefix (key >> sh) as particle j.
+__device__ __forceinline__ int tc_group_start(const uint32_t* __restrict__ key, int j, int sh) {
+    const uint32_t v = key[j] >> sh;
+    int L = 0, R = j;
+    for (int step = 1; R - step >= L; step <<= 1) {
+        if ((key[R - step] >> sh) == v) {
+            R -= step;
+        } else {
+            L = R - step + 1;
+            break;
+        }
+    }
+    while (L < R) {
+        const int mid = (L + R) >> 1;
+        if ((key[mid] >> sh) == v) R = mid;
+        else L = mid + 1;
+    }
+    return L;
+}
+
+// One past the last j' in [lo, cap) with the prefix of particle lo.
+__device__ __forceinline__ int tc_group_end(const uint32_t* __restrict__ key, int lo, int cap, int sh) {
+    const uint32_t v = key[lo] >> sh;
+    int L = lo + 1, R = cap;
+    while (L < R) {
+        const int mid = (L + R) >> 1;
+        if ((key[mid] >> sh) == v) L = mid + 1;
+        else R = mid;
+    }
+    return L;
+}
+
+// pinfo[j] = lvl | (big + 1) << 8: lvl = the first level at which particle j
+// starts a run (kTcLevels + 1 for a key equal to its predecessor's), big =
+// the deepest level at which that run is split (-1: none). The run of level
+// L >= lvl starting at j holds more than max_par particles iff particle
+// j + max_par shares its prefix, more than max_src active ones iff the
+// (max_src + 1)-th active particle from j does.
+__global__ void tc_bigl3d(const uint32_t* __restrict__ key, const uint32_t* __restrict__ as, int n, int max_src,
+                          int max_par, uint32_t* __restrict__ pinfo) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const uint32_t kj = key[j];
+        const int lvl = j == 0 ? 1 : tc_lcp(key[j - 1], kj) + 1;
+        int big = -1;
+        if ((long long)j + max_par < n) big = tc_lcp(kj, key[j + max_par]);
+        const uint32_t target = as[j] + (uint32_t)max_src + 1u;   // as[] < 2^30, max_src < 2^31: no wrap
+        if (as[n] >= target) {
+            const int from = (int)min((long long)n, (long long)j + max_src + 1);
+            const int m = tc_gallop_ge(as, from, n + 1, target);   // particle m-1 is that one
+            big = max(big, tc_lcp(kj, key[m - 1]));
+        }
+        pinfo[j] = (uint32_t)lvl | ((uint32_t)(big + 1) << 8);
+    }
+}
+
+// The levels of the cells particle j starts (first..last, 0 = none; bits
+// 16..23 and 24..31 of pinfo) and the per-tile counts of cells and leaves of
+// every level: rows 0..10 cells, rows 11..21 leaves, tiles columns.
+__global__ void __launch_bounds__(kTcTile)
+tc_cells3d(const uint32_t* __restrict__ key, uint32_t* __restrict__ pinfo, int n, uint32_t* __restrict__ tile_cnt,
+           int tiles, unsigned* err) {
+    __shared__ unsigned s_c[kTcLevels + 1], s_l[kTcLevels + 1];
+    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        if (threadIdx.x <= kTcLevels) s_c[threadIdx.x] = s_l[threadIdx.x] = 0;
+        __syncthreads();
+        const int j = tile * kTcTile + threadIdx.x;
+        if (j < n) {
+            const uint32_t w = pinfo[j];
+            const int lvl = (int)(w & 0xff), big = (int)((w >> 8) & 0xff) - 1;
+            int first = 0, last = 0;
+            if (lvl <= kTcLevels) {
+                bool exists = lvl == 1;   // the root is always split
+                if (!exists) {
+                    const int sp = tc_group_start(key, j, 3 * (kTcLevels - (lvl - 1)));
+                    exists = (int)((pinfo[sp] >> 8) & 0xff) - 1 >= lvl - 1;
+                }
+                if (exists) {
+                    first = lvl;
+                    last = min(kTcLevels, max(lvl, big + 1));
+                    if (big >= kTcLevels) set_err(err, ERR_DEPTH);   // a level-10 cell would need splitting
+                    for (int L = first; L <= last; ++L) atomicAdd(&s_c[L], 1u);
+                    if (big < last) atomicAdd(&s_l[last], 1u);
+                }
+            }
+            pinfo[j] = (w & 0xffffu) | ((uint32_t)first << 16) | ((uint32_t)last << 24);
+        }
+        __syncthreads();
+        if (threadIdx.x <= kTcLevels) {
+            tile_cnt[(size_t)threadIdx.x * tiles + tile] = s_c[threadIdx.x];
+            tile_cnt[(size_t)(kTcLevels + 1 + threadIdx.x) * tiles + tile] = s_l[threadIdx.x];
+        }
+        __syncthreads();
+    }
+}
+
+// One block per row of tile counts: exclusive scan in place, row total.
+__global__ void __launch_bounds__(1024)
+tc_scan_rows3d(uint32_t* __restrict__ tile_cnt, int tiles, uint32_t* __restrict__ row_tot) {
+    __shared__ uint32_t s_w[32];
+    __shared__ uint32_t s_carry;
+    uint32_t* row = tile_cnt + (size_t)blockIdx.x * tiles;
+    if (threadIdx.x == 0) s_carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int b = 0; b < tiles; b += blockDim.x) {
+        const int k = b + threadIdx.x;
+        const uint32_t v = k < tiles ? row[k] : 0u;
+        uint32_t incl = v;
+        #pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) s_w[warp] = incl;
+        __syncthreads();
+        uint32_t before = 0, all = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            before += w < warp ? s_w[w] : 0u;
+            all += s_w[w];
+        }
+        const uint32_t carry = s_carry;
+        if (k < tiles) row[k] = carry + before + incl - v;
+        __syncthreads();
+        if (threadIdx.x == 0) s_carry = carry + all;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) row_tot[blockIdx.x] = s_carry;
+}
+
+// Level starts, depth and the root cell (treeCell.cpp:1117-1133); ERR_LEAF1
+// when a level-1 cell is a leaf and the tree goes deeper: the reference's
+// traversal asks for that leaf's children and throws (fmm3D.cpp:1286).
+__global__ void tc_totals3d(Tree3D t, const uint32_t* __restrict__ row_tot, const uint32_t* __restrict__ as,
+                            unsigned* err) {
+    TreeInfo3D* info = t.info;
+    int cells = 1, depth = 0;
+    info->level_start[0] = 0;
+    for (int L = 1; L < kMaxLevels3D + 2; ++L) {
+        info->level_start[L] = cells;
+        if (L <= kTcLevels) {
+            const int c = (int)row_tot[L];
+            if (c > 0) depth = L;
+            cells += c;
+        }
+    }
+    info->n_cells = cells;
+    info->n_leaves = 0;   // counted after the leaf sort
+    info->depth = depth;
+    info->remaining = 0;
+    info->scan_total = 0;
+    info->p2p_pairs = 0;
+    info->m2p_pairs = 0;
+    if (cells > t.cap_cells) set_err(err, ERR_CELL_CAP);
+    if (depth > 1 && row_tot[kTcLevels + 1 + 1] > 0) set_err(err, ERR_LEAF1);
+    const Geom3D* g = t.geom;
+    t.c_x[0] = xadd(g->piv[0], xmul(0.5, g->root));
+    t.c_y[0] = xadd(g->piv[1], xmul(0.5, g->root));
+    t.c_z[0] = xadd(g->piv[2], xmul(0.5, g->root));
+    t.c_size[0] = g->root;
+    t.c_npar[0] = t.n;
+    t.c_parent[0] = -1;
+    t.c_child0[0] = -1;   // lowered by tc_link3d (unsigned minimum: -1 = none)
+    t.c_chmask[0] = 0;
+    t.c_active[0] = as[t.n] != 0 ? 1 : 0;
+    t.c_level[0] = 0;
+    t.c_lo[0] = 0;
+    t.c_hi[0] = t.n;
+}
+
+// Cell records of every particle's cell levels; cell index = level start +
+// scanned tile count + rank of the particle among the tile's emitters of that
+// level (warp ballots). code[c] = level-L Morton prefix | leaf << 31.
+__global__ void __launch_bounds__(kTcTile)
+tc_emit3d(Tree3D t, const uint32_t* __restrict__ key, const uint32_t* __restrict__ pinfo,
+          const uint32_t* __restrict__ tile_cnt, int tiles, uint32_t* __restrict__ code_out, unsigned* err) {
+    __shared__ int s_wc[kTcLevels + 1][kTcTile / 32];
+    if (block_fatal(err)) return;
+    const int n = t.n;
+    const TreeInfo3D* info = t.info;
+    const Geom3D* g = t.geom;
+    const double root = g->root;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned below = (1u << lane) - 1u;
+    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const int j = tile * kTcTile + threadIdx.x;
+        const uint32_t w = j < n ? pinfo[j] : 0u;
+        const int first = (int)((w >> 16) & 0xff), last = (int)(w >> 24), big = (int)((w >> 8) & 0xff) - 1;
+        if (lane <= kTcLevels) s_wc[lane][warp] = 0;
+        __syncwarp();
+        for (int L = 1; L <= kTcLevels; ++L) {
+            const unsigned m = __ballot_sync(0xffffffffu, first && first <= L && L <= last);
+            if (lane == 0) s_wc[L][warp] = __popc(m);
+        }
+        __syncthreads();
+        for (int L = 1; L <= kTcLevels; ++L) {
+            const bool has = first && first <= L && L <= last;
+            const unsigned m = __ballot_sync(0xffffffffu, has);
+            if (!has) continue;
+            int before = 0;
+            for (int k = 0; k < warp; ++k) before += s_wc[L][k];
+            const int ci = info->level_start[L] + (int)tile_cnt[(size_t)L * tiles + tile] + before + __popc(m & below);
+            if (ci >= t.cap_cells) {
+                set_err(err, ERR_CELL_CAP);
+                continue;
+            }
+            const bool leaf = L == last && big < last;
+            const uint32_t pre = key[j] >> (3 * (kTcLevels - L));
+            const int ix = tc_compact(pre), iy = tc_compact(pre >> 1), iz = tc_compact(pre >> 2);
+            const double len = xdiv(root, ldexp(1.0, L));
+            t.c_x[ci] = xadd(g->piv[0], xmul(xadd(0.5, (double)ix), len));
+            t.c_y[ci] = xadd(g->piv[1], xmul(xadd(0.5, (double)iy), len));
+            t.c_z[ci] = xadd(g->piv[2], xmul(xadd(0.5, (double)iz), len));
+            t.c_size[ci] = len;
+            t.c_lo[ci] = j;
+            t.c_child0[ci] = -1;
+            t.c_chmask[ci] = 0;
+            t.c_level[ci] = (uint8_t)L;
+            code_out[ci] = pre | (leaf ? 0x80000000u : 0u);
+        }
+        __syncthreads();
+    }
+}
+
+// Range, counts and activity of every cell (one search per cell), its parent
+// (the level L-1 cell of its prefix >> 3, by bisection over that level's
+// prefixes), the parent's child mask and first child; every leaf records
+// itself as the cell of its particles.
+__global__ void tc_link3d(Tree3D t, const uint32_t* __restrict__ key, const uint32_t* __restrict__ idx,
+                          const uint32_t* __restrict__ as, const uint32_t* __restrict__ code, int max_par,
+                          unsigned* err) {
+    if (fatal(err)) return;
+    const int nc = t.info->n_cells, n = t.n;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x + 1; c < nc; c += gridDim.x * blockDim.x) {
+        const int L = t.c_level[c];
+        const uint32_t cw = code[c];
+        const bool leaf = (cw >> 31) != 0;
+        const uint32_t pre = cw & 0x7fffffffu;
+        const int lo = t.c_lo[c];
+        const int cap = leaf ? (int)min((long long)n, (long long)lo + max_par) : n;
+        const int hi = tc_group_end(key, lo, cap, 3 * (kTcLevels - L));
+        t.c_hi[c] = hi;
+        t.c_npar[c] = hi - lo;
+        t.c_active[c] = as[hi] != as[lo] ? 1 : 0;
+        int p = 0;
+        if (L >= 2) {
+            int a = t.info->level_start[L - 1], b = t.info->level_start[L];
+            const uint32_t want = pre >> 3;
+            while (a < b) {
+                const int mid = (a + b) >> 1;
+                if ((code[mid] & 0x7fffffffu) < want) a = mid + 1;
+                else b = mid;
+            }
+            p = a;
+            if (p >= t.info->level_start[L] || (code[p] & 0x7fffffffu) != want) {
+                set_err(err, ERR_INDEX);
+                continue;
+            }
+        }
+        t.c_parent[c] = p;
+        atomicOr(&t.c_chmask[p], 1u << (pre & 7u));
+        atomicMin(reinterpret_cast<unsigned*>(&t.c_child0[p]), (unsigned)c);
+        if (leaf)
+            for (int k = lo; k < hi; ++k) t.pcell[idx[k]] = c;
+    }
+}
+
 }  // namespace
+
+static cudaError_t leaves_upward3d(const double* x, const double* y, const double* z, const double* ax,
+                                   const double* ay, const double* az, const uint8_t* act, Tree3D& t, Scratch3D& s,
+                                   unsigned* err, cudaStream_t st, int* launches);
 
 // Tree build (bounding box, levels, leaf order) and upward pass, enqueued on st.
 cudaError_t build_tree3d(const double* x, const double* y, const double* z, const double* ax, const double* ay,
@@ -454,7 +817,7 @@ cudaError_t build_tree3d(const double* x, const double* y, const double* z, cons
     cudaError_t e = cudaMemsetAsync(t.gbar, 0, sizeof(unsigned) * 8, st);
     if (e != cudaSuccess) return e;
     const int bb = std::max(1, std::min(kBBox3Blocks, ceil_div(n, 256)));
-    bbox3d<<<bb, 256, 0, st>>>(x, y, z, n, center[0], center[1], center[2], exp_pct, t.geom, bbox_partial,
+    bbox3d<<<bb, 256, 0, st>>>(x, y, z, n, center[0], center[1], center[2], exp_pct, false, t.geom, bbox_partial,
                                 t.gbar + 6, err);
     root3d<<<gridN, 256, 0, st>>>(t);
     *launches += 2;
@@ -462,7 +825,18 @@ cudaError_t build_tree3d(const double* x, const double* y, const double* z, cons
     e = launch_coop(octree_levels3d, kT3Threads, 0, st, 4, &grid, t, x, y, z, act, kCoopMaxBlocks3D, err);
     if (e != cudaSuccess) return e;
     *launches += 1;
-    // particles in leaf order (stable: ascending index within a leaf)
+    return leaves_upward3d(x, y, z, ax, ay, az, act, t, s, err, st, launches);
+}
+
+// Particles in leaf order (stable: ascending index within a leaf, the
+// reference's parIDList order), leaf ranges, P2M and the M2M levels.
+static cudaError_t leaves_upward3d(const double* x, const double* y, const double* z, const double* ax,
+                                   const double* ay, const double* az, const uint8_t* act, Tree3D& t, Scratch3D& s,
+                                   unsigned* err, cudaStream_t st, int* launches) {
+    const int n = t.n;
+    const int gridN = std::max(1, std::min(148 * 8, ceil_div(n, 256)));
+    cudaError_t e = cudaSuccess;
+    int grid = 0;
     leaf_keys3d<<<gridN, 256, 0, st>>>(t, s.key_a, s.val_a);
     *launches += 1;
     int bits = 1;
@@ -486,6 +860,43 @@ cudaError_t build_tree3d(const double* x, const double* y, const double* z, cons
     }
     *launches += 1;
     return cudaGetLastError();
+}
+
+cudaError_t build_treecell3d(const double* x, const double* y, const double* z, const double* ax,
+                             const double* ay, const double* az, const uint8_t* act, int max_src, int max_par,
+                             double exp_pct, Tree3D& t, Scratch3D& s, double* bbox_partial, unsigned* err,
+                             cudaStream_t st, int* launches) {
+    const int n = t.n;
+    const int gridN = std::max(1, std::min(148 * 8, ceil_div(n, 256)));
+    const int tiles = ceil_div(n, kTcTile);
+    if (tiles > s.tc_tiles) return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemsetAsync(t.gbar, 0, sizeof(unsigned) * 8, st);
+    if (e != cudaSuccess) return e;
+    const int bb = std::max(1, std::min(kBBox3Blocks, ceil_div(n, 256)));
+    bbox3d<<<bb, 256, 0, st>>>(x, y, z, n, 0.0, 0.0, 0.0, exp_pct, true, t.geom, bbox_partial, t.gbar + 6, err);
+    tc_keys3d<<<gridN, 256, 0, st>>>(x, y, z, n, t.geom, s.key_a, s.val_a, err);
+    *launches += 2;
+    uint32_t* keys = s.key_a;
+    uint32_t* vals = s.val_a;
+    e = radix_sort_pairs(&keys, &vals, s.key_b, s.val_b, n, 3 * kTcLevels, s.sort, err, st, launches);
+    if (e != cudaSuccess) return e;
+    tc_act3d<<<gridN, 256, 0, st>>>(act, vals, n, s.tc_act);
+    *launches += 1;
+    e = scan_exclusive(s.tc_act, s.tc_scan, n, s.tc_scan + n, s.scan, err, st);
+    if (e != cudaSuccess) return e;
+    *launches += 1;
+    const int gt = std::max(1, std::min(tiles, 148 * 2));
+    tc_bigl3d<<<gridN, 256, 0, st>>>(keys, s.tc_scan, n, max_src, max_par, s.tc_pinfo);
+    tc_cells3d<<<gt, kTcTile, 0, st>>>(keys, s.tc_pinfo, n, s.tc_tile, tiles, err);
+    tc_scan_rows3d<<<2 * (kTcLevels + 1), 1024, 0, st>>>(s.tc_tile, tiles, s.tc_tot);
+    tc_totals3d<<<1, 1, 0, st>>>(t, s.tc_tot, s.tc_scan, err);
+    tc_emit3d<<<gt, kTcTile, 0, st>>>(t, keys, s.tc_pinfo, s.tc_tile, tiles, s.tc_code, err);
+    const int gc = std::max(1, std::min(148 * 8, ceil_div(t.cap_cells, 256)));
+    tc_link3d<<<gc, 256, 0, st>>>(t, keys, vals, s.tc_scan, s.tc_code, max_par, err);
+    *launches += 6;
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return leaves_upward3d(x, y, z, ax, ay, az, act, t, s, err, st, launches);
 }
 
 }  // namespace vpm

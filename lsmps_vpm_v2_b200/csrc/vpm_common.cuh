@@ -23,6 +23,7 @@ enum ErrBits : unsigned {
     ERR_LIST2 = 1u << 7,        // list 2 longer than 27 (cannot happen)
     ERR_LIST_CAP = 1u << 8,     // CSR list storage too small
     ERR_RANGE = 1u << 9,        // a particle index fell outside its level box
+    ERR_LEAF1 = 1u << 10,       // 3D TreeCell: a level-1 leaf in a deeper tree
 };
 
 // Every spin-wait in this library is bounded by this many polls; on expiry the

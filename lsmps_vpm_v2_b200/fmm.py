@@ -19,7 +19,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _lib
-from ._lib import Params, Stats, VpmError, default_params, lib
+from ._lib import Params, Stats, VpmError, default_params, lib, treecell3d_params
 
 
 def _f64(a):
@@ -179,6 +179,46 @@ class Context:
         self._check(lib().vpm_fmm3d_velocity_device(self._h, x, y, z, ax, ay, az, active, int(n), C.byref(p),
                                                     u, v, w))
 
+    def velocity3d_treecell(self, x, y, z, ax, ay, az, active, target=None, params: Params | None = None,
+                            stats: bool = False):
+        """u = sum_j alpha_j x r / |r|^3 by the treecode on the 3D TreeCell (host
+        arrays); target flags select the evaluated particles (others zero)."""
+        x, y, z = _f64(x), _f64(y), _f64(z)
+        ax, ay, az, a = _f64(ax), _f64(ay), _f64(az), _u8(active)
+        t = None if target is None else _u8(target)
+        n = x.size
+        u, v, w = np.empty(n), np.empty(n), np.empty(n)
+        p = params or treecell3d_params()
+        st = Stats()
+        self._check(lib().vpm_fmm3d_velocity_treecell(self._h, _ptr(x), _ptr(y), _ptr(z), _ptr(ax), _ptr(ay),
+                                                      _ptr(az), _ptr(a), None if t is None else _ptr(t), n,
+                                                      C.byref(p), _ptr(u), _ptr(v), _ptr(w),
+                                                      C.byref(st) if stats else None))
+        return (u, v, w, st) if stats else (u, v, w)
+
+    def velocity3d_treecell_device(self, n, x, y, z, ax, ay, az, active, target, u, v, w,
+                                   params: Params | None = None):
+        """Device-pointer form (target may be None), asynchronous."""
+        p = params or treecell3d_params()
+        self._check(lib().vpm_fmm3d_velocity_treecell_device(self._h, x, y, z, ax, ay, az, active, target, int(n),
+                                                             C.byref(p), u, v, w))
+
+    def build_treecell3d(self, x, y, z, active, params: Params | None = None) -> Stats:
+        x, y, z, a = _f64(x), _f64(y), _f64(z), _u8(active)
+        p = params or treecell3d_params()
+        s = Stats()
+        self._check(lib().vpm_treecell3d_build(self._h, _ptr(x), _ptr(y), _ptr(z), _ptr(a), x.size, C.byref(p),
+                                               C.byref(s)))
+        return s
+
+    def tree3d_cell_ids(self) -> np.ndarray:
+        """Reference cell IDs of the last 3D TreeCell, in library cell order."""
+        nc, nl, depth = C.c_int64(), C.c_int64(), C.c_int32()
+        self._check(lib().vpm_tree3d_counts(self._h, C.byref(nc), C.byref(nl), C.byref(depth)))
+        ids = np.zeros(nc.value, np.int64)
+        self._check(lib().vpm_tree3d_cell_ids(self._h, _ptr(ids)))
+        return ids
+
     def build_tree3d(self, x, y, z, active, params: Params | None = None) -> Stats:
         x, y, z, a = _f64(x), _f64(y), _f64(z), _u8(active)
         p = params or default_params()
@@ -337,14 +377,33 @@ class fmm2D:
 
 
 class fmm3D:
-    """Mirror of fmm3D's fast path (src/FMM/fmm3D.hpp:106-138:
-    calcVelocityFast + get_Field_x/y/z) on the GPU treecode."""
+    """Mirror of fmm3D (src/FMM/fmm3D.hpp:106-138): the fast path
+    calcVelocityFast, the TreeCell path calcVelocity / calcVelocityNearBody,
+    and get_Field_x/y/z, on the GPU treecode."""
 
     def __init__(self, ctx: Context | None = None, params: Params | None = None):
         self.ctx = ctx or default_context()
         self.params = params or default_params()
+        self._tc_params = params or treecell3d_params()
         self._u = self._v = self._w = None
         self.stats: Stats | None = None
+
+    def calcVelocity(self, cellData, parPos, activeMark, alphaX, alphaY, alphaZ):
+        """fmm3D::calcVelocity (fmm3D.cpp:1064-1405) on the 3D TreeCell of the
+        same particles, built on the GPU in the same call; `cellData` is
+        accepted for the reference's signature. Leaf caps: this object's params
+        if given, else the reference's 3D 30/50."""
+        self._treecell(parPos, activeMark, None, alphaX, alphaY, alphaZ)
+
+    def calcVelocityNearBody(self, cellData, parPos, activeMark, targetFlag, alphaX, alphaY, alphaZ):
+        """fmm3D::calcVelocityNearBody (fmm3D.cpp:1406-1606): only flagged
+        targets are evaluated, the others get zero."""
+        self._treecell(parPos, activeMark, targetFlag, alphaX, alphaY, alphaZ)
+
+    def _treecell(self, parPos, activeMark, target, ax, ay, az):
+        pos = np.asarray(parPos, dtype=np.float64)
+        self._u, self._v, self._w, self.stats = self.ctx.velocity3d_treecell(
+            pos[:, 0], pos[:, 1], pos[:, 2], ax, ay, az, activeMark, target, self._tc_params, stats=True)
 
     def calcVelocityFast(self, _parPos, _activeFlag, _targetFlag, _alphaX, _alphaY, _alphaZ):
         """The target flags are accepted and ignored, as the reference ignores them."""

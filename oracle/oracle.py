@@ -47,6 +47,30 @@ def _u8a(a):
     return np.ascontiguousarray(a, dtype=np.uint8)
 
 
+def _vp(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _treecell_dump(call):
+    """Run a TreeCell dump entry twice (size, then fill); cells sorted by ID."""
+    nc = call(None, None, None, None, None)
+    if nc < 0:
+        return None
+    ids = np.zeros(nc, np.int64)
+    ints = np.zeros((nc, 6), np.int32)
+    geom = np.zeros((nc, 4))
+    offs = np.zeros(nc + 1, np.int64)
+    call(None, None, None, _vp(offs), None)
+    pids = np.zeros(max(int(offs[-1]), 1), np.int32)
+    call(_vp(ids), _vp(ints), _vp(geom), _vp(offs), _vp(pids))
+    order = np.argsort(ids, kind="stable")
+    leaves = [pids[offs[k]:offs[k + 1]] for k in order]
+    ints_s = ints[order].copy()
+    ints_s[:, 5] = 0
+    ints_s[0, 5] = ints[:, 5].max()
+    return ids[order], ints_s, geom[order], leaves
+
+
 class Tree2D:
     """A 2D tree dump in the reference's vocabulary (cell IDs, leafList)."""
 
@@ -104,6 +128,11 @@ class Port:
         L.orc_tree3d.argtypes = [_d, _d, _d, _u8, C.c_int64, C.c_int, C.c_double, C.c_void_p, C.c_void_p]
         L.orc_direct3d_velocity.argtypes = [_d, _d, _d, _d, _d, _d, _u8, C.c_int64, _i64, C.c_int64, _d, _d, _d]
         L.orc3_last_error.restype = C.c_char_p
+        L.orc_treecell3d_tree.restype = C.c_int64
+        L.orc_treecell3d_tree.argtypes = [_d, _d, _d, _u8, C.c_int64, C.c_int, C.c_int, C.c_double] + [C.c_void_p] * 5
+        L.orc_treecell3d_velocity.restype = C.c_int
+        L.orc_treecell3d_velocity.argtypes = [_d, _d, _d, _d, _d, _d, _u8, C.c_void_p, C.c_int64, C.c_int, C.c_int,
+                                              C.c_double, _d, _d, _d]
 
     def set_threads(self, n: int) -> None:
         self.lib.orc_set_threads(int(n))
@@ -200,6 +229,28 @@ class Port:
                             geom.ctypes.data_as(C.c_void_p))
         return ints, geom
 
+    def treecell3d(self, x, y, z, active, max_src=30, max_par=50, exp_pct=1.0):
+        """3D TreeCell (treeCell.cpp:1043-1243, DIM 3): (ids, ints, geom, leaf particle lists), by cell ID;
+        ints = parNum, srcParNum, isLeaf, isActive, level, max_level (first row)."""
+        x, y, z, a = _f64(x), _f64(y), _f64(z), _u8a(active)
+        out = _treecell_dump(lambda *o: self.lib.orc_treecell3d_tree(x, y, z, a, x.size, max_src, max_par, exp_pct,
+                                                                      *o))
+        if out is None:
+            raise RuntimeError(self.lib.orc3_last_error().decode())
+        return out
+
+    def treecell3d_velocity(self, x, y, z, ax, ay, az, active, target=None, max_src=30, max_par=50, exp_pct=1.0):
+        """fmm3D::calcVelocity (target None) or calcVelocityNearBody on the 3D TreeCell."""
+        args = [_f64(v) for v in (x, y, z, ax, ay, az)]
+        n = args[0].size
+        t = None if target is None else _u8a(target)
+        u, v, w = np.zeros(n), np.zeros(n), np.zeros(n)
+        rc = self.lib.orc_treecell3d_velocity(*args, _u8a(active), None if t is None else _vp(t), n, max_src, max_par,
+                                              exp_pct, u, v, w)
+        if rc != 0:
+            raise RuntimeError(self.lib.orc3_last_error().decode())
+        return u, v, w
+
     def direct3d_velocity(self, x, y, z, ax, ay, az, active, targets):
         args = [_f64(v) for v in (x, y, z, ax, ay, az)]
         t = np.ascontiguousarray(targets, dtype=np.int64)
@@ -242,6 +293,11 @@ class Reference:
         L3.ref3d_velocity.argtypes = [_d, _d, _d, _d, _d, _d, _u8, C.c_int64, _d, _d, _d]
         L3.ref3d_tree.restype = C.c_int64
         L3.ref3d_tree.argtypes = [_d, _d, _d, _u8, C.c_int64, C.c_void_p, C.c_void_p]
+        L3.ref3d_tc_set.argtypes = [C.c_int, C.c_int, C.c_double]
+        L3.ref3d_tc_velocity.restype = C.c_int
+        L3.ref3d_tc_velocity.argtypes = [_d, _d, _d, _d, _d, _d, _u8, C.c_void_p, C.c_int64, _d, _d, _d]
+        L3.ref3d_tc_tree.restype = C.c_int64
+        L3.ref3d_tc_tree.argtypes = [_d, _d, _d, _u8, C.c_int64] + [C.c_void_p] * 5
 
     def fmm2d_field(self, x, y, q, active, p=10, max_src=50, max_par=75, exp_pct=1.0, exact_binom=False):
         if exact_binom:
@@ -320,3 +376,21 @@ class Reference:
         geom = np.zeros((nc, 4))
         self.lib3.ref3d_tree(x, y, z, a, x.size, ints.ctypes.data_as(C.c_void_p), geom.ctypes.data_as(C.c_void_p))
         return ints, geom
+
+    def treecell3d(self, x, y, z, active, max_src=30, max_par=50, exp_pct=1.0):
+        x, y, z, a = _f64(x), _f64(y), _f64(z), _u8a(active)
+        self.lib3.ref3d_tc_set(max_src, max_par, exp_pct)
+        out = _treecell_dump(lambda *o: self.lib3.ref3d_tc_tree(x, y, z, a, x.size, *o))
+        if out is None:
+            raise RuntimeError(self.lib3.ref3d_last_error().decode())
+        return out
+
+    def treecell3d_velocity(self, x, y, z, ax, ay, az, active, target=None, max_src=30, max_par=50, exp_pct=1.0):
+        args = [_f64(v) for v in (x, y, z, ax, ay, az)]
+        n = args[0].size
+        t = None if target is None else _u8a(target)
+        self.lib3.ref3d_tc_set(max_src, max_par, exp_pct)
+        u, v, w = np.zeros(n), np.zeros(n), np.zeros(n)
+        if self.lib3.ref3d_tc_velocity(*args, _u8a(active), None if t is None else _vp(t), n, u, v, w) != 0:
+            raise RuntimeError(self.lib3.ref3d_last_error().decode())
+        return u, v, w

@@ -9,7 +9,9 @@
 //   * 10-term P2M / M2M       src/FMM/fmm3D.cpp:84-132, fast3DFMM.cpp:164-302
 //   * M2P multipliers         src/FMM/fmm3D.cpp:147-200
 //   * per-target traversal    src/FMM/fast3DFMM.cpp:318-472 (far iff R^2 > (2 size)^2)
-// plus the FP64 direct Biot-Savart sum u_i = sum_j (a_j x r_ij) / |r_ij|^3.
+// the alternative 3D path on the shared TreeCell (VELOCITY_3D_TYPE 2: TreeCell
+// with DIM 3, fmm3D::calcVelocity / calcVelocityNearBody; section below), and
+// the FP64 direct Biot-Savart sum u_i = sum_j (a_j x r_ij) / |r_ij|^3.
 //
 // Geometry decisions (octant comparisons, R^2 against (2 size)^2) use separate
 // IEEE operations in the reference's order; build without -march.
@@ -19,6 +21,7 @@
 #include <cstdint>
 #include <cstring>
 #include <string>
+#include <unordered_map>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
@@ -182,11 +185,271 @@ inline void m2p_mul(double R2, double dx, double dy, double dz, double* gx, doub
     gz[9] = (15 * dz * dx * dz / R7) - (3 * dx / R5);
 }
 
+// ---------------------------------------------------------------------------
+// 3D TreeCell path (VELOCITY_3D_TYPE 2, VELOCITY_CALCULATION_TYPE 2):
+//   tree        TreeCell::initializeTree with DIM 3   src/FMM/treeCell.cpp:1043-1243
+//   cell IDs    start(L) = (8^L - 1) / 7, ID = start + ix + iy 2^L + iz 4^L
+//               (treeCell.cpp:114-148, 223-250); index = (int)((c - pivot) / size_L),
+//               size_L = root / 2^L (treeCell.cpp:101-105, 290-300); children in the
+//               order ix + ((i >> 0) & 1), iy + ((i >> 1) & 1), iz + ((i >> 2) & 1)
+//               (treeCell.cpp:395-417)
+//   P2M, M2M    fmm3D::setupVelocityFMM                src/FMM/fmm3D.cpp:585-784
+//   traversal   fmm3D::calcVelocity / calcVelocityNearBody  fmm3D.cpp:1064-1606:
+//               from the level-1 cells, far iff R^2 > (2 length)^2 (fmm3D.cpp:3),
+//               near leaves by direct sum over ALL their particles (inactive ones
+//               included), j != i.
+// ---------------------------------------------------------------------------
+constexpr int kTcMaxLevel = 10;   // deeper cells overflow the reference's int cell IDs
+
+struct TC3 {
+    double root = 0, piv[3] = {0, 0, 0};
+    std::vector<int64_t> id;
+    std::vector<int> level, npar, nsrc, ix, iy, iz;
+    std::vector<char> leaf, active;
+    std::vector<double> xc, yc, zc, len;
+    std::vector<std::vector<int>> pids;
+    std::vector<int> level_start;       // cells level-major, creation order within a level
+    std::unordered_map<int64_t, int> at;  // cell ID -> index
+    int max_level = 0;
+    int ncell() const { return (int)id.size(); }
+    int find(int64_t cid) const {
+        auto it = at.find(cid);
+        return it == at.end() ? -1 : it->second;
+    }
+};
+
+inline int64_t tc_start(int L) { return ((int64_t)1 << (3 * L)) / 7; }   // (8^L - 1) / 7
+inline int64_t tc_id(int L, int ix, int iy, int iz) {
+    return tc_start(L) + ix + ((int64_t)iy << L) + ((int64_t)iz << (2 * L));
+}
+
+bool build_tc3(TC3& t, const double* x, const double* y, const double* z, const uint8_t* act, int64_t n,
+               int max_src, int max_par, double exp_pct) {
+    const double* p[3] = {x, y, z};
+    double mn[3], mx[3];
+    for (int d = 0; d < 3; ++d) mn[d] = mx[d] = p[d][0];
+    for (int64_t i = 1; i < n; ++i)
+        for (int d = 0; d < 3; ++d) {
+            if (mn[d] > p[d][i]) mn[d] = p[d][i];
+            if (mx[d] < p[d][i]) mx[d] = p[d][i];
+        }
+    t.root = 0.0;
+    for (int d = 0; d < 3; ++d) {
+        const double ext = std::abs(mx[d] - mn[d]);
+        if (ext > t.root) t.root = ext;
+    }
+    t.root *= 1.0 + (exp_pct / 100.0);
+    for (int d = 0; d < 3; ++d) t.piv[d] = (mx[d] + mn[d] - t.root) / 2.0;
+    auto add = [&](int64_t cid, int L, int a, int b, int c, double l) {
+        t.at[cid] = t.ncell();
+        t.id.push_back(cid);
+        t.level.push_back(L);
+        t.npar.push_back(0);
+        t.nsrc.push_back(0);
+        t.ix.push_back(a);
+        t.iy.push_back(b);
+        t.iz.push_back(c);
+        t.leaf.push_back(0);
+        t.active.push_back(0);
+        t.len.push_back(l);
+        t.xc.push_back(t.piv[0] + ((0.5 + a) * l));
+        t.yc.push_back(t.piv[1] + ((0.5 + b) * l));
+        t.zc.push_back(t.piv[2] + ((0.5 + c) * l));
+        t.pids.emplace_back();
+    };
+    add(0, 0, 0, 0, 0, t.root);
+    t.npar[0] = (int)n;
+    for (int64_t i = 0; i < n; ++i) t.nsrc[0] += act[i] ? 1 : 0;
+    t.active[0] = t.nsrc[0] != 0;
+    t.level_start.assign(1, 0);
+    std::vector<char> settled(n, 0);
+    std::vector<int> pcell(n, 0);
+    int64_t unsettled = n;
+    int L = 0;
+    while (unsettled > 0) {
+        ++L;
+        if (L > kTcMaxLevel) {
+            g_err3 = "TreeCell deeper than level 10: the reference's 32-bit cell IDs overflow";
+            return false;
+        }
+        t.level_start.push_back(t.ncell());
+        const double size = t.root / std::pow(2.0, L);
+        const int count = 1 << L;
+        for (int64_t i = 0; i < n; ++i) {
+            if (settled[i]) continue;
+            int idx[3];
+            for (int d = 0; d < 3; ++d) idx[d] = (int)((p[d][i] - t.piv[d]) / size);
+            for (int d = 0; d < 3; ++d)
+                if (idx[d] < 0 || idx[d] >= count) {
+                    g_err3 = "particle outside the root box";
+                    return false;
+                }
+            const int64_t cid = tc_id(L, idx[0], idx[1], idx[2]);
+            int c = t.find(cid);
+            if (c < 0) {
+                c = t.ncell();
+                add(cid, L, idx[0], idx[1], idx[2], size);
+            }
+            pcell[i] = c;
+            t.npar[c] += 1;
+            if (act[i]) t.nsrc[c] += 1;
+        }
+        for (int c = t.level_start[L]; c < t.ncell(); ++c) {
+            if (t.nsrc[c] <= max_src && t.npar[c] <= max_par) t.leaf[c] = 1;
+            if (t.nsrc[c] != 0) t.active[c] = 1;
+        }
+        for (int64_t i = 0; i < n; ++i) {
+            if (settled[i] || !t.leaf[pcell[i]]) continue;
+            t.pids[pcell[i]].push_back((int)i);
+            settled[i] = 1;
+            --unsettled;
+        }
+        t.max_level = L;   // the last leaf created lies on the deepest level
+    }
+    t.level_start.push_back(t.ncell());
+    return true;
+}
+
 }  // namespace
 
 extern "C" {
 
 const char* orc3_last_error() { return g_err3.c_str(); }
+
+// TreeCell dump, cells level-major in creation order: ids = reference cell
+// IDs; ints per cell = nPar, srcParNum, isLeaf, isActive, level, (max_level
+// on cell 0); geom = xc, yc, zc, length; leaf particle IDs (ascending) as
+// CSR leaf_offs[c]..leaf_offs[c+1]. Returns the cell count (-1 on error);
+// call with null outputs first to size them.
+int64_t orc_treecell3d_tree(const double* x, const double* y, const double* z, const uint8_t* act, int64_t n,
+                            int max_src, int max_par, double exp_pct, int64_t* ids, int32_t* ints, double* geom,
+                            int64_t* leaf_offs, int32_t* pids) {
+    TC3 t;
+    if (n < 1 || !build_tc3(t, x, y, z, act, n, max_src, max_par, exp_pct)) return -1;
+    int64_t off = 0;
+    for (int c = 0; c < t.ncell(); ++c) {
+        if (ids) ids[c] = t.id[c];
+        if (ints) {
+            int32_t* r = ints + 6 * (size_t)c;
+            r[0] = t.npar[c]; r[1] = t.nsrc[c]; r[2] = t.leaf[c]; r[3] = t.active[c]; r[4] = t.level[c];
+            r[5] = c == 0 ? t.max_level : 0;
+        }
+        if (geom) {
+            geom[4 * (size_t)c] = t.xc[c]; geom[4 * (size_t)c + 1] = t.yc[c];
+            geom[4 * (size_t)c + 2] = t.zc[c]; geom[4 * (size_t)c + 3] = t.len[c];
+        }
+        if (leaf_offs) leaf_offs[c] = off;
+        for (int i : t.pids[c]) {
+            if (pids) pids[off] = i;
+            ++off;
+        }
+    }
+    if (leaf_offs) leaf_offs[t.ncell()] = off;
+    return t.ncell();
+}
+
+// TreeCell treecode velocity: every particle a target (calcVelocity) when
+// target is null, else only flagged ones (calcVelocityNearBody; the others
+// get zero). Returns -1 with the reference's failure when a level-1 cell is
+// a leaf of a deeper tree (its traversal asks for that leaf's children).
+int orc_treecell3d_velocity(const double* x, const double* y, const double* z, const double* ax, const double* ay,
+                            const double* az, const uint8_t* act, const uint8_t* target, int64_t n, int max_src,
+                            int max_par, double exp_pct, double* u, double* v, double* w) {
+    TC3 t;
+    if (n < 1 || !build_tc3(t, x, y, z, act, n, max_src, max_par, exp_pct)) return -1;
+    const int nc = t.ncell();
+    for (int c = t.level_start[1]; c < t.level_start[2] && t.max_level > 1; ++c)
+        if (t.leaf[c]) {
+            g_err3 = "a level-1 cell is a leaf: the reference's traversal cannot take its children";
+            return -1;
+        }
+    std::vector<double> mx((size_t)nc * 10, 0.0), my((size_t)nc * 10, 0.0), mz((size_t)nc * 10, 0.0);
+    for (int c = 0; c < nc; ++c) {
+        if (!t.leaf[c] || !t.active[c]) continue;
+        for (int i : t.pids[c]) {
+            if (!act[i]) continue;
+            double dx = t.xc[c] - x[i], dy = t.yc[c] - y[i], dz = t.zc[c] - z[i];
+            p2m(&mx[(size_t)c * 10], ax[i], dx, dy, dz);
+            p2m(&my[(size_t)c * 10], ay[i], dx, dy, dz);
+            p2m(&mz[(size_t)c * 10], az[i], dx, dy, dz);
+        }
+    }
+    // children of a non-leaf cell in the reference's order (-1 where absent)
+    auto children = [&](int c, int ch[8]) {
+        const int L = t.level[c] + 1;
+        for (int o = 0; o < 8; ++o)
+            ch[o] = t.find(tc_id(L, 2 * t.ix[c] + (o & 1), 2 * t.iy[c] + ((o >> 1) & 1), 2 * t.iz[c] + ((o >> 2) & 1)));
+    };
+    for (int lv = t.max_level - 1; lv > 0; --lv) {
+        for (int c = t.level_start[lv]; c < t.level_start[lv + 1]; ++c) {
+            if (t.leaf[c] || !t.active[c]) continue;
+            int ch[8];
+            children(c, ch);
+            for (int o = 0; o < 8; ++o) {
+                const int k = ch[o];
+                if (k < 0) continue;
+                double dx = t.xc[c] - t.xc[k], dy = t.yc[c] - t.yc[k], dz = t.zc[c] - t.zc[k];
+                m2m(&mx[(size_t)c * 10], &mx[(size_t)k * 10], dx, dy, dz);
+                m2m(&my[(size_t)c * 10], &my[(size_t)k * 10], dx, dy, dz);
+                m2m(&mz[(size_t)c * 10], &mz[(size_t)k * 10], dx, dy, dz);
+            }
+        }
+    }
+    std::vector<int> first;   // the level-1 cells that exist, in ID order
+    for (int o = 0; o < 8; ++o) {
+        const int c = t.find(1 + o);
+        if (c >= 0) first.push_back(c);
+    }
+    #pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t i = 0; i < n; ++i) {
+        double vx = 0, vy = 0, vz = 0;
+        if (target == nullptr || target[i]) {
+            const double xp = x[i], yp = y[i], zp = z[i];
+            std::vector<int> cur(first), nxt;
+            double gx[10], gy[10], gz[10];
+            for (int lv = 1; lv < t.max_level; ++lv) {
+                nxt.clear();
+                for (int c : cur) {
+                    int ch[8];
+                    children(c, ch);
+                    for (int o = 0; o < 8; ++o) {
+                        const int k = ch[o];
+                        if (k < 0 || !t.active[k]) continue;
+                        double dx = xp - t.xc[k], dy = yp - t.yc[k], dz = zp - t.zc[k];
+                        double R2 = dx * dx + dy * dy + dz * dz;
+                        double Rc = t.len[k] * 2.0;
+                        if (R2 > Rc * Rc) {
+                            m2p_mul(R2, dx, dy, dz, gx, gy, gz);
+                            const double* Mx = &mx[(size_t)k * 10];
+                            const double* My = &my[(size_t)k * 10];
+                            const double* Mz = &mz[(size_t)k * 10];
+                            for (int m = 0; m < 10; ++m) {
+                                vx += My[m] * gz[m] - Mz[m] * gy[m];
+                                vy += Mz[m] * gx[m] - Mx[m] * gz[m];
+                                vz += Mx[m] * gy[m] - My[m] * gx[m];
+                            }
+                        } else if (!t.leaf[k]) {
+                            nxt.push_back(k);
+                        } else {
+                            for (int j : t.pids[k]) {
+                                if (j == i) continue;
+                                double ex = xp - x[j], ey = yp - y[j], ez = zp - z[j];
+                                double r2 = ex * ex + ey * ey + ez * ez;
+                                double r3 = std::sqrt(r2) * r2;
+                                vx += (ay[j] * ez - az[j] * ey) / r3;
+                                vy += (az[j] * ex - ax[j] * ez) / r3;
+                                vz += (ax[j] * ey - ay[j] * ex) / r3;
+                            }
+                        }
+                    }
+                }
+                cur.swap(nxt);
+            }
+        }
+        u[i] = vx; v[i] = vy; w[i] = vz;
+    }
+    return 0;
+}
 
 // Treecode velocity (reference calcVelocityFast with every particle a target).
 int orc_fmm3d_velocity(const double* x, const double* y, const double* z,

@@ -2,12 +2,15 @@
 //
 // C entry points around the reference's default 3D velocity path
 // fmm3D::calcVelocityFast (src/FMM/fast3DFMM.cpp:32-92: FMMCell::generateTree,
-// 10-term P2M/M2M, per-target traversal) compiled by oracle/Makefile from a
+// 10-term P2M/M2M, per-target traversal) and around its TreeCell path
+// (TreeCell::initializeTree with DIM 3, fmm3D::calcVelocity and
+// calcVelocityNearBody, src/FMM/fmm3D.cpp:585-1606), compiled by oracle/Makefile from a
 // build-directory copy of the reference sources with DIM set to 3 (the
 // reference fixes DIM with a #define in global.hpp:85). Output goes to
 // oracle/_ref/libref3d.so only.
 #include "src/FMM/fmm3D.hpp"
 #include "src/FMM/fast3DFMM.hpp"
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -91,6 +94,83 @@ int64_t ref3d_tree(const double* x, const double* y, const double* z, const uint
             }
         }
         return t.cellNum;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return -1;
+    }
+}
+
+// TreeCell leaf caps (read by the TreeCell constructor) and root expansion.
+void ref3d_tc_set(int max_src, int max_par, double exp_pct) { refpars_set(12, exp_pct, max_par, max_src); }
+
+// fmm3D::calcVelocity (target null) or calcVelocityNearBody (target flags)
+// on a TreeCell built from the same particles.
+int ref3d_tc_velocity(const double* x, const double* y, const double* z, const double* ax, const double* ay,
+                      const double* az, const uint8_t* act, const uint8_t* target, int64_t n, double* u, double* v,
+                      double* w) {
+    try {
+        Quiet quiet;
+        std::vector<std::vector<double>> pos;
+        std::vector<bool> mark;
+        pack(x, y, z, act, n, pos, mark);
+        std::vector<double> sx(ax, ax + n), sy(ay, ay + n), sz(az, az + n);
+        TreeCell t;
+        t.initializeTree(pos, mark);
+        fmm3D f;
+        if (target) {
+            std::vector<bool> tg(n, false);
+            for (int64_t i = 0; i < n; ++i) tg[i] = target[i] != 0;
+            f.calcVelocityNearBody(t, pos, mark, tg, sx, sy, sz);
+        } else {
+            f.calcVelocity(t, pos, mark, sx, sy, sz);
+        }
+        std::vector<double> fx = f.get_Field_x(), fy = f.get_Field_y(), fz = f.get_Field_z();
+        std::memcpy(u, fx.data(), sizeof(double) * n);
+        std::memcpy(v, fy.data(), sizeof(double) * n);
+        std::memcpy(w, fz.data(), sizeof(double) * n);
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return -1;
+    }
+    return 0;
+}
+
+// TreeCell dump in ascending cell ID: ids; ints per cell = parNum, srcParNum,
+// isLeaf, isActive, level, max_level (first cell only); geom = centre,
+// length; leaf parIDList as CSR. Returns the cell count; call with null
+// outputs first to size them.
+int64_t ref3d_tc_tree(const double* x, const double* y, const double* z, const uint8_t* act, int64_t n,
+                      int64_t* ids, int32_t* ints, double* geom, int64_t* leaf_offs, int32_t* pids) {
+    try {
+        Quiet quiet;
+        std::vector<std::vector<double>> pos;
+        std::vector<bool> mark;
+        pack(x, y, z, act, n, pos, mark);
+        TreeCell t;
+        t.initializeTree(pos, mark);
+        std::vector<int> keys;
+        for (const auto& kv : t.treeData) keys.push_back(kv.first);
+        std::sort(keys.begin(), keys.end());
+        int64_t off = 0;
+        for (size_t k = 0; k < keys.size(); ++k) {
+            const Cell* c = t.treeData.at(keys[k]);
+            if (ids) ids[k] = c->ID;
+            if (ints) {
+                int32_t* r = ints + 6 * k;
+                r[0] = c->parNum; r[1] = c->srcParNum; r[2] = c->isLeaf ? 1 : 0; r[3] = c->isActive ? 1 : 0;
+                r[4] = c->level; r[5] = k == 0 ? t.max_level : 0;
+            }
+            if (geom)
+                for (int d = 0; d < 3; ++d) geom[4 * k + d] = c->centerPos[d];
+            if (geom) geom[4 * k + 3] = c->length;
+            if (leaf_offs) leaf_offs[k] = off;
+            for (int pid : c->parIDList) {
+                if (pids) pids[off] = pid;
+                ++off;
+            }
+        }
+        if (leaf_offs) leaf_offs[keys.size()] = off;
+        return (int64_t)keys.size();
     } catch (const std::exception& e) {
         g_err = e.what();
         return -1;

@@ -4,7 +4,8 @@ Runs here only (it needs oracle/_ref, built from the reference sources by
 `make -C oracle ref`). Each fixture holds a seeded input set and the
 reference's outputs: the tree dump (cells by ID, leafList, parIDList), lists
 1-4, the field (calcField) and the potential (calcPotential) for 2D; the
-treecode velocity and octree dump for 3D.
+treecode velocity and octree dump for 3D; for the 3D TreeCell path the cell
+dump by ID and the velocities of calcVelocity and calcVelocityNearBody.
 
     python tests/golden/make_golden.py [case ...]   (all cases when none is named)
 """
@@ -51,6 +52,8 @@ def main():
         fn = os.path.join(HERE, f"fmm2d_{name}_p{p}_{ms}_{mp}.npz")
         np.savez_compressed(fn, **out)
         print(fn, x.size, t.ids.size)
+    if not only or "treecell3d" in only:
+        treecell3d(ref)
     if only and "ring3d" not in only:
         return
     # 3D treecode on a coarse ring.
@@ -62,6 +65,29 @@ def main():
     np.savez_compressed(fn, x=r["x"], y=r["y"], z=r["z"], ax=r["ax"], ay=r["ay"], az=r["az"],
                         active=r["active"], u=u, v=v, w=w, ints=ints, geom=geom)
     print(fn, r["x"].size, ints.shape[0])
+
+
+
+def treecell3d(ref):
+    """3D TreeCell path on a coarse ring with every tenth particle inactive
+    (inactive particles are P2P sources there) and every seventh a target."""
+    r = workloads.vortex_ring_3d(h=0.05, seed=11)
+    n = r["x"].size
+    act = r["active"].copy()
+    act[::10] = 0
+    tgt = np.zeros(n, np.uint8)
+    tgt[::7] = 1
+    args = [r[k] for k in ("x", "y", "z", "ax", "ay", "az")]
+    ids, ints, geom, leaves = ref.treecell3d(r["x"], r["y"], r["z"], act, max_src=30, max_par=50)
+    offs = np.concatenate([[0], np.cumsum([len(v) for v in leaves])]).astype(np.int64)
+    pids = np.concatenate(leaves).astype(np.int32)
+    u, v, w = ref.treecell3d_velocity(*args, act, None, max_src=30, max_par=50)
+    ub, vb, wb = ref.treecell3d_velocity(*args, act, tgt, max_src=30, max_par=50)
+    fn = os.path.join(HERE, "treecell3d_ring_h005_30_50.npz")
+    np.savez_compressed(fn, x=r["x"], y=r["y"], z=r["z"], ax=r["ax"], ay=r["ay"], az=r["az"], active=act,
+                        target=tgt, ids=ids, ints=ints, geom=geom, leaf_offs=offs, leaf_pids=pids, u=u, v=v, w=w,
+                        u_nb=ub, v_nb=vb, w_nb=wb)
+    print(fn, n, ids.size)
 
 
 if __name__ == "__main__":

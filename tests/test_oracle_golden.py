@@ -62,3 +62,23 @@ def test_3d_treecode():
     assert np.array_equal(ints, f["ints"]) and np.array_equal(geom, f["geom"])
     u, v, w = P.fmm3d_velocity(f["x"], f["y"], f["z"], f["ax"], f["ay"], f["az"], f["active"])
     assert rel_l2((u, v, w), (f["u"], f["v"], f["w"])) <= 1e-12
+
+
+def test_treecell3d_port_matches_golden():
+    """3D TreeCell path: cells by ID (counts, flags, levels, centres, lengths),
+    leaf particle lists, calcVelocity and calcVelocityNearBody."""
+    f = dict(np.load(os.path.join(GOLD, "treecell3d_ring_h005_30_50.npz")))
+    from oracle import Port
+    P = Port()
+    ids, ints, geom, leaves = P.treecell3d(f["x"], f["y"], f["z"], f["active"], max_src=30, max_par=50)
+    assert np.array_equal(ids, f["ids"]) and np.array_equal(ints, f["ints"]) and np.array_equal(geom, f["geom"])
+    offs = f["leaf_offs"]
+    for k, lst in enumerate(leaves):
+        assert np.array_equal(lst, f["leaf_pids"][offs[k]:offs[k + 1]])
+    args = [f[k] for k in ("x", "y", "z", "ax", "ay", "az")]
+    u, v, w = P.treecell3d_velocity(*args, f["active"], None, max_src=30, max_par=50)
+    assert rel_l2((u, v, w), (f["u"], f["v"], f["w"])) <= 1e-12
+    u, v, w = P.treecell3d_velocity(*args, f["active"], f["target"], max_src=30, max_par=50)
+    assert rel_l2((u, v, w), (f["u_nb"], f["v_nb"], f["w_nb"])) <= 1e-12
+    off = f["target"] == 0
+    assert not np.any(u[off]) and not np.any(v[off]) and not np.any(w[off])

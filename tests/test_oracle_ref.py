@@ -49,3 +49,37 @@ def test_reference_3d(port, ref):
     u, v, w = port.fmm3d_velocity(*args, r["active"])
     ru, rv, rw = ref.fmm3d_velocity(*args, r["active"])
     assert rel_l2((u, v, w), (ru, rv, rw)) <= 1e-12
+
+
+@pytest.mark.parametrize("caps", [(30, 50), (8, 12)])
+def test_reference_treecell3d(port, ref, caps):
+    """3D TreeCell path, cells and velocities, with inactive particles and a
+    target subset."""
+    r = workloads.vortex_ring_3d(h=0.07, seed=3)
+    n = r["x"].size
+    act = r["active"].copy()
+    act[::6] = 0
+    tgt = (np.arange(n) % 5 == 0).astype(np.uint8)
+    ms, mp = caps
+    tp = port.treecell3d(r["x"], r["y"], r["z"], act, max_src=ms, max_par=mp)
+    tr = ref.treecell3d(r["x"], r["y"], r["z"], act, max_src=ms, max_par=mp)
+    for a, b in zip(tp[:3], tr[:3]):
+        assert np.array_equal(a, b)
+    assert all(np.array_equal(a, b) for a, b in zip(tp[3], tr[3]))
+    args = [r[k] for k in ("x", "y", "z", "ax", "ay", "az")]
+    for t in (None, tgt):
+        u = port.treecell3d_velocity(*args, act, t, max_src=ms, max_par=mp)
+        ru = ref.treecell3d_velocity(*args, act, t, max_src=ms, max_par=mp)
+        assert rel_l2(u, ru) <= 1e-12
+
+
+def test_treecell3d_port_refuses_level1_leaf(port):
+    """A level-1 leaf in a deeper TreeCell: the reference's traversal throws
+    (inside its OpenMP loop, which ends the process, so it is not run here);
+    the port reports an error."""
+    rng = np.random.default_rng(2)
+    x, y, z = rng.uniform(-1, 1, (3, 400))
+    x[:3] += 10.0          # three particles alone in a level-1 cell
+    a = rng.normal(size=(3, 400))
+    with pytest.raises(RuntimeError, match="level-1"):
+        port.treecell3d_velocity(x, y, z, *a, np.ones(400, np.uint8))
