@@ -131,6 +131,7 @@ class Port:
         L.orc_treecell3d_tree.restype = C.c_int64
         L.orc_treecell3d_tree.argtypes = [_d, _d, _d, _u8, C.c_int64, C.c_int, C.c_int, C.c_double] + [C.c_void_p] * 5
         L.orc_treecell3d_velocity.restype = C.c_int
+        L.orc_treecell3d_pairs.argtypes = [_i64]
         L.orc_treecell3d_velocity.argtypes = [_d, _d, _d, _d, _d, _d, _u8, C.c_void_p, C.c_int64, C.c_int, C.c_int,
                                               C.c_double, _d, _d, _d]
 
@@ -250,6 +251,12 @@ class Port:
         if rc != 0:
             raise RuntimeError(self.lib.orc3_last_error().decode())
         return u, v, w
+
+    def treecell3d_pairs(self):
+        """(P2P pairs, M2P pairs) of the last treecell3d_velocity call."""
+        out = np.zeros(2, np.int64)
+        self.lib.orc_treecell3d_pairs(out)
+        return int(out[0]), int(out[1])
 
     def direct3d_velocity(self, x, y, z, ax, ay, az, active, targets):
         args = [_f64(v) for v in (x, y, z, ax, ay, az)]

@@ -200,6 +200,7 @@ inline void m2p_mul(double R2, double dx, double dy, double dz, double* gx, doub
 //               included), j != i.
 // ---------------------------------------------------------------------------
 constexpr int kTcMaxLevel = 10;   // deeper cells overflow the reference's int cell IDs
+int64_t g_tc_pairs[2] = {0, 0};   // P2P (target, source) and M2P (target, cell) pairs of the last evaluation
 
 struct TC3 {
     double root = 0, piv[3] = {0, 0, 0};
@@ -400,7 +401,8 @@ int orc_treecell3d_velocity(const double* x, const double* y, const double* z, c
         const int c = t.find(1 + o);
         if (c >= 0) first.push_back(c);
     }
-    #pragma omp parallel for schedule(dynamic, 64)
+    int64_t n_p2p = 0, n_m2p = 0;
+    #pragma omp parallel for schedule(dynamic, 64) reduction(+ : n_p2p, n_m2p)
     for (int64_t i = 0; i < n; ++i) {
         double vx = 0, vy = 0, vz = 0;
         if (target == nullptr || target[i]) {
@@ -419,6 +421,7 @@ int orc_treecell3d_velocity(const double* x, const double* y, const double* z, c
                         double R2 = dx * dx + dy * dy + dz * dz;
                         double Rc = t.len[k] * 2.0;
                         if (R2 > Rc * Rc) {
+                            ++n_m2p;
                             m2p_mul(R2, dx, dy, dz, gx, gy, gz);
                             const double* Mx = &mx[(size_t)k * 10];
                             const double* My = &my[(size_t)k * 10];
@@ -433,6 +436,7 @@ int orc_treecell3d_velocity(const double* x, const double* y, const double* z, c
                         } else {
                             for (int j : t.pids[k]) {
                                 if (j == i) continue;
+                                ++n_p2p;
                                 double ex = xp - x[j], ey = yp - y[j], ez = zp - z[j];
                                 double r2 = ex * ex + ey * ey + ez * ez;
                                 double r3 = std::sqrt(r2) * r2;
@@ -448,7 +452,16 @@ int orc_treecell3d_velocity(const double* x, const double* y, const double* z, c
         }
         u[i] = vx; v[i] = vy; w[i] = vz;
     }
+    g_tc_pairs[0] = n_p2p;
+    g_tc_pairs[1] = n_m2p;
     return 0;
+}
+
+// Pair counts of the last orc_treecell3d_velocity call: out[0] = P2P
+// (target, source) pairs, j != i; out[1] = M2P (target, far cell) pairs.
+void orc_treecell3d_pairs(int64_t* out) {
+    out[0] = g_tc_pairs[0];
+    out[1] = g_tc_pairs[1];
 }
 
 // Treecode velocity (reference calcVelocityFast with every particle a target).
