@@ -11,12 +11,14 @@
 // its TreeCell the same way, with every particle of a near leaf a source.
 // (level-1 cells themselves are never evaluated, as in the reference).
 //
-// One warp per leaf, one lane per target particle of the leaf. The warp
-// walks the union of its targets' lists level by level, each entry carrying
-// the mask of the lanes whose own list holds it; every lane therefore makes
-// exactly its own reference decisions, in its own order. The far/near test
-// uses separately rounded IEEE operations (no contraction) so it decides as
-// the reference does.
+// One warp per 32 consecutive particles in leaf order (leaves hold about 8
+// particles on average, so a warp spans a few neighbouring leaves), one lane
+// per target. The warp walks the union of its targets' lists level by level,
+// each entry carrying the mask of the lanes whose own list holds it; every
+// lane therefore makes exactly its own reference decisions, in its own order,
+// whichever other targets share its warp (results do not depend on the
+// grouping). The far/near test uses separately rounded IEEE operations (no
+// contraction) so it decides as the reference does.
 #include "fmm3d.cuh"
 
 #include <algorithm>
@@ -182,7 +184,8 @@ eval3d_kernel(Tree3D t, const uint8_t* __restrict__ target, double* __restrict__
     int stop = 0;
     if (lane == 0) stop = fatal(err);
     if (__shfl_sync(0xffffffffu, stop, 0)) return;  // warp-uniform
-    const int nc = t.info->n_cells, depth = t.info->depth;
+    const int depth = t.info->depth;
+    const int nchunks = (t.n + 31) >> 5;
     const Src3 src{t.px, t.py, t.pz, t.ax, t.ay, t.az, t.pact};
     const unsigned rm = t.c_chmask[0];
     const int r0 = t.c_child0[0];
@@ -190,9 +193,8 @@ eval3d_kernel(Tree3D t, const uint8_t* __restrict__ target, double* __restrict__
         int c = 0;
         if (lane == 0) c = (int)atomicAdd(ticket, 1u);
         c = __shfl_sync(0xffffffffu, c, 0);
-        if (c >= nc) break;
-        if (t.c_chmask[c] != 0) continue;  // leaves only
-        const int lo = t.c_lo[c], hi = t.c_hi[c];
+        if (c >= nchunks) break;
+        const int lo = c * 32, hi = min(t.n, lo + 32);
         for (int tb = lo; tb < hi; tb += 32) {
             const int slot = tb + lane;
             const bool has = slot < hi;
