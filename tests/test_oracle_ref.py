@@ -83,3 +83,22 @@ def test_treecell3d_port_refuses_level1_leaf(port):
     a = rng.normal(size=(3, 400))
     with pytest.raises(RuntimeError, match="level-1"):
         port.treecell3d_velocity(x, y, z, *a, np.ones(400, np.uint8))
+
+
+@pytest.mark.parametrize("which", ["all_inactive", "max_level_1"])
+def test_reference_treecell3d_edges(port, ref, which):
+    """All particles inactive (every cell inactive, zero velocity), and a tree
+    whose level-1 cells are all leaves (the traversal loop does not run)."""
+    rng = np.random.default_rng(4)
+    n = 1000 if which == "all_inactive" else 40
+    x, y, z = rng.uniform(-1, 1, (3, n))
+    a = rng.normal(size=(3, n))
+    act = np.zeros(n, np.uint8) if which == "all_inactive" else np.ones(n, np.uint8)
+    tp = port.treecell3d(x, y, z, act)
+    tr = ref.treecell3d(x, y, z, act)
+    for p_, r_ in zip(tp[:3], tr[:3]):
+        assert np.array_equal(p_, r_)
+    u = port.treecell3d_velocity(x, y, z, *a, act)
+    ru = ref.treecell3d_velocity(x, y, z, *a, act)
+    for p_, r_ in zip(u, ru):
+        assert np.array_equal(p_, r_) and not np.any(r_)
