@@ -199,21 +199,24 @@ int vpm_tree2d_list(vpm_ctx* ctx, int which, int64_t* cell_ids, int64_t* offs, i
 
 /*
  * vpm_fmm2d_field_device_static: the evaluation of vpm_fmm2d_field_device
- * (device buffers in and out, FP64 or mixed form) without any device
- * allocation, for callers that cannot call cudaMalloc: code running while a
- * CUDA stream capture is open (allocation is not permitted there), host
- * callbacks, and programs whose device memory is owned by another allocator.
- * No counterpart in the reference (its FMM allocates host memory freely).
+ * (device buffers in and out; FP64, mixed or mixed with FP64 M2L) without any
+ * device allocation, for callers that cannot call cudaMalloc: programs whose
+ * device memory is owned by another allocator (a framework's caching
+ * allocator holding the whole budget), and time-step loops that must not
+ * stall on the device synchronisation that cudaMalloc and cudaFree can
+ * cause. No counterpart in the reference (its FMM allocates host memory
+ * freely).
  *
  * All scratch lives in one static device array of 8 MiB that every GPU
  * loading this library keeps until the process exits. Limits: n <= 8192,
  * p <= 12, at most 8192 tree cells; larger requests return VPM_EINVAL, a
  * tree that outgrows the array returns VPM_EOVERFLOW. The first call on a
- * device looks up the array's device address (with that device current) and
- * must come before any stream capture that contains this call. Calls share
- * the array and overwrite it; calls that overlap on the GPU race, so
- * serialise them. Runs on `cuda_stream` (a cudaStream_t, NULL = legacy
- * default stream) and waits for it to report errors. errbuf (may be NULL)
+ * device looks up the array's device address (with that device current);
+ * make that first call before any stream capture begins. Both mixed settings
+ * use the FP64 M2L with the FP32 near field. Calls share the array and
+ * overwrite it; calls that overlap on the GPU race, so serialise them. Runs
+ * on `cuda_stream` (a cudaStream_t, NULL = legacy default stream), then reads
+ * the device error word back and waits for that stream. errbuf (may be NULL)
  * receives a message of at most errlen bytes.
  */
 int vpm_fmm2d_field_device_static(const double* x, const double* y, const double* q,

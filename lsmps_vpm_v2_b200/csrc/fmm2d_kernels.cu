@@ -5,9 +5,10 @@
 //   E_x = Re F, E_y = -Im F,  F = sum of q/(z - z_j) terms.
 //
 // Stage map:
-//   fmm2d_upward  P2M of every active leaf fused with M2M (fmm2D.cpp:309-379):
-//                 the last child to finish computes its parent, so the whole
-//                 upward pass is one launch.
+//   fmm2d_upward  P2M of every active leaf (p2m2d, fmm2D.cpp:237-284), then
+//                 M2M over the levels, deepest first, in one cooperative
+//                 launch with a grid barrier per level (m2m_levels_coop,
+//                 fmm2D.cpp:309-379).
 //   fmm2d_m2l     lists 2 and 4 of every cell at level >= 2 (fmm2D.cpp:396-556).
 //   fmm2d_eval    per leaf: the L2L chain from its level-2 ancestor
 //                 (fmm2D.cpp:587-651), then M2P over list 3 (fmm2D.cpp:1040-1066)

@@ -1,8 +1,9 @@
 // vpm_fmm2d_field_device_static: the 2D evaluation of vpm_fmm2d_field_device
-// for callers that cannot allocate device memory: code that runs while a
-// CUDA stream capture is open (cudaMalloc is not permitted then), host
-// callbacks, or hosts whose device memory is owned by another allocator (a
-// solver that hands its whole budget to a framework's caching allocator).
+// for callers that cannot allocate device memory. Two kinds of caller need
+// it: programs whose device memory belongs to another allocator (a solver
+// that hands its whole budget to a framework's caching allocator, so a
+// cudaMalloc here would fail or fragment that pool), and time-step loops that
+// must not stall, since cudaMalloc and cudaFree can synchronise the device.
 //
 // All scratch (sorted particles, cells, lists, expansions, sort and scan
 // status words, the error word) lives in one file-scope static device array
@@ -10,6 +11,11 @@
 // process exits. The caller passes only its input and output device buffers.
 // No cudaMalloc, cudaFree or allocating library routine is called, on the
 // device or the host.
+//
+// The first call on each device looks up the array's device address with
+// cudaGetSymbolAddress (set-up, once per device, with that device current);
+// make that first call before any stream capture begins. Each call ends by
+// reading the device error word back and waiting for its stream.
 //
 // Limits: n <= kStaticMaxN particles, at most kStaticMaxCells tree cells,
 // p <= kStaticMaxP; larger requests are rejected with VPM_EINVAL, and a tree
@@ -97,8 +103,12 @@ extern "C" int vpm_fmm2d_field_device_static(const double* x, const double* y, c
         set_msg(errbuf, errlen, "p must be in 1..12 for the static-scratch entry point");
         return VPM_EINVAL;
     }
-    if (p.max_src < 0 || p.max_par < 1 || (p.precision != VPM_PREC_FP64 && p.precision != VPM_PREC_MIXED)) {
-        set_msg(errbuf, errlen, "invalid leaf caps or precision");
+    if (p.max_src < 0 || p.max_par < 1) {
+        set_msg(errbuf, errlen, "leaf caps must be max_src >= 0, max_par >= 1");
+        return VPM_EINVAL;
+    }
+    if (p.precision != VPM_PREC_FP64 && p.precision != VPM_PREC_MIXED && p.precision != VPM_PREC_MIXED_FP64_M2L) {
+        set_msg(errbuf, errlen, "precision must be VPM_PREC_FP64, VPM_PREC_MIXED or VPM_PREC_MIXED_FP64_M2L");
         return VPM_EINVAL;
     }
     const int K = (p.max_depth == 31) ? 31 : 16;
@@ -114,8 +124,8 @@ extern "C" int vpm_fmm2d_field_device_static(const double* x, const double* y, c
     }
     void* base_ptr = nullptr;
     {
-        // Set-up, once per device, with that device current. It must run
-        // before any stream capture that contains a call of this function.
+        // Set-up, once per device, with that device current (the first call
+        // on a device; it should come before any stream capture begins).
         std::lock_guard<std::mutex> lock(g_static_mutex);
         if (!g_static_addr[dev]) {
             void* ptr = nullptr;
@@ -223,7 +233,7 @@ extern "C" int vpm_fmm2d_field_device_static(const double* x, const double* y, c
     if (r == cudaSuccess) r = fmm2d_m2l(t, l, xe, P, err, st, &launches);
     if (r == cudaSuccess) r = fmm2d_eval(t, l, xe, P, err, st, &launches);
     if (r == cudaSuccess) {
-        if (p.precision == VPM_PREC_MIXED)
+        if (p.precision == VPM_PREC_MIXED || p.precision == VPM_PREC_MIXED_FP64_M2L)
             r = fmm2d_p2p_f32(t, l, xe, ex, ey, 0, 0.0, 0.0, err, st, &launches);
         else
             r = fmm2d_p2p(t, l, xe, ex, ey, err, st, &launches);

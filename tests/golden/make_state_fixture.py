@@ -12,7 +12,9 @@ on a real particle distribution (tests/cases2d.py: "state500"). Runs here only
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SRC = "/root/reference/input/resume_data/particle_state_00500.csv"
+# The reference checkout: $VPM_REFERENCE_DIR, else "reference" beside the repository.
+REF = os.environ.get("VPM_REFERENCE_DIR") or os.path.abspath(os.path.join(HERE, "..", "..", "..", "reference"))
+SRC = os.path.join(REF, "input", "resume_data", "particle_state_00500.csv")
 DST = os.path.join(HERE, "particle_state_00500_sub8.csv")
 STRIDE = 8
 
