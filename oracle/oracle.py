@@ -124,6 +124,9 @@ class Port:
         L.orc_direct2d_field.argtypes = [_d, _d, _d, _u8, C.c_int64, _i64, C.c_int64, _d, _d]
         L.orc_fmm3d_velocity.restype = C.c_int
         L.orc_fmm3d_velocity.argtypes = [_d, _d, _d, _d, _d, _d, _u8, C.c_int64, C.c_int, C.c_double, _d, _d, _d]
+        L.orc_fmm3d_velocity_at.restype = C.c_int
+        L.orc_fmm3d_velocity_at.argtypes = [_d, _d, _d, _d, _d, _d, _u8, C.c_int64, C.c_int, C.c_double, _i64,
+                                            C.c_int64, _d, _d, _d]
         L.orc_tree3d.restype = C.c_int64
         L.orc_tree3d.argtypes = [_d, _d, _d, _u8, C.c_int64, C.c_int, C.c_double, C.c_void_p, C.c_void_p]
         L.orc_direct3d_velocity.argtypes = [_d, _d, _d, _d, _d, _d, _u8, C.c_int64, _i64, C.c_int64, _d, _d, _d]
@@ -215,6 +218,16 @@ class Port:
         n = args[0].size
         u, v, w = np.zeros(n), np.zeros(n), np.zeros(n)
         rc = self.lib.orc_fmm3d_velocity(*args, a, n, leaf_cap, exp_pct, u, v, w)
+        if rc != 0:
+            raise RuntimeError(self.lib.orc3_last_error().decode())
+        return u, v, w
+
+    def fmm3d_velocity_at(self, x, y, z, ax, ay, az, active, targets, leaf_cap=30, exp_pct=1.0):
+        """The treecode velocity at the sampled targets only (same tree, same per-target walk)."""
+        args = [_f64(v) for v in (x, y, z, ax, ay, az)]
+        t = np.ascontiguousarray(targets, dtype=np.int64)
+        u, v, w = np.zeros(t.size), np.zeros(t.size), np.zeros(t.size)
+        rc = self.lib.orc_fmm3d_velocity_at(*args, _u8a(active), args[0].size, leaf_cap, exp_pct, t, t.size, u, v, w)
         if rc != 0:
             raise RuntimeError(self.lib.orc3_last_error().decode())
         return u, v, w

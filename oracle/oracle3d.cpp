@@ -464,23 +464,34 @@ void orc_treecell3d_pairs(int64_t* out) {
     out[1] = g_tc_pairs[1];
 }
 
-// Treecode velocity (reference calcVelocityFast with every particle a target).
-int orc_fmm3d_velocity(const double* x, const double* y, const double* z,
-                       const double* ax, const double* ay, const double* az, const uint8_t* act,
-                       int64_t n, int leaf_cap, double exp_pct, double* u, double* v, double* w) {
+}  // extern "C"
+
+namespace {
+
+// Octree plus the 10-term moments of every active cell (fast3DFMM.cpp:164-302).
+struct OctMoments {
     Oct t;
-    if (!build_oct(t, x, y, z, act, n, leaf_cap, exp_pct)) return -1;
+    std::vector<double> mx, my, mz;
+};
+
+bool build_moments(OctMoments& om, const double* x, const double* y, const double* z, const double* ax,
+                   const double* ay, const double* az, const uint8_t* act, int64_t n, int leaf_cap,
+                   double exp_pct) {
+    Oct& t = om.t;
+    if (!build_oct(t, x, y, z, act, n, leaf_cap, exp_pct)) return false;
     const int nc = t.ncell();
-    std::vector<double> mx((size_t)nc * 10, 0.0), my((size_t)nc * 10, 0.0), mz((size_t)nc * 10, 0.0);
+    om.mx.assign((size_t)nc * 10, 0.0);
+    om.my.assign((size_t)nc * 10, 0.0);
+    om.mz.assign((size_t)nc * 10, 0.0);
     #pragma omp parallel for schedule(dynamic, 16)
     for (int c = 0; c < nc; ++c) {
         if (!t.leaf(c) || !t.active[c]) continue;
         for (int i : t.pids[c]) {
             if (!act[i]) continue;
             double dx = t.xc[c] - x[i], dy = t.yc[c] - y[i], dz = t.zc[c] - z[i];
-            p2m(&mx[(size_t)c * 10], ax[i], dx, dy, dz);
-            p2m(&my[(size_t)c * 10], ay[i], dx, dy, dz);
-            p2m(&mz[(size_t)c * 10], az[i], dx, dy, dz);
+            p2m(&om.mx[(size_t)c * 10], ax[i], dx, dy, dz);
+            p2m(&om.my[(size_t)c * 10], ay[i], dx, dy, dz);
+            p2m(&om.mz[(size_t)c * 10], az[i], dx, dy, dz);
         }
     }
     for (int lv = t.max_level - 1; lv > 0; --lv) {
@@ -490,58 +501,99 @@ int orc_fmm3d_velocity(const double* x, const double* y, const double* z,
                 if (((t.chd_flag[c] >> o) & 1) == 0) continue;
                 int k = t.chd[c][o];
                 double dx = t.xc[c] - t.xc[k], dy = t.yc[c] - t.yc[k], dz = t.zc[c] - t.zc[k];
-                m2m(&mx[(size_t)c * 10], &mx[(size_t)k * 10], dx, dy, dz);
-                m2m(&my[(size_t)c * 10], &my[(size_t)k * 10], dx, dy, dz);
-                m2m(&mz[(size_t)c * 10], &mz[(size_t)k * 10], dx, dy, dz);
+                m2m(&om.mx[(size_t)c * 10], &om.mx[(size_t)k * 10], dx, dy, dz);
+                m2m(&om.my[(size_t)c * 10], &om.my[(size_t)k * 10], dx, dy, dz);
+                m2m(&om.mz[(size_t)c * 10], &om.mz[(size_t)k * 10], dx, dy, dz);
             }
         }
     }
-    #pragma omp parallel for schedule(dynamic, 64)
-    for (int64_t i = 0; i < n; ++i) {
-        const double xp = x[i], yp = y[i], zp = z[i];
-        double vx = 0, vy = 0, vz = 0;
-        std::vector<int> cur, nxt;
-        for (int o = 0; o < 8; ++o)
-            if ((t.chd_flag[0] >> o) & 1) cur.push_back(t.chd[0][o]);
-        double gx[10], gy[10], gz[10];
-        for (int lv = 1; lv < t.max_level; ++lv) {
-            nxt.clear();
-            for (int c : cur) {
-                for (int o = 0; o < 8; ++o) {
-                    if (((t.chd_flag[c] >> o) & 1) == 0) continue;
-                    int k = t.chd[c][o];
-                    if (!t.active[k]) continue;
-                    double dx = xp - t.xc[k], dy = yp - t.yc[k], dz = zp - t.zc[k];
-                    double R2 = dx * dx + dy * dy + dz * dz;
-                    double Rc = t.size[k] * 2.0;
-                    if (R2 > Rc * Rc) {
-                        m2p_mul(R2, dx, dy, dz, gx, gy, gz);
-                        const double* Mx = &mx[(size_t)k * 10];
-                        const double* My = &my[(size_t)k * 10];
-                        const double* Mz = &mz[(size_t)k * 10];
-                        for (int m = 0; m < 10; ++m) {
-                            vx += My[m] * gz[m] - Mz[m] * gy[m];
-                            vy += Mz[m] * gx[m] - Mx[m] * gz[m];
-                            vz += Mx[m] * gy[m] - My[m] * gx[m];
-                        }
-                    } else if (t.chd_flag[k] != 0) {
-                        nxt.push_back(k);
-                    } else {
-                        for (int j : t.pids[k]) {
-                            if (!act[j] || j == i) continue;
-                            double ex = xp - x[j], ey = yp - y[j], ez = zp - z[j];
-                            double r2 = ex * ex + ey * ey + ez * ez;
-                            double r3 = std::sqrt(r2) * r2;
-                            vx += (ay[j] * ez - az[j] * ey) / r3;
-                            vy += (az[j] * ex - ax[j] * ez) / r3;
-                            vz += (ax[j] * ey - ay[j] * ex) / r3;
-                        }
+    return true;
+}
+
+// One target's walk (fast3DFMM.cpp:340-470): from the root's children, far
+// children (R^2 > (2 size)^2) through their moments, near leaves directly.
+void eval_target(const OctMoments& om, const double* x, const double* y, const double* z, const double* ax,
+                 const double* ay, const double* az, const uint8_t* act, int64_t i, double* out) {
+    const Oct& t = om.t;
+    const double xp = x[i], yp = y[i], zp = z[i];
+    double vx = 0, vy = 0, vz = 0;
+    std::vector<int> cur, nxt;
+    for (int o = 0; o < 8; ++o)
+        if ((t.chd_flag[0] >> o) & 1) cur.push_back(t.chd[0][o]);
+    double gx[10], gy[10], gz[10];
+    for (int lv = 1; lv < t.max_level; ++lv) {
+        nxt.clear();
+        for (int c : cur) {
+            for (int o = 0; o < 8; ++o) {
+                if (((t.chd_flag[c] >> o) & 1) == 0) continue;
+                int k = t.chd[c][o];
+                if (!t.active[k]) continue;
+                double dx = xp - t.xc[k], dy = yp - t.yc[k], dz = zp - t.zc[k];
+                double R2 = dx * dx + dy * dy + dz * dz;
+                double Rc = t.size[k] * 2.0;
+                if (R2 > Rc * Rc) {
+                    m2p_mul(R2, dx, dy, dz, gx, gy, gz);
+                    const double* Mx = &om.mx[(size_t)k * 10];
+                    const double* My = &om.my[(size_t)k * 10];
+                    const double* Mz = &om.mz[(size_t)k * 10];
+                    for (int m = 0; m < 10; ++m) {
+                        vx += My[m] * gz[m] - Mz[m] * gy[m];
+                        vy += Mz[m] * gx[m] - Mx[m] * gz[m];
+                        vz += Mx[m] * gy[m] - My[m] * gx[m];
+                    }
+                } else if (t.chd_flag[k] != 0) {
+                    nxt.push_back(k);
+                } else {
+                    for (int j : t.pids[k]) {
+                        if (!act[j] || j == i) continue;
+                        double ex = xp - x[j], ey = yp - y[j], ez = zp - z[j];
+                        double r2 = ex * ex + ey * ey + ez * ez;
+                        double r3 = std::sqrt(r2) * r2;
+                        vx += (ay[j] * ez - az[j] * ey) / r3;
+                        vy += (az[j] * ex - ax[j] * ez) / r3;
+                        vz += (ax[j] * ey - ay[j] * ex) / r3;
                     }
                 }
             }
-            cur.swap(nxt);
         }
-        u[i] = vx; v[i] = vy; w[i] = vz;
+        cur.swap(nxt);
+    }
+    out[0] = vx; out[1] = vy; out[2] = vz;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Treecode velocity (reference calcVelocityFast with every particle a target).
+int orc_fmm3d_velocity(const double* x, const double* y, const double* z,
+                       const double* ax, const double* ay, const double* az, const uint8_t* act,
+                       int64_t n, int leaf_cap, double exp_pct, double* u, double* v, double* w) {
+    OctMoments om;
+    if (!build_moments(om, x, y, z, ax, ay, az, act, n, leaf_cap, exp_pct)) return -1;
+    #pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t i = 0; i < n; ++i) {
+        double o[3];
+        eval_target(om, x, y, z, ax, ay, az, act, i, o);
+        u[i] = o[0]; v[i] = o[1]; w[i] = o[2];
+    }
+    return 0;
+}
+
+// The same treecode evaluated only at the m targets tgt[0..m-1] (the
+// reference's traversal is per target, fast3DFMM.cpp:340-470, so a sample of
+// targets gives exactly those targets' velocities).
+int orc_fmm3d_velocity_at(const double* x, const double* y, const double* z,
+                          const double* ax, const double* ay, const double* az, const uint8_t* act,
+                          int64_t n, int leaf_cap, double exp_pct, const int64_t* tgt, int64_t m,
+                          double* u, double* v, double* w) {
+    OctMoments om;
+    if (!build_moments(om, x, y, z, ax, ay, az, act, n, leaf_cap, exp_pct)) return -1;
+    #pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t k = 0; k < m; ++k) {
+        double o[3];
+        eval_target(om, x, y, z, ax, ay, az, act, tgt[k], o);
+        u[k] = o[0]; v[k] = o[1]; w[k] = o[2];
     }
     return 0;
 }
