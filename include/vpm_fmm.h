@@ -36,9 +36,12 @@ extern "C" {
 
 /* Arithmetic of the evaluation. */
 #define VPM_PREC_FP64 0    /* plain form: FP64 everywhere                           */
-#define VPM_PREC_MIXED 1   /* chosen form: FP32 near field, list-2 M2L on the tensor
-                              cores as 3xTF32 products (orders 1..20; FP64 above) */
+#define VPM_PREC_MIXED 1   /* chosen form: FP32 near field, list-2 M2L in FP32 per
+                              parent cell (orders 1..16), on the tensor cores as
+                              3xTF32 products (orders 17..20), FP64 above       */
 #define VPM_PREC_MIXED_FP64_M2L 2 /* FP32 near field, FP64 M2L (for comparisons)  */
+#define VPM_PREC_MIXED_TC 3 /* as VPM_PREC_MIXED with the list-2 M2L on the tensor
+                              cores (tcgen05, 3xTF32) at every order 1..20     */
 
 /* Binomial coefficients of the translations. */
 #define VPM_BINOM_REFERENCE 0 /* as the reference's binComb computes them in 32-bit

@@ -22,6 +22,7 @@ VPM_ETIMEDOUT = 110
 PREC_FP64 = 0
 PREC_MIXED = 1
 PREC_MIXED_FP64_M2L = 2
+PREC_MIXED_TC = 3
 BINOM_REFERENCE = 0
 BINOM_EXACT = 1
 

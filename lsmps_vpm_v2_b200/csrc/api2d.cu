@@ -92,7 +92,8 @@ int Ctx::reserve2d(int n, int cap_cells, int P, long long cap_l1, long long cap_
            o_ciy = L.take<int32_t>(C), o_cleaf = L.take<int32_t>(C);
     size_t o_cfl = L.take<uint8_t>(C), o_cmask = L.take<uint8_t>(C), o_clev = L.take<uint8_t>(C);
     size_t o_ccx = L.take<double>(C), o_ccy = L.take<double>(C), o_ccode = L.take<uint64_t>(C);
-    size_t o_leaves = L.take<int32_t>(C);
+    size_t o_leaves = L.take<int32_t>(C), o_nonleaf = L.take<int32_t>(C), o_upcnt = L.take<uint32_t>(C);
+    size_t o_l2blk = L.take<int32_t>(C * 32);
     size_t o_l2 = L.take<int32_t>(C * kList2Cap), o_l2s = L.take<uint8_t>(C * kList2Cap), o_l2n = L.take<uint8_t>(C);
     size_t o_l4 = L.take<int32_t>(C * kList4Cap), o_l4n = L.take<uint8_t>(C);
     size_t o_l1c = L.take<uint32_t>(C), o_l1o = L.take<uint32_t>(C + 1), o_l1s = L.take<int32_t>(cap_l1);
@@ -139,6 +140,9 @@ int Ctx::reserve2d(int n, int cap_cells, int P, long long cap_l1, long long cap_
     tree.c_flags = (uint8_t*)P_(o_cfl); tree.c_chmask = (uint8_t*)P_(o_cmask); tree.c_level = (uint8_t*)P_(o_clev);
     tree.c_cx = (double*)P_(o_ccx); tree.c_cy = (double*)P_(o_ccy); tree.c_code = (uint64_t*)P_(o_ccode);
     tree.leaf_cells = (int32_t*)P_(o_leaves);
+    tree.nonleaf = (int32_t*)P_(o_nonleaf);
+    tree.c_upcnt = (uint32_t*)P_(o_upcnt);
+    lists.l2_blk = (int32_t*)P_(o_l2blk);
     tree.geom = (Geom2D*)P_(o_geom); tree.info = (TreeInfo2D*)P_(o_info);
     tree.dense = (int32_t*)P_(o_dense);
     tree.gbar = ts.lvl_ticket + kBarrierWordsAt;
@@ -190,7 +194,8 @@ int Ctx::check_params(const vpm_fmm_params* prm, vpm_fmm_params& out) {
     if (out.max_src < 0 || out.max_par < 1) return fail(VPM_EINVAL, "leaf caps must be max_src >= 0, max_par >= 1");
     if (out.max_depth != 16 && out.max_depth != 31) out.max_depth = 16;
     if (!(out.exp_tree_pct >= 0.0) || !std::isfinite(out.exp_tree_pct)) return fail(VPM_EINVAL, "exp_tree_pct");
-    if (out.precision != VPM_PREC_FP64 && out.precision != VPM_PREC_MIXED && out.precision != VPM_PREC_MIXED_FP64_M2L)
+    if (out.precision != VPM_PREC_FP64 && out.precision != VPM_PREC_MIXED && out.precision != VPM_PREC_MIXED_FP64_M2L &&
+        out.precision != VPM_PREC_MIXED_TC)
         return fail(VPM_EINVAL, "precision");
     return VPM_OK;
 }
@@ -232,7 +237,7 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
         VPM_CUDA_TRY(cudaStreamWaitEvent(side, fork2, 0));
         VPM_CUDA_TRY(build_int_lists2d(tree, lists, ts.scan, p.eps, d_err, side, &launches));
         VPM_CUDA_TRY(cudaEventRecord(ev_l13, side));
-        if (p.precision == VPM_PREC_MIXED || p.precision == VPM_PREC_MIXED_FP64_M2L)
+        if (p.precision != VPM_PREC_FP64)
             VPM_CUDA_TRY(fmm2d_p2p_f32(tree, lists, ex2, near_x, near_y, 0, 0.0, 0.0, d_err, side, &launches, true));
         else
             VPM_CUDA_TRY(fmm2d_p2p_f64_tma(tree, lists, ex2, (double4*)mixed_base, near_x, near_y, 0, 0.0, 0.0, d_err,
@@ -241,19 +246,14 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
         VPM_CUDA_TRY(cudaStreamWaitEvent(side2, fork2, 0));
         VPM_CUDA_TRY(build_ext_lists2d(tree, lists, p.eps, d_err, side2, &launches));
         VPM_CUDA_TRY(cudaEventRecord(join3, side2));
-        VPM_CUDA_TRY(fmm2d_upward(tree, ex2, p.p, d_err, st, &launches));
+        VPM_CUDA_TRY(fmm2d_upward_direct(tree, ex2, p.p, p.binom == VPM_BINOM_EXACT, d_err, st, &launches));
         VPM_CUDA_TRY(cudaEventRecord(ev_up, st));
         VPM_CUDA_TRY(cudaStreamWaitEvent(side2, ev_up, 0));
         VPM_CUDA_TRY(cudaStreamWaitEvent(side2, ev_l13, 0));
         VPM_CUDA_TRY(fmm2d_m2p(tree, lists, ex2, p.p, d_err, side2, &launches));
         VPM_CUDA_TRY(cudaEventRecord(join4, side2));
         VPM_CUDA_TRY(cudaStreamWaitEvent(st, join3, 0));
-        if (p.precision == VPM_PREC_MIXED && m2l_f32_supported(p.p))
-            VPM_CUDA_TRY(fmm2d_m2l_f32(tree, lists, ex2, p.p, tc_rows, tc_ops, d_err, st, &launches));
-        else if (p.precision == VPM_PREC_MIXED && m2l_tc_supported(p.p))
-            VPM_CUDA_TRY(fmm2d_m2l_tc(tree, lists, ex2, p.p, tc_rows, tc_ops, d_err, st, &launches));
-        else
-            VPM_CUDA_TRY(fmm2d_m2l_only(tree, lists, ex2, p.p, d_err, st, &launches));
+        if (int r = enqueue_m2l(p, st, &launches)) return r;
         if (l2l_direct_ok(p.p, p.binom == VPM_BINOM_EXACT))
             VPM_CUDA_TRY(fmm2d_l2l_leaves(tree, ex2, p.p, d_err, st, &launches));
         else
@@ -274,14 +274,10 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
         for (int i = 4; i < kStageEvents; ++i)
             if (int r = record(i)) return r;
     } else {
-        VPM_CUDA_TRY(fmm2d_upward(tree, ex2, p.p, d_err, st, &launches));
+        VPM_CUDA_TRY(fmm2d_upward_direct(tree, ex2, p.p, p.binom == VPM_BINOM_EXACT, d_err, st, &launches));
         if (int r = record(4)) return r;
-        if (p.precision == VPM_PREC_MIXED && velocity != kModePotential && m2l_f32_supported(p.p))
-            VPM_CUDA_TRY(fmm2d_m2l_f32(tree, lists, ex2, p.p, tc_rows, tc_ops, d_err, st, &launches));
-        else if (p.precision == VPM_PREC_MIXED && velocity != kModePotential && m2l_tc_supported(p.p))
-            VPM_CUDA_TRY(fmm2d_m2l_tc(tree, lists, ex2, p.p, tc_rows, tc_ops, d_err, st, &launches));
-        else
-            VPM_CUDA_TRY(fmm2d_m2l_only(tree, lists, ex2, p.p, d_err, st, &launches));
+        if (velocity == kModePotential) VPM_CUDA_TRY(fmm2d_m2l_only(tree, lists, ex2, p.p, d_err, st, &launches));
+        else if (int r = enqueue_m2l(p, st, &launches)) return r;
         if (velocity == kModePotential) VPM_CUDA_TRY(fmm2d_m2l_b0(tree, lists, ex2, p.p, d_err, st, &launches));
         if (int r = record(5)) return r;
         if (l2l_direct_ok(p.p, p.binom == VPM_BINOM_EXACT))
@@ -298,7 +294,7 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
             if (int r = record(7)) return r;
         }
         if (velocity == kModePotential) {
-        } else if (p.precision == VPM_PREC_MIXED || p.precision == VPM_PREC_MIXED_FP64_M2L) {
+        } else if (p.precision != VPM_PREC_FP64) {
             VPM_CUDA_TRY(fmm2d_p2p_f32(tree, lists, ex2, o0, o1, velocity, uinf, vinf, d_err, st, &launches));
         } else {
             VPM_CUDA_TRY(fmm2d_p2p_f64_tma(tree, lists, ex2, (double4*)mixed_base, o0, o1, velocity, uinf, vinf, d_err,
@@ -313,6 +309,23 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
     return VPM_OK;
 }
 
+// M2L of lists 2 and 4 for the precision setting: the mixed form per parent
+// on the FP32 pipes (orders 1..16), the tensor-core variants for
+// VPM_PREC_MIXED_TC (per parent, orders 1..16) and for the mixed orders 17..20
+// (per offset), FP64 otherwise.
+int Ctx::enqueue_m2l(const vpm_fmm_params& p, cudaStream_t st, int* launches) {
+    const bool exact = p.binom == VPM_BINOM_EXACT;
+    if (p.precision == VPM_PREC_MIXED && m2l_parent_f32_supported(p.p))
+        VPM_CUDA_TRY(fmm2d_m2l_parent_f32(tree, lists, ex2, p.p, exact, d_err, st, launches));
+    else if (p.precision == VPM_PREC_MIXED_TC && m2l_parent_supported(p.p))
+        VPM_CUDA_TRY(fmm2d_m2l_parent(tree, lists, ex2, p.p, tc_rows, tc_ops, d_err, st, launches));
+    else if ((p.precision == VPM_PREC_MIXED || p.precision == VPM_PREC_MIXED_TC) && m2l_tc_supported(p.p))
+        VPM_CUDA_TRY(fmm2d_m2l_tc(tree, lists, ex2, p.p, tc_rows, tc_ops, d_err, st, launches));
+    else
+        VPM_CUDA_TRY(fmm2d_m2l_only(tree, lists, ex2, p.p, d_err, st, launches));
+    return VPM_OK;
+}
+
 // Translation coefficients, list-2 operators (FP64 and tensor-core forms) of
 // order p.p on this context's arena; uploaded when the order, the binomials
 // or the arena changed. The uploads synchronise the stream, so callers that
@@ -322,7 +335,7 @@ int Ctx::ensure_coefs(const vpm_fmm_params& p) {
     if (capturing) return fail(VPM_EINVAL, "coefficient upload inside a graph capture");
     VPM_CUDA_TRY(set_coefficients2d(p.p, p.binom == VPM_BINOM_EXACT, ex2.coef, stream));
     VPM_CUDA_TRY(set_m2l_operators2d(p.p, p.binom == VPM_BINOM_EXACT, ex2.op, stream));
-    if (m2l_f32_supported(p.p)) VPM_CUDA_TRY(set_m2l_f32_operators(p.p, ex2.op, tc_ops, stream));
+    if (m2l_parent_supported(p.p)) VPM_CUDA_TRY(set_m2l_parent_operators(p.p, ex2.op, tc_ops, stream));
     else if (m2l_tc_supported(p.p)) VPM_CUDA_TRY(set_m2l_tc_operators(p.p, ex2.op, tc_ops, stream));
     coef_P = p.p;
     coef_binom = p.binom;

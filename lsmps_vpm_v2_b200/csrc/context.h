@@ -153,6 +153,7 @@ struct Ctx {
     int count_interactions(vpm_fmm_stats* s);
     int fetch_tree(HostTree2D& h);
     int ensure_coefs(const vpm_fmm_params& p);
+    int enqueue_m2l(const vpm_fmm_params& p, cudaStream_t st, int* launches);
     int launch2d(const double* x, const double* y, const double* q, const uint8_t* act, int n,
                  const vpm_fmm_params& p, int K, double* o0, double* o1, int velocity, double uinf, double vinf);
     int reserve3d(int n, int cap_cells);

@@ -40,7 +40,8 @@ struct TreeInfo2D {
     int depth;           // deepest level holding a cell
     int min_leaf_level;
     int max_leaf_level;
-    int pad;
+    int l2_irregular;    // 1 when some list-2 decision is not the integer-offset rule (cells so
+                         // small that the distance tolerance matters): the per-parent M2L is off
     unsigned long long list1_len, list3_len;     // CSR totals
     unsigned long long p2p_pairs, m2l_pairs, m2p_pairs;
 };
@@ -63,6 +64,12 @@ struct Tree2D {
     double *c_cx, *c_cy;
     uint64_t* c_code;
     int32_t* leaf_cells;
+    // Non-leaf cells in cell order (level-major, Morton within a level; the
+    // root first): n_cells - n_leaves entries, or nullptr (not recorded).
+    int32_t* nonleaf;
+    // Per cell: children whose multipole is final (upward pass), zeroed by the
+    // tree build for every cell it emits; nullptr: not kept.
+    uint32_t* c_upcnt;
     // Dense lookup grid: dense[reference cell ID] = cell index for levels
     // <= dense_levels (nullptr: none). Entries are never cleared: a lookup
     // accepts an entry only if that cell has the queried level and index.
@@ -100,6 +107,13 @@ struct Lists2D {
     uint32_t* l3_cnt;
     uint32_t* l3_off;
     int32_t* l3_src;     // [cap_l3]
+    // [cap_cells][32] per non-leaf cell P (indexed by P): the list-2 candidates
+    // of P's children, child d of P's k-th neighbour (k = 0..7 without P itself,
+    // the reference's neighbour order) at entry 4 k + d, or -1 where that cell
+    // is missing, inactive or its parent is a leaf or inactive; written by the
+    // first child of P. Every list 2 of a child of P is the subset of these
+    // entries separated from it (nullptr: not recorded).
+    int32_t* l2_blk;
     int32_t* l1_slot;    // [cap_leaves][kListSlot1] one-pass staging of list 1 (nullptr: two passes)
     int32_t* l3_slot;    // [cap_leaves][kListSlot3]
     int cap_leaves;
@@ -186,6 +200,13 @@ struct Expansions2D {
 };
 
 cudaError_t fmm2d_upward(const Tree2D& t, Expansions2D& e, int P, unsigned* err, cudaStream_t st, int* launches);
+// The same moments without a level loop (cells of up to 1024 particles
+// straight from their particles, the larger ones by M2M in the warp that
+// finishes their last child, counted in t.c_upcnt) when upward_direct_ok;
+// else fmm2d_upward.
+bool upward_direct_ok(int P, bool exact);
+cudaError_t fmm2d_upward_direct(const Tree2D& t, Expansions2D& e, int P, bool exact, unsigned* err, cudaStream_t st,
+                                int* launches);
 cudaError_t fmm2d_m2l(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, unsigned* err, cudaStream_t st,
                       int* launches);  // M2L followed by the L2L levels
 // Potential (fmm2D::calcPotential): b_0 of the M2L after fmm2d_m2l_only, then
@@ -206,6 +227,18 @@ bool m2l_f32_supported(int P);
 cudaError_t set_m2l_f32_operators(int P, const double2* op_dev, float* dst, cudaStream_t st);
 cudaError_t fmm2d_m2l_f32(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, float* rows, const float* ops,
                           unsigned* err, cudaStream_t st, int* launches);
+// List-2 M2L of the mixed form per parent (m2l_tc.cu, m2l_parent_tc): one
+// tensor-core product over all non-leaf cells, orders 1..16; list 4 in FP64.
+bool m2l_parent_supported(int P);
+// The same per-parent list-2 M2L on the FP32 pipes through the operator's
+// diagonal-real-diagonal structure (m2l_parent_f32), orders 1..16; list 4 in
+// FP64.
+bool m2l_parent_f32_supported(int P);
+cudaError_t fmm2d_m2l_parent_f32(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, bool exact,
+                                 unsigned* err, cudaStream_t st, int* launches);
+cudaError_t set_m2l_parent_operators(int P, const double2* op_dev, float* dst, cudaStream_t st);
+cudaError_t fmm2d_m2l_parent(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, float* rows,
+                             const float* ops, unsigned* err, cudaStream_t st, int* launches);
 bool m2l_tc_supported(int P);
 size_t m2l_tc_rows_bytes(int cap_cells);
 size_t m2l_tc_ops_bytes();

@@ -1372,6 +1372,151 @@ cudaError_t set_coefficients2d(int P, bool exact, double* dst, cudaStream_t st) 
     return cudaStreamSynchronize(st);
 }
 
+// ---- upward pass without a level loop ---------------------------------------
+//
+// The multipole of any cell is a_k = sum of q_j (z_j - z_c)^k over the active
+// particles of its subtree (P2M at a leaf, fmm2D.cpp:237-284), and M2M
+// (fmm2D.cpp:309-379) shifts the children's moments with the binomial
+// coefficients C(p, k) = C(p-1, k-1) p / k, which gives the same moments
+// whenever those coefficients are exact (orders up to 18 with the reference's
+// 32-bit binComb, any order with exact binomials). Every cell covers a
+// contiguous range of the sorted particles, so a cell of at most kDirectMax
+// particles takes its moments straight from that range: one warp per cell,
+// all levels at once, no ordering between cells. A larger cell (the top of
+// the tree, about n / kDirectMax cells per level) is computed by M2M as soon
+// as its children are final: each finished cell counts itself into its
+// parent's c_upcnt, and the warp that completes the count computes the
+// parent, then does the same one level up. Sums run in a fixed order (lane
+// order over the particles, then lanes in order; children in child order):
+// the result does not depend on which warp finishes last.
+constexpr int kUpWarps = 8;
+constexpr int kDirectMax = 1024;
+constexpr int kUpMaxP = 18;
+
+template <int P>
+__global__ void __launch_bounds__(32 * kUpWarps)
+upward_direct2d(Tree2D t, double2* __restrict__ a, const double* __restrict__ coef, unsigned* err) {
+    constexpr int Q = P + 1, CS = 2 * Q + 1;   // components per lane, padded row stride
+    extern __shared__ double up_sm[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    double* red = up_sm + (size_t)wib * 32 * CS;   // [lane][component]; M2M: children's moments
+    if (fatal(err)) return;
+    const double* g_m2m = coef + kCoefM2M;
+    const int c_begin = t.info->level_start[1], c_end = t.info->n_cells;
+    const int nw = gridDim.x * kUpWarps;
+    for (int c = c_begin + blockIdx.x * kUpWarps + wib; c < c_end; c += nw) {
+        const int lo = t.c_lo[c], hi = t.c_hi[c];
+        const uint8_t f = t.c_flags[c];
+        if (hi - lo > kDirectMax && !(f & CELL_LEAF)) continue;   // by M2M once its children are final
+        double re[Q], im[Q];
+        #pragma unroll
+        for (int k = 0; k < Q; ++k) re[k] = im[k] = 0.0;
+        if (f & CELL_ACTIVE) {
+            const double zx = t.c_cx[c], zy = t.c_cy[c];
+            for (int j = lo + lane; j < hi; j += 32) {
+                if (!t.pact[j]) continue;
+                const double wx = t.px[j] - zx, wy = t.py[j] - zy;
+                double pr = t.pq[j], pi = 0.0;
+                re[0] += pr;
+                #pragma unroll
+                for (int k = 1; k < Q; ++k) {
+                    const double nr = pr * wx - pi * wy, ni = pr * wy + pi * wx;
+                    pr = nr;
+                    pi = ni;
+                    re[k] += pr;
+                    im[k] += pi;
+                }
+            }
+        }
+        #pragma unroll
+        for (int k = 0; k < Q; ++k) {
+            red[lane * CS + 2 * k] = re[k];
+            red[lane * CS + 2 * k + 1] = im[k];
+        }
+        __syncwarp();
+        for (int comp = lane; comp < 2 * Q; comp += 32) {
+            double sum = 0.0;
+            for (int l = 0; l < 32; ++l) sum += red[l * CS + comp];
+            reinterpret_cast<double*>(a + (size_t)c * Q)[comp] = sum;
+        }
+        __syncwarp();
+        // count this cell into its ancestors while this warp completes them
+        int cur = c;
+        while (true) {
+            const int par = t.c_parent[cur];
+            if (par <= 0) break;                                       // the root's moments are never used
+            if (t.c_hi[par] - t.c_lo[par] <= kDirectMax) break;       // computed directly
+            __threadfence();                                           // cur's moments before the count
+            unsigned done = 0;
+            if (lane == 0) done = atomicAdd(&t.c_upcnt[par], 1u) + 1u;
+            done = __shfl_sync(0xffffffffu, done, 0);
+            const unsigned m = t.c_chmask[par];
+            const int nch = __popc(m);
+            if ((int)done != nch) break;                               // another child completes it
+            __threadfence();
+            // M2M of par: lane k < Q, a_k = sum over children of a_0 t^k + sum_m m2m[k][m] a_m t^(k-m)
+            const int ch0 = t.c_child0[par];
+            double2* sm = reinterpret_cast<double2*>(red);             // [child][Q]
+            for (int i = lane; i < nch * Q; i += 32) sm[i] = __ldcg(a + (size_t)ch0 * Q + i);
+            __syncwarp();
+            double2 acc = make_double2(0.0, 0.0);
+            if (lane < Q && (t.c_flags[par] & CELL_ACTIVE)) {
+                const double pcx = t.c_cx[par], pcy = t.c_cy[par];
+                double2 S[4], tt[4];
+                #pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    const int ch = ch0 + (r < nch ? r : 0);
+                    tt[r] = make_double2(t.c_cx[ch] - pcx, t.c_cy[ch] - pcy);
+                    S[r] = sm[(r < nch ? r : 0) * Q];
+                }
+                for (int mm = 1; mm <= lane; ++mm) {
+                    const double cf = g_m2m[lane * W + mm];
+                    #pragma unroll
+                    for (int r = 0; r < 4; ++r)
+                        if (r < nch) S[r] = cfma(S[r], tt[r], cscale(sm[r * Q + mm], cf));
+                }
+                #pragma unroll
+                for (int r = 0; r < 4; ++r)
+                    if (r < nch) acc = cadd(acc, S[r]);
+            }
+            if (lane < Q) a[(size_t)par * Q + lane] = acc;
+            __syncwarp();
+            cur = par;
+        }
+    }
+}
+
+bool upward_direct_ok(int P, bool exact) { return P >= 1 && P <= kUpMaxP && (exact || P <= 18); }
+static_assert(kUpMaxP <= 18, "the reference's 32-bit M2M binomials wrap from order 19");
+
+template <int P>
+cudaError_t launch_upward_direct(const Tree2D& t, Expansions2D& e, unsigned* err, cudaStream_t st) {
+    const size_t smem = sizeof(double) * kUpWarps * 32 * (2 * (P + 1) + 1);
+    cudaError_t r = cudaFuncSetAttribute(upward_direct2d<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (r != cudaSuccess) return r;
+    upward_direct2d<P><<<148 * 4, 32 * kUpWarps, smem, st>>>(t, e.a, e.coef, err);
+    return cudaGetLastError();
+}
+
+// Upward pass of orders the direct form covers (upward_direct_ok): one launch.
+// Otherwise the P2M + M2M level loop below.
+cudaError_t fmm2d_upward_direct(const Tree2D& t, Expansions2D& e, int P, bool exact, unsigned* err, cudaStream_t st,
+                                int* launches) {
+    if (!upward_direct_ok(P, exact) || !t.c_upcnt) return fmm2d_upward(t, e, P, err, st, launches);
+    cudaError_t r;
+    switch (P) {
+#define VPM_UP_CASE(PP) \
+    case PP: r = launch_upward_direct<PP>(t, e, err, st); break;
+        VPM_UP_CASE(1) VPM_UP_CASE(2) VPM_UP_CASE(3) VPM_UP_CASE(4) VPM_UP_CASE(5) VPM_UP_CASE(6)
+        VPM_UP_CASE(7) VPM_UP_CASE(8) VPM_UP_CASE(9) VPM_UP_CASE(10) VPM_UP_CASE(11) VPM_UP_CASE(12)
+        VPM_UP_CASE(13) VPM_UP_CASE(14) VPM_UP_CASE(15) VPM_UP_CASE(16) VPM_UP_CASE(17) VPM_UP_CASE(18)
+#undef VPM_UP_CASE
+        default: return fmm2d_upward(t, e, P, err, st, launches);
+    }
+    *launches += 1;
+    return r;
+}
+
 // Upward pass: P2M of every active leaf, then M2M level by level from the
 // deepest possible level up to level 1 (levels below the tree's depth exit
 // at once; the launch count does not depend on the data, so the sequence can

@@ -437,7 +437,7 @@ __global__ void int_list_kernel(Tree2D t, double eps, int mode, Lists2D l, unsig
 // which lane 0 then runs exactly as the reference does (it is empty for most
 // cells).
 __device__ void ext_list_warp(const TreeView& v, int c, double eps, int32_t* l2, uint8_t* slot, uint8_t* n2,
-                              int32_t* l4, uint8_t* n4, int* s_e, unsigned* err) {
+                              int32_t* l4, uint8_t* n4, int32_t* blk, int* s_e, unsigned* err) {
     const Tree2D& t = v.t;
     const int lane = threadIdx.x & 31;
     const int L = t.c_level[c], cx = t.c_ix[c], cy = t.c_iy[c];
@@ -456,16 +456,27 @@ __device__ void ext_list_warp(const TreeView& v, int c, double eps, int32_t* l2,
     const bool open = e >= 0 && (f & CELL_ACTIVE) && !(f & CELL_LEAF);
     // list 2: child d of an open neighbour, active and separated from c
     bool take = false;
-    int ch = -1;
+    int ch = -1, cand = -1;
     if (open) {
         const unsigned m = t.c_chmask[e];
         if (m & (1u << d)) {
             ch = t.c_child0[e] + __popc(m & ((1u << d) - 1u));
             if (t.c_flags[ch] & CELL_ACTIVE) {
+                cand = ch;
                 const double min2 = xadd(cur_len, eps);
                 take = (fabs(xsub(t.c_cx[ch], ccx)) > min2) || (fabs(xsub(t.c_cy[ch], ccy)) > min2);
             }
         }
+    }
+    // the candidates of the parent's children, once per parent (by its first child)
+    if (blk && c == t.c_child0[p]) blk[(size_t)p * 32 + lane] = cand;
+    // The per-parent M2L of the mixed form takes list 2 to be the candidates
+    // at an integer offset of 2 or more on some axis; flag a tree where the
+    // tolerance of the separation test decides otherwise.
+    {
+        const int ox = 2 * jx + (d & 1) - cx, oy = 2 * jy + (d >> 1) - cy;
+        const bool far = ox <= -2 || ox >= 2 || oy <= -2 || oy >= 2;
+        if (__any_sync(0xffffffffu, cand >= 0 && take != far) && lane == 0) atomicOr(&t.info->l2_irregular, 1);
     }
     const unsigned tb = __ballot_sync(0xffffffffu, take);
     if (take) {
@@ -536,7 +547,7 @@ __global__ void __launch_bounds__(128) ext_list_kernel(Tree2D t, double eps, Lis
         }
     for (int i = c0 + blockIdx.x * 4 + wib; i < c1; i += warps)
         ext_list_warp(v, i, eps, l.l2_src + (size_t)i * kList2Cap, l.l2_slot + (size_t)i * kList2Cap, &l.l2_n[i],
-                      l.l4_src + (size_t)i * kList4Cap, &l.l4_n[i], s_e[wib], err);
+                      l.l4_src + (size_t)i * kList4Cap, &l.l4_n[i], l.l2_blk, s_e[wib], err);
     (void)lane;
 }
 

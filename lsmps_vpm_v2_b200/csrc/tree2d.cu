@@ -758,6 +758,7 @@ __global__ void flat_totals(Tree2D t, const uint32_t* __restrict__ level_tot, un
     info->n_cells = cells;
     info->n_leaves = leaves;
     info->depth = depth;
+    info->l2_irregular = 0;
     // leaf level range (TreeCell::min_level / max_level, treeCell.cpp:1236-1240)
     int mn = -1, mx = -1;
     for (int L = 1; L <= K; ++L) {
@@ -786,6 +787,8 @@ __global__ void flat_totals(Tree2D t, const uint32_t* __restrict__ level_tot, un
     t.c_cx[0] = xadd(g->pivx, xmul(0.5, g->root));
     t.c_cy[0] = xadd(g->pivy, xmul(0.5, g->root));
     if (t.dense) t.dense[0] = 0;
+    if (t.nonleaf && cells > 1) t.nonleaf[0] = 0;
+    if (t.c_upcnt) t.c_upcnt[0] = 0u;
 }
 
 // Cell records (and leaf entries) of every particle's cell levels, indices
@@ -850,16 +853,19 @@ flat_emit(Tree2D t, const uint32_t* __restrict__ pinfo, const uint32_t* __restri
             t.c_ix[ci] = ix;
             t.c_iy[ci] = iy;
             t.c_code[ci] = code;
+            if (t.c_upcnt) t.c_upcnt[ci] = 0u;
             t.c_cx[ci] = xadd(pivx, xmul(xadd(0.5, (double)ix), len));
             t.c_cy[ci] = xadd(pivy, xmul(xadd(0.5, (double)iy), len));
             if (t.dense && L <= t.dense_levels) t.dense[start_id2(L) + ix + ((int64_t)iy << L)] = ci;
+            // leaves before this cell: of the lower levels, then of this level
+            const int li = info->leaf_start[L] + (int)tile_cnt[(size_t)(kMaxLevels2D + 1 + L) * tiles + tile] + bl +
+                           __popc(ml & below);
             if (lf) {
-                const int li = info->leaf_start[L] + (int)tile_cnt[(size_t)(kMaxLevels2D + 1 + L) * tiles + tile] + bl +
-                               __popc(ml & below);
                 t.c_leafidx[ci] = li;
                 t.leaf_cells[li] = ci;
             } else {
                 t.c_leafidx[ci] = -1;
+                if (t.nonleaf) t.nonleaf[ci - li] = ci;   // the cells before it that are not leaves
             }
         }
         __syncthreads();
