@@ -235,13 +235,30 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
         // writes the output.
         VPM_CUDA_TRY(cudaEventRecord(fork2, st));
         VPM_CUDA_TRY(cudaStreamWaitEvent(side, fork2, 0));
-        VPM_CUDA_TRY(build_int_lists2d(tree, lists, ts.scan, p.eps, d_err, side, &launches));
-        VPM_CUDA_TRY(cudaEventRecord(ev_l13, side));
-        if (p.precision != VPM_PREC_FP64)
-            VPM_CUDA_TRY(fmm2d_p2p_f32(tree, lists, ex2, near_x, near_y, 0, 0.0, 0.0, d_err, side, &launches, true));
-        else
-            VPM_CUDA_TRY(fmm2d_p2p_f64_tma(tree, lists, ex2, (double4*)mixed_base, near_x, near_y, 0, 0.0, 0.0, d_err,
-                                           side, &launches, p.max_par, true));
+        const bool slots = p.precision != VPM_PREC_FP64 && int_lists_slotted(lists);
+        if (slots) {
+            // the mixed near field starts from the list slots; the CSR (for
+            // list 3 and the few leaves that outgrew their slots) is built on a
+            // third side stream meanwhile
+            VPM_CUDA_TRY(build_int_slots2d(tree, lists, p.eps, d_err, side, &launches));
+            VPM_CUDA_TRY(cudaEventRecord(ev_slots, side));
+            VPM_CUDA_TRY(fmm2d_p2p_f32(tree, lists, ex2, near_x, near_y, 0, 0.0, 0.0, d_err, side, &launches, true,
+                                       kP2PListSlots));
+            VPM_CUDA_TRY(cudaStreamWaitEvent(side3, ev_slots, 0));
+            VPM_CUDA_TRY(build_int_csr2d(tree, lists, ts.scan, p.eps, d_err, side3, &launches));
+            VPM_CUDA_TRY(cudaEventRecord(ev_l13, side3));
+            VPM_CUDA_TRY(fmm2d_p2p_f32(tree, lists, ex2, near_x, near_y, 0, 0.0, 0.0, d_err, side3, &launches, true,
+                                       kP2PListSpill));
+            VPM_CUDA_TRY(cudaEventRecord(join5, side3));
+        } else {
+            VPM_CUDA_TRY(build_int_lists2d(tree, lists, ts.scan, p.eps, d_err, side, &launches));
+            VPM_CUDA_TRY(cudaEventRecord(ev_l13, side));
+            if (p.precision != VPM_PREC_FP64)
+                VPM_CUDA_TRY(fmm2d_p2p_f32(tree, lists, ex2, near_x, near_y, 0, 0.0, 0.0, d_err, side, &launches, true));
+            else
+                VPM_CUDA_TRY(fmm2d_p2p_f64_tma(tree, lists, ex2, (double4*)mixed_base, near_x, near_y, 0, 0.0, 0.0,
+                                               d_err, side, &launches, p.max_par, true));
+        }
         VPM_CUDA_TRY(cudaEventRecord(join2, side));
         VPM_CUDA_TRY(cudaStreamWaitEvent(side2, fork2, 0));
         VPM_CUDA_TRY(build_ext_lists2d(tree, lists, p.eps, d_err, side2, &launches));
@@ -260,6 +277,7 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
             VPM_CUDA_TRY(fmm2d_l2l(tree, ex2, p.p, d_err, st, &launches));
         VPM_CUDA_TRY(cudaStreamWaitEvent(st, join2, 0));
         VPM_CUDA_TRY(cudaStreamWaitEvent(st, join4, 0));
+        if (slots) VPM_CUDA_TRY(cudaStreamWaitEvent(st, join5, 0));
         VPM_CUDA_TRY(fmm2d_eval_combine(tree, lists, ex2, p.p, near_x, near_y, o0, o1, velocity, uinf, vinf, d_err, st,
                                         &launches, true));
         last_launches = launches;

@@ -47,10 +47,11 @@ Ctx::~Ctx() {
     if (own_stream) cudaStreamDestroy(own_stream);
     if (side) cudaStreamDestroy(side);
     if (side2) cudaStreamDestroy(side2);
+    if (side3) cudaStreamDestroy(side3);
     if (join3) cudaEventDestroy(join3);
     if (fork2) cudaEventDestroy(fork2);
     if (join2) cudaEventDestroy(join2);
-    for (cudaEvent_t x : {ev_up, ev_l13, join4})
+    for (cudaEvent_t x : {ev_up, ev_l13, join4, ev_slots, join5})
         if (x) cudaEventDestroy(x);
 }
 
@@ -65,6 +66,7 @@ int Ctx::init(int dev) {
     stream = own_stream;
     e = cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&side2, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&side3, cudaStreamNonBlocking);
     if (e != cudaSuccess) return fail_cuda(e, "cudaStreamCreate");
     e = cudaEventCreateWithFlags(&fork2, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&join2, cudaEventDisableTiming);
@@ -72,6 +74,8 @@ int Ctx::init(int dev) {
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_up, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_l13, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&join4, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_slots, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&join5, cudaEventDisableTiming);
     if (e != cudaSuccess) return fail_cuda(e, "cudaEventCreate");
     e = cudaMalloc(&d_err, 64);
     if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc");

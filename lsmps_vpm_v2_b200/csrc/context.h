@@ -54,6 +54,8 @@ struct Ctx {
     cudaStream_t side2 = nullptr;   // lists 2/4 while the main stream runs P2M + M2M
     cudaEvent_t fork2 = nullptr, join2 = nullptr, join3 = nullptr;
     cudaEvent_t ev_up = nullptr, ev_l13 = nullptr, join4 = nullptr;   // upward done, lists 1/3 done, M2P done
+    cudaStream_t side3 = nullptr;   // CSR of lists 1/3 while the near field runs from the slots
+    cudaEvent_t ev_slots = nullptr, join5 = nullptr;   // list slots done, near field of spilled leaves done
     double *near_x = nullptr, *near_y = nullptr;
     std::string last_error;
     unsigned* d_err = nullptr;
@@ -178,10 +180,14 @@ struct Ctx {
 };
 
 // FP32 P2P of the mixed form (packed FP32x2, warp per leaf); near_only: the
-// near field alone in tree order into out0/out1.
+// near field alone in tree order into out0/out1. lists: where list 1 comes
+// from: the CSR (kP2PListCsr), the fixed slots of the one-pass list build
+// (kP2PListSlots: leaves whose list outgrew them are skipped) or, for exactly
+// those leaves, the CSR (kP2PListSpill). Every leaf sums its sources in the
+// same order whichever source is used.
 cudaError_t fmm2d_p2p_f32(const Tree2D& t, const Lists2D& l, const Expansions2D& e, double* out0, double* out1,
                           int velocity, double u_inf, double v_inf, unsigned* err, cudaStream_t st, int* launches,
-                          bool near_only = false);
+                          bool near_only = false, int lists = kP2PListCsr);
 // FP64 P2P on an AoS copy of the particles (`aos`, n entries); kernel choice as
 // for fmm2d_p2p_f32.
 cudaError_t fmm2d_p2p_f64_tma(const Tree2D& t, const Lists2D& l, const Expansions2D& e, double4* aos, double* out0,

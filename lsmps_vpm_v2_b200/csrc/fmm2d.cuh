@@ -120,6 +120,11 @@ struct Lists2D {
     long long cap_l1, cap_l3;
 };
 
+// Where a near-field kernel reads list 1 from: the CSR, the fixed slots of the
+// one-pass build (leaves with more entries than kListSlot1 skipped), or the
+// CSR for exactly those leaves.
+constexpr int kP2PListCsr = 0, kP2PListSlots = 1, kP2PListSpill = 2;
+
 // Scratch of the tree build.
 constexpr int kBBoxBlocks = 296;
 constexpr int kFlatTile = 256;   // particles per block of the flat tree build
@@ -171,6 +176,13 @@ cudaError_t build_ext_lists2d(const Tree2D& t, Lists2D& l, double eps, unsigned*
                               int* launches);
 cudaError_t build_int_lists2d(const Tree2D& t, Lists2D& l, ScanScratch& scan, double eps, unsigned* err,
                               cudaStream_t st, int* launches);
+// The two halves of build_int_lists2d with fixed slots (l.l1_slot, l.l3_slot):
+// counts and the first kListSlot1 / kListSlot3 entries of every leaf; then
+// the CSR (scans, compaction, the leaves that outgrew their slots, totals).
+bool int_lists_slotted(const Lists2D& l);
+cudaError_t build_int_slots2d(const Tree2D& t, Lists2D& l, double eps, unsigned* err, cudaStream_t st, int* launches);
+cudaError_t build_int_csr2d(const Tree2D& t, Lists2D& l, ScanScratch& scan, double eps, unsigned* err,
+                            cudaStream_t st, int* launches);
 // Lists 1-4 (count, scan, fill). Requires the tree on `st`.
 cudaError_t build_lists2d(const Tree2D& t, Lists2D& l, ScanScratch& scan, double eps, unsigned* err,
                           cudaStream_t st, int* launches);

@@ -1152,8 +1152,8 @@ __device__ __forceinline__ void tile_pairs(const ulonglong2* xy, const uint64_t*
 __device__ __forceinline__ float leaf_unit(double x, double c, double ih) { return (float)((x - c) * ih); }
 
 template <int M>
-__device__ __forceinline__ void tile_chunk(TileShared& sm, const Tree2D& t, const Lists2D& l, int c, double ccx,
-                                           double ccy, double ih, uint32_t o1, int n1, int tb, int T, int hs,
+__device__ __forceinline__ void tile_chunk(TileShared& sm, const Tree2D& t, const int32_t* __restrict__ src1, int c,
+                                           double ccx, double ccy, double ih, int n1, int tb, int T, int hs,
                                            const double* fx, const double* fy, double* out0, double* out1,
                                            int velocity, double u_inf, double v_inf, unsigned* err) {
     constexpr int MP = M / 2;
@@ -1212,7 +1212,7 @@ __device__ __forceinline__ void tile_chunk(TileShared& sm, const Tree2D& t, cons
             for (int h = 0; h < 2; ++h) {
                 const int k = lane + 32 * h;
                 if (k < nseg) {
-                    const int sc = l.l1_src[o1 + seg + k];
+                    const int sc = src1[seg + k];
                     const int slo = t.c_lo[sc];
                     sz[h] = t.c_hi[sc] - slo;
                     sm.meta[wib][k] = make_int2(slo, sz[h]);
@@ -1295,19 +1295,31 @@ __device__ __forceinline__ void tile_chunk(TileShared& sm, const Tree2D& t, cons
 __global__ void __launch_bounds__(32 * kTileWarps, 3)
 p2p2d_tile_f32(Tree2D t, Lists2D l, const double* __restrict__ fx,
                const double* __restrict__ fy, double* __restrict__ out0, double* __restrict__ out1, int velocity,
-               double u_inf, double v_inf, unsigned* err) {
+               double u_inf, double v_inf, int lists, unsigned* err) {
     __shared__ TileShared sm;
     if (fatal(err)) return;
     const int wib = threadIdx.x >> 5;
     const int nl = t.info->n_leaves;
     for (int li = blockIdx.x * kTileWarps + wib; li < nl; li += gridDim.x * kTileWarps) {
+        // list 1 of the leaf: CSR, or the fixed slots of int_list_slots (the
+        // leaves whose list outgrew them come in a second pass, from the CSR)
+        const int32_t* src1;
+        int n1;
+        if (lists == kP2PListCsr) {
+            src1 = l.l1_src + l.l1_off[li];
+            n1 = (int)(l.l1_off[li + 1] - l.l1_off[li]);
+        } else {
+            const uint32_t cnt = l.l1_cnt[li];
+            const bool spill = cnt > (uint32_t)kListSlot1;
+            if (spill != (lists == kP2PListSpill)) continue;
+            src1 = spill ? l.l1_src + l.l1_off[li] : l.l1_slot + (size_t)li * kListSlot1;
+            n1 = spill ? (int)(l.l1_off[li + 1] - l.l1_off[li]) : (int)cnt;
+        }
         const int c = t.leaf_cells[li];
         const int lo = t.c_lo[c], hi = t.c_hi[c];
         const double ccx = t.c_cx[c], ccy = t.c_cy[c];
         const int lev = t.c_level[c];
         const double ih = ldexp(1.0, lev) / t.geom->root;   // 1 / leaf size
-        const uint32_t o1 = l.l1_off[li];
-        const int n1 = (int)(l.l1_off[li + 1] - o1);
         for (int tb = lo; tb < hi; tb += kTileChunk) {
             const int T = min(kTileChunk, hi - tb);
             int hs = 0;   // the smallest H = 2^hs with ceil(T / H) <= kTileMaxM (H <= 16)
@@ -1316,7 +1328,7 @@ p2p2d_tile_f32(Tree2D t, Lists2D l, const double* __restrict__ fx,
             switch (M) {
 #define VPM_TILE_CASE(MM)                                                                                           \
     case MM:                                                                                                        \
-        tile_chunk<MM>(sm, t, l, c, ccx, ccy, ih, o1, n1, tb, T, hs, fx, fy, out0, out1, velocity, u_inf,             \
+        tile_chunk<MM>(sm, t, src1, c, ccx, ccy, ih, n1, tb, T, hs, fx, fy, out0, out1, velocity, u_inf,              \
                        v_inf, err);                                                                                 \
         break;
                 VPM_TILE_CASE(1) VPM_TILE_CASE(2) VPM_TILE_CASE(3) VPM_TILE_CASE(4) VPM_TILE_CASE(5) VPM_TILE_CASE(6)
@@ -1751,14 +1763,16 @@ cudaError_t fmm2d_p2p_out(const Tree2D& t, const Lists2D& l, const Expansions2D&
 
 cudaError_t fmm2d_p2p_f32(const Tree2D& t, const Lists2D& l, const Expansions2D& e, double* out0, double* out1,
                           int velocity, double u_inf, double v_inf, unsigned* err, cudaStream_t st, int* launches,
-                          bool near_only) {
+                          bool near_only, int lists) {
     Expansions2D en = e;
     if (near_only) en.fx = en.fy = nullptr;
     // Many short blocks (a leaf or a few per warp) rather than one persistent
     // wave: blocks retire all through the launch, so the far-field kernels
     // running concurrently on the other streams get SM room as they queue.
-    p2p2d_tile_f32<<<148 * 3 * 8, 32 * kTileWarps, 0, st>>>(t, l, en.fx, en.fy, out0, out1, velocity, u_inf, v_inf,
-                                                           err);
+    // the pass over the few leaves whose list 1 outgrew its slots: one wave
+    const int grid = lists == kP2PListSpill ? 148 : 148 * 3 * 8;
+    p2p2d_tile_f32<<<grid, 32 * kTileWarps, 0, st>>>(t, l, en.fx, en.fy, out0, out1, velocity, u_inf, v_inf, lists,
+                                                    err);
     *launches += 1;
     return cudaGetLastError();
 }

@@ -578,20 +578,37 @@ cudaError_t build_lists2d(const Tree2D& t, Lists2D& l, ScanScratch& scan, double
     return build_int_lists2d(t, l, scan, eps, err, st, launches);
 }
 
+bool int_lists_slotted(const Lists2D& l) { return l.l1_slot && l.l3_slot; }
+
+cudaError_t build_int_slots2d(const Tree2D& t, Lists2D& l, double eps, unsigned* err, cudaStream_t st, int* launches) {
+    if (!int_lists_slotted(l)) return cudaErrorInvalidValue;
+    int_list_slots<<<148 * 16, 128, 0, st>>>(t, eps, l, err);
+    *launches += 1;
+    return cudaGetLastError();
+}
+
+cudaError_t build_int_csr2d(const Tree2D& t, Lists2D& l, ScanScratch& scan, double eps, unsigned* err,
+                            cudaStream_t st, int* launches) {
+    if (!int_lists_slotted(l)) return cudaErrorInvalidValue;
+    const int gl = std::max(1, std::min(148 * 4, ceil_div(l.cap_leaves, 128)));
+    cudaError_t e = scan_exclusive(l.l1_cnt, l.l1_off, l.cap_leaves, l.l1_off + l.cap_leaves, scan, err, st);
+    if (e != cudaSuccess) return e;
+    e = scan_exclusive(l.l3_cnt, l.l3_off, l.cap_leaves, l.l3_off + l.cap_leaves, scan, err, st);
+    if (e != cudaSuccess) return e;
+    int_list_compact<<<148 * 8, 256, 0, st>>>(t, l, err);
+    int_list_overflow<<<gl, 128, 0, st>>>(t, eps, l, err);
+    list_totals<<<1, 32, 0, st>>>(t, l, err);
+    *launches += 5;
+    return cudaGetLastError();
+}
+
 cudaError_t build_int_lists2d(const Tree2D& t, Lists2D& l, ScanScratch& scan, double eps, unsigned* err,
                               cudaStream_t st, int* launches) {
     const int gl = std::max(1, std::min(148 * 4, ceil_div(l.cap_leaves, 128)));
-    if (l.l1_slot && l.l3_slot) {
-        int_list_slots<<<148 * 16, 128, 0, st>>>(t, eps, l, err);
-        cudaError_t e = scan_exclusive(l.l1_cnt, l.l1_off, l.cap_leaves, l.l1_off + l.cap_leaves, scan, err, st);
+    if (int_lists_slotted(l)) {
+        cudaError_t e = build_int_slots2d(t, l, eps, err, st, launches);
         if (e != cudaSuccess) return e;
-        e = scan_exclusive(l.l3_cnt, l.l3_off, l.cap_leaves, l.l3_off + l.cap_leaves, scan, err, st);
-        if (e != cudaSuccess) return e;
-        int_list_compact<<<148 * 8, 256, 0, st>>>(t, l, err);
-        int_list_overflow<<<gl, 128, 0, st>>>(t, eps, l, err);
-        list_totals<<<1, 32, 0, st>>>(t, l, err);
-        *launches += 6;
-        return cudaGetLastError();
+        return build_int_csr2d(t, l, scan, eps, err, st, launches);
     }
     int_list_kernel<<<gl, 128, 0, st>>>(t, eps, 0, l, err);
     *launches += 1;
