@@ -1124,17 +1124,24 @@ __device__ __forceinline__ uint64_t pack2(float lo, float hi) {
 __device__ __forceinline__ float lo2(uint64_t v) { return __uint_as_float((uint32_t)v); }
 __device__ __forceinline__ float hi2(uint64_t v) { return __uint_as_float((uint32_t)(v >> 32)); }
 
-// Staged sources j0, j0 + ns, ... < cnt applied to the lane's M targets.
-template <int M>
-__device__ __forceinline__ void tile_pairs(const ulonglong2* xy, const uint64_t* qq, int j0, int cnt, int ns,
+// Staged sources split, split + NS, ... below cnt applied to the lane's M
+// targets: a loop with constant bounds and strides (NS = 32 >> HS), so no
+// index arithmetic is left between the pair updates.
+template <int M, int HS>
+__device__ __forceinline__ void tile_pairs(const ulonglong2* xy, const uint64_t* qq, int split, int cnt,
                                            const uint64_t* nx, const uint64_t* ny, float nxo, float nyo, uint64_t* px,
                                            uint64_t* py, float& pxo, float& pyo) {
-    constexpr int MP = M / 2;
+    constexpr int MP = M / 2, NS = 32 >> HS, PER = kTileStage / NS;
     constexpr bool ODD = (M & 1) != 0;
     const uint64_t eps = pack2(kTileEps, kTileEps);
-    for (int j = j0; j < cnt; j += ns) {
-        const ulonglong2 sv = xy[j];   // (x, x), (y, y)
-        const uint64_t sq = qq[j];     // (q, q)
+    const ulonglong2* xs = xy + split;
+    const uint64_t* qs = qq + split;
+    const int nrun = (cnt - split + NS - 1) / NS;   // sources of this split in the stage
+    #pragma unroll
+    for (int u = 0; u < PER; ++u) {
+        if (u >= nrun) break;
+        const ulonglong2 sv = xs[u * NS];   // (x, x), (y, y)
+        const uint64_t sq = qs[u * NS];     // (q, q)
         #pragma unroll
         for (int h = 0; h < MP; ++h) tile_pair2(nx[h], ny[h], sv.x, sv.y, sq, eps, px[h], py[h]);
         if (ODD) {
@@ -1151,15 +1158,15 @@ __device__ __forceinline__ void tile_pairs(const ulonglong2* xy, const uint64_t*
 // as a target and as a source).
 __device__ __forceinline__ float leaf_unit(double x, double c, double ih) { return (float)((x - c) * ih); }
 
-template <int M>
+template <int M, int HS>
 __device__ __forceinline__ void tile_chunk(TileShared& sm, const Tree2D& t, const int32_t* __restrict__ src1, int c,
-                                           double ccx, double ccy, double ih, int n1, int tb, int T, int hs,
+                                           double ccx, double ccy, double ih, int n1, int tb, int T,
                                            const double* fx, const double* fy, double* out0, double* out1,
                                            int velocity, double u_inf, double v_inf, unsigned* err) {
     constexpr int MP = M / 2;
     constexpr int NP = MP > 0 ? MP : 1;
+    constexpr int hs = HS, H = 1 << HS, ns = 32 >> HS;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int H = 1 << hs, ns = 32 >> hs;
     const int tt = lane & (H - 1), split = lane >> hs;
     // negated target coordinates (leaf frame); target k of this lane is chunk slot tt + k H
     uint64_t nx[NP], ny[NP], px[NP], py[NP];
@@ -1269,8 +1276,9 @@ __device__ __forceinline__ void tile_chunk(TileShared& sm, const Tree2D& t, cons
             advance(k1, q1);
             pv0 = fetch(k0, q0);
             pv1 = fetch(k1, q1);
-            tile_pairs<M>(reinterpret_cast<const ulonglong2*>(sm.xy[wib]), reinterpret_cast<const uint64_t*>(sm.qq[wib]),
-                          split, min(kTileStage, total - cb), ns, nx, ny, nxo, nyo, px, py, pxo, pyo);
+            tile_pairs<M, HS>(reinterpret_cast<const ulonglong2*>(sm.xy[wib]),
+                              reinterpret_cast<const uint64_t*>(sm.qq[wib]), split, min(kTileStage, total - cb), nx,
+                              ny, nxo, nyo, px, py, pxo, pyo);
             __syncwarp();
             steps += kTileStage;
             if (steps >= kTileFlush * ns) {
@@ -1325,13 +1333,15 @@ p2p2d_tile_f32(Tree2D t, Lists2D l, const double* __restrict__ fx,
             int hs = 0;   // the smallest H = 2^hs with ceil(T / H) <= kTileMaxM (H <= 16)
             while (((T + (1 << hs) - 1) >> hs) > kTileMaxM) ++hs;
             const int M = (T + (1 << hs) - 1) >> hs;
-            switch (M) {
-#define VPM_TILE_CASE(MM)                                                                                           \
-    case MM:                                                                                                        \
-        tile_chunk<MM>(sm, t, src1, c, ccx, ccy, ih, n1, tb, T, hs, fx, fy, out0, out1, velocity, u_inf,              \
-                       v_inf, err);                                                                                 \
+            switch ((hs << 4) | M) {
+#define VPM_TILE_CASE(HH, MM)                                                                                       \
+    case (HH << 4) | MM:                                                                                            \
+        tile_chunk<MM, HH>(sm, t, src1, c, ccx, ccy, ih, n1, tb, T, fx, fy, out0, out1, velocity, u_inf, v_inf, err); \
         break;
-                VPM_TILE_CASE(1) VPM_TILE_CASE(2) VPM_TILE_CASE(3) VPM_TILE_CASE(4) VPM_TILE_CASE(5) VPM_TILE_CASE(6)
+#define VPM_TILE_ROW(HH) VPM_TILE_CASE(HH, 1) VPM_TILE_CASE(HH, 2) VPM_TILE_CASE(HH, 3) VPM_TILE_CASE(HH, 4)         \
+    VPM_TILE_CASE(HH, 5) VPM_TILE_CASE(HH, 6)
+                VPM_TILE_ROW(0) VPM_TILE_ROW(1) VPM_TILE_ROW(2) VPM_TILE_ROW(3) VPM_TILE_ROW(4)
+#undef VPM_TILE_ROW
 #undef VPM_TILE_CASE
                 default: break;
             }
