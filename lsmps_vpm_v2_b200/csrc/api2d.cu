@@ -92,7 +92,7 @@ int Ctx::reserve2d(int n, int cap_cells, int P, long long cap_l1, long long cap_
            o_ciy = L.take<int32_t>(C), o_cleaf = L.take<int32_t>(C);
     size_t o_cfl = L.take<uint8_t>(C), o_cmask = L.take<uint8_t>(C), o_clev = L.take<uint8_t>(C);
     size_t o_ccx = L.take<double>(C), o_ccy = L.take<double>(C), o_ccode = L.take<uint64_t>(C);
-    size_t o_leaves = L.take<int32_t>(C), o_nonleaf = L.take<int32_t>(C), o_upcnt = L.take<uint32_t>(C);
+    size_t o_leaves = L.take<int32_t>(C), o_nonleaf = L.take<int32_t>(C);
     size_t o_l2blk = L.take<int32_t>(C * 32);
     size_t o_l2 = L.take<int32_t>(C * kList2Cap), o_l2s = L.take<uint8_t>(C * kList2Cap), o_l2n = L.take<uint8_t>(C);
     size_t o_l4 = L.take<int32_t>(C * kList4Cap), o_l4n = L.take<uint8_t>(C);
@@ -141,7 +141,6 @@ int Ctx::reserve2d(int n, int cap_cells, int P, long long cap_l1, long long cap_
     tree.c_cx = (double*)P_(o_ccx); tree.c_cy = (double*)P_(o_ccy); tree.c_code = (uint64_t*)P_(o_ccode);
     tree.leaf_cells = (int32_t*)P_(o_leaves);
     tree.nonleaf = (int32_t*)P_(o_nonleaf);
-    tree.c_upcnt = (uint32_t*)P_(o_upcnt);
     lists.l2_blk = (int32_t*)P_(o_l2blk);
     tree.geom = (Geom2D*)P_(o_geom); tree.info = (TreeInfo2D*)P_(o_info);
     tree.dense = (int32_t*)P_(o_dense);

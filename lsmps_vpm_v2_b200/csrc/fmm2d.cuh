@@ -67,9 +67,6 @@ struct Tree2D {
     // Non-leaf cells in cell order (level-major, Morton within a level; the
     // root first): n_cells - n_leaves entries, or nullptr (not recorded).
     int32_t* nonleaf;
-    // Per cell: children whose multipole is final (upward pass), zeroed by the
-    // tree build for every cell it emits; nullptr: not kept.
-    uint32_t* c_upcnt;
     // Dense lookup grid: dense[reference cell ID] = cell index for levels
     // <= dense_levels (nullptr: none). Entries are never cleared: a lookup
     // accepts an entry only if that cell has the queried level and index.
@@ -212,10 +209,10 @@ struct Expansions2D {
 };
 
 cudaError_t fmm2d_upward(const Tree2D& t, Expansions2D& e, int P, unsigned* err, cudaStream_t st, int* launches);
-// The same moments without a level loop (cells of up to 1024 particles
-// straight from their particles, the larger ones by M2M in the warp that
-// finishes their last child, counted in t.c_upcnt) when upward_direct_ok;
-// else fmm2d_upward.
+// The same moments in two launches (cells of up to 1024 particles straight
+// from their particles, the larger ones by a cooperative M2M level loop from
+// the deepest level holding one) when upward_direct_ok; else fmm2d_upward.
+// Uses grid-barrier words 2 and 3 of t.gbar (zeroed before every evaluation).
 bool upward_direct_ok(int P, bool exact);
 cudaError_t fmm2d_upward_direct(const Tree2D& t, Expansions2D& e, int P, bool exact, unsigned* err, cudaStream_t st,
                                 int* launches);

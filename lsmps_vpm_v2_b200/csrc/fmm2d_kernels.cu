@@ -109,7 +109,7 @@ constexpr int kLevelWarps = 8;
 // Child expansions are read through L2 (ld.cg): in the cooperative kernel the
 // level below was written by other blocks of the same launch.
 __device__ __forceinline__ void m2m_level_body(const Tree2D& t, double2* __restrict__ a,
-                                               const double* __restrict__ coef, int P, int L) {
+                                               const double* __restrict__ coef, int P, int L, int min_count = -1) {
     __shared__ double2 s_child[kLevelWarps][4][32];  // [warp][child][g * (P+1) + k]
     __shared__ double2 s_tt[kLevelWarps][4][16];     // [warp][child][g]
     const double* g_m2m = coef + kCoefM2M;
@@ -123,7 +123,7 @@ __device__ __forceinline__ void m2m_level_body(const Tree2D& t, double2* __restr
         bool ok = g < G && c < c1;
         if (ok) {
             const uint8_t f = t.c_flags[c];
-            ok = !(f & CELL_LEAF) && (f & CELL_ACTIVE);
+            ok = !(f & CELL_LEAF) && (f & CELL_ACTIVE) && t.c_hi[c] - t.c_lo[c] > min_count;
         }
         unsigned m = 0;
         int ch0 = -1;
@@ -181,6 +181,19 @@ m2m_levels_coop(Tree2D t, double2* __restrict__ a, const double* __restrict__ co
     const int depth = t.info->depth;
     for (int L = depth - 1; L >= 1; --L) {
         if (!block_fatal(err)) m2m_level_body(t, a, coef, P, L);
+        grid_sync_counter(bar, err);
+    }
+}
+
+// The same level loop over the cells of more than min_count particles only
+// (the others are final already), from the deepest level holding one
+// (*top_level, written by upward_direct2d) up to level 1.
+__global__ void __launch_bounds__(32 * kLevelWarps)
+m2m_big_levels_coop(Tree2D t, double2* __restrict__ a, const double* __restrict__ coef, int P, int min_count,
+                    const unsigned* top_level, unsigned* bar, unsigned* err) {
+    const int top = (int)*top_level;
+    for (int L = top; L >= 1; --L) {
+        if (!block_fatal(err)) m2m_level_body(t, a, coef, P, L, min_count);
         grid_sync_counter(bar, err);
     }
 }
@@ -1394,7 +1407,7 @@ cudaError_t set_coefficients2d(int P, bool exact, double* dst, cudaStream_t st) 
     return cudaStreamSynchronize(st);
 }
 
-// ---- upward pass without a level loop ---------------------------------------
+// ---- upward pass in two launches ----------------------------------------------
 //
 // The multipole of any cell is a_k = sum of q_j (z_j - z_c)^k over the active
 // particles of its subtree (P2M at a leaf, fmm2D.cpp:237-284), and M2M
@@ -1403,33 +1416,33 @@ cudaError_t set_coefficients2d(int P, bool exact, double* dst, cudaStream_t st) 
 // whenever those coefficients are exact (orders up to 18 with the reference's
 // 32-bit binComb, any order with exact binomials). Every cell covers a
 // contiguous range of the sorted particles, so a cell of at most kDirectMax
-// particles takes its moments straight from that range: one warp per cell,
-// all levels at once, no ordering between cells. A larger cell (the top of
-// the tree, about n / kDirectMax cells per level) is computed by M2M as soon
-// as its children are final: each finished cell counts itself into its
-// parent's c_upcnt, and the warp that completes the count computes the
-// parent, then does the same one level up. Sums run in a fixed order (lane
-// order over the particles, then lanes in order; children in child order):
-// the result does not depend on which warp finishes last.
+// particles takes its moments straight from that range (upward_direct2d: one
+// warp per cell, all levels at once, no ordering between cells). The larger
+// cells (the top of the tree, about n / kDirectMax per level) follow by M2M
+// from their children in the cooperative level loop m2m_big_levels_coop,
+// from the deepest level holding one. Sums run in a fixed order (lane order
+// over the particles, then lanes in order; children in child order).
 constexpr int kUpWarps = 8;
 constexpr int kDirectMax = 1024;
 constexpr int kUpMaxP = 18;
 
 template <int P>
 __global__ void __launch_bounds__(32 * kUpWarps)
-upward_direct2d(Tree2D t, double2* __restrict__ a, const double* __restrict__ coef, unsigned* err) {
+upward_direct2d(Tree2D t, double2* __restrict__ a, unsigned* __restrict__ top_level, unsigned* err) {
     constexpr int Q = P + 1, CS = 2 * Q + 1;   // components per lane, padded row stride
     extern __shared__ double up_sm[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    double* red = up_sm + (size_t)wib * 32 * CS;   // [lane][component]; M2M: children's moments
+    double* red = up_sm + (size_t)wib * 32 * CS;   // [lane][component]
     if (fatal(err)) return;
-    const double* g_m2m = coef + kCoefM2M;
     const int c_begin = t.info->level_start[1], c_end = t.info->n_cells;
     const int nw = gridDim.x * kUpWarps;
     for (int c = c_begin + blockIdx.x * kUpWarps + wib; c < c_end; c += nw) {
         const int lo = t.c_lo[c], hi = t.c_hi[c];
         const uint8_t f = t.c_flags[c];
-        if (hi - lo > kDirectMax && !(f & CELL_LEAF)) continue;   // by M2M once its children are final
+        if (hi - lo > kDirectMax && !(f & CELL_LEAF)) {   // by M2M afterwards (m2m_big_levels_coop)
+            if (lane == 0) atomicMax(top_level, (unsigned)t.c_level[c]);
+            continue;
+        }
         double re[Q], im[Q];
         #pragma unroll
         for (int k = 0; k < Q; ++k) re[k] = im[k] = 0.0;
@@ -1462,49 +1475,6 @@ upward_direct2d(Tree2D t, double2* __restrict__ a, const double* __restrict__ co
             reinterpret_cast<double*>(a + (size_t)c * Q)[comp] = sum;
         }
         __syncwarp();
-        // count this cell into its ancestors while this warp completes them
-        int cur = c;
-        while (true) {
-            const int par = t.c_parent[cur];
-            if (par <= 0) break;                                       // the root's moments are never used
-            if (t.c_hi[par] - t.c_lo[par] <= kDirectMax) break;       // computed directly
-            __threadfence();                                           // cur's moments before the count
-            unsigned done = 0;
-            if (lane == 0) done = atomicAdd(&t.c_upcnt[par], 1u) + 1u;
-            done = __shfl_sync(0xffffffffu, done, 0);
-            const unsigned m = t.c_chmask[par];
-            const int nch = __popc(m);
-            if ((int)done != nch) break;                               // another child completes it
-            __threadfence();
-            // M2M of par: lane k < Q, a_k = sum over children of a_0 t^k + sum_m m2m[k][m] a_m t^(k-m)
-            const int ch0 = t.c_child0[par];
-            double2* sm = reinterpret_cast<double2*>(red);             // [child][Q]
-            for (int i = lane; i < nch * Q; i += 32) sm[i] = __ldcg(a + (size_t)ch0 * Q + i);
-            __syncwarp();
-            double2 acc = make_double2(0.0, 0.0);
-            if (lane < Q && (t.c_flags[par] & CELL_ACTIVE)) {
-                const double pcx = t.c_cx[par], pcy = t.c_cy[par];
-                double2 S[4], tt[4];
-                #pragma unroll
-                for (int r = 0; r < 4; ++r) {
-                    const int ch = ch0 + (r < nch ? r : 0);
-                    tt[r] = make_double2(t.c_cx[ch] - pcx, t.c_cy[ch] - pcy);
-                    S[r] = sm[(r < nch ? r : 0) * Q];
-                }
-                for (int mm = 1; mm <= lane; ++mm) {
-                    const double cf = g_m2m[lane * W + mm];
-                    #pragma unroll
-                    for (int r = 0; r < 4; ++r)
-                        if (r < nch) S[r] = cfma(S[r], tt[r], cscale(sm[r * Q + mm], cf));
-                }
-                #pragma unroll
-                for (int r = 0; r < 4; ++r)
-                    if (r < nch) acc = cadd(acc, S[r]);
-            }
-            if (lane < Q) a[(size_t)par * Q + lane] = acc;
-            __syncwarp();
-            cur = par;
-        }
     }
 }
 
@@ -1516,15 +1486,18 @@ cudaError_t launch_upward_direct(const Tree2D& t, Expansions2D& e, unsigned* err
     const size_t smem = sizeof(double) * kUpWarps * 32 * (2 * (P + 1) + 1);
     cudaError_t r = cudaFuncSetAttribute(upward_direct2d<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (r != cudaSuccess) return r;
-    upward_direct2d<P><<<148 * 4, 32 * kUpWarps, smem, st>>>(t, e.a, e.coef, err);
-    return cudaGetLastError();
+    upward_direct2d<P><<<148 * 4, 32 * kUpWarps, smem, st>>>(t, e.a, t.gbar + 3, err);
+    int grid = 0;
+    r = launch_coop(m2m_big_levels_coop, 32 * kLevelWarps, 0, st, 1, &grid, t, e.a, (const double*)e.coef, P,
+                    kDirectMax, (const unsigned*)(t.gbar + 3), t.gbar + 2, err);
+    return r != cudaSuccess ? r : cudaGetLastError();
 }
 
 // Upward pass of orders the direct form covers (upward_direct_ok): one launch.
 // Otherwise the P2M + M2M level loop below.
 cudaError_t fmm2d_upward_direct(const Tree2D& t, Expansions2D& e, int P, bool exact, unsigned* err, cudaStream_t st,
                                 int* launches) {
-    if (!upward_direct_ok(P, exact) || !t.c_upcnt) return fmm2d_upward(t, e, P, err, st, launches);
+    if (!upward_direct_ok(P, exact) || !t.gbar) return fmm2d_upward(t, e, P, err, st, launches);
     cudaError_t r;
     switch (P) {
 #define VPM_UP_CASE(PP) \
@@ -1535,7 +1508,11 @@ cudaError_t fmm2d_upward_direct(const Tree2D& t, Expansions2D& e, int P, bool ex
 #undef VPM_UP_CASE
         default: return fmm2d_upward(t, e, P, err, st, launches);
     }
-    *launches += 1;
+    if (r != cudaSuccess) {   // cooperative launch refused: the level loop over all cells instead
+        (void)cudaGetLastError();
+        return fmm2d_upward(t, e, P, err, st, launches);
+    }
+    *launches += 2;
     return r;
 }
 

@@ -788,7 +788,6 @@ __global__ void flat_totals(Tree2D t, const uint32_t* __restrict__ level_tot, un
     t.c_cy[0] = xadd(g->pivy, xmul(0.5, g->root));
     if (t.dense) t.dense[0] = 0;
     if (t.nonleaf && cells > 1) t.nonleaf[0] = 0;
-    if (t.c_upcnt) t.c_upcnt[0] = 0u;
 }
 
 // Cell records (and leaf entries) of every particle's cell levels, indices
@@ -853,7 +852,6 @@ flat_emit(Tree2D t, const uint32_t* __restrict__ pinfo, const uint32_t* __restri
             t.c_ix[ci] = ix;
             t.c_iy[ci] = iy;
             t.c_code[ci] = code;
-            if (t.c_upcnt) t.c_upcnt[ci] = 0u;
             t.c_cx[ci] = xadd(pivx, xmul(xadd(0.5, (double)ix), len));
             t.c_cy[ci] = xadd(pivy, xmul(xadd(0.5, (double)iy), len));
             if (t.dense && L <= t.dense_levels) t.dense[start_id2(L) + ix + ((int64_t)iy << L)] = ci;
