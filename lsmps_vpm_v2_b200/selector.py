@@ -116,6 +116,15 @@ class Selector:
                                                       float(target_err), _p(f)))
         return f
 
+    def features_device(self, x, y, q, active, target_err: float) -> np.ndarray:
+        """The same features from device arrays (torch CUDA tensors: float64
+        x, y, q and uint8 active): the particles are not copied to the host;
+        the 228 floats come back."""
+        f = np.zeros(N_FEAT, np.float32)
+        self.ctx._check(lib().vpm_selector_features2d_device(
+            self.ctx._h, *[C.c_void_p(v.data_ptr()) for v in (x, y, q, active)], x.numel(), float(target_err), _p(f)))
+        return f
+
     def choose(self, feat, target_err: float, margin: float = 0.3):
         """(max_src, max_par, p) and the 70 predictions for a feature vector."""
         f = np.ascontiguousarray(feat, dtype=np.float32)
@@ -126,8 +135,12 @@ class Selector:
         return (ms.value, mp.value, p.value), pred
 
     def params_for(self, x, y, q, active, target_err: float = 1e-4, margin: float = 0.3, **over) -> Params:
-        """vpm_fmm_params of the mixed form with the chosen caps and order."""
-        (ms, mp, p), _ = self.choose(self.features(x, y, q, active, target_err), target_err, margin)
+        """vpm_fmm_params of the mixed form with the chosen caps and order
+        (host arrays, or torch CUDA tensors: the features are then computed
+        from the device buffers)."""
+        feat = (self.features_device(x, y, q, active, target_err) if hasattr(x, "data_ptr")
+                else self.features(x, y, q, active, target_err))
+        (ms, mp, p), _ = self.choose(feat, target_err, margin)
         prm = default_params(max_src=ms, max_par=mp, p=p, precision=1, binom=1)
         for k, v in over.items():
             setattr(prm, k, v)

@@ -4,7 +4,9 @@ the GPU (python -m lsmps_vpm_v2_b200.selector_train).
 Each random 2D field (multi-vortex lattices, boundary-layer plates at random
 resolution, Gaussian clusters; N log-uniform in [10k, 2M]) is evaluated by
 the mixed form at all 35 (caps, p) candidates: the label of a candidate is
-its measured device time (CUDA events, median of two after a warm-up) and
+its measured device time (CUDA events around a replay of the evaluation's
+CUDA graph, the way a time-stepping caller runs it; median of three after
+the capture) and
 its relative L2 error against the FP64 direct sum on 4,096 sampled targets
 (the library's direct-sum kernel). One field gives one row of 228 features
 and 70 labels; the target-error feature is drawn at random per row (the
@@ -81,10 +83,10 @@ def label_field(ctx, sel, d, cands, rng, torch):
     mask = np.ones(N_OUT, np.float32)
     st = torch.cuda.current_stream()
     for k, (ms, mp, p) in enumerate(cands):
-        prm = default_params(max_src=ms, max_par=mp, p=p, precision=1, binom=1)
+        prm = default_params(max_src=ms, max_par=mp, p=p, precision=1, binom=1, use_graph=1)
         times = []
         ok = True
-        for rep in range(3):
+        for rep in range(4):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(st)
             r = lib().vpm_fmm2d_field_device(ctx._h, x.data_ptr(), y.data_ptr(), q.data_ptr(), a.data_ptr(), n,
@@ -102,7 +104,7 @@ def label_field(ctx, sel, d, cands, rng, torch):
         err = num / den if den > 0 else 0.0
         labels[k] = math.log10(max(err, 1e-12))
         labels[N_CAND + k] = math.log10(max(float(np.median(times)), 1e-3))
-    feat = sel.features(d["x"], d["y"], d["q"], d["active"], 1e-4)
+    feat = sel.features_device(x, y, q, a, 1e-4)
     return feat, labels, mask
 
 
