@@ -7,9 +7,11 @@ p = 10, leaf caps 50/75).
 
 Prints one JSON line (rank 0). Our arm measures both forms - the plain FP64
 form (the reference's caps 50/75 and p = 10) and the mixed form (FP32 near
-field, tensor-core M2L, caps and p from the learned selector for a 1e-4
-target) - with their errors against the FP64 direct sum on 4,096 targets, and
-reports the --form one (default mixed) as the headline: `value` is particle
+field, FP32 list-2 M2L per parent cell, caps and p from the learned selector
+for a 1e-4 target; the same form with the M2L on the tensor cores is reported
+beside it as forms.mixed_tc) - with their errors against the FP64 direct sum
+on 4,096 targets, and reports the --form one (default mixed) as the headline:
+`value` is particle
 velocities per second of device-resident evaluations (inputs in HBM, CUDA
 events on the launching stream, L2 flushed by a 256 MiB write between steps); `e2e` is the
 same metric through the public host API (pinned host buffers, H2D + D2H
@@ -43,6 +45,7 @@ from lsmps_vpm_v2_b200 import workloads  # noqa: E402
 METRIC = "2D FMM particle velocities/sec @780k, mixed vs FP64 GPU at ≤1e-4 rel L2"
 UNIT = "particle velocities/s"
 L2_FLUSH_BYTES = 256 << 20
+SELECT_EVERY = 100   # steps between two (caps, p) choices of a time-stepping caller
 P2P_FLOPS_PER_PAIR = 12  # 2 sub, 3 for r^2, 1 reciprocal, 2 x 3 multiply-add
 
 
@@ -86,7 +89,7 @@ def cpu_baseline(wl, budget_s=12.0, max_reps=20):
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks / throttle reasons sampled every 25 ms."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -100,7 +103,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "25"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
 
@@ -191,7 +194,7 @@ def run_ours(args):
     import torch.distributed as dist
 
     from lsmps_vpm_v2_b200 import Context, default_params, PREC_FP64, PREC_MIXED
-    from lsmps_vpm_v2_b200._lib import lib
+    from lsmps_vpm_v2_b200._lib import PREC_MIXED_TC, lib
     from lsmps_vpm_v2_b200.selector import Selector
 
     world, rank, local = _dist_env()
@@ -222,12 +225,19 @@ def run_ours(args):
     # no trained network is present) ----
     p64 = default_params(precision=PREC_FP64, use_graph=graph)
     sel = Selector(ctx)
-    t0 = time.perf_counter()
     have_net = sel.load()
-    feat = sel.features(wl["x"], wl["y"], wl["q"], wl["active"], 1e-4)
-    (ms_, mp_, pp_), _ = sel.choose(feat, 1e-4)
+    # the choice from the device buffers (features, BF16 inference); timed warm,
+    # once per particle set: a time-stepping caller renews it every
+    # SELECT_EVERY steps, so its cost per step is the amortised figure
+    sel.params_for(x, y, q, act, 1e-4)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    psel = sel.params_for(x, y, q, act, 1e-4)
+    torch.cuda.synchronize()
     t_sel = (time.perf_counter() - t0) * 1e3
+    ms_, mp_, pp_ = int(psel.max_src), int(psel.max_par), int(psel.p)
     pmx = default_params(precision=PREC_MIXED, binom=1, max_src=ms_, max_par=mp_, p=pp_, use_graph=graph)
+    ptc = default_params(precision=PREC_MIXED_TC, binom=1, max_src=ms_, max_par=mp_, p=pp_, use_graph=graph)
     forms = {"fp64": p64, "mixed": pmx}
     headline = args.form
     prm = forms[headline]
@@ -239,7 +249,7 @@ def run_ours(args):
     ctx._check(lib().vpm_direct2d_field_device(ctx._h, x.data_ptr(), y.data_ptr(), q.data_ptr(), act.data_ptr(), n,
                                                tg.data_ptr(), tg.numel(), dx.data_ptr(), dy.data_ptr()))
     err = {}
-    for name, p_ in forms.items():
+    for name, p_ in list(forms.items()) + [("mixed_tc", ptc)]:
         ctx.field2d_device(x, y, q, act, ex, ey, p_)
         ctx.sync()
         num = torch.sqrt(((ex[tg] - dx) ** 2).sum() + ((ey[tg] - dy) ** 2).sum())
@@ -264,6 +274,13 @@ def run_ours(args):
             dist.barrier()
         ms[name] = max_over_ranks(ms[name], world, dev)
     clk = clocks.stop()
+    # the same mixed form with its list-2 M2L on the tensor cores (reported beside it)
+    for _ in range(max(args.warmup, 3)):
+        ctx.field2d_device(x, y, q, act, ex, ey, ptc)
+    ctx.sync()
+    ms["mixed_tc"] = max_over_ranks(time_steps(ctx, stream, flush, lambda: ctx.field2d_device(x, y, q, act, ex, ey,
+                                                                                             ptc), args.steps),
+                                    world, dev)
     ms_step = ms[headline]
     value = world * n / (ms_step * 1e-3)
     ctx.field2d_device(x, y, q, act, ex, ey, prm)
@@ -295,16 +312,20 @@ def run_ours(args):
     ha = torch.from_numpy(wl["active"]).pin_memory().numpy()
     hu = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
     hv = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
-    e2e_ms = []
-    for k in range(max(3, min(args.steps, 20)) + 2):
-        flush.fill_(k)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        ctx.velocity2d(hx, hy, hw, hs, ha, 0.0, 0.0, prm, out=(hu, hv))
-        t1 = time.perf_counter()
-        if k >= 2:
-            e2e_ms.append((t1 - t0) * 1e3)
-    e2e_step = max_over_ranks(float(np.mean(e2e_ms)), world, dev)
+    e2e_of = {}
+    for name in ("fp64", "mixed"):
+        e2e_ms = []
+        for k in range(max(3, min(args.steps, 20)) + 2):
+            flush.fill_(k)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ctx.velocity2d(hx, hy, hw, hs, ha, 0.0, 0.0, forms[name], out=(hu, hv))
+            t1 = time.perf_counter()
+            if k >= 2:
+                e2e_ms.append((t1 - t0) * 1e3)
+        e2e_of[name] = max_over_ranks(float(np.mean(e2e_ms)), world, dev)
+    e2e_step = e2e_of[headline]
+    h2d_bytes, d2h_bytes = n * (8 * 4 + 1), n * 16
 
     # ---- roofline of the dominant kernel (near-field P2P) ----
     fp64_peak, fp32_peak = ctx.fma_peaks()
@@ -335,16 +356,25 @@ def run_ours(args):
                    "l2": "256 MiB write between steps (outside the per-step events)",
                    "launch": "CUDA graph replay" if prm.use_graph else "eager",
                    "mixed_params": "learned selector, target 1e-4" if have_net else "reference pair (no network)",
-                   "selector_ms": t_sel},
+                   "selector_ms": t_sel, "selector_every_steps": SELECT_EVERY,
+                   "selector_ms_per_step_amortised": t_sel / SELECT_EVERY},
         "forms": {"fp64": {"value": world * n / (ms["fp64"] * 1e-3), "ms_per_step": ms["fp64"],
-                           "rel_l2_vs_direct": err["fp64"], "p": int(p64.p), "caps": [50, 75]},
+                           "rel_l2_vs_direct": err["fp64"], "p": int(p64.p), "caps": [50, 75],
+                           "e2e": {"value": world * n / (e2e_of["fp64"] * 1e-3), "ms_per_step": e2e_of["fp64"]}},
                   "mixed": {"value": world * n / (ms["mixed"] * 1e-3), "ms_per_step": ms["mixed"],
                             "rel_l2_vs_direct": err["mixed"], "p": int(pmx.p),
-                            "caps": [int(pmx.max_src), int(pmx.max_par)]},
+                            "caps": [int(pmx.max_src), int(pmx.max_par)], "m2l": "FP32 per parent cell",
+                            "e2e": {"value": world * n / (e2e_of["mixed"] * 1e-3), "ms_per_step": e2e_of["mixed"]}},
+                  "mixed_tc": {"value": world * n / (ms["mixed_tc"] * 1e-3), "ms_per_step": ms["mixed_tc"],
+                               "rel_l2_vs_direct": err["mixed_tc"], "p": int(ptc.p),
+                               "caps": [int(ptc.max_src), int(ptc.max_par)],
+                               "m2l": "tcgen05 3xTF32 per parent cell (VPM_PREC_MIXED_TC)"},
                   "mixed_over_fp64": ms["fp64"] / ms["mixed"],
+                  "e2e_mixed_over_fp64": e2e_of["fp64"] / e2e_of["mixed"],
+                  "pcie_ms_per_step_at_50GBps": (h2d_bytes + d2h_bytes) / 50e9 * 1e3,
                   "direct_sum": "FP64 direct sum on 4,096 sampled targets (vpm_direct2d_field_device)"},
         "e2e": {"value": world * n / (e2e_step * 1e-3), "unit": UNIT, "ms_per_step": e2e_step,
-                "h2d_bytes_per_step": n * (8 * 4 + 1), "d2h_bytes_per_step": n * 16,
+                "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes,
                 "api": "vpm_velocity2d (host buffers)"},
         "gpu_launches": launches_per_step * args.steps,
         "stages_ms": stage,
@@ -368,16 +398,16 @@ def run_ours(args):
 def mixed_dtype(form, p):
     """Arithmetic types of the timed form: the plain form is FP64 throughout;
     the mixed form runs its near field and list-2 M2L in FP32 (3xTF32 on the
-    tensor cores for orders 13-20) and everything else in FP64."""
+    tensor cores for orders 17-20) and everything else in FP64."""
     if form == "fp64":
         return "f64"
-    return "f32+tf32+f64" if p >= 13 else "f32+f64"
+    return "f32+tf32+f64" if p >= 17 else "f32+f64"
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--form", choices=["mixed", "fp64"], default="mixed",
