@@ -304,6 +304,28 @@ def run_ours(args):
     ctx.sync()
     st = ctx.last_stats()
 
+    # ---- batched uneven solves: 64 multi-vortex fields, N log-uniform in
+    # [4,096, 400,000], p = 12, mixed form, one graph over all solves (its
+    # stream count tuned on the first call) ----
+    bl = workloads.batched_2d(n_solves=64, lo=4096, hi=400_000, seed=3)
+    boffs = np.zeros(len(bl) + 1, np.int64)
+    boffs[1:] = np.cumsum([f["x"].size for f in bl])
+    bdev = [torch.from_numpy(np.concatenate([f[k] for f in bl])).to(dev) for k in ("x", "y", "q", "active")]
+    bN = int(boffs[-1])
+    bex = torch.empty(bN, dtype=torch.float64, device=dev)
+    bey = torch.empty_like(bex)
+    pb = default_params(p=12, precision=PREC_MIXED, binom=1, use_graph=graph)
+    bargs = [t.data_ptr() for t in bdev] + [bex.data_ptr(), bey.data_ptr()]
+    run_batch = lambda: ctx.field2d_batched_device(boffs, *bargs, pb)  # noqa: E731
+    for _ in range(max(args.warmup, 3)):
+        run_batch()
+    ctx.sync()
+    ms_batch = max_over_ranks(time_steps(ctx, stream, flush, run_batch, max(3, min(args.steps, 40))), world, dev)
+    batched = {"workload": f"64 multi-vortex solves, N log-uniform 4,096-400,000 ({bN} particles)", "p": 12,
+               "form": "mixed", "value": world * bN / (ms_batch * 1e-3), "unit": UNIT, "ms_per_step": ms_batch,
+               "streams": ctx.batch_streams(), "launch": "one CUDA graph over all solves" if graph else "eager"}
+    del bdev, bex, bey
+
     # ---- end to end through the public host API (pinned buffers) ----
     hx = torch.from_numpy(wl["x"]).pin_memory().numpy()
     hy = torch.from_numpy(wl["y"]).pin_memory().numpy()
@@ -376,6 +398,7 @@ def run_ours(args):
         "e2e": {"value": world * n / (e2e_step * 1e-3), "unit": UNIT, "ms_per_step": e2e_step,
                 "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes,
                 "api": "vpm_velocity2d (host buffers)"},
+        "batched": batched,
         "gpu_launches": launches_per_step * args.steps,
         "stages_ms": stage,
         "interactions": {"p2p_pairs": pairs, "m2l_pairs": int(st.m2l_pairs), "m2p_pairs": int(st.m2p_pairs),

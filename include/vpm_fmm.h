@@ -247,6 +247,13 @@ int vpm_fmm2d_field_batched_device(vpm_ctx* ctx, int32_t n_solves, const int64_t
                                    const vpm_fmm_params* prm, double* ex, double* ey);
 
 /*
+ * Streams the last batched call of this context ran its solves on: with
+ * use_graph the count chosen by timing the batch's graph with 4, 8, 12 and 16
+ * streams on its first call (no counterpart in the reference).
+ */
+int vpm_batch_streams(vpm_ctx* ctx, int32_t* streams);
+
+/*
  * 3D velocity of the vortex particles (x_j, alpha_j) by the octree treecode
  * of the reference's default 3D path (VELOCITY_3D_TYPE 1):
  *   u(x_i) = sum_j alpha_j x (x_i - x_j) / |x_i - x_j|^3

@@ -105,6 +105,7 @@ SIGNATURES = {
     "vpm_measure_fma_peaks": (C.c_int, [_vp, _dp, _dp]),
     "vpm_stage_history": (C.c_int, [_vp, C.c_int32, C.c_int32, _vp, C.POINTER(C.c_int32)]),
     "vpm_fmm2d_field_batched": (C.c_int, [_vp, C.c_int32, _vp, _vp, _vp, _vp, _vp, C.POINTER(Params), _vp, _vp]),
+    "vpm_batch_streams": (C.c_int, [_vp, _vp]),
     "vpm_fmm2d_field_batched_device": (C.c_int, [_vp, C.c_int32, _vp, _vp, _vp, _vp, _vp, C.POINTER(Params), _vp,
                                                  _vp]),
     "vpm_mlp_param_count": (C.c_int64, []),

@@ -126,6 +126,8 @@ struct Ctx {
     cudaGraphExec_t batch_exec = nullptr;
     std::vector<int64_t> batch_key;
     int batch_subs = 0;
+    int batch_streams = 0;                       // streams of the tuned batch graph
+    cudaEvent_t tune_ev[2] = {nullptr, nullptr};  // timing of the stream-count tuning
     void* batch_in = nullptr;
     size_t batch_in_bytes = 0;
 
@@ -172,6 +174,13 @@ struct Ctx {
     int batch2d(int ns, const int64_t* offs, const double* x, const double* y, const double* q, const uint8_t* act,
                 const vpm_fmm_params& p, double* ex, double* ey);
     int batch_errors(unsigned* bits);
+    int prepare_batch(int ns, const int64_t* offs, const vpm_fmm_params& p, int S, const std::vector<int>& stream_of);
+    int enqueue_batch(int ns, const int64_t* offs, const double* x, const double* y, const double* q,
+                      const uint8_t* act, const vpm_fmm_params& p, double* ex, double* ey, int S,
+                      const std::vector<int>& stream_of, const std::vector<int>& order);
+    int capture_batch(int ns, const int64_t* offs, const double* x, const double* y, const double* q,
+                      const uint8_t* act, const vpm_fmm_params& p, double* ex, double* ey, int S,
+                      cudaGraphExec_t* out);
     void drop_batch();
     void drop_graph();
     void begin_ring();

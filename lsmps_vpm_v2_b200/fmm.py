@@ -100,6 +100,12 @@ class Context:
         self._check(lib().vpm_fmm2d_field_batched_device(self._h, offs.size - 1, _ptr(offs), x, y, q, active,
                                                          C.byref(p), ex, ey))
 
+    def batch_streams(self) -> int:
+        """Streams the last batched call ran on (tuned on the first graph call of a layout)."""
+        v = C.c_int32()
+        self._check(lib().vpm_batch_streams(self._h, C.byref(v)))
+        return int(v.value)
+
     def potential2d(self, x, y, q, active, params: Params | None = None, stats: bool = False):
         """phi_i = sum_j q_j log|x_i - x_j| by the 2D FMM (host arrays)."""
         x, y, q, a = _f64(x), _f64(y), _f64(q), _u8(active)
