@@ -326,6 +326,36 @@ def run_ours(args):
                "streams": ctx.batch_streams(), "launch": "one CUDA graph over all solves" if graph else "eager"}
     del bdev, bex, bey
 
+    # ---- 3D: the thin vortex ring at h = 0.0096 (2,009,183 particles), the
+    # octree treecode of the reference's default 3D path in both forms, against
+    # the FP64 direct sum on 1,024 sampled targets ----
+    rg = workloads.vortex_ring_3d(h=0.0096)
+    n3 = int(rg["x"].size)
+    r3 = [torch.from_numpy(np.ascontiguousarray(rg[k])).to(dev) for k in ("x", "y", "z", "ax", "ay", "az", "active")]
+    o3 = [torch.empty(n3, dtype=torch.float64, device=dev) for _ in range(3)]
+    tg3 = torch.from_numpy(workloads.sample_targets(n3, 1024, seed=3)).to(dev)
+    d3 = [torch.empty(tg3.numel(), dtype=torch.float64, device=dev) for _ in range(3)]
+    p3ptr = [t.data_ptr() for t in r3]
+    o3ptr = [t.data_ptr() for t in o3]
+    ctx._check(lib().vpm_direct3d_velocity_device(ctx._h, *p3ptr, n3, tg3.data_ptr(), tg3.numel(),
+                                                  *[t.data_ptr() for t in d3]))
+    den3 = torch.sqrt(sum((t * t).sum() for t in d3))
+    res3 = {}
+    for name, prec in (("fp64", PREC_FP64), ("mixed", PREC_MIXED)):
+        p3 = default_params(precision=prec)
+        run3 = lambda: ctx.velocity3d_device(n3, *p3ptr, *o3ptr, p3)  # noqa: E731
+        for _ in range(3):
+            run3()
+        ctx.sync()
+        t3 = max_over_ranks(time_steps(ctx, stream, flush, run3, 5), world, dev)
+        e3 = float((torch.sqrt(sum(((o[tg3] - d) ** 2).sum() for o, d in zip(o3, d3))) / den3).item())
+        res3[name] = {"value": world * n3 / (t3 * 1e-3), "ms_per_step": t3, "rel_l2_vs_direct": e3}
+    bench_3d = {"workload": f"vortex ring 3D h=0.0096 N={n3}", "leaf_cap": 30, "far_test": "R > 2 size",
+                "forms": res3, "mixed_over_fp64": res3["fp64"]["ms_per_step"] / res3["mixed"]["ms_per_step"],
+                "direct_sum": "FP64 direct sum on 1,024 sampled targets (vpm_direct3d_velocity_device)",
+                "launch": "eager"}
+    del r3, o3
+
     # ---- end to end through the public host API (pinned buffers) ----
     hx = torch.from_numpy(wl["x"]).pin_memory().numpy()
     hy = torch.from_numpy(wl["y"]).pin_memory().numpy()
@@ -399,6 +429,7 @@ def run_ours(args):
                 "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes,
                 "api": "vpm_velocity2d (host buffers)"},
         "batched": batched,
+        "bench_3d": bench_3d,
         "gpu_launches": launches_per_step * args.steps,
         "stages_ms": stage,
         "interactions": {"p2p_pairs": pairs, "m2l_pairs": int(st.m2l_pairs), "m2p_pairs": int(st.m2p_pairs),

@@ -405,6 +405,17 @@ int vpm_direct2d_field_device(vpm_ctx* ctx, const double* x, const double* y, co
                               double* ey);
 
 /*
+ * FP64 direct sum of the 3D velocity at m sampled targets (device pointers,
+ * int64 target indices on the device): u_t = sum over active j != t of
+ * alpha_j x (x_t - x_j) / |x_t - x_j|^3, the yardstick of the 3D treecode's
+ * error (the reference's near-field kernel, fast3DFMM.cpp:437-459, over all
+ * sources). Asynchronous on the context's stream.
+ */
+int vpm_direct3d_velocity_device(vpm_ctx* ctx, const double* x, const double* y, const double* z,
+                                 const double* ax, const double* ay, const double* az, const uint8_t* active,
+                                 int64_t n, const int64_t* targets, int64_t m, double* u, double* v, double* w);
+
+/*
  * FMA-throughput microbenchmark of the device (TFLOP/s of dependent FMA
  * chains in FP64 and FP32): the pipe peaks the near-field roofline fractions
  * are quoted against. No counterpart in the reference (measurement utility).

@@ -121,6 +121,8 @@ SIGNATURES = {
     "vpm_selector_features2d_device": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int64, C.c_double, _vp]),
     "vpm_select2d": (C.c_int, [_vp, _vp, C.c_double, C.c_double, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                C.POINTER(C.c_int32), _vp]),
+    "vpm_direct3d_velocity_device": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int64, _vp, C.c_int64,
+                                              _vp, _vp, _vp]),
     "vpm_direct2d_field_device": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int64, _vp, C.c_int64, _vp, _vp]),
     "vpm_fmm3d_velocity": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int64, C.POINTER(Params),
                                      _vp, _vp, _vp, C.POINTER(Stats)]),

@@ -323,6 +323,98 @@ __global__ void direct2d_sum(const double* __restrict__ part, int m, double* __r
     }
 }
 
+// The 3D Biot-Savart sum at sampled targets in the same arrangement:
+// partial[split][k] = sum over active j != t_k of alpha_j x r / |r|^3,
+// r = x_t - x_j (fast3DFMM.cpp:437-459 over all sources).
+__global__ void __launch_bounds__(256)
+direct3d_partial(const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ z,
+                 const double* __restrict__ ax, const double* __restrict__ ay, const double* __restrict__ az,
+                 const uint8_t* __restrict__ act, int n, const int64_t* __restrict__ tgt, int m,
+                 double* __restrict__ part) {
+    constexpr int T = kDirTargets / 2;   // targets per block (three sums each)
+    __shared__ double s_p[3][T];
+    __shared__ int64_t s_t[T];
+    __shared__ double s_red[3][8][T];
+    const int t0 = blockIdx.x * T;
+    if (threadIdx.x < T) {
+        const int k = t0 + threadIdx.x;
+        const int64_t ti = k < m ? tgt[k] : -1;
+        s_t[threadIdx.x] = ti;
+        s_p[0][threadIdx.x] = ti >= 0 ? x[ti] : 0.0;
+        s_p[1][threadIdx.x] = ti >= 0 ? y[ti] : 0.0;
+        s_p[2][threadIdx.x] = ti >= 0 ? z[ti] : 0.0;
+    }
+    __syncthreads();
+    const int split = blockIdx.y;
+    const long long per = (n + kDirSplits - 1) / kDirSplits;
+    const long long j0 = split * per, j1 = min((long long)n, j0 + per);
+    double u[T], v[T], w[T];
+    #pragma unroll
+    for (int k = 0; k < T; ++k) u[k] = v[k] = w[k] = 0.0;
+    for (long long j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+        if (!act[j]) continue;
+        const double xj = x[j], yj = y[j], zj = z[j], a1 = ax[j], a2 = ay[j], a3 = az[j];
+        #pragma unroll
+        for (int k = 0; k < T; ++k) {
+            const double ex = s_p[0][k] - xj, ey = s_p[1][k] - yj, ez = s_p[2][k] - zj;
+            const double r2 = ex * ex + ey * ey + ez * ez;
+            const double r3 = sqrt(r2) * r2;
+            const double f = (j == s_t[k]) ? 0.0 : 1.0 / r3;
+            u[k] = fma(f, a2 * ez - a3 * ey, u[k]);
+            v[k] = fma(f, a3 * ex - a1 * ez, v[k]);
+            w[k] = fma(f, a1 * ey - a2 * ex, w[k]);
+        }
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    #pragma unroll
+    for (int k = 0; k < T; ++k) {
+        double a = u[k], b = v[k], c = w[k];
+        #pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_xor_sync(0xffffffffu, a, o);
+            b += __shfl_xor_sync(0xffffffffu, b, o);
+            c += __shfl_xor_sync(0xffffffffu, c, o);
+        }
+        if (lane == 0) {
+            s_red[0][warp][k] = a;
+            s_red[1][warp][k] = b;
+            s_red[2][warp][k] = c;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < T) {
+        double a = 0.0, b = 0.0, c = 0.0;
+        for (int wv = 0; wv < 8; ++wv) {
+            a += s_red[0][wv][threadIdx.x];
+            b += s_red[1][wv][threadIdx.x];
+            c += s_red[2][wv][threadIdx.x];
+        }
+        const int k = t0 + threadIdx.x;
+        if (k < m) {
+            double* o = part + ((size_t)split * m + k) * 3;
+            o[0] = a;
+            o[1] = b;
+            o[2] = c;
+        }
+    }
+}
+
+__global__ void direct3d_sum(const double* __restrict__ part, int m, double* __restrict__ u, double* __restrict__ v,
+                             double* __restrict__ w) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
+        double a = 0.0, b = 0.0, c = 0.0;
+        for (int sp = 0; sp < kDirSplits; ++sp) {
+            const double* o = part + ((size_t)sp * m + k) * 3;
+            a += o[0];
+            b += o[1];
+            c += o[2];
+        }
+        u[k] = a;
+        v[k] = b;
+        w[k] = c;
+    }
+}
+
 }  // namespace
 
 // ---- host side -------------------------------------------------------------------
@@ -862,6 +954,37 @@ int vpm_direct2d_field_device(vpm_ctx* ctx, const double* x, const double* y, co
     dim3 grid((unsigned)((m + vpm::kDirTargets - 1) / vpm::kDirTargets), vpm::kDirSplits);
     vpm::direct2d_partial<<<grid, 256, 0, c->stream>>>(x, y, q, active, (int)n, targets, (int)m, s->dir_part);
     vpm::direct2d_sum<<<vpm::grid_for(m), 256, 0, c->stream>>>(s->dir_part, (int)m, ex, ey);
+    SEL_TRY(cudaGetLastError());
+    return VPM_OK;
+}
+
+// FP64 direct 3D velocity at m sampled targets (device pointers).
+int vpm_direct3d_velocity_device(vpm_ctx* ctx, const double* x, const double* y, const double* z, const double* ax,
+                                 const double* ay, const double* az, const uint8_t* active, int64_t n,
+                                 const int64_t* targets, int64_t m, double* u, double* v, double* w) {
+    if (!ctx) return VPM_EINVAL;
+    Ctx* c = (Ctx*)ctx;
+    if (n < 1 || n >= (1ll << 31) || m < 0 || m >= (1ll << 31)) return c->fail(VPM_EINVAL, "n or m out of range");
+    if (m == 0) return VPM_OK;
+    if (!x || !y || !z || !ax || !ay || !az || !active || !targets || !u || !v || !w)
+        return c->fail(VPM_EINVAL, "null buffer");
+    SEL_TRY(cudaSetDevice(c->device));
+    Selector* s = selector_of(c);
+    if (!s) return c->fail(VPM_ENOMEM, "selector");
+    SEL_TRY(vpm::sel_alloc(*s));
+    const size_t need = sizeof(double) * 3 * vpm::kDirSplits * (size_t)m;
+    if (s->dir_part_cap < need) {
+        if (s->dir_part) cudaFree(s->dir_part);
+        s->dir_part = nullptr;
+        s->dir_part_cap = 0;
+        SEL_TRY(cudaMalloc(&s->dir_part, need));
+        s->dir_part_cap = need;
+    }
+    const int T = vpm::kDirTargets / 2;
+    dim3 grid((unsigned)((m + T - 1) / T), vpm::kDirSplits);
+    vpm::direct3d_partial<<<grid, 256, 0, c->stream>>>(x, y, z, ax, ay, az, active, (int)n, targets, (int)m,
+                                                       s->dir_part);
+    vpm::direct3d_sum<<<vpm::grid_for(m), 256, 0, c->stream>>>(s->dir_part, (int)m, u, v, w);
     SEL_TRY(cudaGetLastError());
     return VPM_OK;
 }

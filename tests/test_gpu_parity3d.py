@@ -182,3 +182,30 @@ def test_coincident_particles_report_error(ctx):
         d[k][:40] = 0.25
     with pytest.raises(VpmError):
         ctx.velocity3d_alpha(d["x"], d["y"], d["z"], d["ax"], d["ay"], d["az"], d["active"], params())
+
+
+def test_direct3d_device_matches_oracle(ctx, port):
+    """The library's FP64 3D direct sum (the yardstick of the 3D error in the
+    bench) against the oracle's on sampled targets of a partly inactive ring."""
+    import ctypes as C
+    import torch
+    from lsmps_vpm_v2_b200._lib import lib
+    r = workloads.vortex_ring_3d(h=0.05)
+    act = r["active"].copy()
+    act[::7] = 0
+    args = (r["x"], r["y"], r["z"], r["ax"], r["ay"], r["az"], act)
+    tg = workloads.sample_targets(r["x"].size, 777, seed=2)
+    dev = [torch.from_numpy(np.ascontiguousarray(v)).cuda() for v in args]
+    t = torch.from_numpy(tg).cuda()
+    out = [torch.empty(tg.size, dtype=torch.float64, device="cuda") for _ in range(3)]
+    ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+    try:
+        ctx._check(lib().vpm_direct3d_velocity_device(ctx._h, *[C.c_void_p(v.data_ptr()) for v in dev], r["x"].size,
+                                                       C.c_void_p(t.data_ptr()), tg.size,
+                                                       *[C.c_void_p(o.data_ptr()) for o in out]))
+        torch.cuda.synchronize()
+    finally:
+        ctx.set_stream(None)
+    ref = port.direct3d_velocity(*args, tg)
+    got = [o.cpu().numpy() for o in out]
+    assert workloads.rel_l2(got, ref) <= 1e-13
