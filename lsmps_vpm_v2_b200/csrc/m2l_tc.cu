@@ -593,12 +593,13 @@ m2l_parent_tc(Tree2D t, const int32_t* __restrict__ blk, const float* __restrict
 // operations per (child, source) instead of 288 for the dense 2P x 2(P+1)
 // operator. C and the powers tau^-k of the 49 offsets are kernel parameters
 // (constant bank, read as broadcast operands). A block takes 32 parents, one
-// per lane; warp q computes child q of every parent. The block first gathers
-// the scaled moments of all 32 x 32 (position, parent) sources into shared
-// memory (one round of independent loads, FP64 moments rounded once after
-// scaling by the child level's 1 / length^k); then each warp walks the 27
-// positions not adjacent to its child. Sums run in position order, so the
-// result does not depend on the schedule.
+// per lane; warps q and q + 4 compute child q of every parent over positions
+// 0..15 and 16..31. The block first gathers the scaled moments of all 32 x 32
+// (position, parent) sources into shared memory (one round of independent
+// loads, FP64 moments rounded once after scaling by the child level's
+// 1 / length^k); then each warp walks its positions not adjacent to its
+// child, and the first half's sums are added to the second's. Sums run in
+// position order, so the result does not depend on the schedule.
 constexpr int kPF32MaxP = 16;
 
 template <int P>
@@ -608,15 +609,17 @@ struct ParF32Args {
 };
 
 template <int P>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(256)
 m2l_parent_f32(Tree2D t, const int32_t* __restrict__ blk, const double2* __restrict__ a, double2* __restrict__ b,
                const __grid_constant__ ParF32Args<P> args, unsigned* err) {
     constexpr int Q = P + 1;
     extern __shared__ float2 pf_A[];             // [32 positions][Q][32 parents]
     __shared__ int s_src[kParPos][32];           // [position][parent]
     __shared__ double s_rp[32][Q];               // [parent][k]: (1 / child length)^k
+    __shared__ float s_half[4][2 * P][32];       // the first position half's sums [child][output][parent]
     if (fatal(err)) return;
-    const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
+    const int q = wq & 3, half = wq >> 2;
     const int qx = q & 1, qy = q >> 1;
     const int np = t.info->n_cells - t.info->n_leaves;   // non-leaf cells; the root is the first
     const int nparents = np > 1 ? np - 1 : 0;
@@ -625,7 +628,7 @@ m2l_parent_f32(Tree2D t, const int32_t* __restrict__ blk, const double2* __restr
     for (int tile = blockIdx.x; tile * 32 < nparents; tile += gridDim.x) {
         const int pi = 1 + tile * 32 + lane;
         const int par = pi < np ? t.nonleaf[pi] : -1;
-        if (q == 0) {
+        if (wq == 0) {
             const double rinv = par >= 0 ? ldexp(1.0, (int)t.c_level[par] + 1) / root : 0.0;
             double r = 1.0;
             #pragma unroll
@@ -634,7 +637,7 @@ m2l_parent_f32(Tree2D t, const int32_t* __restrict__ blk, const double2* __restr
                 r *= rinv;
             }
         }
-        if (q == 1) {
+        if (wq == 1) {
             if (par >= 0 && !irregular) {
                 const int4* bp = reinterpret_cast<const int4*>(blk + (size_t)par * kParPos);
                 #pragma unroll
@@ -667,7 +670,7 @@ m2l_parent_f32(Tree2D t, const int32_t* __restrict__ blk, const double2* __restr
         float accr[P], acci[P];
         #pragma unroll
         for (int p = 0; p < P; ++p) accr[p] = acci[p] = 0.f;
-        for (int j = 0; j < kParPos; ++j) {
+        for (int j = half * (kParPos / 2); j < (half + 1) * (kParPos / 2); ++j) {
             const int k8 = j >> 2, d = j & 3, nb = k8 < 4 ? k8 : k8 + 1;
             const int tx = 2 * (nb % 3 - 1) + (d & 1) - qx, ty = 2 * (nb / 3 - 1) + (d >> 1) - qy;
             if (tx >= -1 && tx <= 1 && ty >= -1 && ty <= 1) continue;   // adjacent: not in this child's list 2
@@ -693,7 +696,20 @@ m2l_parent_f32(Tree2D t, const int32_t* __restrict__ blk, const double2* __restr
                 acci[p] = fmaf(w.x, bi, fmaf(w.y, br, acci[p]));
             }
         }
-        if (par >= 0) {
+        if (half == 0) {
+            #pragma unroll
+            for (int p = 0; p < P; ++p) {
+                s_half[q][p][lane] = accr[p];
+                s_half[q][P + p][lane] = acci[p];
+            }
+        }
+        __syncthreads();
+        if (half == 1 && par >= 0) {
+            #pragma unroll
+            for (int p = 0; p < P; ++p) {
+                accr[p] = s_half[q][p][lane] + accr[p];
+                acci[p] = s_half[q][P + p][lane] + acci[p];
+            }
             const unsigned m = t.c_chmask[par];
             if (m & (1u << q)) {
                 const int ch = t.c_child0[par] + __popc(m & ((1u << q) - 1u));
@@ -733,9 +749,9 @@ cudaError_t launch_m2l_parent_f32(const Tree2D& t, const Lists2D& l, Expansions2
     cudaError_t r = cudaFuncSetAttribute(m2l_parent_f32<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (r != cudaSuccess) return r;
     int occ = 0;
-    r = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, m2l_parent_f32<P>, 128, smem);
+    r = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, m2l_parent_f32<P>, 256, smem);
     if (r != cudaSuccess) return r;
-    m2l_parent_f32<P><<<148 * (occ > 0 ? occ : 1), 128, smem, st>>>(t, l.l2_blk, e.a, e.b, args, err);
+    m2l_parent_f32<P><<<148 * (occ > 0 ? occ : 1), 256, smem, st>>>(t, l.l2_blk, e.a, e.b, args, err);
     return cudaGetLastError();
 }
 
