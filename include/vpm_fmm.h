@@ -128,6 +128,12 @@ const char* vpm_last_error(vpm_ctx* ctx);
  *   fmm2D::get_Field_x / get_Field_y                src/FMM/fmm2D.cpp:1146-1157
  * ex/ey are the reference's Ex/Ey (the velocity is u = Ey, v = -Ex).
  * Host buffers of n elements. stats may be NULL.
+ * Host entry points (this one, vpm_fmm2d_potential, vpm_velocity2d) upload
+ * positions and flags first and build the tree and lists while the strengths
+ * (vorticity and core sizes) are still being copied; with page-locked host
+ * buffers those copies overlap the tree build. The outputs come back in the
+ * same round trip as the error word, so on a non-zero status they may have
+ * been partly written.
  */
 int vpm_fmm2d_field(vpm_ctx* ctx, const double* x, const double* y, const double* q,
                     const uint8_t* active, int64_t n, const vpm_fmm_params* prm,

@@ -221,7 +221,11 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
     VPM_CUDA_TRY(cudaMemsetAsync(d_err, 0, sizeof(unsigned), st));
     if (int r = ensure_coefs(p)) return r;
     if (int r = record(0)) return r;
-    VPM_CUDA_TRY(keys_sort2d(x, y, q, act, tree, ts, p.exp_tree_pct, d_err, st, &launches,
+    // Strengths still in flight on `upload` (q_ready): sort without them and
+    // gather them in tree order just before their first reader.
+    const bool deferred = q_ready != nullptr && !tree_only;
+    const unsigned wait_flags = capturing ? cudaEventWaitExternal : 0u;
+    VPM_CUDA_TRY(keys_sort2d(x, y, deferred ? nullptr : q, act, tree, ts, p.exp_tree_pct, d_err, st, &launches,
                              std::min(p.max_src, p.max_par)));
     if (int r = record(1)) return r;
     VPM_CUDA_TRY(levels2d(tree, ts, p.max_src, p.max_par, d_err, st, &launches));
@@ -234,6 +238,11 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
         // writes the output.
         VPM_CUDA_TRY(cudaEventRecord(fork2, st));
         VPM_CUDA_TRY(cudaStreamWaitEvent(side, fork2, 0));
+        if (deferred) {
+            VPM_CUDA_TRY(cudaStreamWaitEvent(st, q_ready, wait_flags));
+            VPM_CUDA_TRY(gather_strengths2d(tree, q, d_err, st, &launches));
+            VPM_CUDA_TRY(cudaEventRecord(ev_qg, st));
+        }
         const bool slots = p.precision != VPM_PREC_FP64 && int_lists_slotted(lists);
         if (slots) {
             // the mixed near field starts from the list slots; the CSR (for
@@ -241,17 +250,20 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
             // third side stream meanwhile
             VPM_CUDA_TRY(build_int_slots2d(tree, lists, p.eps, d_err, side, &launches));
             VPM_CUDA_TRY(cudaEventRecord(ev_slots, side));
+            if (deferred) VPM_CUDA_TRY(cudaStreamWaitEvent(side, ev_qg, 0));
             VPM_CUDA_TRY(fmm2d_p2p_f32(tree, lists, ex2, near_x, near_y, 0, 0.0, 0.0, d_err, side, &launches, true,
                                        kP2PListSlots));
             VPM_CUDA_TRY(cudaStreamWaitEvent(side3, ev_slots, 0));
             VPM_CUDA_TRY(build_int_csr2d(tree, lists, ts.scan, p.eps, d_err, side3, &launches));
             VPM_CUDA_TRY(cudaEventRecord(ev_l13, side3));
+            if (deferred) VPM_CUDA_TRY(cudaStreamWaitEvent(side3, ev_qg, 0));
             VPM_CUDA_TRY(fmm2d_p2p_f32(tree, lists, ex2, near_x, near_y, 0, 0.0, 0.0, d_err, side3, &launches, true,
                                        kP2PListSpill));
             VPM_CUDA_TRY(cudaEventRecord(join5, side3));
         } else {
             VPM_CUDA_TRY(build_int_lists2d(tree, lists, ts.scan, p.eps, d_err, side, &launches));
             VPM_CUDA_TRY(cudaEventRecord(ev_l13, side));
+            if (deferred) VPM_CUDA_TRY(cudaStreamWaitEvent(side, ev_qg, 0));
             if (p.precision != VPM_PREC_FP64)
                 VPM_CUDA_TRY(fmm2d_p2p_f32(tree, lists, ex2, near_x, near_y, 0, 0.0, 0.0, d_err, side, &launches, true));
             else
@@ -291,6 +303,10 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
         for (int i = 4; i < kStageEvents; ++i)
             if (int r = record(i)) return r;
     } else {
+        if (deferred) {
+            VPM_CUDA_TRY(cudaStreamWaitEvent(st, q_ready, wait_flags));
+            VPM_CUDA_TRY(gather_strengths2d(tree, q, d_err, st, &launches));
+        }
         VPM_CUDA_TRY(fmm2d_upward_direct(tree, ex2, p.p, p.binom == VPM_BINOM_EXACT, d_err, st, &launches));
         if (int r = record(4)) return r;
         if (velocity == kModePotential) VPM_CUDA_TRY(fmm2d_m2l_only(tree, lists, ex2, p.p, d_err, st, &launches));
@@ -425,6 +441,7 @@ int Ctx::launch2d(const double* x, const double* y, const double* q, const uint8
     k.ptr[0] = x; k.ptr[1] = y; k.ptr[2] = q; k.ptr[3] = act; k.ptr[4] = o0; k.ptr[5] = o1;
     k.n = n; k.K = K; k.velocity = velocity; k.uinf = uinf; k.vinf = vinf; k.p = p; k.stream = stream;
     k.arena = arena2d;
+    k.deferred = q_ready != nullptr;
     const bool split = p.use_graph == 2;
     const bool have = split ? stage_exec[0] != nullptr : gexec != nullptr;
     if (have && std::memcmp(&k, &gkey, sizeof(k)) == 0) {
@@ -541,26 +558,46 @@ int Ctx::run2d_host(const double* x, const double* y, const double* q_or_omega, 
         }
         r = reserve2d(n, cells, p.p, l1, l3);
         if (r) return r;
+        // Positions and flags first on the main stream: the sort and the tree
+        // and list builds need nothing else. The strengths (or vorticity and
+        // core size) follow on `upload`, ordered after them on the copy
+        // engine, and are waited for only where P2M and P2P first read them.
         VPM_CUDA_TRY(cudaMemcpyAsync(in_x, x, sizeof(double) * n, cudaMemcpyHostToDevice, stream));
         VPM_CUDA_TRY(cudaMemcpyAsync(in_y, y, sizeof(double) * n, cudaMemcpyHostToDevice, stream));
         VPM_CUDA_TRY(cudaMemcpyAsync(in_act, act, n, cudaMemcpyHostToDevice, stream));
         if (tree_only) {
             VPM_CUDA_TRY(cudaMemsetAsync(in_q, 0, sizeof(double) * n, stream));
-        } else if (velocity == 1) {
-            VPM_CUDA_TRY(cudaMemcpyAsync(in_q, q_or_omega, sizeof(double) * n, cudaMemcpyHostToDevice, stream));
-            VPM_CUDA_TRY(cudaMemcpyAsync(out0, s, sizeof(double) * n, cudaMemcpyHostToDevice, stream));
-            source_from_vorticity<<<std::min(1184, ceil_div(n, 256)), 256, 0, stream>>>(in_q, out0, n, in_q);
-            VPM_CUDA_TRY(cudaGetLastError());
         } else {
-            VPM_CUDA_TRY(cudaMemcpyAsync(in_q, q_or_omega, sizeof(double) * n, cudaMemcpyHostToDevice, stream));
+            VPM_CUDA_TRY(cudaEventRecord(ev_upload, stream));
+            VPM_CUDA_TRY(cudaStreamWaitEvent(upload, ev_upload, 0));
+            VPM_CUDA_TRY(cudaMemcpyAsync(in_q, q_or_omega, sizeof(double) * n, cudaMemcpyHostToDevice, upload));
+            if (velocity == 1) {
+                // the core sizes pass through out0, which the evaluation
+                // writes only after it has waited for ev_q
+                VPM_CUDA_TRY(cudaMemcpyAsync(out0, s, sizeof(double) * n, cudaMemcpyHostToDevice, upload));
+                source_from_vorticity<<<std::min(1184, ceil_div(n, 256)), 256, 0, upload>>>(in_q, out0, n, in_q);
+                VPM_CUDA_TRY(cudaGetLastError());
+            }
+            VPM_CUDA_TRY(cudaEventRecord(ev_q, upload));
+            q_ready = ev_q;
         }
         last_was_graph = p.use_graph != 0 && !tree_only;
         if (tree_only) last_timed = true;
         r = tree_only ? enqueue2d(in_x, in_y, in_q, in_act, n, p, K, out0, out1, velocity, uinf, vinf, true)
                       : launch2d(in_x, in_y, in_q, in_act, n, p, K, out0, out1, velocity, uinf, vinf);
-        if (r) return r;
+        q_ready = nullptr;
+        if (r) {
+            cudaStreamSynchronize(upload);
+            return r;
+        }
+        // The error word and the outputs in one round trip: on an error the
+        // outputs are discarded (retried, or the call fails).
         unsigned bits = 0;
         VPM_CUDA_TRY(cudaMemcpyAsync(&bits, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+        if (!tree_only) {
+            VPM_CUDA_TRY(cudaMemcpyAsync(o0, out0, sizeof(double) * n, cudaMemcpyDeviceToHost, stream));
+            if (o1) VPM_CUDA_TRY(cudaMemcpyAsync(o1, out1, sizeof(double) * n, cudaMemcpyDeviceToHost, stream));
+        }
         VPM_CUDA_TRY(cudaStreamSynchronize(stream));
         if (bits & ERR_DEPTH) {
             if (K < kMaxLevels2D) { K = kMaxLevels2D; depth_retry = 1; continue; }
@@ -569,9 +606,6 @@ int Ctx::run2d_host(const double* x, const double* y, const double* q_or_omega, 
         if (bits & (ERR_CELL_CAP | ERR_LIST_CAP)) { grow = true; continue; }
         if (bits) return map_err(bits);
         if (tree_only) return stats ? collect_stats(stats) : VPM_OK;
-        VPM_CUDA_TRY(cudaMemcpyAsync(o0, out0, sizeof(double) * n, cudaMemcpyDeviceToHost, stream));
-        if (o1) VPM_CUDA_TRY(cudaMemcpyAsync(o1, out1, sizeof(double) * n, cudaMemcpyDeviceToHost, stream));
-        VPM_CUDA_TRY(cudaStreamSynchronize(stream));
         if (stats) return collect_stats(stats);
         return VPM_OK;
     }

@@ -48,10 +48,11 @@ Ctx::~Ctx() {
     if (side) cudaStreamDestroy(side);
     if (side2) cudaStreamDestroy(side2);
     if (side3) cudaStreamDestroy(side3);
+    if (upload) cudaStreamDestroy(upload);
     if (join3) cudaEventDestroy(join3);
     if (fork2) cudaEventDestroy(fork2);
     if (join2) cudaEventDestroy(join2);
-    for (cudaEvent_t x : {ev_up, ev_l13, join4, ev_slots, join5})
+    for (cudaEvent_t x : {ev_up, ev_l13, join4, ev_slots, join5, ev_upload, ev_q, ev_qg})
         if (x) cudaEventDestroy(x);
 }
 
@@ -67,6 +68,7 @@ int Ctx::init(int dev) {
     e = cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&side2, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&side3, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&upload, cudaStreamNonBlocking);
     if (e != cudaSuccess) return fail_cuda(e, "cudaStreamCreate");
     e = cudaEventCreateWithFlags(&fork2, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&join2, cudaEventDisableTiming);
@@ -76,6 +78,9 @@ int Ctx::init(int dev) {
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&join4, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_slots, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&join5, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_upload, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_q, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_qg, cudaEventDisableTiming);
     if (e != cudaSuccess) return fail_cuda(e, "cudaEventCreate");
     e = cudaMalloc(&d_err, 64);
     if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc");

@@ -56,6 +56,13 @@ struct Ctx {
     cudaEvent_t ev_up = nullptr, ev_l13 = nullptr, join4 = nullptr;   // upward done, lists 1/3 done, M2P done
     cudaStream_t side3 = nullptr;   // CSR of lists 1/3 while the near field runs from the slots
     cudaEvent_t ev_slots = nullptr, join5 = nullptr;   // list slots done, near field of spilled leaves done
+    // Host entry points: the strengths (or vorticity and core size) are
+    // copied on `upload` while the main stream sorts the particles and builds
+    // the tree and lists; `q_ready` (recorded on `upload`) is set while an
+    // evaluation waits for them, and `ev_qg` marks the strengths in tree order.
+    cudaStream_t upload = nullptr;
+    cudaEvent_t ev_upload = nullptr, ev_q = nullptr, ev_qg = nullptr;
+    cudaEvent_t q_ready = nullptr;
     double *near_x = nullptr, *near_y = nullptr;
     std::string last_error;
     unsigned* d_err = nullptr;
@@ -85,6 +92,7 @@ struct Ctx {
         vpm_fmm_params p;
         cudaStream_t stream;
         void* arena;
+        int deferred;   // the strengths arrive on `upload` (q_ready)
     };
     cudaGraphExec_t gexec = nullptr;
     GraphKey gkey{};

@@ -161,9 +161,14 @@ cudaError_t build_tree2d(const double* x, const double* y, const double* q, cons
 // active-count scan; then the level-by-level cell construction.
 // shallow_cap = min(max_src, max_par): lets the cooperative sort try three
 // radix passes first (see sort2d_coop); 0 always sorts the full keys.
+// q = null sorts without the strengths: t.pq is then left for
+// gather_strengths2d, so that the strengths can still be in flight from the
+// host while the tree and the lists are built.
 cudaError_t keys_sort2d(const double* x, const double* y, const double* q, const uint8_t* act, Tree2D& t,
                         TreeScratch2D& s, double exp_pct, unsigned* err, cudaStream_t st, int* launches,
                         int shallow_cap = 0);
+// t.pq[i] = q[t.perm[i]] for i < t.n.
+cudaError_t gather_strengths2d(const Tree2D& t, const double* q, unsigned* err, cudaStream_t st, int* launches);
 cudaError_t levels2d(Tree2D& t, TreeScratch2D& s, int max_src, int max_par, unsigned* err, cudaStream_t st,
                      int* launches);
 

@@ -132,7 +132,8 @@ __global__ void keys2d(const double* __restrict__ x, const double* __restrict__ 
 
 // Sorted copies of the particle data and the active flags as 0/1 words; the
 // sorted keys (from whichever buffer the sort ended in, 32- or 64-bit) and
-// permutation land in the tree's own arrays.
+// permutation land in the tree's own arrays. q may be null: the strengths are
+// then gathered later (gather_strengths2d).
 template <typename KT>
 __global__ void gather2d(const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ q,
                          const uint8_t* __restrict__ act, const KT* __restrict__ skey,
@@ -148,7 +149,7 @@ __global__ void gather2d(const double* __restrict__ x, const double* __restrict_
         }
         px[i] = x[j];
         py[i] = y[j];
-        pq[i] = q[j];
+        if (q) pq[i] = q[j];
         uint8_t a = act[j] ? 1 : 0;
         pact[i] = a;
         act_u32[i] = a;
@@ -271,7 +272,7 @@ sort2d_coop(const double* __restrict__ x, const double* __restrict__ y, const do
         #pragma unroll 6
         for (int i = c0 + tid; i < c1; i += kCoopSortThreads) {
             const double a = x[i], c = y[i];
-            aos[i] = make_double4(a, c, q[i], act[i] ? 1.0 : 0.0);
+            aos[i] = make_double4(a, c, q ? q[i] : 0.0, act[i] ? 1.0 : 0.0);
             bad |= !isfinite(a) || !isfinite(c);
             mnx = fmin(mnx, a); mxx = fmax(mxx, a);
             mny = fmin(mny, c); mxy = fmax(mxy, c);
@@ -515,7 +516,7 @@ sort2d_coop(const double* __restrict__ x, const double* __restrict__ y, const do
                 t.perm[pos] = val;
                 t.px[pos] = e.x;
                 t.py[pos] = e.y;
-                t.pq[pos] = e.z;
+                if (q) t.pq[pos] = e.z;
                 t.pact[pos] = (uint8_t)(vf >> 31);
                 t.actscan[pos] = s_abase[d] + s_rank[j];
             }
@@ -1004,6 +1005,30 @@ cudaError_t keys_sort2d(const double* x, const double* y, const double* q, const
     *launches += 1;
     e = scan_exclusive(s.act_u32, t.actscan, n, t.actscan + n, s.scan, err, st);
     if (e != cudaSuccess) return e;
+    *launches += 1;
+    return cudaGetLastError();
+}
+
+namespace {
+// pq[i] = q[perm[i]]: the strengths in tree order, for a sort that ran
+// without them (keys_sort2d with q = null).
+__global__ void __launch_bounds__(256) gather_strengths2d(const uint32_t* __restrict__ perm,
+                                                          const double* __restrict__ q, double* __restrict__ pq, int n,
+                                                          unsigned* err) {
+    if (fatal(err)) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t j = __ldg(perm + i);
+        if (j >= (uint32_t)n) {
+            set_err(err, ERR_INDEX);
+            continue;
+        }
+        pq[i] = __ldg(q + j);
+    }
+}
+}  // namespace
+
+cudaError_t gather_strengths2d(const Tree2D& t, const double* q, unsigned* err, cudaStream_t st, int* launches) {
+    gather_strengths2d<<<std::max(1, std::min(148 * 8, ceil_div(t.n, 256))), 256, 0, st>>>(t.perm, q, t.pq, t.n, err);
     *launches += 1;
     return cudaGetLastError();
 }
