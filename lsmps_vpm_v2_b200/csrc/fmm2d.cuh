@@ -234,13 +234,6 @@ cudaError_t fmm2d_potential_eval(const Tree2D& t, const Lists2D& l, Expansions2D
 // order P).
 bool l2l_direct_ok(int P, bool exact);
 cudaError_t fmm2d_l2l_leaves(const Tree2D& t, Expansions2D& e, int P, unsigned* err, cudaStream_t st, int* launches);
-// List-2 M2L of the mixed form (m2l_tc.cu) on scaled expansions: on the FP32
-// pipes for orders 1..12 (fmm2d_m2l_f32), on the tensor cores (tcgen05,
-// 3xTF32) for orders 13..20; both add list 4 in FP64 afterwards.
-bool m2l_f32_supported(int P);
-cudaError_t set_m2l_f32_operators(int P, const double2* op_dev, float* dst, cudaStream_t st);
-cudaError_t fmm2d_m2l_f32(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, float* rows, const float* ops,
-                          unsigned* err, cudaStream_t st, int* launches);
 // List-2 M2L of the mixed form per parent (m2l_tc.cu, m2l_parent_tc): one
 // tensor-core product over all non-leaf cells, orders 1..16; list 4 in FP64.
 bool m2l_parent_supported(int P);

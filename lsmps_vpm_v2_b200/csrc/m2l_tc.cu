@@ -755,151 +755,6 @@ cudaError_t launch_m2l_parent_f32(const Tree2D& t, const Lists2D& l, Expansions2
     return cudaGetLastError();
 }
 
-// ---- the same scaled list-2 M2L on the FP32 pipes (orders 1..kF32MaxP) ----
-//
-// b~ = sum over offsets tau of T_tau a~ in FP32. A warp takes 32 / NG
-// consecutive target cells, NG = (2P rounded up to 4) / 4 lanes per target,
-// each lane four of the target's 2P real outputs. The warp walks the offsets
-// present in its targets' lists in increasing order; at offset tau every
-// lane applies its four rows of the same operator (shared memory, one
-// 16-byte read per input) to the scaled row of its target's source (zero
-// when it has none), accumulating in registers. The next offset's rows are
-// loaded while the current one is applied. FP32 products and sums carry
-// about 24 bits, as the 3xTF32 tensor-core form; the order of the sums is
-// fixed.
-constexpr int kF32MaxP = 12;
-constexpr int kF32Warps = 8;
-
-__host__ __device__ constexpr int f32_rp(int P) { return ((2 * (P + 1) + 3) / 4) * 4; }   // row stride (floats)
-__host__ __device__ constexpr int f32_nrp(int P) { return ((2 * P + 3) / 4) * 4; }       // outputs, padded
-
-// Scaled multipole rows [Re a~_0..Re a~_P, Im a~_0..Im a~_P, 0..] in FP32, and
-// after the last cell (row n_cells) a row of zeros: the source of an empty slot.
-__global__ void m2l_rows_f32(Tree2D t, const double2* __restrict__ a, float* __restrict__ rows, int P, int RP,
-                             unsigned* err) {
-    if (fatal(err)) return;
-    const int nc = t.info->n_cells;
-    const double root = t.geom->root;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < (long long)(nc + 1) * RP;
-         i += (long long)gridDim.x * blockDim.x) {
-        const int c = (int)(i / RP), k = (int)(i - (long long)c * RP);
-        float v = 0.f;
-        if (c < nc && k < 2 * (P + 1)) {
-            const int kk = k <= P ? k : k - (P + 1);
-            const double rinv = ldexp(1.0, (int)t.c_level[c]) / root;
-            double sc = 1.0;
-            for (int e = 0; e < kk; ++e) sc *= rinv;
-            const double2 ak = a[(size_t)c * (P + 1) + kk];
-            v = (float)((k <= P ? ak.x : ak.y) * sc);
-        }
-        rows[i] = v;
-    }
-}
-
-// One instantiation per order P (all loops have constant bounds).
-template <int P>
-__global__ void __launch_bounds__(32 * kF32Warps)
-m2l2d_f32(Tree2D t, Lists2D l, const float* __restrict__ rows, const float* __restrict__ ops,
-          double2* __restrict__ b, unsigned* err) {
-    extern __shared__ __align__(16) float f32_smem[];
-    constexpr int NRP = f32_nrp(P), NG = NRP / 4, TPW = 32 / NG;
-    constexpr int RP = f32_rp(P), RQ = RP / 4, K2 = 2 * (P + 1);
-    float* s_op = f32_smem;                                                         // [49][K2][NRP]
-    int* s_src = reinterpret_cast<int*>(s_op + (size_t)49 * K2 * NRP);              // [warps][49][TPW]
-    if (fatal(err)) return;
-    for (int i = threadIdx.x; i < 49 * K2 * NRP / 4; i += blockDim.x)
-        reinterpret_cast<float4*>(s_op)[i] = reinterpret_cast<const float4*>(ops)[i];
-    __syncthreads();
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int tl = lane / NG, g = lane - tl * NG;   // target of the lane, output group
-    int* my_src = s_src + (size_t)wib * 49 * TPW;
-    const int c_begin = t.info->level_start[2], c_end = t.info->n_cells;
-    const int ntasks = (c_end - c_begin + TPW - 1) / TPW;
-    const double root = t.geom->root;
-    for (int task = blockIdx.x * kF32Warps + wib; task < ntasks; task += gridDim.x * kF32Warps) {
-        const int c = c_begin + task * TPW + tl;
-        const bool valid = tl < TPW && c < c_end;
-        for (int i = lane; i < 49 * TPW; i += 32) my_src[i] = c_end;   // the zero row
-        __syncwarp();
-        uint32_t m_lo = 0, m_hi = 0;   // offsets present in this target's list
-        if (valid && g == 0) {
-            const int n2 = l.l2_n[c];
-            for (int k = 0; k < n2; ++k) {
-                const int slot = l.l2_slot[(size_t)c * kList2Cap + k];
-                my_src[slot * TPW + tl] = l.l2_src[(size_t)c * kList2Cap + k];
-                if (slot < 32) m_lo |= 1u << slot;
-                else m_hi |= 1u << (slot - 32);
-            }
-        }
-        __syncwarp();
-        uint64_t mask = ((uint64_t)__reduce_or_sync(0xffffffffu, m_hi) << 32) | __reduce_or_sync(0xffffffffu, m_lo);
-        float acc[4] = {0.f, 0.f, 0.f, 0.f};
-        // row of this lane's target's source at offset tau (the zero row when it has none)
-        auto load_row = [&](int tau, float4* dst) {
-            const int src = valid ? my_src[tau * TPW + tl] : c_end;
-            const float4* row = reinterpret_cast<const float4*>(rows + (size_t)src * RP);
-            #pragma unroll
-            for (int q = 0; q < RQ; ++q) dst[q] = __ldg(row + q);
-        };
-        auto apply = [&](int tau, const float4* row) {
-            const float4* T = reinterpret_cast<const float4*>(s_op + (size_t)tau * K2 * NRP) + g;
-            #pragma unroll
-            for (int q = 0; q < RQ; ++q) {
-                const float av[4] = {row[q].x, row[q].y, row[q].z, row[q].w};
-                #pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int k = 4 * q + u;
-                    if (k >= K2) break;
-                    const float4 w = T[k * NG];
-                    acc[0] = fmaf(w.x, av[u], acc[0]);
-                    acc[1] = fmaf(w.y, av[u], acc[1]);
-                    acc[2] = fmaf(w.z, av[u], acc[2]);
-                    acc[3] = fmaf(w.w, av[u], acc[3]);
-                }
-            }
-        };
-        auto next_tau = [&]() {
-            const int tt = mask ? __ffsll((long long)mask) - 1 : 49;
-            mask &= mask - 1;
-            return tt;
-        };
-        // offsets in increasing order, two row buffers in turn (the next row
-        // loads while the current one is applied)
-        float4 ra[RQ], rb[RQ];
-        int ta = next_tau();
-        if (ta < 49) load_row(ta, ra);
-        while (ta < 49) {
-            const int tb = next_tau();
-            if (tb < 49) load_row(tb, rb);
-            apply(ta, ra);
-            if (tb >= 49) break;
-            ta = next_tau();
-            if (ta < 49) load_row(ta, ra);
-            apply(tb, rb);
-        }
-        if (valid) {
-            // output r = 4 g + i is Re b~_{r+1} (r < P) or Im b~_{r-P+1} (P <= r < 2P)
-            const double rinv = ldexp(1.0, (int)t.c_level[c]) / root;
-            double* bc = reinterpret_cast<double*>(b + (size_t)c * (P + 1));
-            if (g == 0) {
-                bc[0] = 0.0;
-                bc[1] = 0.0;
-            }
-            #pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                const int r = 4 * g + i;
-                if (r < 2 * P) {
-                    const int pp = r < P ? r + 1 : r - P + 1;
-                    double rk = 1.0;
-                    for (int e = 0; e < pp; ++e) rk *= rinv;
-                    bc[2 * pp + (r < P ? 0 : 1)] = (double)acc[i] * rk;
-                }
-            }
-        }
-        __syncwarp();
-    }
-}
-
 // List 4 of every cell (FP64, direct formula of fmm2D.cpp:504-520), added
 // to b; with with_list2 on a tree flagged l2_irregular, list 2 as well (the
 // per-parent M2L then left b at zero). One warp per cell with sources; the
@@ -958,7 +813,6 @@ m2l_list4_add(Tree2D t, Lists2D l, const double2* __restrict__ a, double2* __res
 }  // namespace
 
 bool m2l_tc_supported(int P) { return P >= 1 && P <= 20; }
-bool m2l_f32_supported(int P) { return P >= 1 && P <= kF32MaxP; }
 bool m2l_parent_supported(int P) { return P >= 1 && P <= kParMaxP && par_stages(P) >= 2; }
 
 size_t m2l_tc_rows_bytes(int cap_cells) { return sizeof(float) * (size_t)cap_cells * 2 * kTcMaxK; }
@@ -1115,70 +969,6 @@ cudaError_t fmm2d_m2l_tc(const Tree2D& t, const Lists2D& l, Expansions2D& e, int
     cudaError_t r = cudaFuncSetAttribute(m2l2d_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (r != cudaSuccess) return r;
     m2l2d_tc<<<148 * 2, kTcRows, smem, st>>>(t, l, rows, ops, e.b, P, KP, NP, err);
-    m2l_list4_add<<<148 * 8, 128, 0, st>>>(t, l, e.a, e.b, e.coef, P, false, err);
-    *launches += 3;
-    return cudaGetLastError();
-}
-
-
-// The 49 list-2 operators for m2l2d_f32 as FP32 [slot][k][r]: k the input
-// (Re a~_0..P, Im a~_0..P), r the output (Re b~_1..P, Im b~_1..P, padding).
-// Synchronises.
-cudaError_t set_m2l_f32_operators(int P, const double2* op_dev, float* dst, cudaStream_t st) {
-    const int K2 = 2 * (P + 1), NRP = f32_nrp(P);
-    std::vector<double2> op((size_t)49 * (P + 1) * P);
-    cudaError_t e = cudaMemcpyAsync(op.data(), op_dev, sizeof(double2) * op.size(), cudaMemcpyDeviceToHost, st);
-    if (e != cudaSuccess) return e;
-    e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return e;
-    std::vector<float> h((size_t)49 * K2 * NRP, 0.f);
-    for (int slot = 0; slot < 49; ++slot) {
-        float* T = h.data() + (size_t)slot * K2 * NRP;
-        for (int p = 1; p <= P; ++p) {
-            for (int k = 0; k <= P; ++k) {
-                const double2 Tc = op[((size_t)slot * (P + 1) + k) * P + (p - 1)];
-                // Re b_p = Tr Re a_k - Ti Im a_k ; Im b_p = Ti Re a_k + Tr Im a_k
-                T[(size_t)k * NRP + (p - 1)] = (float)Tc.x;
-                T[(size_t)(P + 1 + k) * NRP + (p - 1)] = (float)(-Tc.y);
-                T[(size_t)k * NRP + (P + p - 1)] = (float)Tc.y;
-                T[(size_t)(P + 1 + k) * NRP + (P + p - 1)] = (float)Tc.x;
-            }
-        }
-    }
-    e = cudaMemcpyAsync(dst, h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice, st);
-    if (e != cudaSuccess) return e;
-    return cudaStreamSynchronize(st);
-}
-
-template <int P>
-cudaError_t launch_m2l_f32(const Tree2D& t, const Lists2D& l, Expansions2D& e, const float* rows, const float* ops,
-                           unsigned* err, cudaStream_t st) {
-    const size_t smem = sizeof(float) * (size_t)49 * 2 * (P + 1) * f32_nrp(P) + sizeof(int) * kF32Warps * 49 * (32 / (f32_nrp(P) / 4));
-    cudaError_t r = cudaFuncSetAttribute(m2l2d_f32<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (r != cudaSuccess) return r;
-    int occ = 0;
-    r = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, m2l2d_f32<P>, 32 * kF32Warps, smem);
-    if (r != cudaSuccess) return r;
-    m2l2d_f32<P><<<148 * (occ > 0 ? occ : 1), 32 * kF32Warps, smem, st>>>(t, l, rows, ops, e.b, err);
-    return cudaGetLastError();
-}
-
-cudaError_t fmm2d_m2l_f32(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, float* rows, const float* ops,
-                          unsigned* err, cudaStream_t st, int* launches) {
-    if (!m2l_f32_supported(P)) return cudaErrorInvalidValue;
-    const int RP = f32_rp(P);
-    m2l_rows_f32<<<148 * 8, 256, 0, st>>>(t, e.a, rows, P, RP, err);
-    cudaError_t r;
-    switch (P) {
-#define VPM_M2L_F32_CASE(PP) \
-    case PP: r = launch_m2l_f32<PP>(t, l, e, rows, ops, err, st); break;
-        VPM_M2L_F32_CASE(1) VPM_M2L_F32_CASE(2) VPM_M2L_F32_CASE(3) VPM_M2L_F32_CASE(4) VPM_M2L_F32_CASE(5)
-        VPM_M2L_F32_CASE(6) VPM_M2L_F32_CASE(7) VPM_M2L_F32_CASE(8) VPM_M2L_F32_CASE(9) VPM_M2L_F32_CASE(10)
-        VPM_M2L_F32_CASE(11) VPM_M2L_F32_CASE(12)
-#undef VPM_M2L_F32_CASE
-        default: return cudaErrorInvalidValue;
-    }
-    if (r != cudaSuccess) return r;
     m2l_list4_add<<<148 * 8, 128, 0, st>>>(t, l, e.a, e.b, e.coef, P, false, err);
     *launches += 3;
     return cudaGetLastError();
