@@ -1421,7 +1421,9 @@ cudaError_t set_coefficients2d(int P, bool exact, double* dst, cudaStream_t st) 
 // cells (the top of the tree, about n / kDirectMax per level) follow by M2M
 // from their children in the cooperative level loop m2m_big_levels_coop,
 // from the deepest level holding one. Sums run in a fixed order (lane order
-// over the particles, then lanes in order; children in child order).
+// over the particles, then lanes in order; children in child order). A large
+// cell without active particles gets zero moments from the first launch, so
+// every cell's moments are written in every evaluation.
 constexpr int kUpWarps = 8;
 constexpr int kDirectMax = 1024;
 constexpr int kUpMaxP = 18;
@@ -1439,8 +1441,12 @@ upward_direct2d(Tree2D t, double2* __restrict__ a, unsigned* __restrict__ top_le
     for (int c = c_begin + blockIdx.x * kUpWarps + wib; c < c_end; c += nw) {
         const int lo = t.c_lo[c], hi = t.c_hi[c];
         const uint8_t f = t.c_flags[c];
-        if (hi - lo > kDirectMax && !(f & CELL_LEAF)) {   // by M2M afterwards (m2m_big_levels_coop)
-            if (lane == 0) atomicMax(top_level, (unsigned)t.c_level[c]);
+        if (hi - lo > kDirectMax && !(f & CELL_LEAF)) {
+            if (f & CELL_ACTIVE) {   // by M2M afterwards (m2m_big_levels_coop)
+                if (lane == 0) atomicMax(top_level, (unsigned)t.c_level[c]);
+            } else {                 // no active particle: zero moments (its parent's M2M reads them)
+                for (int comp = lane; comp < 2 * Q; comp += 32) reinterpret_cast<double*>(a + (size_t)c * Q)[comp] = 0.0;
+            }
             continue;
         }
         double re[Q], im[Q];

@@ -127,3 +127,27 @@ def test_coincident_cluster_retries_deeper_keys(ctx, port):
     assert st.depth_retry == 1
     rx, ry = port.fmm2d_field(x, y, q, a)
     assert rel_l2((ex, ey), (rx, ry)) <= TOL
+
+
+def test_inactive_large_cell_after_active_evaluation(ctx, port):
+    """A cell of more than 1024 particles, all of them inactive, under an active
+    parent: its moments must be zero, also when the same context evaluated the
+    particles active just before (the arena then holds that cell's old moments),
+    in both precision settings' upward passes."""
+    rng = np.random.default_rng(77)
+    xb, yb = rng.uniform(0.0, 1.0, 40_000), rng.uniform(0.0, 1.0, 40_000)
+    keep = ~((xb > 0.08) & (xb < 0.18) & (yb > 0.08) & (yb < 0.18))   # no active particle near the cluster
+    xb, yb = xb[keep], yb[keep]
+    xc, yc = rng.uniform(0.10, 0.16, 12_000), rng.uniform(0.10, 0.16, 12_000)
+    x, y = np.concatenate([xb, xc]), np.concatenate([yb, yc])
+    q = rng.normal(0.0, 1.0, x.size) * 1e-3
+    on = np.ones(x.size, np.uint8)
+    off = on.copy()
+    off[xb.size:] = 0
+    for prm in (default_params(), default_params(precision=1, binom=BINOM_EXACT, p=8, max_src=100, max_par=150)):
+        ctx.field2d(x, y, q, on, prm)
+        ex, ey = ctx.field2d(x, y, q, off, prm)
+        rx, ry = port.fmm2d_field(x, y, q, off, p=prm.p, max_src=prm.max_src, max_par=prm.max_par,
+                                  exact_binom=prm.binom == BINOM_EXACT)
+        tol = TOL if prm.precision == 0 else 1e-5
+        assert rel_l2((ex, ey), (rx, ry)) <= tol, prm.precision
