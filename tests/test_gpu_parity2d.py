@@ -151,3 +151,29 @@ def test_inactive_large_cell_after_active_evaluation(ctx, port):
                                   exact_binom=prm.binom == BINOM_EXACT)
         tol = TOL if prm.precision == 0 else 1e-5
         assert rel_l2((ex, ey), (rx, ry)) <= tol, prm.precision
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_reused_context_matches_fresh(ctx, prec):
+    """One context evaluating a sequence of different particle sets (sizes,
+    clustering, inactive regions) gives, for each, the bits a fresh context
+    gives: nothing read from the arena outlives the evaluation that wrote it.
+    Eager launches and graph replay both."""
+    from lsmps_vpm_v2_b200 import Context
+    seq = [cases2d.clustered(), cases2d.partly_inactive(), cases2d.plate_small(), cases2d.deep()]
+    d = dict(cases2d.clustered())
+    a = d["active"].copy()
+    a[(d["x"] > np.median(d["x"])) & (d["y"] > np.median(d["y"]))] = 0   # one inactive quadrant
+    d["active"] = a
+    seq.append(d)
+    seq.append(cases2d.clustered())
+    for use_graph in (0, 1):
+        prm = default_params(use_graph=use_graph) if prec == 0 else \
+            default_params(precision=1, binom=BINOM_EXACT, p=8, max_src=100, max_par=150, use_graph=use_graph)
+        for k, d in enumerate(seq):
+            x, y, q, act = d["x"], d["y"], d["q"], d["active"]
+            ex, ey = ctx.field2d(x, y, q, act, prm)
+            fresh = Context(0)
+            fx, fy = fresh.field2d(x, y, q, act, prm)
+            del fresh
+            assert np.array_equal(ex, fx, equal_nan=True) and np.array_equal(ey, fy, equal_nan=True), (use_graph, k)
