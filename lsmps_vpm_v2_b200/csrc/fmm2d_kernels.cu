@@ -5,16 +5,24 @@
 //   E_x = Re F, E_y = -Im F,  F = sum of q/(z - z_j) terms.
 //
 // Stage map:
-//   fmm2d_upward  P2M of every active leaf (p2m2d, fmm2D.cpp:237-284), then
-//                 M2M over the levels, deepest first, in one cooperative
-//                 launch with a grid barrier per level (m2m_levels_coop,
-//                 fmm2D.cpp:309-379).
-//   fmm2d_m2l     lists 2 and 4 of every cell at level >= 2 (fmm2D.cpp:396-556).
-//   fmm2d_eval    per leaf: the L2L chain from its level-2 ancestor
-//                 (fmm2D.cpp:587-651), then M2P over list 3 (fmm2D.cpp:1040-1066)
-//                 and L2P (fmm2D.cpp:1076-1093) for its particles.
-//   fmm2d_p2p     per leaf: direct sum over list 1, j != i (fmm2D.cpp:135-179),
-//                 added to the far field and written in the caller's order.
+//   fmm2d_upward_direct  moments of every cell of at most 1024 particles
+//                 straight from its particles (upward_direct2d), then M2M of
+//                 the larger cells level by level in one cooperative launch
+//                 (m2m_big_levels_coop); fmm2D.cpp:237-284, 309-379.
+//   fmm2d_upward  P2M of every active leaf, then M2M over all levels (p2m2d,
+//                 m2m_levels_coop), for orders the direct form does not cover.
+//   fmm2d_m2l_only  lists 2 and 4 of every cell at level >= 2 in FP64 with the
+//                 49 precomputed list-2 operators (m2l2d_op, fmm2D.cpp:396-556);
+//                 the mixed forms' per-parent list-2 M2L is in m2l_tc.cu.
+//   fmm2d_l2l_leaves, fmm2d_l2l  every leaf's local expansion from its
+//                 ancestors' M2L parts, or the level loop (fmm2D.cpp:587-651).
+//   fmm2d_eval, fmm2d_m2p, fmm2d_eval_combine  M2P over list 3
+//                 (fmm2D.cpp:1040-1066) and L2P (fmm2D.cpp:1076-1093), warp per
+//                 leaf; the combine pass adds the near field and writes the
+//                 output in the caller's order.
+//   fmm2d_p2p_f64_tma, fmm2d_p2p_f32  near field over list 1, j != i
+//                 (fmm2D.cpp:135-179): FP64 warp kernel for the plain form,
+//                 packed FP32 tiles for the mixed forms.
 #include "fmm2d.cuh"
 
 #include <complex>
