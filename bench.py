@@ -17,7 +17,11 @@ events on the launching stream, L2 flushed by a 256 MiB write between steps); `e
 same metric through the public host API (pinned host buffers, H2D + D2H
 inside the timed region); `roofline` covers the dominant kernel; and
 `cpu_baseline` is the reference's own FMM compiled from its sources
-(oracle/_ref), timed on the host cores. With --gpus N (torchrun) each rank
+(oracle/_ref), timed on the host cores. `batched`, `named_configs` (the
+65,536-particle Lamb-Oseen lattice at p = 10, the boundary layer at p = 16)
+and `bench_3d` (the 2M-particle vortex ring) report the other named
+workloads, each form with its error against the FP64 direct sum. With
+--gpus N (torchrun) each rank
 evaluates its own copy of the workload (independent solves, no collective)
 and `value` is the aggregate.
 
@@ -326,6 +330,42 @@ def run_ours(args):
                "streams": ctx.batch_streams(), "launch": "one CUDA graph over all solves" if graph else "eager"}
     del bdev, bex, bey
 
+    # ---- the other named 2D workloads: the 65,536-particle Lamb-Oseen lattice
+    # at the reference's order and caps, and the boundary layer at p = 16 (both
+    # mixed M2L variants); each form against the FP64 direct sum ----
+    named = {}
+    lo_ = workloads.lamb_oseen_2d(n_side=256)
+    cfgs = [("lamb_oseen_65536_p10", lo_,
+             {"fp64": default_params(precision=PREC_FP64, use_graph=graph),
+              "mixed": default_params(precision=PREC_MIXED, binom=1, use_graph=graph)}),
+            ("boundary_layer_778377_p16", None,
+             {"fp64": default_params(precision=PREC_FP64, p=16, use_graph=graph),
+              "mixed": default_params(precision=PREC_MIXED, binom=1, p=16, use_graph=graph),
+              "mixed_tc": default_params(precision=PREC_MIXED_TC, binom=1, p=16, use_graph=graph)})]
+    for cname, d_, cforms in cfgs:
+        if d_ is None:
+            cx, cy, cq, ca, cex, cey = x, y, q, act, ex, ey
+        else:
+            cx, cy, cq, ca = (torch.from_numpy(d_[k]).to(dev) for k in ("x", "y", "q", "active"))
+            cex, cey = torch.empty_like(cx), torch.empty_like(cx)
+        cn = int(cx.numel())
+        ctg = torch.from_numpy(workloads.sample_targets(cn, 4096)).to(dev)
+        cdx, cdy = torch.empty(ctg.numel(), dtype=torch.float64, device=dev), torch.empty(ctg.numel(), dtype=torch.float64, device=dev)
+        ctx._check(lib().vpm_direct2d_field_device(ctx._h, cx.data_ptr(), cy.data_ptr(), cq.data_ptr(), ca.data_ptr(),
+                                                   cn, ctg.data_ptr(), ctg.numel(), cdx.data_ptr(), cdy.data_ptr()))
+        entry = {"n": cn}
+        for fname, p_ in cforms.items():
+            for _ in range(max(args.warmup, 3)):
+                ctx.field2d_device(cx, cy, cq, ca, cex, cey, p_)
+            ctx.sync()
+            num = torch.sqrt(((cex[ctg] - cdx) ** 2).sum() + ((cey[ctg] - cdy) ** 2).sum())
+            den = torch.sqrt((cdx * cdx).sum() + (cdy * cdy).sum())
+            cms = max_over_ranks(time_steps(ctx, stream, flush, lambda: ctx.field2d_device(cx, cy, cq, ca, cex, cey, p_),
+                                            max(3, min(args.steps, 50))), world, dev)
+            entry[fname] = {"ms_per_step": cms, "value": world * cn / (cms * 1e-3), "p": int(p_.p),
+                            "caps": [int(p_.max_src), int(p_.max_par)], "rel_l2_vs_direct": float((num / den).item())}
+        named[cname] = entry
+
     # ---- 3D: the thin vortex ring at h = 0.0096 (2,009,183 particles), the
     # octree treecode of the reference's default 3D path in both forms, against
     # the FP64 direct sum on 1,024 sampled targets ----
@@ -429,6 +469,7 @@ def run_ours(args):
                 "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes,
                 "api": "vpm_velocity2d (host buffers)"},
         "batched": batched,
+        "named_configs": named,
         "bench_3d": bench_3d,
         "gpu_launches": launches_per_step * args.steps,
         "stages_ms": stage,

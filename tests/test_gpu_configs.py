@@ -3,9 +3,10 @@
 * Lamb-Oseen, 256 x 256 jittered lattice (N = 65,536), p = 10, caps 50/75:
   tree, leafList, parIDList and lists 1-4 bit-exact against the oracle, field
   within 1e-10 of the oracle.
-* Boundary layer (N = 778,377) at p = 16, mixed form (tensor-core M2L): within
-  1e-4 of the FP64 direct sum on 4,096 sampled targets and within 1e-5 of the
-  same form with the FP64 M2L; plain FP64 at p = 16 within 1e-10 of the oracle.
+* Boundary layer (N = 778,377) at p = 16, mixed form (per-parent M2L on the
+  FP32 pipes, and on the tensor cores): within 1e-4 of the FP64 direct sum on
+  4,096 sampled targets and within 1e-5 of the same form with the FP64 M2L;
+  plain FP64 at p = 16 within 1e-10 of the oracle.
 * 64 uneven solves (N log-uniform in 4,096..400,000, multi-vortex fields),
   p = 12, mixed: every solve of the batch equal to the same solve run alone,
   bit for bit, and sampled solves within 1e-4 of the direct sum.
@@ -17,7 +18,7 @@ import numpy as np
 import pytest
 
 from lsmps_vpm_v2_b200 import PREC_MIXED, default_params, workloads
-from lsmps_vpm_v2_b200._lib import PREC_MIXED_FP64_M2L
+from lsmps_vpm_v2_b200._lib import PREC_MIXED_FP64_M2L, PREC_MIXED_TC
 from lsmps_vpm_v2_b200.workloads import rel_l2, sample_targets
 
 pytestmark = pytest.mark.gpu
@@ -55,12 +56,13 @@ def plate():
 def test_boundary_layer_p16_mixed(ctx, port, plate):
     d = plate
     x, y, q, a = d["x"], d["y"], d["q"], d["active"]
-    tc = ctx.field2d(x, y, q, a, default_params(p=16, precision=PREC_MIXED, binom=1))
     ref = ctx.field2d(x, y, q, a, default_params(p=16, precision=PREC_MIXED_FP64_M2L, binom=1))
-    assert rel_l2(tc, ref) <= TOL_MIXED
     tg = sample_targets(x.size, 4096)
     dx, dy = port.direct2d_field(x, y, q, a, tg)
-    assert rel_l2((tc[0][tg], tc[1][tg]), (dx, dy)) <= TOL_DIRECT
+    for prec in (PREC_MIXED, PREC_MIXED_TC):
+        f = ctx.field2d(x, y, q, a, default_params(p=16, precision=prec, binom=1))
+        assert rel_l2(f, ref) <= TOL_MIXED, prec
+        assert rel_l2((f[0][tg], f[1][tg]), (dx, dy)) <= TOL_DIRECT, prec
 
 
 def test_boundary_layer_p16_fp64(ctx, port, plate):
