@@ -55,8 +55,8 @@ typedef struct vpm_ctx vpm_ctx;
  * Knobs of the evaluation. Defaults (vpm_fmm_params_default) are the
  * reference's 2D values: global.cpp:303 (expTree = 1.0), :311 (P_max = 10),
  * :312 (par_count_max = 75), :313 (src_count_max = 50); treeCell.cpp:5
- * (EPSILON_TOLERANCE = 1e-9); fast3DFMM.cpp:4 (support factor 2.0) with the
- * 3D leaf cap src_count_max = 30 (global.cpp:779).
+ * (EPSILON_TOLERANCE = 1e-9); fast3DFMM.cpp:4 (support factor 2.0, support_3d) with
+ * the 3D leaf cap src_count_max = 30 (global.cpp:779).
  */
 typedef struct vpm_fmm_params {
     int32_t p;            /* expansion order, 1..30                                 */
@@ -76,6 +76,12 @@ typedef struct vpm_fmm_params {
                              recorded between them (profiling)                    */
     double center_3d[3];  /* 3D domain centre joined into the root box
                              (Pars::xcenter/ycenter/zcenter, fast3DFMM.cpp:506-508) */
+    double support_3d;    /* 3D far test: a cell is far from a target when
+                             R > support_3d x its size; the reference's support
+                             factor is 2.0 (fast3DFMM.cpp:4, fmm3D.cpp:3), the
+                             default (0 is taken as 2.0); larger values trade
+                             time for accuracy (4.0: <= 1e-4 against the direct
+                             sum on the vortex rings of the tests); >= 1.0   */
 } vpm_fmm_params;
 
 /* Per-call figures (counts are exact; times are CUDA-event milliseconds). */

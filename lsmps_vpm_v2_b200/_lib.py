@@ -41,6 +41,7 @@ class Params(C.Structure):
         ("max_depth", C.c_int32),
         ("use_graph", C.c_int32),
         ("center_3d", C.c_double * 3),
+        ("support_3d", C.c_double),
     ]
 
 

@@ -193,6 +193,9 @@ int Ctx::check_params(const vpm_fmm_params* prm, vpm_fmm_params& out) {
     if (out.max_src < 0 || out.max_par < 1) return fail(VPM_EINVAL, "leaf caps must be max_src >= 0, max_par >= 1");
     if (out.max_depth != 16 && out.max_depth != 31) out.max_depth = 16;
     if (!(out.exp_tree_pct >= 0.0) || !std::isfinite(out.exp_tree_pct)) return fail(VPM_EINVAL, "exp_tree_pct");
+    if (out.support_3d == 0.0) out.support_3d = 2.0;
+    if (!(out.support_3d >= 1.0) || !std::isfinite(out.support_3d))
+        return fail(VPM_EINVAL, "support_3d must be a finite factor >= 1");
     if (out.precision != VPM_PREC_FP64 && out.precision != VPM_PREC_MIXED && out.precision != VPM_PREC_MIXED_FP64_M2L &&
         out.precision != VPM_PREC_MIXED_TC)
         return fail(VPM_EINVAL, "precision");
@@ -680,6 +683,7 @@ void vpm_fmm_params_default(vpm_fmm_params* p) {
     p->precision = VPM_PREC_FP64;
     p->binom = VPM_BINOM_REFERENCE;
     p->max_depth = 16;
+    p->support_3d = 2.0;
 }
 
 int vpm_ctx_create(int device, vpm_ctx** out) {

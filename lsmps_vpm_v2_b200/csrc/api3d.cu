@@ -133,8 +133,8 @@ int Ctx::enqueue3d(const double* x, const double* y, const double* z, const doub
         VPM_CUDA_TRY(build_tree3d(x, y, z, ax, ay, az, act, p.center_3d, p.exp_tree_pct, tree3, s3, bbox3, d_err,
                                   st, &launches));
     if (!tree_only)
-        VPM_CUDA_TRY(eval3d(tree3, p.precision == VPM_PREC_MIXED, treecell, target, u, v, w, uinf, vinf, winf, d_err,
-                            st, &launches));
+        VPM_CUDA_TRY(eval3d(tree3, p.precision == VPM_PREC_MIXED, treecell, target, p.support_3d, u, v, w, uinf, vinf,
+                            winf, d_err, st, &launches));
     VPM_CUDA_TRY(cudaEventRecord(ev[1], st));
     last_launches3 = launches;
     have_tree3 = true;

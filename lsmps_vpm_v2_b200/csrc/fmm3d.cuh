@@ -109,9 +109,10 @@ cudaError_t build_treecell3d(const double* x, const double* y, const double* z, 
 // leaf is a P2P source (TreeCell path, fmm3D.cpp:1337-1352) instead of the
 // active ones only (octree path). target (caller order, may be null): only
 // flagged particles are evaluated, the others get zero (the free stream is
-// not added to them).
-cudaError_t eval3d(const Tree3D& t, bool mixed, bool all_src, const uint8_t* target, double* u, double* v,
-                   double* w, double uinf, double vinf, double winf, unsigned* err, cudaStream_t st,
+// not added to them). support: a child cell is far when R > support x its
+// size (the reference's support factor 2).
+cudaError_t eval3d(const Tree3D& t, bool mixed, bool all_src, const uint8_t* target, double support, double* u,
+                   double* v, double* w, double uinf, double vinf, double winf, unsigned* err, cudaStream_t st,
                    int* launches);
 
 }  // namespace vpm

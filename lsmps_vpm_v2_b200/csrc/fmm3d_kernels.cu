@@ -1,7 +1,7 @@
 // 3D treecode evaluation (fastFMM3Dutils::evaluateFMM, src/FMM/fast3DFMM.cpp:318-472):
 // every particle is a target; from the root's children down, each active
 // child k of a cell on the target's list is
-//   far   if R^2 > (2 size_k)^2   -> M2P with the derivative multipliers of
+//   far   if R^2 > (s size_k)^2   -> M2P with the derivative multipliers of
 //                                    fmm3D::M2P_mul_calc (fmm3D.cpp:147-200)
 //   else a non-leaf               -> onto the target's list for the next level
 //   else a leaf                   -> P2P  u += (alpha_j x r) / |r|^3, j != i,
@@ -10,6 +10,8 @@
 // 2, fmm3D.cpp:1264-1360; calcVelocityNearBody, fmm3D.cpp:1406-1606) walks
 // its TreeCell the same way, with every particle of a near leaf a source.
 // (level-1 cells themselves are never evaluated, as in the reference).
+// s is the reference's support factor 2 (fast3DFMM.cpp:4) unless the caller
+// asks for a stricter far test (a larger s: more accurate, slower).
 //
 // One warp per 32 consecutive particles in leaf order (leaves hold about 8
 // particles on average, so a warp spans a few neighbouring leaves), one lane
@@ -22,6 +24,7 @@
 #include "fmm3d.cuh"
 
 #include <algorithm>
+#include <cmath>
 
 namespace vpm {
 
@@ -176,11 +179,15 @@ __device__ __forceinline__ void p2p3(const Src3& s, int lo, int hi, int self, do
 
 template <bool F32, bool ALL>
 __global__ void __launch_bounds__(32 * kEval3DWarps)
-eval3d_kernel(Tree3D t, const uint8_t* __restrict__ target, double* __restrict__ u, double* __restrict__ v,
-              double* __restrict__ w, double uinf, double vinf, double winf, unsigned* ticket, unsigned* err) {
-    __shared__ int s_cell[kEval3DWarps][2][kWork3DCap];
-    __shared__ unsigned s_mask[kEval3DWarps][2][kWork3DCap];
+eval3d_kernel(Tree3D t, const uint8_t* __restrict__ target, double support, int cap, double* __restrict__ u,
+              double* __restrict__ v, double* __restrict__ w, double uinf, double vinf, double winf, unsigned* ticket,
+              unsigned* err) {
+    // per warp two work lists of `cap` entries (cell, lane mask): dynamic
+    // shared memory sized from the support factor by the launcher
+    extern __shared__ int s_work[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    int* s_cell0 = s_work + (size_t)wib * 4 * cap;
+    unsigned* s_mask0 = reinterpret_cast<unsigned*>(s_cell0 + 2 * cap);
     int stop = 0;
     if (lane == 0) stop = fatal(err);
     if (__shfl_sync(0xffffffffu, stop, 0)) return;  // warp-uniform
@@ -205,15 +212,15 @@ eval3d_kernel(Tree3D t, const uint8_t* __restrict__ target, double* __restrict__
             int which = 0;
             int ncur = __popc(rm);
             if (lane < ncur) {
-                s_cell[wib][0][lane] = r0 + lane;
-                s_mask[wib][0][lane] = full;
+                s_cell0[lane] = r0 + lane;
+                s_mask0[lane] = full;
             }
             __syncwarp();
             for (int lv = 1; lv < depth && ncur > 0; ++lv) {
-                const int* cur_c = s_cell[wib][which];
-                const unsigned* cur_m = s_mask[wib][which];
-                int* nxt_c = s_cell[wib][which ^ 1];
-                unsigned* nxt_m = s_mask[wib][which ^ 1];
+                const int* cur_c = s_cell0 + which * cap;
+                const unsigned* cur_m = s_mask0 + which * cap;
+                int* nxt_c = s_cell0 + (which ^ 1) * cap;
+                unsigned* nxt_m = s_mask0 + (which ^ 1) * cap;
                 int nn = 0;
                 for (int e = 0; e < ncur; ++e) {
                     const int cc = cur_c[e];
@@ -232,7 +239,7 @@ eval3d_kernel(Tree3D t, const uint8_t* __restrict__ target, double* __restrict__
                             dy = xsub(yp, t.c_y[k]);
                             dz = xsub(zp, t.c_z[k]);
                             R2 = xadd(xadd(xmul(dx, dx), xmul(dy, dy)), xmul(dz, dz));
-                            const double Rc = xmul(t.c_size[k], 2.0);
+                            const double Rc = xmul(t.c_size[k], support);
                             far = R2 > xmul(Rc, Rc);
                             if (far) {
                                 if (F32) m2p32(&t.mom[(size_t)k * 30], dx, dy, dz, vx, vy, vz);
@@ -242,7 +249,7 @@ eval3d_kernel(Tree3D t, const uint8_t* __restrict__ target, double* __restrict__
                         const unsigned near = __ballot_sync(0xffffffffu, mine && !far);
                         if (!near) continue;
                         if (t.c_chmask[k] != 0) {
-                            if (nn < kWork3DCap) {
+                            if (nn < cap) {
                                 if (lane == 0) {
                                     nxt_c[nn] = k;
                                     nxt_m[nn] = near;
@@ -258,7 +265,7 @@ eval3d_kernel(Tree3D t, const uint8_t* __restrict__ target, double* __restrict__
                 }
                 __syncwarp();
                 which ^= 1;
-                ncur = min(nn, kWork3DCap);
+                ncur = min(nn, cap);
             }
             if (has) {
                 const uint32_t i = t.perm[slot];
@@ -273,17 +280,31 @@ eval3d_kernel(Tree3D t, const uint8_t* __restrict__ target, double* __restrict__
 
 }  // namespace
 
-cudaError_t eval3d(const Tree3D& t, bool mixed, bool all_src, const uint8_t* target, double* u, double* v,
-                   double* w, double uinf, double vinf, double winf, unsigned* err, cudaStream_t st,
+cudaError_t eval3d(const Tree3D& t, bool mixed, bool all_src, const uint8_t* target, double support, double* u,
+                   double* v, double* w, double uinf, double vinf, double winf, unsigned* err, cudaStream_t st,
                    int* launches) {
     unsigned* ticket = t.gbar + 4;
     cudaError_t e = cudaMemsetAsync(ticket, 0, sizeof(unsigned), st);
     if (e != cudaSuccess) return e;
+    // work-list entries per level: kWork3DCap at the reference's factor 2
+    // (which needs a few dozen), times (factor / 2)^1.5 beyond it (the near
+    // shell of a level widens with the factor; on the 2M-particle ring 3.5
+    // and 4 fit with room to spare, and an overflow sets ERR_QUEUE)
+    const double f = support > 2.0 ? support / 2.0 : 1.0;
+    const int cap = std::min(8 * kWork3DCap, (int)std::ceil(kWork3DCap * std::pow(f, 1.5) / 32.0) * 32);
+    const size_t smem = sizeof(int) * 4 * (size_t)cap * kEval3DWarps;
     const dim3 g(148 * 8), b(32 * kEval3DWarps);
-    if (mixed && all_src) eval3d_kernel<true, true><<<g, b, 0, st>>>(t, target, u, v, w, uinf, vinf, winf, ticket, err);
-    else if (mixed) eval3d_kernel<true, false><<<g, b, 0, st>>>(t, target, u, v, w, uinf, vinf, winf, ticket, err);
-    else if (all_src) eval3d_kernel<false, true><<<g, b, 0, st>>>(t, target, u, v, w, uinf, vinf, winf, ticket, err);
-    else eval3d_kernel<false, false><<<g, b, 0, st>>>(t, target, u, v, w, uinf, vinf, winf, ticket, err);
+#define VPM_EVAL3D(F, A)                                                                                     \
+    do {                                                                                                     \
+        e = cudaFuncSetAttribute(eval3d_kernel<F, A>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+        if (e != cudaSuccess) return e;                                                                      \
+        eval3d_kernel<F, A><<<g, b, smem, st>>>(t, target, support, cap, u, v, w, uinf, vinf, winf, ticket, err); \
+    } while (0)
+    if (mixed && all_src) VPM_EVAL3D(true, true);
+    else if (mixed) VPM_EVAL3D(true, false);
+    else if (all_src) VPM_EVAL3D(false, true);
+    else VPM_EVAL3D(false, false);
+#undef VPM_EVAL3D
     *launches += 1;
     return cudaGetLastError();
 }

@@ -123,10 +123,11 @@ class Port:
                                           C.c_int, _d]
         L.orc_direct2d_field.argtypes = [_d, _d, _d, _u8, C.c_int64, _i64, C.c_int64, _d, _d]
         L.orc_fmm3d_velocity.restype = C.c_int
-        L.orc_fmm3d_velocity.argtypes = [_d, _d, _d, _d, _d, _d, _u8, C.c_int64, C.c_int, C.c_double, _d, _d, _d]
+        L.orc_fmm3d_velocity.argtypes = [_d, _d, _d, _d, _d, _d, _u8, C.c_int64, C.c_int, C.c_double, C.c_double,
+                                         _d, _d, _d]
         L.orc_fmm3d_velocity_at.restype = C.c_int
-        L.orc_fmm3d_velocity_at.argtypes = [_d, _d, _d, _d, _d, _d, _u8, C.c_int64, C.c_int, C.c_double, _i64,
-                                            C.c_int64, _d, _d, _d]
+        L.orc_fmm3d_velocity_at.argtypes = [_d, _d, _d, _d, _d, _d, _u8, C.c_int64, C.c_int, C.c_double, C.c_double,
+                                            _i64, C.c_int64, _d, _d, _d]
         L.orc_tree3d.restype = C.c_int64
         L.orc_tree3d.argtypes = [_d, _d, _d, _u8, C.c_int64, C.c_int, C.c_double, C.c_void_p, C.c_void_p]
         L.orc_direct3d_velocity.argtypes = [_d, _d, _d, _d, _d, _d, _u8, C.c_int64, _i64, C.c_int64, _d, _d, _d]
@@ -136,7 +137,7 @@ class Port:
         L.orc_treecell3d_velocity.restype = C.c_int
         L.orc_treecell3d_pairs.argtypes = [_i64]
         L.orc_treecell3d_velocity.argtypes = [_d, _d, _d, _d, _d, _d, _u8, C.c_void_p, C.c_int64, C.c_int, C.c_int,
-                                              C.c_double, _d, _d, _d]
+                                              C.c_double, C.c_double, _d, _d, _d]
 
     def set_threads(self, n: int) -> None:
         self.lib.orc_set_threads(int(n))
@@ -212,22 +213,23 @@ class Port:
             self.lib.orc_tree2d_free(h)
 
     # ---- 3D ---------------------------------------------------------------
-    def fmm3d_velocity(self, x, y, z, ax, ay, az, active, leaf_cap=30, exp_pct=1.0):
+    def fmm3d_velocity(self, x, y, z, ax, ay, az, active, leaf_cap=30, exp_pct=1.0, support=2.0):
         args = [_f64(v) for v in (x, y, z, ax, ay, az)]
         a = _u8a(active)
         n = args[0].size
         u, v, w = np.zeros(n), np.zeros(n), np.zeros(n)
-        rc = self.lib.orc_fmm3d_velocity(*args, a, n, leaf_cap, exp_pct, u, v, w)
+        rc = self.lib.orc_fmm3d_velocity(*args, a, n, leaf_cap, exp_pct, support, u, v, w)
         if rc != 0:
             raise RuntimeError(self.lib.orc3_last_error().decode())
         return u, v, w
 
-    def fmm3d_velocity_at(self, x, y, z, ax, ay, az, active, targets, leaf_cap=30, exp_pct=1.0):
+    def fmm3d_velocity_at(self, x, y, z, ax, ay, az, active, targets, leaf_cap=30, exp_pct=1.0, support=2.0):
         """The treecode velocity at the sampled targets only (same tree, same per-target walk)."""
         args = [_f64(v) for v in (x, y, z, ax, ay, az)]
         t = np.ascontiguousarray(targets, dtype=np.int64)
         u, v, w = np.zeros(t.size), np.zeros(t.size), np.zeros(t.size)
-        rc = self.lib.orc_fmm3d_velocity_at(*args, _u8a(active), args[0].size, leaf_cap, exp_pct, t, t.size, u, v, w)
+        rc = self.lib.orc_fmm3d_velocity_at(*args, _u8a(active), args[0].size, leaf_cap, exp_pct, support, t, t.size,
+                                            u, v, w)
         if rc != 0:
             raise RuntimeError(self.lib.orc3_last_error().decode())
         return u, v, w
@@ -253,14 +255,16 @@ class Port:
             raise RuntimeError(self.lib.orc3_last_error().decode())
         return out
 
-    def treecell3d_velocity(self, x, y, z, ax, ay, az, active, target=None, max_src=30, max_par=50, exp_pct=1.0):
-        """fmm3D::calcVelocity (target None) or calcVelocityNearBody on the 3D TreeCell."""
+    def treecell3d_velocity(self, x, y, z, ax, ay, az, active, target=None, max_src=30, max_par=50, exp_pct=1.0,
+                            support=2.0):
+        """fmm3D::calcVelocity (target None) or calcVelocityNearBody on the 3D TreeCell; far iff
+        R > support x length (the reference's support factor is 2)."""
         args = [_f64(v) for v in (x, y, z, ax, ay, az)]
         n = args[0].size
         t = None if target is None else _u8a(target)
         u, v, w = np.zeros(n), np.zeros(n), np.zeros(n)
         rc = self.lib.orc_treecell3d_velocity(*args, _u8a(active), None if t is None else _vp(t), n, max_src, max_par,
-                                              exp_pct, u, v, w)
+                                              exp_pct, support, u, v, w)
         if rc != 0:
             raise RuntimeError(self.lib.orc3_last_error().decode())
         return u, v, w

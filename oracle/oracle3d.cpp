@@ -8,7 +8,8 @@
 //   * octant rule             src/FMM/fast3DFMM.hpp:17-22
 //   * 10-term P2M / M2M       src/FMM/fmm3D.cpp:84-132, fast3DFMM.cpp:164-302
 //   * M2P multipliers         src/FMM/fmm3D.cpp:147-200
-//   * per-target traversal    src/FMM/fast3DFMM.cpp:318-472 (far iff R^2 > (2 size)^2)
+//   * per-target traversal    src/FMM/fast3DFMM.cpp:318-472 (far iff R^2 > (2 size)^2; the
+//                             factor 2 is the reference's support factor, a parameter here)
 // the alternative 3D path on the shared TreeCell (VELOCITY_3D_TYPE 2: TreeCell
 // with DIM 3, fmm3D::calcVelocity / calcVelocityNearBody; section below), and
 // the FP64 direct Biot-Savart sum u_i = sum_j (a_j x r_ij) / |r_ij|^3.
@@ -355,7 +356,7 @@ int64_t orc_treecell3d_tree(const double* x, const double* y, const double* z, c
 // a leaf of a deeper tree (its traversal asks for that leaf's children).
 int orc_treecell3d_velocity(const double* x, const double* y, const double* z, const double* ax, const double* ay,
                             const double* az, const uint8_t* act, const uint8_t* target, int64_t n, int max_src,
-                            int max_par, double exp_pct, double* u, double* v, double* w) {
+                            int max_par, double exp_pct, double support, double* u, double* v, double* w) {
     TC3 t;
     if (n < 1 || !build_tc3(t, x, y, z, act, n, max_src, max_par, exp_pct)) return -1;
     const int nc = t.ncell();
@@ -419,7 +420,7 @@ int orc_treecell3d_velocity(const double* x, const double* y, const double* z, c
                         if (k < 0 || !t.active[k]) continue;
                         double dx = xp - t.xc[k], dy = yp - t.yc[k], dz = zp - t.zc[k];
                         double R2 = dx * dx + dy * dy + dz * dz;
-                        double Rc = t.len[k] * 2.0;
+                        double Rc = t.len[k] * support;
                         if (R2 > Rc * Rc) {
                             ++n_m2p;
                             m2p_mul(R2, dx, dy, dz, gx, gy, gz);
@@ -511,9 +512,10 @@ bool build_moments(OctMoments& om, const double* x, const double* y, const doubl
 }
 
 // One target's walk (fast3DFMM.cpp:340-470): from the root's children, far
-// children (R^2 > (2 size)^2) through their moments, near leaves directly.
+// children (R^2 > (support size)^2; the reference's support factor is 2,
+// fast3DFMM.cpp:4) through their moments, near leaves directly.
 void eval_target(const OctMoments& om, const double* x, const double* y, const double* z, const double* ax,
-                 const double* ay, const double* az, const uint8_t* act, int64_t i, double* out) {
+                 const double* ay, const double* az, const uint8_t* act, int64_t i, double support, double* out) {
     const Oct& t = om.t;
     const double xp = x[i], yp = y[i], zp = z[i];
     double vx = 0, vy = 0, vz = 0;
@@ -530,7 +532,7 @@ void eval_target(const OctMoments& om, const double* x, const double* y, const d
                 if (!t.active[k]) continue;
                 double dx = xp - t.xc[k], dy = yp - t.yc[k], dz = zp - t.zc[k];
                 double R2 = dx * dx + dy * dy + dz * dz;
-                double Rc = t.size[k] * 2.0;
+                double Rc = t.size[k] * support;
                 if (R2 > Rc * Rc) {
                     m2p_mul(R2, dx, dy, dz, gx, gy, gz);
                     const double* Mx = &om.mx[(size_t)k * 10];
@@ -568,13 +570,13 @@ extern "C" {
 // Treecode velocity (reference calcVelocityFast with every particle a target).
 int orc_fmm3d_velocity(const double* x, const double* y, const double* z,
                        const double* ax, const double* ay, const double* az, const uint8_t* act,
-                       int64_t n, int leaf_cap, double exp_pct, double* u, double* v, double* w) {
+                       int64_t n, int leaf_cap, double exp_pct, double support, double* u, double* v, double* w) {
     OctMoments om;
     if (!build_moments(om, x, y, z, ax, ay, az, act, n, leaf_cap, exp_pct)) return -1;
     #pragma omp parallel for schedule(dynamic, 64)
     for (int64_t i = 0; i < n; ++i) {
         double o[3];
-        eval_target(om, x, y, z, ax, ay, az, act, i, o);
+        eval_target(om, x, y, z, ax, ay, az, act, i, support, o);
         u[i] = o[0]; v[i] = o[1]; w[i] = o[2];
     }
     return 0;
@@ -585,14 +587,14 @@ int orc_fmm3d_velocity(const double* x, const double* y, const double* z,
 // targets gives exactly those targets' velocities).
 int orc_fmm3d_velocity_at(const double* x, const double* y, const double* z,
                           const double* ax, const double* ay, const double* az, const uint8_t* act,
-                          int64_t n, int leaf_cap, double exp_pct, const int64_t* tgt, int64_t m,
+                          int64_t n, int leaf_cap, double exp_pct, double support, const int64_t* tgt, int64_t m,
                           double* u, double* v, double* w) {
     OctMoments om;
     if (!build_moments(om, x, y, z, ax, ay, az, act, n, leaf_cap, exp_pct)) return -1;
     #pragma omp parallel for schedule(dynamic, 16)
     for (int64_t k = 0; k < m; ++k) {
         double o[3];
-        eval_target(om, x, y, z, ax, ay, az, act, tgt[k], o);
+        eval_target(om, x, y, z, ax, ay, az, act, tgt[k], support, o);
         u[k] = o[0]; v[k] = o[1]; w[k] = o[2];
     }
     return 0;

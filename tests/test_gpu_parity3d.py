@@ -209,3 +209,36 @@ def test_direct3d_device_matches_oracle(ctx, port):
     ref = port.direct3d_velocity(*args, tg)
     got = [o.cpu().numpy() for o in out]
     assert workloads.rel_l2(got, ref) <= 1e-13
+
+
+@pytest.mark.parametrize("support", [3.0, 3.5, 4.0])
+@pytest.mark.parametrize("name", ["ring_h006", "clustered_30k", "cube_20k_inactive"])
+def test_stricter_far_test_vs_oracle(ctx, port, name, support):
+    """The far test R > support x size with a factor above the reference's 2
+    (support_3d): the same per-target walk as the oracle's with that factor,
+    within 1e-10, and closer to the FP64 direct sum than the factor-2 walk."""
+    d = CASES[name]()
+    args = (d["x"], d["y"], d["z"], d["ax"], d["ay"], d["az"])
+    p = params()
+    p.support_3d = support
+    u, v, w = ctx.velocity3d_alpha(*args, d["active"], p)
+    ru, rv, rw = port.fmm3d_velocity(*args, d["active"], support=support)
+    assert rel_l2((u, v, w), (ru, rv, rw)) <= TOL
+    tg = np.random.default_rng(1).choice(d["x"].size, 512, replace=False)
+    du, dv, dw = port.direct3d_velocity(*args, d["active"], tg)
+    u2, v2, w2 = ctx.velocity3d_alpha(*args, d["active"], params())
+    assert rel_l2((u[tg], v[tg], w[tg]), (du, dv, dw)) < rel_l2((u2[tg], v2[tg], w2[tg]), (du, dv, dw))
+
+
+def test_support_factor_validation(ctx):
+    from lsmps_vpm_v2_b200 import VpmError
+    d = ring(0.06)
+    args = (d["x"], d["y"], d["z"], d["ax"], d["ay"], d["az"])
+    p = params()
+    p.support_3d = 0.0                    # taken as the reference's 2.0
+    assert rel_l2(ctx.velocity3d_alpha(*args, d["active"], p), ctx.velocity3d_alpha(*args, d["active"], params())) == 0
+    for bad in (0.5, float("nan"), float("inf")):
+        p.support_3d = bad
+        with pytest.raises(VpmError) as e:
+            ctx.velocity3d_alpha(*args, d["active"], p)
+        assert e.value.status == 22

@@ -204,3 +204,18 @@ def test_inputs_the_reference_cannot_run_report_errors(ctx, port):
     args = [d[k] for k in ("x", "y", "z", "ax", "ay", "az")]
     u = ctx.velocity3d_treecell(*args, d["active"], None, params())
     assert rel_l2(u, port.treecell3d_velocity(*args, d["active"], None)) <= TOL
+
+
+@pytest.mark.parametrize("name", ["ring_inactive", "clustered"])
+def test_stricter_far_test_vs_oracle(ctx, port, name):
+    """support_3d = 3.5 on the TreeCell path: the oracle's walk with the same
+    factor, within 1e-10, for all particles and for a target subset."""
+    d = CASES[name]()
+    args = [d[k] for k in ("x", "y", "z", "ax", "ay", "az")]
+    p = params()
+    p.support_3d = 3.5
+    u = ctx.velocity3d_treecell(*args, d["active"], None, p)
+    assert rel_l2(u, port.treecell3d_velocity(*args, d["active"], None, support=3.5)) <= TOL
+    tgt = (np.arange(d["x"].size) % 5 == 2).astype(np.uint8)
+    ub = ctx.velocity3d_treecell(*args, d["active"], tgt, p)
+    assert rel_l2(ub, port.treecell3d_velocity(*args, d["active"], tgt, support=3.5)) <= TOL
