@@ -61,6 +61,7 @@ int Ctx::reserve3d(int n, int cap_cells) {
            o_lo = L.take<int32_t>(C), o_hi = L.take<int32_t>(C);
     size_t o_mask = L.take<uint32_t>(C), o_act2 = L.take<uint8_t>(C), o_lev = L.take<uint8_t>(C);
     size_t o_mom = L.take<double>(C * 30), o_leaves = L.take<int32_t>(C);
+    size_t o_ps32 = L.take<float4>(n), o_as32 = L.take<float4>(n), o_mom32 = L.take<float>(C * 30);
     size_t o_gbar = L.take<unsigned>(8), o_blk = L.take<uint32_t>(kCoopMaxBlocks3D);
     size_t o_geom = L.take<Geom3D>(1), o_info = L.take<TreeInfo3D>(1), o_bbox = L.take<double>(296 * 6);
     size_t o_ka = L.take<uint32_t>(n), o_kb = L.take<uint32_t>(n), o_va = L.take<uint32_t>(n),
@@ -98,6 +99,7 @@ int Ctx::reserve3d(int n, int cap_cells) {
     t.c_lo = (int32_t*)P_(o_lo); t.c_hi = (int32_t*)P_(o_hi);
     t.c_chmask = (uint32_t*)P_(o_mask); t.c_active = (uint8_t*)P_(o_act2); t.c_level = (uint8_t*)P_(o_lev);
     t.mom = (double*)P_(o_mom); t.leaf_cells = (int32_t*)P_(o_leaves);
+    t.ps32 = (float4*)P_(o_ps32); t.as32 = (float4*)P_(o_as32); t.mom32 = (float*)P_(o_mom32);
     t.gbar = (unsigned*)P_(o_gbar); t.blk = (uint32_t*)P_(o_blk);
     t.geom = (Geom3D*)P_(o_geom); t.info = (TreeInfo3D*)P_(o_info);
     t.cap_cells = cap_cells;
@@ -132,9 +134,12 @@ int Ctx::enqueue3d(const double* x, const double* y, const double* z, const doub
     else
         VPM_CUDA_TRY(build_tree3d(x, y, z, ax, ay, az, act, p.center_3d, p.exp_tree_pct, tree3, s3, bbox3, d_err,
                                   st, &launches));
-    if (!tree_only)
-        VPM_CUDA_TRY(eval3d(tree3, p.precision == VPM_PREC_MIXED, treecell, target, p.support_3d, u, v, w, uinf, vinf,
-                            winf, d_err, st, &launches));
+    if (!tree_only) {
+        const bool mixed = p.precision == VPM_PREC_MIXED;
+        if (mixed) VPM_CUDA_TRY(prep3d_f32(tree3, d_err, st, &launches));
+        VPM_CUDA_TRY(eval3d(tree3, mixed, treecell, target, p.support_3d, u, v, w, uinf, vinf, winf, d_err, st,
+                            &launches));
+    }
     VPM_CUDA_TRY(cudaEventRecord(ev[1], st));
     last_launches3 = launches;
     have_tree3 = true;

@@ -68,6 +68,10 @@ struct Tree3D {
     uint32_t* c_chmask;               // child octants present (reference chdFlag)
     uint8_t *c_active, *c_level;
     double* mom;                      // [cap_cells][30]: moments of alpha_x, alpha_y, alpha_z
+    // mixed form: FP32 copies made once per evaluation (prep3d_f32)
+    float4* ps32;                     // position minus its leaf's centre, active flag in .w
+    float4* as32;                     // alpha
+    float* mom32;                     // [cap_cells][30]
     int32_t* leaf_cells;              // leaves in cell order
     unsigned* gbar;                   // grid barrier words (2), zeroed per evaluation
     uint32_t* blk;                    // per-block scan partials [gridDim]
@@ -101,6 +105,11 @@ cudaError_t build_treecell3d(const double* x, const double* y, const double* z, 
                              const double* ay, const double* az, const uint8_t* act, int max_src, int max_par,
                              double exp_pct, Tree3D& t, Scratch3D& s, double* bbox_partial, unsigned* err,
                              cudaStream_t st, int* launches);
+
+// FP32 copies for the mixed traversal: each particle's offset from its
+// leaf's centre (formed in FP64, rounded once) with its active flag, its
+// alpha, and every cell's moments.
+cudaError_t prep3d_f32(const Tree3D& t, unsigned* err, cudaStream_t st, int* launches);
 
 // Per-target traversal (M2P of far cells, P2P of near leaves) writing the
 // velocity u = sum alpha x r / |r|^3 (+ free stream) in the caller's order.

@@ -88,8 +88,9 @@ __device__ __forceinline__ void m2p64(const double* __restrict__ M, double R2, d
 }
 
 // The same in FP32 (mixed form): offsets rounded to float after the FP64
-// subtraction, the cell's sum formed in FP32 and added to the FP64 total.
-__device__ __forceinline__ void m2p32(const double* __restrict__ M, double dxd, double dyd, double dzd,
+// subtraction, moments from their FP32 copy, the cell's sum formed in FP32
+// and added to the FP64 total.
+__device__ __forceinline__ void m2p32(const float* __restrict__ M, double dxd, double dyd, double dzd,
                                       double& vx, double& vy, double& vz) {
     const float dx = (float)dxd, dy = (float)dyd, dz = (float)dzd;
     const float R2 = dx * dx + dy * dy + dz * dz;
@@ -133,7 +134,7 @@ __device__ __forceinline__ void m2p32(const double* __restrict__ M, double dxd, 
     float sx = 0.f, sy = 0.f, sz = 0.f;
     #pragma unroll
     for (int m = 0; m < 10; ++m) {
-        const float mx = (float)M[m], my = (float)M[10 + m], mz = (float)M[20 + m];
+        const float mx = M[m], my = M[10 + m], mz = M[20 + m];
         sx += my * gz[m] - mz * gy[m];
         sy += mz * gx[m] - mx * gz[m];
         sz += mx * gy[m] - my * gx[m];
@@ -145,21 +146,27 @@ __device__ __forceinline__ void m2p32(const double* __restrict__ M, double dxd, 
 
 // P2P of one near leaf [lo, hi) onto target slot `self` at (xp, yp, zp);
 // ALL: inactive particles are sources too (TreeCell path).
+// F32: the target's offset from the leaf's centre (cx, cy, cz) is formed in
+// FP64 once and rounded; the sources' offsets and alphas come from their FP32
+// copies (prep3d_f32), so the pair loop is FP32 only.
 template <bool F32, bool ALL>
-__device__ __forceinline__ void p2p3(const Src3& s, int lo, int hi, int self, double xp, double yp, double zp,
-                                     double& vx, double& vy, double& vz) {
+__device__ __forceinline__ void p2p3(const Src3& s, const float4* __restrict__ ps32, const float4* __restrict__ as32,
+                                     int lo, int hi, int self, double xp, double yp, double zp, double cx, double cy,
+                                     double cz, double& vx, double& vy, double& vz) {
     if (F32) {
+        const float tx = (float)(xp - cx), ty = (float)(yp - cy), tz = (float)(zp - cz);
         float sx = 0.f, sy = 0.f, sz = 0.f;
         for (int j = lo; j < hi; ++j) {
-            if ((!ALL && !s.act[j]) || j == self) continue;
-            const float ex = (float)(xp - s.px[j]), ey = (float)(yp - s.py[j]), ez = (float)(zp - s.pz[j]);
+            const float4 sp = ps32[j];
+            if ((!ALL && sp.w == 0.f) || j == self) continue;
+            const float ex = tx - sp.x, ey = ty - sp.y, ez = tz - sp.z;
             const float r2 = ex * ex + ey * ey + ez * ez;
             const float ir = rsqrtf(r2);
             const float ir3 = ir * ir * ir;
-            const float ax = (float)s.ax[j], ay = (float)s.ay[j], az = (float)s.az[j];
-            sx += (ay * ez - az * ey) * ir3;
-            sy += (az * ex - ax * ez) * ir3;
-            sz += (ax * ey - ay * ex) * ir3;
+            const float4 al = as32[j];
+            sx += (al.y * ez - al.z * ey) * ir3;
+            sy += (al.z * ex - al.x * ez) * ir3;
+            sz += (al.x * ey - al.y * ex) * ir3;
         }
         vx += sx;
         vy += sy;
@@ -175,6 +182,27 @@ __device__ __forceinline__ void p2p3(const Src3& s, int lo, int hi, int self, do
             vz += (s.ax[j] * ey - s.ay[j] * ex) * ir3;
         }
     }
+}
+
+// One warp per cell: for a leaf (no children), the offsets from its centre
+// and the alphas of its particles; then every cell's moments (grid-stride).
+__global__ void __launch_bounds__(256) prep3d_f32_kernel(Tree3D t, unsigned* err) {
+    if (fatal(err)) return;
+    const int lane = threadIdx.x & 31;
+    const int nc = t.info->n_cells;
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    for (int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < nc; c += warps) {
+        if (t.c_chmask[c] != 0) continue;
+        const double cx = t.c_x[c], cy = t.c_y[c], cz = t.c_z[c];
+        for (int j = t.c_lo[c] + lane; j < t.c_hi[c]; j += 32) {
+            t.ps32[j] = make_float4((float)(t.px[j] - cx), (float)(t.py[j] - cy), (float)(t.pz[j] - cz),
+                                    t.pact[j] ? 1.f : 0.f);
+            t.as32[j] = make_float4((float)t.ax[j], (float)t.ay[j], (float)t.az[j], 0.f);
+        }
+    }
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < (long long)nc * 30;
+         i += (long long)gridDim.x * blockDim.x)
+        t.mom32[i] = (float)t.mom[i];
 }
 
 template <bool F32, bool ALL>
@@ -242,7 +270,7 @@ eval3d_kernel(Tree3D t, const uint8_t* __restrict__ target, double support, int 
                             const double Rc = xmul(t.c_size[k], support);
                             far = R2 > xmul(Rc, Rc);
                             if (far) {
-                                if (F32) m2p32(&t.mom[(size_t)k * 30], dx, dy, dz, vx, vy, vz);
+                                if (F32) m2p32(&t.mom32[(size_t)k * 30], dx, dy, dz, vx, vy, vz);
                                 else m2p64(&t.mom[(size_t)k * 30], R2, dx, dy, dz, vx, vy, vz);
                             }
                         }
@@ -259,7 +287,8 @@ eval3d_kernel(Tree3D t, const uint8_t* __restrict__ target, double support, int 
                             }
                             ++nn;
                         } else if ((near >> lane) & 1u) {
-                            p2p3<F32, ALL>(src, t.c_lo[k], t.c_hi[k], slot, xp, yp, zp, vx, vy, vz);
+                            p2p3<F32, ALL>(src, t.ps32, t.as32, t.c_lo[k], t.c_hi[k], slot, xp, yp, zp, t.c_x[k],
+                                           t.c_y[k], t.c_z[k], vx, vy, vz);
                         }
                     }
                 }
@@ -279,6 +308,12 @@ eval3d_kernel(Tree3D t, const uint8_t* __restrict__ target, double support, int 
 }
 
 }  // namespace
+
+cudaError_t prep3d_f32(const Tree3D& t, unsigned* err, cudaStream_t st, int* launches) {
+    prep3d_f32_kernel<<<148 * 8, 256, 0, st>>>(t, err);
+    *launches += 1;
+    return cudaGetLastError();
+}
 
 cudaError_t eval3d(const Tree3D& t, bool mixed, bool all_src, const uint8_t* target, double support, double* u,
                    double* v, double* w, double uinf, double vinf, double winf, unsigned* err, cudaStream_t st,
