@@ -177,3 +177,32 @@ def test_reused_context_matches_fresh(ctx, prec):
             fx, fy = fresh.field2d(x, y, q, act, prm)
             del fresh
             assert np.array_equal(ex, fx, equal_nan=True) and np.array_equal(ey, fy, equal_nan=True), (use_graph, k)
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+@pytest.mark.parametrize("use_graph", [0, 1])
+def test_host_entry_matches_device_entry(ctx, prec, use_graph):
+    """The host entry points upload positions first and gather the strengths
+    into tree order after the sort; the device entry point sorts with them.
+    Both give the same bits, for the field and (through vpm_velocity2d) the
+    velocity, from page-locked and from ordinary host memory."""
+    import torch
+    d = cases2d.clustered()
+    x, y, q, a = d["x"], d["y"], d["q"], d["active"]
+    prm = default_params(use_graph=use_graph) if prec == 0 else \
+        default_params(precision=1, binom=BINOM_EXACT, p=8, max_src=100, max_par=150, use_graph=use_graph)
+    dev = [torch.from_numpy(np.ascontiguousarray(v)).cuda() for v in (x, y, q, a)]
+    ex_d, ey_d = torch.empty_like(dev[0]), torch.empty_like(dev[0])
+    ctx.field2d_device(*dev, ex_d, ey_d, prm)
+    ctx.sync()
+    ex_d, ey_d = ex_d.cpu().numpy(), ey_d.cpu().numpy()
+    ex, ey = ctx.field2d(x, y, q, a, prm)
+    assert np.array_equal(ex, ex_d) and np.array_equal(ey, ey_d)
+    pinned = [torch.from_numpy(np.ascontiguousarray(v)).pin_memory().numpy() for v in (x, y, q, a)]
+    ex2, ey2 = ctx.field2d(*pinned, prm)
+    assert np.array_equal(ex2, ex_d) and np.array_equal(ey2, ey_d)
+    # velocity: q = -omega s^2 / (2 pi) formed on the upload stream; u = Ey, v = -Ex
+    s = np.full(x.size, 0.02)
+    omega = -q * 2.0 * np.pi / (s * s)
+    u, v = ctx.velocity2d(x, y, omega, s, a, 0.0, 0.0, prm)
+    assert rel_l2((u, v), (ey_d, -ex_d)) <= 1e-14
