@@ -440,6 +440,15 @@ def run_ours(args):
                 "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                 "traffic": traffic, "peak_source": "measured FMA-chain peak (vpm_measure_fma_peaks)",
                 "work": f"{P2P_FLOPS_PER_PAIR} flops x {pairs} list-1 pairs per launch"}
+    if form != "fp64":
+        # the FP32 near field issues one reciprocal per pair: its tighter bound
+        # is the special-function unit, measured by a reciprocal-chain kernel
+        rcp_peak = ctx.rcp_peak()
+        pair_rate = pairs / (p2p_ms * 1e-3) / 1e9
+        roofline["reciprocal_bound"] = {"achieved": pair_rate, "peak": rcp_peak, "unit": "G pairs/s",
+                                        "frac": pair_rate / rcp_peak,
+                                        "peak_source": "measured rcp.approx.f32 chain throughput (vpm_measure_rcp_peak)",
+                                        "work": "one reciprocal per list-1 pair"}
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

@@ -434,6 +434,14 @@ int vpm_direct3d_velocity_device(vpm_ctx* ctx, const double* x, const double* y,
  */
 int vpm_measure_fma_peaks(vpm_ctx* ctx, double* fp64_tflops, double* fp32_tflops);
 
+/*
+ * Reciprocal-throughput microbenchmark (G reciprocals/s of dependent
+ * rcp.approx.ftz.f32 chains): the special-function-unit peak that bounds the
+ * FP32 near field, which issues one reciprocal per pair. No counterpart in
+ * the reference (measurement utility).
+ */
+int vpm_measure_rcp_peak(vpm_ctx* ctx, double* grcp_per_s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -104,6 +104,7 @@ SIGNATURES = {
     "vpm_tree2d_leaves": (C.c_int, [_vp, _vp, _vp, _vp]),
     "vpm_tree2d_list": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp]),
     "vpm_measure_fma_peaks": (C.c_int, [_vp, _dp, _dp]),
+    "vpm_measure_rcp_peak": (C.c_int, [_vp, _dp]),
     "vpm_stage_history": (C.c_int, [_vp, C.c_int32, C.c_int32, _vp, C.POINTER(C.c_int32)]),
     "vpm_fmm2d_field_batched": (C.c_int, [_vp, C.c_int32, _vp, _vp, _vp, _vp, _vp, C.POINTER(Params), _vp, _vp]),
     "vpm_batch_streams": (C.c_int, [_vp, _vp]),

@@ -40,8 +40,57 @@ int run(Ctx* c, int iters, double* tflops) {
     return VPM_OK;
 }
 
+// Reciprocal-throughput microbenchmark (rcp.approx.ftz.f32, the special
+// function unit the FP32 near field issues one reciprocal per pair to): 8
+// independent chains x <- 1/x + 1 per thread (the add keeps consecutive
+// reciprocals from cancelling and runs on the FMA pipe, which is 8x wider).
+__global__ void __launch_bounds__(256) rcp_chains(float* out, int iters) {
+    float x[8];
+    #pragma unroll
+    for (int k = 0; k < 8; ++k) x[k] = 1.0f + 0.125f * (float)(threadIdx.x + k);
+    for (int i = 0; i < iters; ++i) {
+        #pragma unroll
+        for (int u = 0; u < 16; ++u) {
+            #pragma unroll
+            for (int k = 0; k < 8; ++k)
+                asm volatile("rcp.approx.ftz.f32 %0, %0;\n\tadd.f32 %0, %0, 0f3F800000;" : "+f"(x[k]));
+        }
+    }
+    float s = 0.f;
+    #pragma unroll
+    for (int k = 0; k < 8; ++k) s += x[k];
+    if (s == -12345.0f) out[0] = s;
+}
+
+int run_rcp(Ctx* c, int iters, double* grcp) {
+    const int blocks = 148 * 8, threads = 256;
+    float* d = nullptr;
+    cudaError_t e = cudaMalloc(&d, 64);
+    if (e != cudaSuccess) return c->fail_cuda(e, "cudaMalloc");
+    rcp_chains<<<blocks, threads, 0, c->stream>>>(d, 4);  // warm-up
+    cudaEventRecord(c->ev[0], c->stream);
+    rcp_chains<<<blocks, threads, 0, c->stream>>>(d, iters);
+    cudaEventRecord(c->ev[1], c->stream);
+    e = cudaEventSynchronize(c->ev[1]);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+    cudaFree(d);
+    if (e != cudaSuccess) return c->fail_cuda(e, "rcp_chains");
+    const double n = 8.0 * 16 * (double)iters * blocks * threads;
+    *grcp = n / (ms * 1e-3) / 1e9;
+    return VPM_OK;
+}
+
 }  // namespace
 }  // namespace vpm
+
+extern "C" int vpm_measure_rcp_peak(vpm_ctx* ctx, double* grcp_per_s) {
+    if (!ctx || !grcp_per_s) return VPM_EINVAL;
+    vpm::Ctx* c = (vpm::Ctx*)ctx;
+    cudaError_t e = cudaSetDevice(c->device);
+    if (e != cudaSuccess) return c->fail_cuda(e, "cudaSetDevice");
+    return vpm::run_rcp(c, 1024, grcp_per_s);
+}
 
 extern "C" int vpm_measure_fma_peaks(vpm_ctx* ctx, double* fp64_tflops, double* fp32_tflops) {
     if (!ctx || !fp64_tflops || !fp32_tflops) return VPM_EINVAL;

@@ -256,6 +256,12 @@ class Context:
         self._check(lib().vpm_measure_fma_peaks(self._h, C.byref(a), C.byref(b)))
         return a.value, b.value
 
+    def rcp_peak(self):
+        """FP32 reciprocal (rcp.approx) throughput of the device in G/s."""
+        a = C.c_double()
+        self._check(lib().vpm_measure_rcp_peak(self._h, C.byref(a)))
+        return a.value
+
     def last_stats(self) -> Stats:
         s = Stats()
         self._check(lib().vpm_last_stats(self._h, C.byref(s)))
