@@ -18,7 +18,8 @@
 namespace vpm {
 
 constexpr int kMaxLevels3D = 60;     // octree depth limit (coincident particles)
-constexpr int kWork3DCap = 512;      // union work list of one leaf's traversal, per level
+constexpr int kWork3DCap = 512;      // union work list of a warp's traversal per level, at support
+                                     // factor 2 (eval3d scales it for larger factors)
 constexpr int kEval3DWarps = 4;      // warps (leaves) per evaluation block
 constexpr int kCoopMaxBlocks3D = 148 * 8;  // size of the per-block scan partials
 
