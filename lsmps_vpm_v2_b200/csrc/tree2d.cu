@@ -884,7 +884,14 @@ __global__ void flat_link(Tree2D t, int max_par, unsigned* err) {
         {
             const int lo = t.c_lo[c];
             const bool leaf = t.c_flags[c] & CELL_LEAF;
-            const int hi = group_end(t.key, lo, leaf ? min(n, lo + max_par) : n, 2 * (K - L));
+            // a split cell's children partition its range, so a cell's range
+            // ends where its next sibling's starts; only a parent's last child
+            // needs the search for the end of its key group
+            int hi;
+            if (c + 1 < nc && t.c_level[c + 1] == L && (t.c_code[c + 1] >> 2) == (code >> 2))
+                hi = t.c_lo[c + 1];
+            else
+                hi = group_end(t.key, lo, leaf ? min(n, lo + max_par) : n, 2 * (K - L));
             const int src = (int)(t.actscan[hi] - t.actscan[lo]);
             t.c_hi[c] = hi;
             t.c_src[c] = src;
