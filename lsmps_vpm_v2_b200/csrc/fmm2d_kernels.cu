@@ -1501,9 +1501,14 @@ cudaError_t launch_upward_direct(const Tree2D& t, Expansions2D& e, unsigned* err
     cudaError_t r = cudaFuncSetAttribute(upward_direct2d<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (r != cudaSuccess) return r;
     upward_direct2d<P><<<148 * 4, 32 * kUpWarps, smem, st>>>(t, e.a, t.gbar + 3, err);
+    // A small grid: the large cells are a few hundred per level, and the
+    // blocks of this loop wait at its barriers most of the time while the
+    // near field runs beside it on the other streams, so every block it does
+    // not hold is SM room for that (16 blocks: mixed step 0.442 -> 0.430 ms
+    // at 778k against one block per SM).
     int grid = 0;
-    r = launch_coop(m2m_big_levels_coop, 32 * kLevelWarps, 0, st, 1, &grid, t, e.a, (const double*)e.coef, P,
-                    kDirectMax, (const unsigned*)(t.gbar + 3), t.gbar + 2, err);
+    r = launch_coop_max(m2m_big_levels_coop, 32 * kLevelWarps, 0, st, 1, std::max(16, t.n >> 16), &grid, t, e.a,
+                        (const double*)e.coef, P, kDirectMax, (const unsigned*)(t.gbar + 3), t.gbar + 2, err);
     return r != cudaSuccess ? r : cudaGetLastError();
 }
 

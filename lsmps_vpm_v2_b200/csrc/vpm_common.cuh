@@ -211,12 +211,12 @@ __host__ __device__ __forceinline__ int64_t start_id2(int L) { return (((int64_t
 __host__ __device__ inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
 
 // Cooperative launch with every block co-resident: grid = SMs x the
-// occupancy of `kernel` at `block` threads (at most max_blocks_per_sm). The
-// grid size is returned in *grid. Fails (no launch) when the device cannot
-// make the blocks co-resident.
+// occupancy of `kernel` at `block` threads (at most max_blocks_per_sm), and at
+// most max_grid blocks. The grid size is returned in *grid. Fails (no launch)
+// when the device cannot make the blocks co-resident.
 template <typename... KArgs, typename... Args>
-cudaError_t launch_coop(void (*kernel)(KArgs...), int block, size_t smem, cudaStream_t st, int max_blocks_per_sm,
-                        int* grid, Args... args) {
+cudaError_t launch_coop_max(void (*kernel)(KArgs...), int block, size_t smem, cudaStream_t st, int max_blocks_per_sm,
+                            int max_grid, int* grid, Args... args) {
     int dev = 0, sms = 0, occ = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
@@ -226,8 +226,9 @@ cudaError_t launch_coop(void (*kernel)(KArgs...), int block, size_t smem, cudaSt
     if (e != cudaSuccess) return e;
     if (occ < 1) return cudaErrorCooperativeLaunchTooLarge;
     if (occ > max_blocks_per_sm) occ = max_blocks_per_sm;
+    const int g = sms * occ < max_grid ? sms * occ : (max_grid > 0 ? max_grid : 1);
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(sms * occ);
+    cfg.gridDim = dim3(g);
     cfg.blockDim = dim3(block);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = st;
@@ -236,8 +237,14 @@ cudaError_t launch_coop(void (*kernel)(KArgs...), int block, size_t smem, cudaSt
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (grid) *grid = sms * occ;
+    if (grid) *grid = g;
     return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
+template <typename... KArgs, typename... Args>
+cudaError_t launch_coop(void (*kernel)(KArgs...), int block, size_t smem, cudaStream_t st, int max_blocks_per_sm,
+                        int* grid, Args... args) {
+    return launch_coop_max(kernel, block, smem, st, max_blocks_per_sm, 1 << 30, grid, args...);
 }
 
 }  // namespace vpm
