@@ -229,7 +229,7 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
     const bool deferred = q_ready != nullptr && !tree_only;
     const unsigned wait_flags = capturing ? cudaEventWaitExternal : 0u;
     VPM_CUDA_TRY(keys_sort2d(x, y, deferred ? nullptr : q, act, tree, ts, p.exp_tree_pct, d_err, st, &launches,
-                             std::min(p.max_src, p.max_par)));
+                             std::min(p.max_src, p.max_par), sort_items));
     if (int r = record(1)) return r;
     VPM_CUDA_TRY(levels2d(tree, ts, p.max_src, p.max_par, d_err, st, &launches));
     if (int r = record(2)) return r;

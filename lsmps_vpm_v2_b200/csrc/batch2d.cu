@@ -62,6 +62,9 @@ int Ctx::prepare_batch(int ns, const int64_t* offs, const vpm_fmm_params& p, int
             delete c;
             return fail(r, "sub-context: " + m);
         }
+        // 8192 particles per sort block: a batch's sorts run side by side
+        // (64 uneven solves: 5.11 -> 4.54 ms against 2048)
+        c->sort_items = 8192;
         subs.push_back(c);
         cudaEvent_t e = nullptr;
         VPM_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));

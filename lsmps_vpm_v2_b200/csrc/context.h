@@ -127,6 +127,10 @@ struct Ctx {
 
     Selector* selector = nullptr;
 
+    // particles per block of the cooperative sort (keys_sort2d): more in the
+    // sub-contexts of a batch, whose solves share the GPU
+    int sort_items = 2048;
+
     // batched solves (batch2d.cu)
     std::vector<Ctx*> subs;
     std::vector<cudaEvent_t> join_ev;

@@ -928,17 +928,19 @@ __global__ void flat_link(Tree2D t, int max_par, unsigned* err) {
 
 }  // namespace
 
-// Grid and per-block share of the cooperative sort for n particles, or false
-// when it does not apply (share above kCoopSortMaxChunk, or fewer than one
-// resident block per SM).
-bool coop_sort_shape(int n, int* grid, int* chunk) {
+// Grid and per-block share of the cooperative sort for n particles (about
+// `items` per block, at most one block per SM), or false when it does not
+// apply (share above kCoopSortMaxChunk, or fewer than one resident block per
+// SM).
+bool coop_sort_shape(int n, int items, int* grid, int* chunk) {
     static int sms = 0, smem_set = 0;
     if (sms == 0) {
         int dev = 0;
         if (cudaGetDevice(&dev) != cudaSuccess) return false;
         if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return false;
     }
-    const int g = std::max(1, std::min(std::min(sms, kCoopSortGridMax), ceil_div(n, 2048)));
+    const int g = std::max(std::max(1, ceil_div(n, kCoopSortMaxChunk)),
+                           std::min(std::min(sms, kCoopSortGridMax), ceil_div(n, items)));
     const int c = ceil_div(n, g);
     if (c > kCoopSortMaxChunk) return false;
     if (smem_set == 0) {
@@ -959,7 +961,7 @@ bool coop_sort_shape(int n, int* grid, int* chunk) {
 
 cudaError_t keys_sort2d(const double* x, const double* y, const double* q, const uint8_t* act, Tree2D& t,
                         TreeScratch2D& s, double exp_pct, unsigned* err, cudaStream_t st, int* launches,
-                        int shallow_cap) {
+                        int shallow_cap, int items_per_block) {
     const int n = t.n;
     const int K = t.key_levels;
     const int gridN = std::max(1, std::min(148 * 8, ceil_div(n, 256)));
@@ -969,7 +971,7 @@ cudaError_t keys_sort2d(const double* x, const double* y, const double* q, const
     if (e != cudaSuccess) return e;
     *launches += 1;
     int coop_grid = 0, coop_chunk = 0;
-    if (2 * K <= 32 && s.coop_words && s.sort_aos && coop_sort_shape(n, &coop_grid, &coop_chunk)) {
+    if (2 * K <= 32 && s.coop_words && s.sort_aos && coop_sort_shape(n, items_per_block, &coop_grid, &coop_chunk)) {
         uint32_t* k32 = reinterpret_cast<uint32_t*>(s.key_alt);
         const size_t smem = (size_t)coop_chunk * 10;
         cudaLaunchConfig_t cfg = {};
