@@ -127,9 +127,11 @@ struct Ctx {
 
     Selector* selector = nullptr;
 
-    // particles per block of the cooperative sort (keys_sort2d): more in the
-    // sub-contexts of a batch, whose solves share the GPU
-    int sort_items = 2048;
+    // particles per block of the cooperative sort (keys_sort2d; at most one
+    // block per SM): 1024 for a solve with the GPU to itself (the 65,536-
+    // particle lattice spreads over 64 SMs: 0.183 -> 0.179 ms against 2048),
+    // more in the sub-contexts of a batch, whose solves share the GPU
+    int sort_items = 1024;
 
     // batched solves (batch2d.cu)
     std::vector<Ctx*> subs;

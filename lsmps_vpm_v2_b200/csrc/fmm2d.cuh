@@ -164,12 +164,13 @@ cudaError_t build_tree2d(const double* x, const double* y, const double* q, cons
 // q = null sorts without the strengths: t.pq is then left for
 // gather_strengths2d, so that the strengths can still be in flight from the
 // host while the tree and the lists are built.
-// items_per_block: particles per block of the cooperative sort (2048: a
-// solve with the GPU to itself spreads over every SM; solves sharing the GPU
-// in a batch take fewer, fuller blocks so that several sorts fit at once).
+// items_per_block: particles per block of the cooperative sort (a solve with
+// the GPU to itself spreads over as many SMs as it can fill; solves sharing
+// the GPU in a batch take fewer, fuller blocks so that several sorts fit at
+// once).
 cudaError_t keys_sort2d(const double* x, const double* y, const double* q, const uint8_t* act, Tree2D& t,
                         TreeScratch2D& s, double exp_pct, unsigned* err, cudaStream_t st, int* launches,
-                        int shallow_cap = 0, int items_per_block = 2048);
+                        int shallow_cap = 0, int items_per_block = 1024);
 // t.pq[i] = q[t.perm[i]] for i < t.n.
 cudaError_t gather_strengths2d(const Tree2D& t, const double* q, unsigned* err, cudaStream_t st, int* launches);
 cudaError_t levels2d(Tree2D& t, TreeScratch2D& s, int max_src, int max_par, unsigned* err, cudaStream_t st,
