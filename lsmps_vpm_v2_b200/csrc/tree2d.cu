@@ -632,6 +632,31 @@ __device__ __forceinline__ int group_start(const uint64_t* __restrict__ key, int
     return L;
 }
 
+// group_start with the whole warp on one query (i and sh the same in every
+// lane): 32 probes per round, galloping back from i by 1, 2, 4, ... 2^30,
+// then 32-way splits of the bracket, so a group of d particles takes about
+// 1 + log_31(d) rounds of loads instead of 2 log_2(d) dependent ones.
+__device__ __forceinline__ int group_start_warp(const uint64_t* __restrict__ key, int i, int sh) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t v = key[i] >> sh;
+    const int p0 = lane < 31 ? max(0, i - (1 << lane)) : 0;
+    const unsigned in0 = __ballot_sync(0xffffffffu, (key[p0] >> sh) == v);
+    if (in0 == 0xffffffffu) return 0;                  // the group reaches particle 0
+    const int t0 = __ffs(~in0) - 1;                     // first probe outside the group
+    int lo = __shfl_sync(0xffffffffu, p0, t0) + 1;
+    int hi = t0 == 0 ? i : __shfl_sync(0xffffffffu, p0, t0 - 1);
+    while (lo < hi) {                                   // the answer is in [lo, hi]; hi is in the group
+        const int q = lo + (int)(((long long)(hi - lo) * lane) / 31);
+        const unsigned in = __ballot_sync(0xffffffffu, (key[q] >> sh) == v);
+        const int t = __ffs(in) - 1;                    // lane 31 probes hi: t >= 0
+        if (t == 0) return lo;
+        const int qt = __shfl_sync(0xffffffffu, q, t), qp = __shfl_sync(0xffffffffu, q, t - 1);
+        lo = qp + 1;
+        hi = qt;
+    }
+    return lo;
+}
+
 __device__ __forceinline__ uint32_t compact2(uint64_t x) {
     x &= 0x5555555555555555ull;
     x = (x | (x >> 1)) & 0x3333333333333333ull;
@@ -664,27 +689,57 @@ flat_bigl(Tree2D t, int max_src, int max_par, uint32_t* __restrict__ pinfo, unsi
 }
 
 // The cell levels of every particle (pinfo bits 16..23 first, 24..31 last; 0 =
-// none) and the per-tile counts of cells and leaves of every level.
+// none) and the per-tile counts of cells and leaves of every level. A particle
+// starting a group at level lvl starts cells only if the parent group (level
+// lvl-1) is big; that group starts at the last particle before it that starts
+// a group at level <= lvl-1, found from per-warp ballots of the tile (most
+// parents start in the same tile) and otherwise by a search of the keys back
+// from the tile's first particle.
 __global__ void __launch_bounds__(kFlatTile)
 flat_cells(Tree2D t, uint32_t* __restrict__ pinfo, uint32_t* __restrict__ tile_cnt, int tiles, unsigned* err) {
     __shared__ unsigned s_c[kMaxLevels2D + 1], s_l[kMaxLevels2D + 1];
+    __shared__ uint32_t s_pi[kFlatTile];                          // the tile's pinfo words
+    __shared__ unsigned s_mk[kMaxLevels2D + 1][kFlatTile / 32];   // per warp: lanes starting a group at level <= m
     const int n = t.n, K = t.key_levels;
     const uint64_t* __restrict__ key = t.key;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         for (int k = threadIdx.x; k <= K; k += blockDim.x) s_c[k] = s_l[k] = 0;
+        const int tb = tile * kFlatTile;
+        const int i = tb + threadIdx.x;
+        const uint32_t w = i < n ? pinfo[i] : 0xffu;   // past the end: no group start
+        const int lvl = (int)(w & 0xff);
+        s_pi[threadIdx.x] = w;
+        for (int m = 1; m <= K; ++m) {
+            const unsigned mk = __ballot_sync(0xffffffffu, lvl <= m);
+            if (lane == 0) s_mk[m][warp] = mk;
+        }
         __syncthreads();
-        const int i = tile * kFlatTile + threadIdx.x;
+        // pinfo word of the parent group's first particle (only bits 0..15,
+        // lvl and big, are read: they are not rewritten below)
+        const bool starts = lvl <= K;   // implies i < n
+        const int m = lvl - 1;
+        uint32_t wp = 0;
+        bool need = false;
+        if (starts && lvl > 1) {
+            unsigned mk = s_mk[m][warp] & ((1u << lane) - 1u);
+            int wq = warp;
+            while (!mk && wq > 0) mk = s_mk[m][--wq];
+            if (mk) wp = s_pi[wq * 32 + 31 - __clz(mk)];
+            else need = true;
+        }
+        // parents starting before the tile: one cooperative search per level
+        for (unsigned qm = __ballot_sync(0xffffffffu, need); qm;) {
+            const int mq = __shfl_sync(0xffffffffu, m, __ffs(qm) - 1);
+            const uint32_t wg = pinfo[group_start_warp(key, tb, 2 * (K - mq))];
+            if (need && m == mq) wp = wg;
+            qm &= ~__ballot_sync(0xffffffffu, need && m == mq);
+        }
         if (i < n) {
-            const uint32_t w = pinfo[i];
-            const int lvl = (int)(w & 0xff), big = (int)((w >> 8) & 0xff) - 1;
+            const int big = (int)((w >> 8) & 0xff) - 1;
             int first = 0, last = 0;
-            if (lvl <= K) {
-                bool exists = lvl == 1;
-                if (!exists) {
-                    const int sp = group_start(key, i, 2 * (K - (lvl - 1)));
-                    const int bigp = (int)((pinfo[sp] >> 8) & 0xff) - 1;
-                    exists = bigp >= lvl - 1;
-                }
+            if (starts) {
+                const bool exists = lvl == 1 || (int)((wp >> 8) & 0xff) - 1 >= m;
                 if (exists) {
                     first = lvl;
                     last = min(K, max(lvl, big + 1));
@@ -704,13 +759,68 @@ flat_cells(Tree2D t, uint32_t* __restrict__ pinfo, uint32_t* __restrict__ tile_c
     }
 }
 
-// One block per (kind, level) row: exclusive scan of the tile counts in place
-// and the row total.
+// Level starts, totals and the root cell (treeCell.cpp:1117-1133), from the
+// row totals of flat_scan (one thread).
+__device__ void flat_totals(Tree2D t, const uint32_t* __restrict__ level_tot, unsigned* err) {
+    const int K = t.key_levels;
+    TreeInfo2D* info = t.info;
+    int cells = 1, leaves = 0, depth = 0;
+    info->level_start[0] = 0;
+    info->leaf_start[0] = 0;
+    int mn = -1, mx = -1;   // leaf level range (TreeCell::min_level / max_level, treeCell.cpp:1236-1240)
+    for (int L = 1; L < kMaxLevels2D + 3; ++L) {
+        info->level_start[L] = cells;
+        info->leaf_start[L] = leaves;
+        if (L <= K) {
+            const int c = (int)__ldcg(level_tot + L), lf = (int)__ldcg(level_tot + kMaxLevels2D + 1 + L);
+            if (c > 0) depth = L;
+            if (lf > 0) {
+                if (mn < 0) mn = L;
+                mx = L;
+            }
+            cells += c;
+            leaves += lf;
+        }
+    }
+    info->n_cells = cells;
+    info->n_leaves = leaves;
+    info->depth = depth;
+    info->l2_irregular = 0;
+    info->min_leaf_level = mn;
+    info->max_leaf_level = mx;
+    if (cells > t.cap_cells) set_err(err, ERR_CELL_CAP);
+    const Geom2D* g = t.geom;
+    t.c_lo[0] = 0;
+    t.c_hi[0] = t.n;
+    const int src = (int)t.actscan[t.n];
+    t.c_src[0] = src;
+    t.c_flags[0] = src != 0 ? CELL_ACTIVE : 0;
+    t.c_parent[0] = -1;
+    t.c_child0[0] = -1;   // lowered by flat_link (unsigned minimum, so -1 = none)
+    t.c_chmask[0] = 0;
+    t.c_level[0] = 0;
+    t.c_ix[0] = 0;
+    t.c_iy[0] = 0;
+    t.c_code[0] = 0;
+    t.c_leafidx[0] = -1;
+    t.c_cx[0] = xadd(g->pivx, xmul(0.5, g->root));
+    t.c_cy[0] = xadd(g->pivy, xmul(0.5, g->root));
+    if (t.dense) t.dense[0] = 0;
+    if (t.nonleaf && cells > 1) t.nonleaf[0] = 0;
+}
+
+// One block per (kind, level) row of levels 0..K: exclusive scan of the tile
+// counts in place and the row total; the last block to finish then sets the
+// level starts, totals and root cell (flat_totals). ticket: zero on entry.
 __global__ void __launch_bounds__(1024)
-flat_scan(uint32_t* __restrict__ tile_cnt, int tiles, uint32_t* __restrict__ level_tot) {
+flat_scan(Tree2D t, uint32_t* __restrict__ tile_cnt, int tiles, uint32_t* __restrict__ level_tot, unsigned* ticket,
+          unsigned* err) {
     __shared__ uint32_t s_w[32];
     __shared__ uint32_t s_carry;
-    uint32_t* row = tile_cnt + (size_t)blockIdx.x * tiles;
+    __shared__ bool s_last;
+    const int K = t.key_levels;
+    const int r = blockIdx.x <= K ? (int)blockIdx.x : kMaxLevels2D + 1 + ((int)blockIdx.x - K - 1);
+    uint32_t* row = tile_cnt + (size_t)r * tiles;
     if (threadIdx.x == 0) s_carry = 0;
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -736,59 +846,16 @@ flat_scan(uint32_t* __restrict__ tile_cnt, int tiles, uint32_t* __restrict__ lev
         if (threadIdx.x == 0) s_carry = carry + tot;
         __syncthreads();
     }
-    if (threadIdx.x == 0) level_tot[blockIdx.x] = s_carry;
-}
-
-// Level starts, totals and the root cell (treeCell.cpp:1117-1133).
-__global__ void flat_totals(Tree2D t, const uint32_t* __restrict__ level_tot, unsigned* err) {
-    const int K = t.key_levels;
-    TreeInfo2D* info = t.info;
-    int cells = 1, leaves = 0, depth = 0;
-    info->level_start[0] = 0;
-    info->leaf_start[0] = 0;
-    for (int L = 1; L < kMaxLevels2D + 3; ++L) {
-        info->level_start[L] = cells;
-        info->leaf_start[L] = leaves;
-        if (L <= K) {
-            const int c = (int)level_tot[L], lf = (int)level_tot[kMaxLevels2D + 1 + L];
-            if (c > 0) depth = L;
-            cells += c;
-            leaves += lf;
-        }
+    if (threadIdx.x == 0) {
+        level_tot[r] = s_carry;
+        __threadfence();
+        s_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
     }
-    info->n_cells = cells;
-    info->n_leaves = leaves;
-    info->depth = depth;
-    info->l2_irregular = 0;
-    // leaf level range (TreeCell::min_level / max_level, treeCell.cpp:1236-1240)
-    int mn = -1, mx = -1;
-    for (int L = 1; L <= K; ++L) {
-        if (level_tot[kMaxLevels2D + 1 + L] > 0) {
-            if (mn < 0) mn = L;
-            mx = L;
-        }
+    __syncthreads();
+    if (s_last && threadIdx.x == 0) {
+        __threadfence();
+        flat_totals(t, level_tot, err);
     }
-    info->min_leaf_level = mn;
-    info->max_leaf_level = mx;
-    if (cells > t.cap_cells) set_err(err, ERR_CELL_CAP);
-    const Geom2D* g = t.geom;
-    t.c_lo[0] = 0;
-    t.c_hi[0] = t.n;
-    const int src = (int)t.actscan[t.n];
-    t.c_src[0] = src;
-    t.c_flags[0] = src != 0 ? CELL_ACTIVE : 0;
-    t.c_parent[0] = -1;
-    t.c_child0[0] = -1;   // lowered by flat_link (unsigned minimum, so -1 = none)
-    t.c_chmask[0] = 0;
-    t.c_level[0] = 0;
-    t.c_ix[0] = 0;
-    t.c_iy[0] = 0;
-    t.c_code[0] = 0;
-    t.c_leafidx[0] = -1;
-    t.c_cx[0] = xadd(g->pivx, xmul(0.5, g->root));
-    t.c_cy[0] = xadd(g->pivy, xmul(0.5, g->root));
-    if (t.dense) t.dense[0] = 0;
-    if (t.nonleaf && cells > 1) t.nonleaf[0] = 0;
 }
 
 // Cell records (and leaf entries) of every particle's cell levels, indices
@@ -797,15 +864,23 @@ __global__ void __launch_bounds__(kFlatTile)
 flat_emit(Tree2D t, const uint32_t* __restrict__ pinfo, const uint32_t* __restrict__ tile_cnt, int tiles,
           int max_par, unsigned* err) {
     __shared__ int s_wc[kMaxLevels2D + 1][kFlatTile / 32], s_wl[kMaxLevels2D + 1][kFlatTile / 32];
+    __shared__ int s_c0[kMaxLevels2D + 1], s_l0[kMaxLevels2D + 1];   // the tile's first cell / leaf of each level
+    __shared__ double s_len[kMaxLevels2D + 1];                        // cell size of each level
     if (block_fatal(err)) return;
     const int n = t.n, K = t.key_levels;
     const TreeInfo2D* info = t.info;
     const double root = t.geom->root, pivx = t.geom->pivx, pivy = t.geom->pivy;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned below = (1u << lane) - 1u;
+    for (int k = threadIdx.x; k <= K; k += blockDim.x) s_len[k] = xdiv(root, ldexp(1.0, k));
     for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         const int i = tile * kFlatTile + threadIdx.x;
         const uint32_t w = i < n ? pinfo[i] : 0u;
+        const uint64_t ki = i < n ? t.key[i] : 0ull;
+        for (int k = threadIdx.x; k <= K; k += blockDim.x) {
+            s_c0[k] = info->level_start[k] + (int)tile_cnt[(size_t)k * tiles + tile];
+            s_l0[k] = info->leaf_start[k] + (int)tile_cnt[(size_t)(kMaxLevels2D + 1 + k) * tiles + tile];
+        }
         const int first = (int)((w >> 16) & 0xff), last = (int)(w >> 24), big = (int)((w >> 8) & 0xff) - 1;
         // the levels at which this warp's particles start cells (most warps: one or two)
         const int Llo = (int)__reduce_min_sync(0xffffffffu, first ? (unsigned)first : 255u);
@@ -836,15 +911,15 @@ flat_emit(Tree2D t, const uint32_t* __restrict__ pinfo, const uint32_t* __restri
                 bc += s_wc[L][k];
                 bl += s_wl[L][k];
             }
-            const int ci = info->level_start[L] + (int)tile_cnt[(size_t)L * tiles + tile] + bc + __popc(mc & below);
+            const int ci = s_c0[L] + bc + __popc(mc & below);
             if (ci >= t.cap_cells) {
                 set_err(err, ERR_CELL_CAP);
                 continue;
             }
             const int sh = 2 * (K - L);
-            const uint64_t code = t.key[i] >> sh;
+            const uint64_t code = ki >> sh;
             const int ix = (int)compact2(code), iy = (int)compact2(code >> 1);
-            const double len = xdiv(root, ldexp(1.0, L));
+            const double len = s_len[L];
             t.c_lo[ci] = i;
             t.c_flags[ci] = lf ? CELL_LEAF : 0;   // range end, counts and activity: flat_link
             t.c_child0[ci] = -1;
@@ -857,8 +932,7 @@ flat_emit(Tree2D t, const uint32_t* __restrict__ pinfo, const uint32_t* __restri
             t.c_cy[ci] = xadd(pivy, xmul(xadd(0.5, (double)iy), len));
             if (t.dense && L <= t.dense_levels) t.dense[start_id2(L) + ix + ((int64_t)iy << L)] = ci;
             // leaves before this cell: of the lower levels, then of this level
-            const int li = info->leaf_start[L] + (int)tile_cnt[(size_t)(kMaxLevels2D + 1 + L) * tiles + tile] + bl +
-                           __popc(ml & below);
+            const int li = s_l0[L] + bl + __popc(ml & below);
             if (lf) {
                 t.c_leafidx[ci] = li;
                 t.leaf_cells[li] = ci;
@@ -1050,12 +1124,12 @@ cudaError_t levels2d_flat(Tree2D& t, TreeScratch2D& s, int max_src, int max_par,
     const int grid = std::max(1, std::min(tiles, 148 * 8));
     flat_bigl<<<grid, kFlatTile, 0, st>>>(t, max_src, max_par, s.pinfo, err);
     flat_cells<<<grid, kFlatTile, 0, st>>>(t, s.pinfo, s.tile_cnt, tiles, err);
-    flat_scan<<<2 * (kMaxLevels2D + 1), 1024, 0, st>>>(s.tile_cnt, tiles, s.level_tot);
-    flat_totals<<<1, 1, 0, st>>>(t, s.level_tot, err);
+    // lvl_ticket[0]: zeroed with the other tickets before the sort
+    flat_scan<<<2 * (t.key_levels + 1), 1024, 0, st>>>(t, s.tile_cnt, tiles, s.level_tot, s.lvl_ticket, err);
     flat_emit<<<grid, kFlatTile, 0, st>>>(t, s.pinfo, s.tile_cnt, tiles, max_par, err);
     const int gc = std::max(1, std::min(148 * 8, ceil_div(t.cap_cells, 256)));
     flat_link<<<gc, 256, 0, st>>>(t, max_par, err);
-    *launches += 6;
+    *launches += 5;
     return cudaGetLastError();
 }
 
