@@ -587,29 +587,6 @@ __device__ __forceinline__ int gallop_ge(const uint32_t* __restrict__ a, int lo,
     return L;
 }
 
-// First j in (i, lim] with key prefix (>> sh) different from particle i's,
-// or lim (the group is known to end at or before lim). Galloping from i, then
-// bisection: the search costs the logarithm of the group's size, not of n.
-__device__ __forceinline__ int group_end(const uint64_t* __restrict__ key, int i, int lim, int sh) {
-    const uint64_t v = key[i] >> sh;
-    int L = i + 1, R = lim;   // answer in [L, R]
-    for (int step = 1; L + step - 1 < R; step <<= 1) {
-        const int probe = L + step - 1;
-        if ((key[probe] >> sh) == v) {
-            L = probe + 1;
-        } else {
-            R = probe;
-            break;
-        }
-    }
-    while (L < R) {
-        const int mid = (L + R) >> 1;
-        if ((key[mid] >> sh) == v) L = mid + 1;
-        else R = mid;
-    }
-    return L;
-}
-
 // First j <= i with the same key prefix (>> sh) as particle i: galloping
 // back from i, then bisection.
 __device__ __forceinline__ int group_start(const uint64_t* __restrict__ key, int i, int sh) {
@@ -646,7 +623,8 @@ __device__ __forceinline__ int group_start_warp(const uint64_t* __restrict__ key
     int lo = __shfl_sync(0xffffffffu, p0, t0) + 1;
     int hi = t0 == 0 ? i : __shfl_sync(0xffffffffu, p0, t0 - 1);
     while (lo < hi) {                                   // the answer is in [lo, hi]; hi is in the group
-        const int q = lo + (int)(((long long)(hi - lo) * lane) / 31);
+        const int step = (hi - lo + 30) / 31;
+        const int q = min(hi, lo + step * lane);
         const unsigned in = __ballot_sync(0xffffffffu, (key[q] >> sh) == v);
         const int t = __ffs(in) - 1;                    // lane 31 probes hi: t >= 0
         if (t == 0) return lo;
@@ -796,7 +774,7 @@ __device__ void flat_totals(Tree2D t, const uint32_t* __restrict__ level_tot, un
     t.c_src[0] = src;
     t.c_flags[0] = src != 0 ? CELL_ACTIVE : 0;
     t.c_parent[0] = -1;
-    t.c_child0[0] = -1;   // lowered by flat_link (unsigned minimum, so -1 = none)
+    t.c_child0[0] = -1;   // set by flat_emit (the first level-1 cell)
     t.c_chmask[0] = 0;
     t.c_level[0] = 0;
     t.c_ix[0] = 0;
@@ -859,8 +837,12 @@ flat_scan(Tree2D t, uint32_t* __restrict__ tile_cnt, int tiles, uint32_t* __rest
 }
 
 // Cell records (and leaf entries) of every particle's cell levels, indices
-// from the scanned tile counts plus the rank inside the tile.
-__global__ void __launch_bounds__(kFlatTile)
+// from the scanned tile counts plus the rank inside the tile. The parent of a
+// level-L cell starting at particle i is the last level-(L-1) cell starting
+// at or before i (cells of a level are disjoint and in particle order), so it
+// too is a count; a split cell's first child starts at the same particle, so
+// the thread that emits both links them. Range ends: flat_link.
+__global__ void __launch_bounds__(kFlatTile, 8)
 flat_emit(Tree2D t, const uint32_t* __restrict__ pinfo, const uint32_t* __restrict__ tile_cnt, int tiles,
           int max_par, unsigned* err) {
     __shared__ int s_wc[kMaxLevels2D + 1][kFlatTile / 32], s_wl[kMaxLevels2D + 1][kFlatTile / 32];
@@ -874,7 +856,8 @@ flat_emit(Tree2D t, const uint32_t* __restrict__ pinfo, const uint32_t* __restri
     const unsigned below = (1u << lane) - 1u;
     for (int k = threadIdx.x; k <= K; k += blockDim.x) s_len[k] = xdiv(root, ldexp(1.0, k));
     for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-        const int i = tile * kFlatTile + threadIdx.x;
+        const int tb = tile * kFlatTile;
+        const int i = tb + threadIdx.x;
         const uint32_t w = i < n ? pinfo[i] : 0u;
         const uint64_t ki = i < n ? t.key[i] : 0ull;
         for (int k = threadIdx.x; k <= K; k += blockDim.x) {
@@ -901,28 +884,36 @@ flat_emit(Tree2D t, const uint32_t* __restrict__ pinfo, const uint32_t* __restri
             }
         }
         __syncthreads();
+        unsigned mcp = 0u;   // lanes with a cell at level L-1 (none below Llo)
         for (int L = Llo; L <= Lhi; ++L) {
             const bool has = first && first <= L && L <= last;
             const bool lf = has && L == last && big < last;
             const unsigned mc = __ballot_sync(0xffffffffu, has), ml = __ballot_sync(0xffffffffu, lf);
+            const unsigned mprev = mcp;
+            mcp = mc;
             if (!has) continue;
-            int bc = 0, bl = 0;
+            int bc = 0, bl = 0, bp = 0;
             for (int k = 0; k < warp; ++k) {
                 bc += s_wc[L][k];
                 bl += s_wl[L][k];
+                bp += s_wc[L - 1][k];
             }
             const int ci = s_c0[L] + bc + __popc(mc & below);
             if (ci >= t.cap_cells) {
                 set_err(err, ERR_CELL_CAP);
                 continue;
             }
+            // parent: level-(L-1) cells starting at or before particle i, minus one
+            const int p = L == 1 ? 0 : s_c0[L - 1] + bp + __popc(mprev & (below | (1u << lane))) - 1;
             const int sh = 2 * (K - L);
             const uint64_t code = ki >> sh;
             const int ix = (int)compact2(code), iy = (int)compact2(code >> 1);
             const double len = s_len[L];
             t.c_lo[ci] = i;
-            t.c_flags[ci] = lf ? CELL_LEAF : 0;   // range end, counts and activity: flat_link
-            t.c_child0[ci] = -1;
+            t.c_parent[ci] = p;
+            t.c_flags[ci] = lf ? CELL_LEAF : 0;   // counts and activity: flat_link
+            t.c_child0[ci] = -1;                  // a split cell's first child: set at level L+1 below
+            if (L > first || i == 0) t.c_child0[p] = ci;   // the parent starts at this particle too
             t.c_chmask[ci] = 0;
             t.c_level[ci] = (uint8_t)L;
             t.c_ix[ci] = ix;
@@ -945,58 +936,47 @@ flat_emit(Tree2D t, const uint32_t* __restrict__ pinfo, const uint32_t* __restri
     }
 }
 
-// Range end, source count and activity of every cell (one search per cell,
-// all in parallel; a leaf holds at most max_par particles), then the parent
-// (level L-1 cell holding its prefix), the parent's child mask and first
-// child.
+// Range end, source count and activity of every cell, and the parent's child
+// mask. The children of a split cell partition its range, so a cell's range
+// ends where the next sibling of its nearest ancestor-or-self that has one
+// starts (a walk up the parent links, one level per step; most cells stop at
+// their own next sibling), or at n.
 __global__ void flat_link(Tree2D t, int max_par, unsigned* err) {
     if (fatal(err)) return;
-    const int nc = t.info->n_cells, n = t.n, K = t.key_levels;
+    const int nc = t.info->n_cells, n = t.n;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x + 1; c < nc; c += gridDim.x * blockDim.x) {
         const int L = t.c_level[c];
         const uint64_t code = t.c_code[c];
+        const uint8_t fl = t.c_flags[c];
+        const int lo = t.c_lo[c], p = t.c_parent[c];
+        int hi = n;
         {
-            const int lo = t.c_lo[c];
-            const bool leaf = t.c_flags[c] & CELL_LEAF;
-            // a split cell's children partition its range, so a cell's range
-            // ends where its next sibling's starts; only a parent's last child
-            // needs the search for the end of its key group
-            int hi;
-            if (c + 1 < nc && t.c_level[c + 1] == L && (t.c_code[c + 1] >> 2) == (code >> 2))
-                hi = t.c_lo[c + 1];
-            else
-                hi = group_end(t.key, lo, leaf ? min(n, lo + max_par) : n, 2 * (K - L));
-            const int src = (int)(t.actscan[hi] - t.actscan[lo]);
-            t.c_hi[c] = hi;
-            t.c_src[c] = src;
-            if (src != 0) t.c_flags[c] = (leaf ? CELL_LEAF : 0) | CELL_ACTIVE;
-        }
-        int p = 0;
-        if (L >= 2) {
-            const int px = t.c_ix[c] >> 1, py = t.c_iy[c] >> 1;
-            p = -1;
-            if (t.dense && L - 1 <= t.dense_levels) {
-                p = t.dense[start_id2(L - 1) + px + ((int64_t)py << (L - 1))];
-            } else {
-                int lo = t.info->level_start[L - 1], hi = t.info->level_start[L];
-                const uint64_t pc = code >> 2;
-                while (lo < hi) {
-                    const int mid = (lo + hi) >> 1;
-                    if (t.c_code[mid] < pc) lo = mid + 1;
-                    else hi = mid;
+            int a = c, ap = p, aL = L;
+            uint64_t acode = code;
+            while (aL >= 1) {
+                const int s = a + 1;
+                if (s < nc && t.c_level[s] == aL && (t.c_code[s] >> 2) == (acode >> 2)) {
+                    hi = t.c_lo[s];
+                    break;
                 }
-                p = lo;
-            }
-            if (p < 0 || p >= nc || t.c_level[p] != L - 1 || t.c_code[p] != (code >> 2)) {
-                set_err(err, ERR_INDEX);
-                continue;
+                if (ap <= 0) break;   // the parent is the root: the range runs to n
+                a = ap;
+                ap = t.c_parent[a];
+                aL -= 1;
+                acode >>= 2;
             }
         }
-        t.c_parent[c] = p;
+        if (hi <= lo || hi > n || p < 0 || p >= nc || t.c_level[p] != L - 1 || t.c_code[p] != (code >> 2)) {
+            set_err(err, ERR_INDEX);
+            continue;
+        }
+        const int src = (int)(t.actscan[hi] - t.actscan[lo]);
+        t.c_hi[c] = hi;
+        t.c_src[c] = src;
+        if (src != 0) t.c_flags[c] = fl | CELL_ACTIVE;
         unsigned* word = reinterpret_cast<unsigned*>(reinterpret_cast<uintptr_t>(&t.c_chmask[p]) & ~(uintptr_t)3);
         const unsigned shift = 8u * (unsigned)(reinterpret_cast<uintptr_t>(&t.c_chmask[p]) & 3);
         atomicOr(word, (1u << (unsigned)(code & 3)) << shift);
-        atomicMin(reinterpret_cast<unsigned*>(&t.c_child0[p]), (unsigned)c);   // -1 is the largest unsigned
     }
 }
 
