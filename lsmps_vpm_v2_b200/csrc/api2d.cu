@@ -162,7 +162,6 @@ int Ctx::reserve2d(int n, int cap_cells, int P, long long cap_l1, long long cap_
     ex2.op = (double2*)P_(o_op);
     coef_P = -1;  // the new arena holds no coefficients yet
     mixed_base = P_(o_mixed);
-    ts.sort_aos = mixed_base;   // the near-field work area is free while the tree is built
     {
         const size_t r0 = ((sizeof(double4) * (size_t)n + 1023) & ~(size_t)1023);
         tc_rows = (float*)((char*)mixed_base + r0);

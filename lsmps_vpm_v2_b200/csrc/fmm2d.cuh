@@ -146,7 +146,6 @@ struct TreeScratch2D {
     uint32_t* level_tot;    // [2][kMaxLevels2D + 1] cells / leaves per level
     int flat_tiles;         // tiles of kFlatTile particles
     uint32_t* coop_words;   // [kCoopSortWords] count tables of the cooperative sort (nullptr: multi-kernel sort)
-    void* sort_aos;         // [n] double4 staging of the cooperative sort (free again once the tree is built)
     SortScratch sort;
     ScanScratch scan;
 };

@@ -219,9 +219,8 @@ static_assert(kCwFlag + 1 <= kCoopSortWords, "count tables of the cooperative so
 // kb0/kb1: 32-bit key ping-pong buffers (pass 0's keys are computed into
 // kb0); vb0/vb1: index ping-pong buffers, vb1 may alias t.perm (the last
 // pass reads vb0). An index carries its particle's active flag in bit 31.
-// aos: n entries of (x, y, q, active) in input order, written while the
-// bounding box is read, so that the last pass fetches one 32-byte sector per
-// particle. The last pass also produces the active-count scan: a block's
+// The last pass gathers x, y and q by index (from L2: the bounding box has
+// just read them) and also produces the active-count scan: a block's
 // sorted items form one run per digit, so the count before an item is the
 // digit's global start, the runs of that digit in earlier blocks, and the
 // item's place in its own run.
@@ -237,7 +236,7 @@ static_assert(kCwFlag + 1 <= kCoopSortWords, "count tables of the cooperative so
 __global__ void __launch_bounds__(kCoopSortThreads, 1)
 sort2d_coop(const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ q,
             const uint8_t* __restrict__ act, double exp_pct, int passes, int shallow_cap, Tree2D t, double* partial,
-            double4* aos, uint32_t* kb0, uint32_t* kb1, uint32_t* vb0, uint32_t* vb1, uint32_t* words, int chunk_cap,
+            uint32_t* kb0, uint32_t* kb1, uint32_t* vb0, uint32_t* vb1, uint32_t* words, int chunk_cap,
             unsigned* err) {
     extern __shared__ __align__(16) unsigned char cs_sm[];
     __shared__ uint32_t s_wh[kCoopSortWarps][256];   // per-warp digit counts, then warp-exclusive prefixes
@@ -265,14 +264,13 @@ sort2d_coop(const double* __restrict__ x, const double* __restrict__ y, const do
     const int w0 = min(c1, c0 + warp * S), w1 = min(c1, w0 + S);
 
     // 1. bounding box (block partials, barrier, every block reduces all of
-    //    them) and the AoS copy of the particles
+    //    them)
     {
         double mnx = x[0], mxx = x[0], mny = y[0], mxy = y[0];
         bool bad = false;
         #pragma unroll 6
         for (int i = c0 + tid; i < c1; i += kCoopSortThreads) {
             const double a = x[i], c = y[i];
-            aos[i] = make_double4(a, c, q ? q[i] : 0.0, act[i] ? 1.0 : 0.0);
             bad |= !isfinite(a) || !isfinite(c);
             mnx = fmin(mnx, a); mxx = fmax(mxx, a);
             mny = fmin(mny, c); mxy = fmax(mxy, c);
@@ -511,12 +509,12 @@ sort2d_coop(const double* __restrict__ x, const double* __restrict__ y, const do
                 kout[pos] = key;
                 vout[pos] = vf;
             } else {
-                const double4 e = aos[val];
+                const double px = x[val], py = y[val], pq = q ? q[val] : 0.0;
                 t.key[pos] = key & kmask;
                 t.perm[pos] = val;
-                t.px[pos] = e.x;
-                t.py[pos] = e.y;
-                if (q) t.pq[pos] = e.z;
+                t.px[pos] = px;
+                t.py[pos] = py;
+                if (q) t.pq[pos] = pq;
                 t.pact[pos] = (uint8_t)(vf >> 31);
                 t.actscan[pos] = s_abase[d] + s_rank[j];
             }
@@ -738,34 +736,42 @@ flat_cells(Tree2D t, uint32_t* __restrict__ pinfo, uint32_t* __restrict__ tile_c
 }
 
 // Level starts, totals and the root cell (treeCell.cpp:1117-1133), from the
-// row totals of flat_scan (one thread).
+// row totals of flat_scan: one warp, lane l for level l + 1 (K <= 31).
 __device__ void flat_totals(Tree2D t, const uint32_t* __restrict__ level_tot, unsigned* err) {
-    const int K = t.key_levels;
+    const int K = t.key_levels, lane = threadIdx.x & 31, L = lane + 1;
     TreeInfo2D* info = t.info;
-    int cells = 1, leaves = 0, depth = 0;
+    const int c = L <= K ? (int)__ldcg(level_tot + L) : 0;
+    const int lf = L <= K ? (int)__ldcg(level_tot + kMaxLevels2D + 1 + L) : 0;
+    int ci = c, li = lf;   // inclusive sums over levels 1..L
+    #pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int yc = __shfl_up_sync(0xffffffffu, ci, o), yl = __shfl_up_sync(0xffffffffu, li, o);
+        if (lane >= o) {
+            ci += yc;
+            li += yl;
+        }
+    }
+    const int cells = 1 + __shfl_sync(0xffffffffu, ci, 31), leaves = __shfl_sync(0xffffffffu, li, 31);
+    // first cell / leaf of each level: the root, then the levels below it
+    info->level_start[L] = 1 + ci - c;
+    info->leaf_start[L] = li - lf;
+    const int depth = (int)__reduce_max_sync(0xffffffffu, c > 0 ? (unsigned)L : 0u);
+    // leaf level range (TreeCell::min_level / max_level, treeCell.cpp:1236-1240)
+    const unsigned mn = __reduce_min_sync(0xffffffffu, lf > 0 ? (unsigned)L : 255u);
+    const unsigned mx = __reduce_max_sync(0xffffffffu, lf > 0 ? (unsigned)L : 0u);
+    if (lane != 0) return;
     info->level_start[0] = 0;
     info->leaf_start[0] = 0;
-    int mn = -1, mx = -1;   // leaf level range (TreeCell::min_level / max_level, treeCell.cpp:1236-1240)
-    for (int L = 1; L < kMaxLevels2D + 3; ++L) {
-        info->level_start[L] = cells;
-        info->leaf_start[L] = leaves;
-        if (L <= K) {
-            const int c = (int)__ldcg(level_tot + L), lf = (int)__ldcg(level_tot + kMaxLevels2D + 1 + L);
-            if (c > 0) depth = L;
-            if (lf > 0) {
-                if (mn < 0) mn = L;
-                mx = L;
-            }
-            cells += c;
-            leaves += lf;
-        }
+    for (int k = 33; k < kMaxLevels2D + 3; ++k) {
+        info->level_start[k] = cells;
+        info->leaf_start[k] = leaves;
     }
     info->n_cells = cells;
     info->n_leaves = leaves;
     info->depth = depth;
     info->l2_irregular = 0;
-    info->min_leaf_level = mn;
-    info->max_leaf_level = mx;
+    info->min_leaf_level = mn == 255u ? -1 : (int)mn;
+    info->max_leaf_level = mx == 0u ? -1 : (int)mx;
     if (cells > t.cap_cells) set_err(err, ERR_CELL_CAP);
     const Geom2D* g = t.geom;
     t.c_lo[0] = 0;
@@ -788,24 +794,30 @@ __device__ void flat_totals(Tree2D t, const uint32_t* __restrict__ level_tot, un
 }
 
 // One block per (kind, level) row of levels 0..K: exclusive scan of the tile
-// counts in place and the row total; the last block to finish then sets the
-// level starts, totals and root cell (flat_totals). ticket: zero on entry.
+// counts in place (kScanPer consecutive counts per thread and round) and the
+// row total; the last block to finish then sets the level starts, totals and
+// root cell (flat_totals). ticket: zero on entry.
+constexpr int kScanPer = 4;
+
 __global__ void __launch_bounds__(1024)
 flat_scan(Tree2D t, uint32_t* __restrict__ tile_cnt, int tiles, uint32_t* __restrict__ level_tot, unsigned* ticket,
           unsigned* err) {
     __shared__ uint32_t s_w[32];
-    __shared__ uint32_t s_carry;
     __shared__ bool s_last;
     const int K = t.key_levels;
     const int r = blockIdx.x <= K ? (int)blockIdx.x : kMaxLevels2D + 1 + ((int)blockIdx.x - K - 1);
     uint32_t* row = tile_cnt + (size_t)r * tiles;
-    if (threadIdx.x == 0) s_carry = 0;
-    __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int b = 0; b < tiles; b += blockDim.x) {
-        const int k = b + threadIdx.x;
-        const uint32_t v = k < tiles ? row[k] : 0u;
-        uint32_t x = v;
+    uint32_t carry = 0;
+    for (int b0 = 0; b0 < tiles; b0 += 1024 * kScanPer) {
+        const int k0 = b0 + threadIdx.x * kScanPer;
+        uint32_t v[kScanPer], sum = 0;
+        #pragma unroll
+        for (int u = 0; u < kScanPer; ++u) {
+            v[u] = k0 + u < tiles ? row[k0 + u] : 0u;
+            sum += v[u];
+        }
+        uint32_t x = sum;
         #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
@@ -813,24 +825,32 @@ flat_scan(Tree2D t, uint32_t* __restrict__ tile_cnt, int tiles, uint32_t* __rest
         }
         if (lane == 31) s_w[warp] = x;
         __syncthreads();
-        uint32_t base = 0, tot = 0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-            if (w < warp) base += s_w[w];
-            tot += s_w[w];
+        if (warp == 0) {
+            uint32_t y = s_w[lane];
+            #pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t z = __shfl_up_sync(0xffffffffu, y, o);
+                if (lane >= o) y += z;
+            }
+            s_w[lane] = y;   // inclusive over warps
         }
-        const uint32_t carry = s_carry;
-        if (k < tiles) row[k] = carry + base + x - v;
         __syncthreads();
-        if (threadIdx.x == 0) s_carry = carry + tot;
+        uint32_t e = carry + (warp ? s_w[warp - 1] : 0u) + x - sum;
+        #pragma unroll
+        for (int u = 0; u < kScanPer; ++u) {
+            if (k0 + u < tiles) row[k0 + u] = e;
+            e += v[u];
+        }
+        carry += s_w[31];
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        level_tot[r] = s_carry;
+        level_tot[r] = carry;
         __threadfence();
         s_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
     }
     __syncthreads();
-    if (s_last && threadIdx.x == 0) {
+    if (s_last && warp == 0) {
         __threadfence();
         flat_totals(t, level_tot, err);
     }
@@ -1025,7 +1045,7 @@ cudaError_t keys_sort2d(const double* x, const double* y, const double* q, const
     if (e != cudaSuccess) return e;
     *launches += 1;
     int coop_grid = 0, coop_chunk = 0;
-    if (2 * K <= 32 && s.coop_words && s.sort_aos && coop_sort_shape(n, items_per_block, &coop_grid, &coop_chunk)) {
+    if (2 * K <= 32 && s.coop_words && coop_sort_shape(n, items_per_block, &coop_grid, &coop_chunk)) {
         uint32_t* k32 = reinterpret_cast<uint32_t*>(s.key_alt);
         const size_t smem = (size_t)coop_chunk * 10;
         cudaLaunchConfig_t cfg = {};
@@ -1040,7 +1060,7 @@ cudaError_t keys_sort2d(const double* x, const double* y, const double* q, const
         cfg.numAttrs = 1;
         e = cudaLaunchKernelEx(&cfg, sort2d_coop, x, y, q, act, exp_pct, (2 * K + 7) / 8, shallow_cap, t,
                                s.bbox_partial,
-                               (double4*)s.sort_aos, k32, k32 + n, s.val_alt, t.perm, s.coop_words, coop_chunk,
+                               k32, k32 + n, s.val_alt, t.perm, s.coop_words, coop_chunk,
                                err);
         if (e != cudaSuccess) return e;
         *launches += 1;
