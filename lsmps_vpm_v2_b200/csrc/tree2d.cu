@@ -860,12 +860,16 @@ flat_scan(Tree2D t, uint32_t* __restrict__ tile_cnt, int tiles, uint32_t* __rest
 // from the scanned tile counts plus the rank inside the tile. The parent of a
 // level-L cell starting at particle i is the last level-(L-1) cell starting
 // at or before i (cells of a level are disjoint and in particle order), so it
-// too is a count; a split cell's first child starts at the same particle, so
-// the thread that emits both links them. Range ends: flat_link.
+// too is a count; a split cell's first child starts at the same particle and
+// sets the parent's child0 (the only writer: leaves set their own -1). Range
+// ends: flat_link. A warp's (particle, level) cells are spread over its lanes,
+// one per lane and round, so a particle starting many levels does not hold
+// the block at its barrier.
 __global__ void __launch_bounds__(kFlatTile, 8)
 flat_emit(Tree2D t, const uint32_t* __restrict__ pinfo, const uint32_t* __restrict__ tile_cnt, int tiles,
           int max_par, unsigned* err) {
-    __shared__ int s_wc[kMaxLevels2D + 1][kFlatTile / 32], s_wl[kMaxLevels2D + 1][kFlatTile / 32];
+    constexpr int NW = kFlatTile / 32;
+    __shared__ unsigned s_mc[kMaxLevels2D + 1][NW], s_ml[kMaxLevels2D + 1][NW];   // lanes with a cell / leaf at L
     __shared__ int s_c0[kMaxLevels2D + 1], s_l0[kMaxLevels2D + 1];   // the tile's first cell / leaf of each level
     __shared__ double s_len[kMaxLevels2D + 1];                        // cell size of each level
     if (block_fatal(err)) return;
@@ -873,7 +877,6 @@ flat_emit(Tree2D t, const uint32_t* __restrict__ pinfo, const uint32_t* __restri
     const TreeInfo2D* info = t.info;
     const double root = t.geom->root, pivx = t.geom->pivx, pivy = t.geom->pivy;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const unsigned below = (1u << lane) - 1u;
     for (int k = threadIdx.x; k <= K; k += blockDim.x) s_len[k] = xdiv(root, ldexp(1.0, k));
     for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         const int tb = tile * kFlatTile;
@@ -885,13 +888,13 @@ flat_emit(Tree2D t, const uint32_t* __restrict__ pinfo, const uint32_t* __restri
             s_l0[k] = info->leaf_start[k] + (int)tile_cnt[(size_t)(kMaxLevels2D + 1 + k) * tiles + tile];
         }
         const int first = (int)((w >> 16) & 0xff), last = (int)(w >> 24), big = (int)((w >> 8) & 0xff) - 1;
-        // the levels at which this warp's particles start cells (most warps: one or two)
+        const int ncell = first ? last - first + 1 : 0;
+        // lane masks of every level (zero outside the warp's range), then one barrier
         const int Llo = (int)__reduce_min_sync(0xffffffffu, first ? (unsigned)first : 255u);
         const int Lhi = (int)__reduce_max_sync(0xffffffffu, first ? (unsigned)last : 0u);
-        // per-warp counts of every level (zero outside the warp's range), then one barrier
         if (lane <= K) {
-            s_wc[lane][warp] = 0;
-            s_wl[lane][warp] = 0;
+            s_mc[lane][warp] = 0u;
+            s_ml[lane][warp] = 0u;
         }
         __syncwarp();
         for (int L = Llo; L <= Lhi; ++L) {
@@ -899,41 +902,58 @@ flat_emit(Tree2D t, const uint32_t* __restrict__ pinfo, const uint32_t* __restri
             const bool lf = has && L == last && big < last;
             const unsigned mc = __ballot_sync(0xffffffffu, has), ml = __ballot_sync(0xffffffffu, lf);
             if (lane == 0) {
-                s_wc[L][warp] = __popc(mc);
-                s_wl[L][warp] = __popc(ml);
+                s_mc[L][warp] = mc;
+                s_ml[L][warp] = ml;
             }
         }
         __syncthreads();
-        unsigned mcp = 0u;   // lanes with a cell at level L-1 (none below Llo)
-        for (int L = Llo; L <= Lhi; ++L) {
-            const bool has = first && first <= L && L <= last;
-            const bool lf = has && L == last && big < last;
-            const unsigned mc = __ballot_sync(0xffffffffu, has), ml = __ballot_sync(0xffffffffu, lf);
-            const unsigned mprev = mcp;
-            mcp = mc;
-            if (!has) continue;
+        // the warp's cells in (lane, level) order, 32 per round
+        int incl = ncell;
+        #pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        for (int r0 = 0; r0 < total; r0 += 32) {
+            const int q = r0 + lane;
+            // owner lane of cell q: the number of lanes whose inclusive count is <= q
+            int ol = 0;
+            #pragma unroll
+            for (int step = 16; step >= 1; step >>= 1)
+                if (__shfl_sync(0xffffffffu, incl, ol + step - 1) <= q) ol += step;
+            ol = min(ol, 31);
+            const int ofirst = __shfl_sync(0xffffffffu, first, ol), olast = __shfl_sync(0xffffffffu, last, ol);
+            const int obig = __shfl_sync(0xffffffffu, big, ol);
+            const int oexcl = __shfl_sync(0xffffffffu, incl - ncell, ol);
+            const uint64_t okey = __shfl_sync(0xffffffffu, ki, ol);
+            if (q >= total) continue;
+            const int L = ofirst + (q - oexcl);
+            const bool lf = L == olast && obig < olast;
+            const unsigned lt = (1u << ol) - 1u;
             int bc = 0, bl = 0, bp = 0;
             for (int k = 0; k < warp; ++k) {
-                bc += s_wc[L][k];
-                bl += s_wl[L][k];
-                bp += s_wc[L - 1][k];
+                bc += __popc(s_mc[L][k]);
+                bl += __popc(s_ml[L][k]);
+                bp += __popc(s_mc[L - 1][k]);
             }
-            const int ci = s_c0[L] + bc + __popc(mc & below);
+            const int ci = s_c0[L] + bc + __popc(s_mc[L][warp] & lt);
             if (ci >= t.cap_cells) {
                 set_err(err, ERR_CELL_CAP);
                 continue;
             }
-            // parent: level-(L-1) cells starting at or before particle i, minus one
-            const int p = L == 1 ? 0 : s_c0[L - 1] + bp + __popc(mprev & (below | (1u << lane))) - 1;
+            const int io = tb + warp * 32 + ol;   // the particle starting the cell
+            // parent: level-(L-1) cells starting at or before particle io, minus one
+            const int p = L == 1 ? 0 : s_c0[L - 1] + bp + __popc(s_mc[L - 1][warp] & (lt | (1u << ol))) - 1;
             const int sh = 2 * (K - L);
-            const uint64_t code = ki >> sh;
+            const uint64_t code = okey >> sh;
             const int ix = (int)compact2(code), iy = (int)compact2(code >> 1);
             const double len = s_len[L];
-            t.c_lo[ci] = i;
+            t.c_lo[ci] = io;
             t.c_parent[ci] = p;
             t.c_flags[ci] = lf ? CELL_LEAF : 0;   // counts and activity: flat_link
-            t.c_child0[ci] = -1;                  // a split cell's first child: set at level L+1 below
-            if (L > first || i == 0) t.c_child0[p] = ci;   // the parent starts at this particle too
+            if (L == olast) t.c_child0[ci] = -1;  // no child (split cells: set by their first child)
+            if (L > ofirst || io == 0) t.c_child0[p] = ci;   // the parent starts at this particle too
             t.c_chmask[ci] = 0;
             t.c_level[ci] = (uint8_t)L;
             t.c_ix[ci] = ix;
@@ -943,7 +963,7 @@ flat_emit(Tree2D t, const uint32_t* __restrict__ pinfo, const uint32_t* __restri
             t.c_cy[ci] = xadd(pivy, xmul(xadd(0.5, (double)iy), len));
             if (t.dense && L <= t.dense_levels) t.dense[start_id2(L) + ix + ((int64_t)iy << L)] = ci;
             // leaves before this cell: of the lower levels, then of this level
-            const int li = s_l0[L] + bl + __popc(ml & below);
+            const int li = s_l0[L] + bl + __popc(s_ml[L][warp] & lt);
             if (lf) {
                 t.c_leafidx[ci] = li;
                 t.leaf_cells[li] = ci;
