@@ -247,9 +247,9 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
         }
         const bool slots = p.precision != VPM_PREC_FP64 && int_lists_slotted(lists);
         if (slots) {
-            // the mixed near field starts from the list slots; the CSR (for
-            // list 3 and the few leaves that outgrew their slots) is built on a
-            // third side stream meanwhile
+            // the mixed near field and M2P start from the list slots; the CSR
+            // (for the few leaves whose lists outgrew their slots) is built on
+            // a third side stream meanwhile
             VPM_CUDA_TRY(build_int_slots2d(tree, lists, p.eps, d_err, side, &launches));
             VPM_CUDA_TRY(cudaEventRecord(ev_slots, side));
             if (deferred) VPM_CUDA_TRY(cudaStreamWaitEvent(side, ev_qg, 0));
@@ -261,7 +261,6 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
             if (deferred) VPM_CUDA_TRY(cudaStreamWaitEvent(side3, ev_qg, 0));
             VPM_CUDA_TRY(fmm2d_p2p_f32(tree, lists, ex2, near_x, near_y, 0, 0.0, 0.0, d_err, side3, &launches, true,
                                        kP2PListSpill));
-            VPM_CUDA_TRY(cudaEventRecord(join5, side3));
         } else {
             VPM_CUDA_TRY(build_int_lists2d(tree, lists, ts.scan, p.eps, d_err, side, &launches));
             VPM_CUDA_TRY(cudaEventRecord(ev_l13, side));
@@ -278,9 +277,16 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
         VPM_CUDA_TRY(cudaEventRecord(join3, side2));
         VPM_CUDA_TRY(fmm2d_upward_direct(tree, ex2, p.p, p.binom == VPM_BINOM_EXACT, d_err, st, &launches));
         VPM_CUDA_TRY(cudaEventRecord(ev_up, st));
+        if (slots) {
+            // M2P of the leaves whose list 3 outgrew its slots, after their
+            // CSR (the others: from the slots on the third stream below)
+            VPM_CUDA_TRY(cudaStreamWaitEvent(side3, ev_up, 0));
+            VPM_CUDA_TRY(fmm2d_m2p(tree, lists, ex2, p.p, d_err, side3, &launches, kP2PListSpill));
+            VPM_CUDA_TRY(cudaEventRecord(join5, side3));
+        }
         VPM_CUDA_TRY(cudaStreamWaitEvent(side2, ev_up, 0));
-        VPM_CUDA_TRY(cudaStreamWaitEvent(side2, ev_l13, 0));
-        VPM_CUDA_TRY(fmm2d_m2p(tree, lists, ex2, p.p, d_err, side2, &launches));
+        VPM_CUDA_TRY(cudaStreamWaitEvent(side2, slots ? ev_slots : ev_l13, 0));
+        VPM_CUDA_TRY(fmm2d_m2p(tree, lists, ex2, p.p, d_err, side2, &launches, slots ? kP2PListSlots : kP2PListCsr));
         VPM_CUDA_TRY(cudaEventRecord(join4, side2));
         VPM_CUDA_TRY(cudaStreamWaitEvent(st, join3, 0));
         if (int r = enqueue_m2l(p, st, &launches)) return r;

@@ -222,9 +222,11 @@ cudaError_t fmm2d_p2p_f64_tma(const Tree2D& t, const Lists2D& l, const Expansion
 cudaError_t fmm2d_eval_combine(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, const double* nx,
                                const double* ny, double* out0, double* out1, int velocity, double u_inf, double v_inf,
                                unsigned* err, cudaStream_t st, int* launches, bool m2p_done = false);
-// M2P over list 3 of every leaf's particles into e.fx/e.fy (tree order).
+// M2P over list 3 of every leaf's particles into e.fx/e.fy (tree order);
+// lists: where list 3 comes from, as for fmm2d_p2p_f32 (the slots pass skips
+// the leaves whose list outgrew them, the spill pass takes exactly those).
 cudaError_t fmm2d_m2p(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, unsigned* err, cudaStream_t st,
-                      int* launches);
+                      int* launches, int lists = kP2PListCsr);
 cudaError_t fmm2d_p2p_out(const Tree2D& t, const Lists2D& l, const Expansions2D& e, double* out0, double* out1,
                           int velocity, double u_inf, double v_inf, unsigned* err, cudaStream_t st, int* launches);
 

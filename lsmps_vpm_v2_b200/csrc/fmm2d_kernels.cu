@@ -442,7 +442,7 @@ constexpr int kEvalFull = 0, kEvalM2P = 1, kEvalL2P = 2;
 template <bool TWO, int MODE>
 __device__ __forceinline__ void eval_targets(const Tree2D& t, const Lists2D& l, const double2* __restrict__ a,
                                              const double2* s_b, int P, int i0, int i1, bool h0, bool h1, double zx,
-                                             double zy, uint32_t o3, uint32_t e3, double* fx, double* fy,
+                                             double zy, const int32_t* src3, uint32_t n3, double* fx, double* fy,
                                              const double* nx, const double* ny, double* out0, double* out1,
                                              int velocity, double u_inf, double v_inf, unsigned* err) {
     double x[2], y[2], ex[2] = {0.0, 0.0}, ey[2] = {0.0, 0.0};
@@ -460,10 +460,10 @@ __device__ __forceinline__ void eval_targets(const Tree2D& t, const Lists2D& l, 
                 ex[u] = fx[ii[u]];
                 ey[u] = fy[ii[u]];
             }
-        o3 = e3;
+        n3 = 0;
     }
-    for (uint32_t k = o3; k < e3; ++k) {
-        const int s = l.l3_src[k];
+    for (uint32_t k = 0; k < n3; ++k) {
+        const int s = src3[k];
         const double sx = t.c_cx[s], sy = t.c_cy[s];
         const double2* A = a + (size_t)s * (P + 1);
         double2 w[2], S[2];
@@ -532,7 +532,7 @@ template <int MODE>
 __global__ void __launch_bounds__(kEvalThreads)
 eval2d(Tree2D t, Lists2D l, const double2* __restrict__ a, const double2* __restrict__ b, double* __restrict__ fx,
        double* __restrict__ fy, int P, const double* __restrict__ nx, const double* __restrict__ ny,
-       double* __restrict__ out0, double* __restrict__ out1, int velocity, double u_inf, double v_inf,
+       double* __restrict__ out0, double* __restrict__ out1, int velocity, double u_inf, double v_inf, int lists,
        unsigned* err) {
     __shared__ double2 s_bw[kEvalWarps][W];
     if (fatal(err)) return;
@@ -548,14 +548,36 @@ eval2d(Tree2D t, Lists2D l, const double2* __restrict__ a, const double2* __rest
         __syncwarp();
         const int lo = t.c_lo[c], hi = t.c_hi[c];
         const double zx = t.c_cx[c], zy = t.c_cy[c];
-        const uint32_t o3 = l.l3_off[li], e3 = l.l3_off[li + 1];
+        // list 3 of the leaf: the CSR, or (M2P) the fixed slots of
+        // int_list_slots, the leaves whose list outgrew them coming in a
+        // second pass from the CSR
+        const int32_t* src3 = nullptr;
+        uint32_t n3 = 0;
+        if (MODE != kEvalL2P) {
+            bool csr = lists == kP2PListCsr;
+            if (!csr) {
+                const uint32_t cnt = l.l3_cnt[li];
+                const bool spill = cnt > (uint32_t)kListSlot3;
+                if (spill != (lists == kP2PListSpill)) continue;   // the other pass takes this leaf
+                csr = spill;
+                if (!spill) {
+                    src3 = l.l3_slot + (size_t)li * kListSlot3;
+                    n3 = cnt;
+                }
+            }
+            if (csr) {
+                const uint32_t o3 = l.l3_off[li];
+                src3 = l.l3_src + o3;
+                n3 = l.l3_off[li + 1] - o3;
+            }
+        }
         for (int i0 = lo; i0 < hi; i0 += 64) {
             const int ia = i0 + lane, ib = i0 + 32 + lane;
             if (i0 + 32 < hi)   // warp-uniform
-                eval_targets<true, MODE>(t, l, a, s_b, P, ia, ib, ia < hi, ib < hi, zx, zy, o3, e3, fx, fy, nx, ny,
+                eval_targets<true, MODE>(t, l, a, s_b, P, ia, ib, ia < hi, ib < hi, zx, zy, src3, n3, fx, fy, nx, ny,
                                          out0, out1, velocity, u_inf, v_inf, err);
             else
-                eval_targets<false, MODE>(t, l, a, s_b, P, ia, ib, ia < hi, false, zx, zy, o3, e3, fx, fy, nx, ny,
+                eval_targets<false, MODE>(t, l, a, s_b, P, ia, ib, ia < hi, false, zx, zy, src3, n3, fx, fy, nx, ny,
                                           out0, out1, velocity, u_inf, v_inf, err);
         }
         __syncwarp();
@@ -1734,15 +1756,15 @@ cudaError_t fmm2d_m2l(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P,
 cudaError_t fmm2d_eval(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, unsigned* err, cudaStream_t st,
                        int* launches) {
     eval2d<kEvalFull><<<148 * 16, kEvalThreads, 0, st>>>(t, l, e.a, e.b, e.fx, e.fy, P, nullptr, nullptr, nullptr,
-                                                         nullptr, 0, 0.0, 0.0, err);
+                                                         nullptr, 0, 0.0, 0.0, kP2PListCsr, err);
     *launches += 1;
     return cudaGetLastError();
 }
 
 cudaError_t fmm2d_m2p(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, unsigned* err, cudaStream_t st,
-                      int* launches) {
+                      int* launches, int lists) {
     eval2d<kEvalM2P><<<148 * 16, kEvalThreads, 0, st>>>(t, l, e.a, e.b, e.fx, e.fy, P, nullptr, nullptr, nullptr,
-                                                        nullptr, 0, 0.0, 0.0, err);
+                                                        nullptr, 0, 0.0, 0.0, lists, err);
     *launches += 1;
     return cudaGetLastError();
 }
@@ -1752,10 +1774,10 @@ cudaError_t fmm2d_eval_combine(const Tree2D& t, const Lists2D& l, Expansions2D& 
                                unsigned* err, cudaStream_t st, int* launches, bool m2p_done) {
     if (m2p_done)
         eval2d<kEvalL2P><<<148 * 16, kEvalThreads, 0, st>>>(t, l, e.a, e.b, e.fx, e.fy, P, nx, ny, out0, out1, velocity,
-                                                            u_inf, v_inf, err);
+                                                            u_inf, v_inf, kP2PListCsr, err);
     else
         eval2d<kEvalFull><<<148 * 16, kEvalThreads, 0, st>>>(t, l, e.a, e.b, e.fx, e.fy, P, nx, ny, out0, out1,
-                                                             velocity, u_inf, v_inf, err);
+                                                             velocity, u_inf, v_inf, kP2PListCsr, err);
     *launches += 1;
     return cudaGetLastError();
 }
