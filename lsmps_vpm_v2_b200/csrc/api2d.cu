@@ -275,8 +275,20 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
         VPM_CUDA_TRY(cudaStreamWaitEvent(side2, fork2, 0));
         VPM_CUDA_TRY(build_ext_lists2d(tree, lists, p.eps, d_err, side2, &launches));
         VPM_CUDA_TRY(cudaEventRecord(join3, side2));
-        VPM_CUDA_TRY(fmm2d_upward_direct(tree, ex2, p.p, p.binom == VPM_BINOM_EXACT, d_err, st, &launches));
+        // mixed form: the per-parent M2L of the levels below the cells left
+        // to the M2M loop runs on the lists-2/4 stream as soon as the other
+        // moments are final, beside that loop; the rest follows it
+        const bool split_m2l = p.precision == VPM_PREC_MIXED && m2l_parent_f32_supported(p.p) && lists.l2_blk &&
+                               tree.nonleaf && tree.gbar;
+        VPM_CUDA_TRY(fmm2d_upward_direct(tree, ex2, p.p, p.binom == VPM_BINOM_EXACT, d_err, st, &launches,
+                                         split_m2l ? ev_small : nullptr));
         VPM_CUDA_TRY(cudaEventRecord(ev_up, st));
+        if (split_m2l) {
+            VPM_CUDA_TRY(cudaStreamWaitEvent(side2, ev_small, 0));
+            VPM_CUDA_TRY(fmm2d_m2l_parent_f32(tree, lists, ex2, p.p, p.binom == VPM_BINOM_EXACT, d_err, side2,
+                                              &launches, 1));
+            VPM_CUDA_TRY(cudaEventRecord(ev_m2ld, side2));
+        }
         if (slots) {
             // M2P of the leaves whose list 3 outgrew its slots, after their
             // CSR (the others: from the slots on the third stream below)
@@ -289,7 +301,14 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
         VPM_CUDA_TRY(fmm2d_m2p(tree, lists, ex2, p.p, d_err, side2, &launches, slots ? kP2PListSlots : kP2PListCsr));
         VPM_CUDA_TRY(cudaEventRecord(join4, side2));
         VPM_CUDA_TRY(cudaStreamWaitEvent(st, join3, 0));
-        if (int r = enqueue_m2l(p, st, &launches)) return r;
+        if (split_m2l) {
+            VPM_CUDA_TRY(fmm2d_m2l_parent_f32(tree, lists, ex2, p.p, p.binom == VPM_BINOM_EXACT, d_err, st,
+                                              &launches, 2));
+            VPM_CUDA_TRY(cudaStreamWaitEvent(st, ev_m2ld, 0));
+            VPM_CUDA_TRY(fmm2d_m2l_list4(tree, lists, ex2, p.p, d_err, st, &launches));
+        } else if (int r = enqueue_m2l(p, st, &launches)) {
+            return r;
+        }
         if (l2l_direct_ok(p.p, p.binom == VPM_BINOM_EXACT))
             VPM_CUDA_TRY(fmm2d_l2l_leaves(tree, ex2, p.p, d_err, st, &launches));
         else

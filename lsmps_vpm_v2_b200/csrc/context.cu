@@ -52,7 +52,7 @@ Ctx::~Ctx() {
     if (join3) cudaEventDestroy(join3);
     if (fork2) cudaEventDestroy(fork2);
     if (join2) cudaEventDestroy(join2);
-    for (cudaEvent_t x : {ev_up, ev_l13, join4, ev_slots, join5, ev_upload, ev_q, ev_qg})
+    for (cudaEvent_t x : {ev_up, ev_l13, join4, ev_slots, join5, ev_upload, ev_q, ev_qg, ev_small, ev_m2ld})
         if (x) cudaEventDestroy(x);
 }
 
@@ -81,6 +81,8 @@ int Ctx::init(int dev) {
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_upload, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_q, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_qg, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_small, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_m2ld, cudaEventDisableTiming);
     if (e != cudaSuccess) return fail_cuda(e, "cudaEventCreate");
     e = cudaMalloc(&d_err, 64);
     if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc");

@@ -56,6 +56,8 @@ struct Ctx {
     cudaEvent_t ev_up = nullptr, ev_l13 = nullptr, join4 = nullptr;   // upward done, lists 1/3 done, M2P done
     cudaStream_t side3 = nullptr;   // CSR of lists 1/3 while the near field runs from the slots
     cudaEvent_t ev_slots = nullptr, join5 = nullptr;   // list slots done, near field of spilled leaves done
+    // moments of all but the M2M loop's cells done; M2L of the parents below them done
+    cudaEvent_t ev_small = nullptr, ev_m2ld = nullptr;
     // Host entry points: the strengths (or vorticity and core size) are
     // copied on `upload` while the main stream sorts the particles and builds
     // the tree and lists; `q_ready` (recorded on `upload`) is set while an

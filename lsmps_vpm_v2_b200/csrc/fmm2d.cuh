@@ -222,8 +222,10 @@ cudaError_t fmm2d_upward(const Tree2D& t, Expansions2D& e, int P, unsigned* err,
 // the deepest level holding one) when upward_direct_ok; else fmm2d_upward.
 // Uses grid-barrier words 2 and 3 of t.gbar (zeroed before every evaluation).
 bool upward_direct_ok(int P, bool exact);
+// mid (may be null): recorded on st once every cell's moments except those of
+// the cells left to the M2M loop are final (at the end when there is no loop).
 cudaError_t fmm2d_upward_direct(const Tree2D& t, Expansions2D& e, int P, bool exact, unsigned* err, cudaStream_t st,
-                                int* launches);
+                                int* launches, cudaEvent_t mid = nullptr);
 cudaError_t fmm2d_m2l(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, unsigned* err, cudaStream_t st,
                       int* launches);  // M2L followed by the L2L levels
 // Potential (fmm2D::calcPotential): b_0 of the M2L after fmm2d_m2l_only, then
@@ -243,9 +245,16 @@ bool m2l_parent_supported(int P);
 // The same per-parent list-2 M2L on the FP32 pipes through the operator's
 // diagonal-real-diagonal structure (m2l_parent_f32), orders 1..16; list 4 in
 // FP64.
+// part 0: every parent, then list 4 (fmm2d_m2l_list4); part 1: the parents
+// at levels >= the deepest level holding a cell moved by the M2M loop (their
+// children's sources are final once upward_direct2d is done); part 2: the
+// other parents. Parts 1 and 2 leave list 4 to the caller, after both.
 bool m2l_parent_f32_supported(int P);
 cudaError_t fmm2d_m2l_parent_f32(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, bool exact,
-                                 unsigned* err, cudaStream_t st, int* launches);
+                                 unsigned* err, cudaStream_t st, int* launches, int part = 0);
+// List 4 (and list 2 of an irregular tree) added to b in FP64.
+cudaError_t fmm2d_m2l_list4(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, unsigned* err, cudaStream_t st,
+                            int* launches);
 cudaError_t set_m2l_parent_operators(int P, const double2* op_dev, float* dst, cudaStream_t st);
 cudaError_t fmm2d_m2l_parent(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, float* rows,
                              const float* ops, unsigned* err, cudaStream_t st, int* launches);

@@ -8,7 +8,8 @@
 //   fmm2d_upward_direct  moments of every cell of at most 1024 particles
 //                 straight from its particles (upward_direct2d), then M2M of
 //                 the larger cells level by level in one cooperative launch
-//                 (m2m_big_levels_coop); fmm2D.cpp:237-284, 309-379.
+//                 (m2m_big_levels_coop), with an optional event between the
+//                 two; fmm2D.cpp:237-284, 309-379.
 //   fmm2d_upward  P2M of every active leaf, then M2M over all levels (p2m2d,
 //                 m2m_levels_coop), for orders the direct form does not cover.
 //   fmm2d_m2l_only  lists 2 and 4 of every cell at level >= 2 in FP64 with the
@@ -1518,11 +1519,15 @@ bool upward_direct_ok(int P, bool exact) { return P >= 1 && P <= kUpMaxP && (exa
 static_assert(kUpMaxP <= 18, "the reference's 32-bit M2M binomials wrap from order 19");
 
 template <int P>
-cudaError_t launch_upward_direct(const Tree2D& t, Expansions2D& e, unsigned* err, cudaStream_t st) {
+cudaError_t launch_upward_direct(const Tree2D& t, Expansions2D& e, unsigned* err, cudaStream_t st, cudaEvent_t mid) {
     const size_t smem = sizeof(double) * kUpWarps * 32 * (2 * (P + 1) + 1);
     cudaError_t r = cudaFuncSetAttribute(upward_direct2d<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (r != cudaSuccess) return r;
     upward_direct2d<P><<<148 * 4, 32 * kUpWarps, smem, st>>>(t, e.a, t.gbar + 3, err);
+    if (mid) {
+        r = cudaEventRecord(mid, st);
+        if (r != cudaSuccess) return r;
+    }
     // A small grid: the large cells are a few hundred per level, and the
     // blocks of this loop wait at its barriers most of the time while the
     // near field runs beside it on the other streams, so every block it does
@@ -1537,21 +1542,27 @@ cudaError_t launch_upward_direct(const Tree2D& t, Expansions2D& e, unsigned* err
 // Upward pass of orders the direct form covers (upward_direct_ok): one launch.
 // Otherwise the P2M + M2M level loop below.
 cudaError_t fmm2d_upward_direct(const Tree2D& t, Expansions2D& e, int P, bool exact, unsigned* err, cudaStream_t st,
-                                int* launches) {
-    if (!upward_direct_ok(P, exact) || !t.gbar) return fmm2d_upward(t, e, P, err, st, launches);
+                                int* launches, cudaEvent_t mid) {
+    // the level loop over all cells: every moment is final only at its end
+    auto full = [&]() -> cudaError_t {
+        cudaError_t r = fmm2d_upward(t, e, P, err, st, launches);
+        if (r == cudaSuccess && mid) r = cudaEventRecord(mid, st);
+        return r;
+    };
+    if (!upward_direct_ok(P, exact) || !t.gbar) return full();
     cudaError_t r;
     switch (P) {
 #define VPM_UP_CASE(PP) \
-    case PP: r = launch_upward_direct<PP>(t, e, err, st); break;
+    case PP: r = launch_upward_direct<PP>(t, e, err, st, mid); break;
         VPM_UP_CASE(1) VPM_UP_CASE(2) VPM_UP_CASE(3) VPM_UP_CASE(4) VPM_UP_CASE(5) VPM_UP_CASE(6)
         VPM_UP_CASE(7) VPM_UP_CASE(8) VPM_UP_CASE(9) VPM_UP_CASE(10) VPM_UP_CASE(11) VPM_UP_CASE(12)
         VPM_UP_CASE(13) VPM_UP_CASE(14) VPM_UP_CASE(15) VPM_UP_CASE(16) VPM_UP_CASE(17) VPM_UP_CASE(18)
 #undef VPM_UP_CASE
-        default: return fmm2d_upward(t, e, P, err, st, launches);
+        default: return full();
     }
     if (r != cudaSuccess) {   // cooperative launch refused: the level loop over all cells instead
         (void)cudaGetLastError();
-        return fmm2d_upward(t, e, P, err, st, launches);
+        return full();
     }
     *launches += 2;
     return r;

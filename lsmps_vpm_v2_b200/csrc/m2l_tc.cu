@@ -611,7 +611,8 @@ struct ParF32Args {
 template <int P>
 __global__ void __launch_bounds__(256)
 m2l_parent_f32(Tree2D t, const int32_t* __restrict__ blk, const double2* __restrict__ a, double2* __restrict__ b,
-               const __grid_constant__ ParF32Args<P> args, unsigned* err) {
+               const __grid_constant__ ParF32Args<P> args, int part, const unsigned* __restrict__ top_level,
+               unsigned* err) {
     constexpr int Q = P + 1;
     extern __shared__ float2 pf_A[];             // [32 positions][Q][32 parents]
     __shared__ int s_src[kParPos][32];           // [position][parent]
@@ -622,12 +623,21 @@ m2l_parent_f32(Tree2D t, const int32_t* __restrict__ blk, const double2* __restr
     const int q = wq & 3, half = wq >> 2;
     const int qx = q & 1, qy = q >> 1;
     const int np = t.info->n_cells - t.info->n_leaves;   // non-leaf cells; the root is the first
-    const int nparents = np > 1 ? np - 1 : 0;
+    // parents [pb, pe) of the non-leaf list (level-major): all, or those at
+    // levels >= *top_level (part 1: their children's sources are final once
+    // the small cells' moments are), or the others (part 2)
+    int pb = 1, pe = np;
+    if (part != 0) {
+        const int top = (int)*top_level;
+        const int split = max(1, t.info->level_start[top] - t.info->leaf_start[top]);
+        if (part == 1) pb = max(pb, split);
+        else pe = min(pe, split);
+    }
     const bool irregular = t.info->l2_irregular != 0;
     const double root = t.geom->root;
-    for (int tile = blockIdx.x; tile * 32 < nparents; tile += gridDim.x) {
-        const int pi = 1 + tile * 32 + lane;
-        const int par = pi < np ? t.nonleaf[pi] : -1;
+    for (int tile = blockIdx.x; pb + tile * 32 < pe; tile += gridDim.x) {
+        const int pi = pb + tile * 32 + lane;
+        const int par = pi < pe ? t.nonleaf[pi] : -1;
         if (wq == 0) {
             const double rinv = par >= 0 ? ldexp(1.0, (int)t.c_level[par] + 1) / root : 0.0;
             double r = 1.0;
@@ -728,7 +738,7 @@ m2l_parent_f32(Tree2D t, const int32_t* __restrict__ blk, const double2* __restr
 
 template <int P>
 cudaError_t launch_m2l_parent_f32(const Tree2D& t, const Lists2D& l, Expansions2D& e, bool exact, unsigned* err,
-                                  cudaStream_t st) {
+                                  cudaStream_t st, int part) {
     ParF32Args<P> args;
     for (int p = 1; p <= P; ++p) {
         args.C[p - 1][0] = (float)(-1.0 / (double)p);
@@ -751,7 +761,8 @@ cudaError_t launch_m2l_parent_f32(const Tree2D& t, const Lists2D& l, Expansions2
     int occ = 0;
     r = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, m2l_parent_f32<P>, 256, smem);
     if (r != cudaSuccess) return r;
-    m2l_parent_f32<P><<<148 * (occ > 0 ? occ : 1), 256, smem, st>>>(t, l.l2_blk, e.a, e.b, args, err);
+    m2l_parent_f32<P><<<148 * (occ > 0 ? occ : 1), 256, smem, st>>>(t, l.l2_blk, e.a, e.b, args, part,
+                                                                     t.gbar ? t.gbar + 3 : nullptr, err);
     return cudaGetLastError();
 }
 
@@ -882,12 +893,13 @@ cudaError_t set_m2l_parent_operators(int P, const double2* op_dev, float* dst, c
 bool m2l_parent_f32_supported(int P) { return P >= 1 && P <= kPF32MaxP; }
 
 cudaError_t fmm2d_m2l_parent_f32(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, bool exact,
-                                 unsigned* err, cudaStream_t st, int* launches) {
-    if (!m2l_parent_f32_supported(P) || !l.l2_blk || !t.nonleaf) return cudaErrorInvalidValue;
+                                 unsigned* err, cudaStream_t st, int* launches, int part) {
+    if (!m2l_parent_f32_supported(P) || !l.l2_blk || !t.nonleaf || (part != 0 && !t.gbar))
+        return cudaErrorInvalidValue;
     cudaError_t r;
     switch (P) {
 #define VPM_PF32_CASE(PP) \
-    case PP: r = launch_m2l_parent_f32<PP>(t, l, e, exact, err, st); break;
+    case PP: r = launch_m2l_parent_f32<PP>(t, l, e, exact, err, st, part); break;
         VPM_PF32_CASE(1) VPM_PF32_CASE(2) VPM_PF32_CASE(3) VPM_PF32_CASE(4) VPM_PF32_CASE(5) VPM_PF32_CASE(6)
         VPM_PF32_CASE(7) VPM_PF32_CASE(8) VPM_PF32_CASE(9) VPM_PF32_CASE(10) VPM_PF32_CASE(11) VPM_PF32_CASE(12)
         VPM_PF32_CASE(13) VPM_PF32_CASE(14) VPM_PF32_CASE(15) VPM_PF32_CASE(16)
@@ -895,8 +907,15 @@ cudaError_t fmm2d_m2l_parent_f32(const Tree2D& t, const Lists2D& l, Expansions2D
         default: return cudaErrorInvalidValue;
     }
     if (r != cudaSuccess) return r;
+    *launches += 1;
+    if (part != 0) return cudaGetLastError();
+    return fmm2d_m2l_list4(t, l, e, P, err, st, launches);
+}
+
+cudaError_t fmm2d_m2l_list4(const Tree2D& t, const Lists2D& l, Expansions2D& e, int P, unsigned* err, cudaStream_t st,
+                            int* launches) {
     m2l_list4_add<<<148 * 8, 128, 0, st>>>(t, l, e.a, e.b, e.coef, P, true, err);
-    *launches += 2;
+    *launches += 1;
     return cudaGetLastError();
 }
 
