@@ -278,12 +278,12 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
         // mixed form: the per-parent M2L of the levels below the cells left
         // to the M2M loop runs on the lists-2/4 stream as soon as the other
         // moments are final, beside that loop; the rest follows it
-        const bool split_m2l = p.precision == VPM_PREC_MIXED && m2l_parent_f32_supported(p.p) && lists.l2_blk &&
-                               tree.nonleaf && tree.gbar;
+        const bool split = split_m2l && p.precision == VPM_PREC_MIXED && m2l_parent_f32_supported(p.p) &&
+                           lists.l2_blk && tree.nonleaf && tree.gbar;
         VPM_CUDA_TRY(fmm2d_upward_direct(tree, ex2, p.p, p.binom == VPM_BINOM_EXACT, d_err, st, &launches,
-                                         split_m2l ? ev_small : nullptr));
+                                         split ? ev_small : nullptr));
         VPM_CUDA_TRY(cudaEventRecord(ev_up, st));
-        if (split_m2l) {
+        if (split) {
             VPM_CUDA_TRY(cudaStreamWaitEvent(side2, ev_small, 0));
             VPM_CUDA_TRY(fmm2d_m2l_parent_f32(tree, lists, ex2, p.p, p.binom == VPM_BINOM_EXACT, d_err, side2,
                                               &launches, 1));
@@ -301,7 +301,7 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
         VPM_CUDA_TRY(fmm2d_m2p(tree, lists, ex2, p.p, d_err, side2, &launches, slots ? kP2PListSlots : kP2PListCsr));
         VPM_CUDA_TRY(cudaEventRecord(join4, side2));
         VPM_CUDA_TRY(cudaStreamWaitEvent(st, join3, 0));
-        if (split_m2l) {
+        if (split) {
             VPM_CUDA_TRY(fmm2d_m2l_parent_f32(tree, lists, ex2, p.p, p.binom == VPM_BINOM_EXACT, d_err, st,
                                               &launches, 2));
             VPM_CUDA_TRY(cudaStreamWaitEvent(st, ev_m2ld, 0));

@@ -65,6 +65,7 @@ int Ctx::prepare_batch(int ns, const int64_t* offs, const vpm_fmm_params& p, int
         // 8192 particles per sort block: a batch's sorts run side by side
         // (64 uneven solves: 5.11 -> 4.54 ms against 2048)
         c->sort_items = 8192;
+        c->split_m2l = false;
         subs.push_back(c);
         cudaEvent_t e = nullptr;
         VPM_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));

@@ -134,6 +134,10 @@ struct Ctx {
     // particle lattice spreads over 64 SMs: 0.183 -> 0.179 ms against 2048),
     // more in the sub-contexts of a batch, whose solves share the GPU
     int sort_items = 1024;
+    // mixed form: the M2L of the levels below the large cells beside their M2M
+    // loop (one graph per solve); off in the sub-contexts of a batch, whose
+    // small solves share the GPU and gain nothing from the extra launch
+    bool split_m2l = true;
 
     // batched solves (batch2d.cu)
     std::vector<Ctx*> subs;
