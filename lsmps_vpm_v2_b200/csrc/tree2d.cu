@@ -585,32 +585,11 @@ __device__ __forceinline__ int gallop_ge(const uint32_t* __restrict__ a, int lo,
     return L;
 }
 
-// First j <= i with the same key prefix (>> sh) as particle i: galloping
-// back from i, then bisection.
-__device__ __forceinline__ int group_start(const uint64_t* __restrict__ key, int i, int sh) {
-    const uint64_t v = key[i] >> sh;
-    int L = 0, R = i;   // answer in [L, R]
-    for (int step = 1; R - step >= L; step <<= 1) {
-        const int probe = R - step;
-        if ((key[probe] >> sh) == v) {
-            R = probe;
-        } else {
-            L = probe + 1;
-            break;
-        }
-    }
-    while (L < R) {
-        const int mid = (L + R) >> 1;
-        if ((key[mid] >> sh) == v) R = mid;
-        else L = mid + 1;
-    }
-    return L;
-}
-
-// group_start with the whole warp on one query (i and sh the same in every
-// lane): 32 probes per round, galloping back from i by 1, 2, 4, ... 2^30,
-// then 32-way splits of the bracket, so a group of d particles takes about
-// 1 + log_31(d) rounds of loads instead of 2 log_2(d) dependent ones.
+// First j <= i with the same key prefix (>> sh) as particle i, with the whole
+// warp on one query (i and sh the same in every lane): 32 probes per round,
+// galloping back from i by 1, 2, 4, ... 2^30, then 32-way splits of the
+// bracket, so a group of d particles takes about 1 + log_31(d) rounds of loads
+// instead of 2 log_2(d) dependent ones for one thread alone.
 __device__ __forceinline__ int group_start_warp(const uint64_t* __restrict__ key, int i, int sh) {
     const int lane = threadIdx.x & 31;
     const uint64_t v = key[i] >> sh;
