@@ -552,10 +552,17 @@ sort2d_coop(const double* __restrict__ x, const double* __restrict__ y, const do
 //            particle from i, iff the keys share that many leading digits;
 //   cells    particle i starts the cells at levels lvl(i) .. min(K,
 //            max(lvl(i), bigL(i) + 1)) when the parent group of its first
-//            one (the level lvl(i)-1 group containing i, found by search) is
-//            big; the deepest of them is a leaf unless it is big.
+//            one (the level lvl(i)-1 group containing i: it starts at the
+//            last particle before i with lvl <= lvl(i)-1) is big; the
+//            deepest of them is a leaf unless it is big.
 // Cell and leaf indices then come from per-tile, per-level counts (scan over
-// tiles, in tile order = Morton order within each level).
+// tiles, in tile order = Morton order within each level); so do parents (the
+// last cell of the level above starting at or before a cell's particle).
+// Range ends follow from the children partitioning their parent: a cell ends
+// where the next sibling of its nearest ancestor-or-self that has one starts.
+// Kernels: flat_bigl (lvl, bigL), flat_cells (cell levels, tile counts),
+// flat_scan (scanned counts, level totals), flat_emit (cell records, parents,
+// first children), flat_link (range ends, counts, activity, child masks).
 
 __device__ __forceinline__ int lcp_levels(uint64_t a, uint64_t b, int K) {
     const uint64_t x = a ^ b;
