@@ -236,8 +236,11 @@ int Ctx::enqueue2d(const double* x, const double* y, const double* q, const uint
         // One captured graph: the near field (lists 1/3, P2P) runs on the side
         // stream concurrently with lists 2/4 and the far field (P2M, M2M, M2L,
         // L2L); M2P follows lists 2/4 on the third stream once the upward pass
-        // and list 3 are done; L2P then adds the M2P and near-field sums and
-        // writes the output.
+        // and list 3 are done (the mixed form: list 3 from the slots, the few
+        // leaves that outgrew them after the CSR on the fourth stream; its M2L
+        // of the levels below the large cells also runs on the third stream,
+        // beside the large cells' M2M loop); L2P then adds the M2P and
+        // near-field sums and writes the output.
         VPM_CUDA_TRY(cudaEventRecord(fork2, st));
         VPM_CUDA_TRY(cudaStreamWaitEvent(side, fork2, 0));
         if (deferred) {
